@@ -1,0 +1,177 @@
+// flow_device.cuh - per-face / per-node device math of the nonlinear iteration.
+//
+// Every expression keeps the operand order of the reference line it cites and
+// the translation unit is compiled with --fmad=false, so each function returns
+// the same bits as the reference's host code (IEEE double +,-,*,/ and sqrt are
+// correctly rounded on both sides).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace flow {
+
+// flux.C:37-68 Incompressible_Euler_Flux (the physical Euler flux).
+__device__ __forceinline__ void euler_flux(const double* Q, double* F, double nx, double ny,
+                                           double len, double gamma) {
+  double rho = Q[0];
+  double u = Q[1] / Q[0];
+  double v = Q[2] / Q[0];
+  double E = Q[3];
+  double P = (gamma - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+  double theta = u * nx + v * ny;
+  F[0] = rho * theta * len;
+  F[1] = rho * u * theta * len + P * nx * len;
+  F[2] = rho * v * theta * len + P * ny * len;
+  F[3] = theta * (E + P) * len;
+}
+
+// Roe-averaged dissipation matrix |A| = T |Lambda| T^-1, row-major
+// (flux.C:355-524; the same block is repeated in jacobian.C:764-866).
+__device__ __forceinline__ void roe_matrix(double nx, double ny, double gamma, const double* ql,
+                                           const double* qr, double* Rm) {
+  double rhoL = ql[0], uL = ql[1] / ql[0], vL = ql[2] / ql[0], EL = ql[3];
+  double pL = (gamma - 1.) * (EL - 0.5 * rhoL * (uL * uL + vL * vL));
+  double HL = EL + pL, hL = HL / rhoL;
+  double rhoR = qr[0], uR = qr[1] / qr[0], vR = qr[2] / qr[0], ER = qr[3];
+  double pR = (gamma - 1.) * (ER - 0.5 * rhoR * (uR * uR + vR * vR));
+  double HR = ER + pR, hR = HR / rhoR;
+  double rhobar = sqrt(rhoL * rhoR);
+  double bg = rhobar / (rhoL + rhobar);
+  double ubar = uL + bg * (uR - uL);
+  double vbar = vL + bg * (vR - vL);
+  double hbar = hL + bg * (hR - hL);
+  double thetabar = ubar * nx + vbar * ny;
+  double V2bar = (ubar * ubar + vbar * vbar);
+  double cbar = sqrt((gamma - 1.0) * (hbar - 0.5 * V2bar));
+  double lam[4], T[16], Ti[16];
+  lam[0] = fabs(thetabar);
+  lam[1] = fabs(thetabar);
+  lam[2] = fabs(thetabar + cbar);
+  lam[3] = fabs(thetabar - cbar);
+  double c2 = cbar * cbar;
+  T[0] = 1.0;
+  T[1] = 0.0;
+  T[2] = 1.0 / c2;
+  T[3] = 1.0 / c2;
+  T[4] = ubar;
+  T[5] = -ny;
+  T[6] = ubar / c2 + nx / cbar;
+  T[7] = ubar / c2 - nx / cbar;
+  T[8] = vbar;
+  T[9] = nx;
+  T[10] = vbar / c2 + ny / cbar;
+  T[11] = vbar / c2 - ny / cbar;
+  T[12] = 0.5 * V2bar;
+  T[13] = ubar * (-ny) + vbar * nx;
+  double ogm1 = 1.0 / (gamma - 1.0), tc = thetabar / cbar, hv = (0.5 * V2bar) / c2;
+  T[14] = ogm1 + tc + hv;
+  T[15] = ogm1 - tc + hv;
+  Ti[0] = 1.0 - (gamma - 1.0) * (0.5 * V2bar) / c2;
+  Ti[1] = (gamma - 1.0) * ubar / c2;
+  Ti[2] = (gamma - 1.0) * vbar / c2;
+  Ti[3] = -1.0 * (gamma - 1.0) / c2;
+  Ti[4] = -1.0 * (ubar * (-ny) + vbar * nx);
+  Ti[5] = -ny;
+  Ti[6] = nx;
+  Ti[7] = 0.;
+  Ti[8] = 0.5 * (-cbar * thetabar + (gamma - 1.0) * 0.5 * V2bar);
+  Ti[9] = 0.5 * (cbar * nx - (gamma - 1.0) * ubar);
+  Ti[10] = 0.5 * (cbar * ny - (gamma - 1.0) * vbar);
+  Ti[11] = 0.5 * (gamma - 1.0);
+  Ti[12] = 0.5 * (cbar * thetabar + (gamma - 1.0) * 0.5 * V2bar);
+  Ti[13] = -0.5 * (cbar * nx + (gamma - 1.0) * ubar);
+  Ti[14] = -0.5 * (cbar * ny + (gamma - 1.0) * vbar);
+  Ti[15] = 0.5 * (gamma - 1.0);
+  // linear_algebra.C:657-736: MMMult_DtG (Lambda * Tinv) then MMMult_GtG.
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      double s = 0.;
+#pragma unroll
+      for (int k = 0; k < 4; k++) s += T[i * 4 + k] * (lam[k] * Ti[k * 4 + j]);
+      Rm[i * 4 + j] = s;
+    }
+}
+
+// flux.C:299-541 Roe_flux_centered.
+__device__ __forceinline__ void roe_flux(double nx, double ny, double len, double gamma,
+                                         const double* ql, const double* qr, double* flux) {
+  double Rm[16], FL[4], FR[4];
+  roe_matrix(nx, ny, gamma, ql, qr, Rm);
+  double dq[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) dq[i] = qr[i] - ql[i];
+  double diss[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double s = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) s += Rm[i * 4 + j] * dq[j];
+    diss[i] = s * len;
+  }
+  euler_flux(ql, FL, nx, ny, len, gamma);
+  euler_flux(qr, FR, nx, ny, len, gamma);
+#pragma unroll
+  for (int i = 0; i < 4; i++) flux[i] = 0.5 * (FL[i] + FR[i] - diss[i]);
+}
+
+// cv_calc.C:840-866: max(|theta+c|, |theta-c|) for one node state.
+__device__ __forceinline__ double max_wave(const double* q, double nx, double ny, double gamma) {
+  double rho = q[0];
+  double u = q[1] / rho;
+  double v = q[2] / rho;
+  double P = (gamma - 1.0) * (q[3] - 0.5 * rho * (u * u + v * v));
+  double c = sqrt((gamma * P) / rho);
+  double theta = u * nx + v * ny;
+  double tpc = fabs(theta + c), tmc = fabs(theta - c);
+  return tpc >= tmc ? tpc : tmc;
+}
+
+// limiter.C:672-700: one reconstructed value's Venkatakrishnan bound
+// (phi(y) = (y^2+2y)/(y^2+y+2), no epsilon), folded into phi with MIN().
+__device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0, double qmin,
+                                              double qmax) {
+  double d = qrec - q0;
+  if (d > 0.) {
+    double t = (qmax - q0) / (qrec - q0);
+    t = (t * t + 2. * t) / (t * t + t + 2.);
+    return ph <= t ? ph : t;
+  } else if (d < 0.) {
+    double t = (qmin - q0) / (qrec - q0);
+    t = (t * t + 2. * t) / (t * t + t + 2.);
+    return ph <= t ? ph : t;
+  }
+  return ph <= 1.0 ? ph : 1.0;
+}
+
+// linear_algebra.C:571-596 lu() on a 4x4 row-major block, in place.
+__device__ __forceinline__ void lu4(double* A) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+#pragma unroll
+    for (int i = k + 1; i < 4; i++) A[i * 4 + k] = A[i * 4 + k] / A[k * 4 + k];
+#pragma unroll
+    for (int j = k + 1; j < 4; j++)
+#pragma unroll
+      for (int i = k + 1; i < 4; i++) A[i * 4 + j] = A[i * 4 + j] - A[i * 4 + k] * A[k * 4 + j];
+  }
+}
+
+// linear_algebra.C:611-638 forwardstab() then backstab().
+__device__ __forceinline__ void lu_solve4(const double* M, const double* b, double* x) {
+  double y0 = b[0];
+  double y1 = b[1] - M[4] * y0;
+  double y2 = b[2] - M[8] * y0 - M[9] * y1;
+  double y3 = b[3] - M[12] * y0 - M[13] * y1 - M[14] * y2;
+  x[3] = y3 / M[15];
+  x[2] = (y2 - M[11] * x[3]) / M[10];
+  x[1] = (y1 - M[6] * x[2] - M[7] * x[3]) / M[5];
+  x[0] = (y0 - M[1] * x[1] - M[2] * x[2] - M[3] * x[3]) / M[0];
+}
+
+// A[r,:] . d in the reference's grouping (linear_algebra.C:200-221).
+__device__ __forceinline__ double row_dot(const double* A, int r, const double* d) {
+  return (A[r * 4] * d[0] + A[r * 4 + 1] * d[1] + A[r * 4 + 2] * d[2] + A[r * 4 + 3] * d[3]);
+}
+
+}  // namespace flow

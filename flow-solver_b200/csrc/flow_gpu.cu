@@ -1,0 +1,730 @@
+// flow_gpu.cu - C ABI of the B200 nonlinear iteration (include/flow_gpu.h).
+//
+// A flow_ctx owns one mesh resident in HBM (the reference GRID/SYS_MEM
+// arrays re-laid out for per-face and per-node gathers, see flow_state.h),
+// the solver state, and one CUDA stream.  Host work per step is a fixed
+// sequence of kernel launches; nothing is copied back unless asked for.
+//
+// Compiled with --fmad=false: the face and node kernels reproduce the
+// reference's double-precision results bit for bit.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "flow_gpu.h"
+#include "flow_kernels.cuh"
+#include "host/curved.h"
+
+using namespace flow;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const char* msg) { g_last_error = msg; }
+
+struct Buffers {
+  std::vector<void*> ptrs;
+  template <class T>
+  T* alloc(size_t n) {
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  void release() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+}  // namespace
+
+struct flow_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Buffers buf;
+  DevMesh m{};
+  DevState s{};
+  int order = 1;
+  int nsm = 148;
+  int epoch = 0;
+  int citer = 0;
+  int sweep_mode = 0;
+  long launches = 0;
+  double last_ms = 0.;
+  bool ok = false;
+  // host copies needed to answer flow_get in the reference layout
+  int nn = 0, ng = 0, ns = 0, nbe = 0, nnz = 0;
+  double* d_hist = nullptr;  // 2 x hist_cap device history of (dq, r_rho)
+  int hist_cap = 0;
+};
+
+namespace {
+
+bool upload(flow_ctx* c, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return true;
+  return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+template <class T>
+T* upload_vec(flow_ctx* c, const std::vector<T>& v) {
+  T* d = c->buf.alloc<T>(v.size());
+  if (!d) return nullptr;
+  if (!upload(c, d, v.data(), v.size() * sizeof(T))) return nullptr;
+  return d;
+}
+
+// Build a CSR list: for each node, items appended in call order.
+struct Csr {
+  std::vector<int> ptr, idx;
+  void build(int n, const std::vector<std::pair<int, int>>& items) {
+    ptr.assign(n + 2, 0);
+    for (auto& it : items) ptr[it.first + 1]++;
+    for (int i = 1; i <= n + 1; i++) ptr[i] += ptr[i - 1];
+    idx.assign(items.size(), 0);
+    std::vector<int> pos(ptr.begin(), ptr.end());
+    for (auto& it : items) idx[pos[it.first]++] = it.second;
+  }
+};
+
+int launch_check(flow_ctx* c) {
+  c->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return FLOW_ERR_CUDA;
+  }
+  return 0;
+}
+
+double ramp_cfl(const flow_params* p, int citer) {
+  // init_memory.C:200-216
+  if (p->method == 1) {
+    if (citer < p->ramp) return 1. + (1. * (citer - 1)) / (1. * p->ramp) * (p->CFL - 1.);
+    return p->CFL;
+  }
+  if (p->method == 0) return 1.0;
+  return p->CFL;
+}
+
+StepArgs make_args(const flow_params* p, int ts) {
+  StepArgs a{};
+  a.gamma = p->gamma;
+  a.cfl = ramp_cfl(p, ts);
+  double angle = p->alpha * M_PI / 180.;
+  a.uinf = p->mach * cos(angle);
+  a.vinf = p->mach * sin(angle);
+  a.pinf = 1. / p->gamma;
+  double angle2 = p->alpha * M_PI / 180;  // grid_io.C:1432
+  a.cos_a = cos(angle2);
+  a.sin_a = sin(angle2);
+  const int hi = ts > (p->foits + p->soits);
+  a.do_grad = (p->order == 1 && ts > p->foits) || (p->order == 3 && ts > p->foits && !hi);
+  a.do_derivs = (p->order == 3 && hi);
+  a.do_lim = (p->order == 1 && p->limit > 0 && ts > p->foits) || (p->order == 3 && p->limit > 0 && hi);
+  a.recon = (p->order == 1) ? (ts > p->foits ? 1 : 0) : (ts > p->foits && !hi ? 1 : 0);
+  a.gauss = (p->order == 3 && hi);
+  a.jac = p->method != 0;
+  a.steady_diag = 1;
+  return a;
+}
+
+int check_params(flow_ctx* c, const flow_params* p) {
+  if (!p) return FLOW_ERR_ARG;
+  if (p->order != c->order) { set_error("params.order differs from the context's"); return FLOW_ERR_ARG; }
+  if (p->method != 1) { set_error("only the implicit method (method=1) is supported"); return FLOW_ERR_ARG; }
+  if (p->unsteady != 0 || p->tacc != 0) { set_error("only steady runs are supported"); return FLOW_ERR_ARG; }
+  if (p->limit != 0 && p->limit != 2) { set_error("only limit=0 or limit=2 is supported"); return FLOW_ERR_ARG; }
+  if (p->iter < 1 || p->jufreq < 1 || p->subits < 0) { set_error("bad iter/jufreq/subits"); return FLOW_ERR_ARG; }
+  if (p->order == 3 && p->soits > 0) { set_error("order 3 with soits > 0 is not supported"); return FLOW_ERR_ARG; }
+  return 0;
+}
+
+int grid_blocks(int n, int t) { return (n + t - 1) / t; }
+
+int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
+  int nb = grid_blocks(c->nn, 128);
+  if (c->order == 1)
+    k_node_prepare<1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+  else
+    k_node_prepare<3><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+  return launch_check(c);
+}
+
+int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
+  int rc = 0;
+  int nbs = grid_blocks(c->ns, 128);
+  if (a.recon == 1) {
+    if (jac) k_subedge_flux<1, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+    else k_subedge_flux<1, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+  } else {
+    if (jac) k_subedge_flux<0, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+    else k_subedge_flux<0, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+  }
+  rc |= launch_check(c);
+  int nbb = grid_blocks(c->nbe, 128);
+  if (nbb > 0) {
+    if (jac) k_boundary<true><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
+    else k_boundary<false><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
+    rc |= launch_check(c);
+  }
+  int nbn = grid_blocks(c->nn, 128);
+  if (jac) k_assemble<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+  else k_assemble<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+  rc |= launch_check(c);
+  return rc;
+}
+
+// linear_solve (linear_algebra.C:122-401): subits sweeps, alternating
+// forward/backward, each followed by the b-Ax RMS that may stop the loop.
+int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
+  int rc = 0;
+  cudaMemsetAsync(c->s.dQ, 0, sizeof(double) * 4 * (c->nn + 1), c->stream);
+  cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream);
+  const long max_spin = 1L << 21;  // ~0.1-0.2 s per wait at most
+  for (int it = 0; it < p->subits; it++) {
+    cudaMemsetAsync(c->s.counter, 0, sizeof(unsigned), c->stream);
+    int ep = ++c->epoch;
+    int blocks = c->nsm * 4;
+    if (it % 2 == 0)
+      k_sweep_ordered<true><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
+    else
+      k_sweep_ordered<false><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
+    rc |= launch_check(c);
+    if (it < p->subits - 1 || final_rms) {
+      k_lin_residual<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->m, c->s);
+      rc |= launch_check(c);
+      k_finalize_rms<<<1, kRedThreads, 0, c->stream>>>(c->s, kRedBlocks, c->nn);
+      rc |= launch_check(c);
+    }
+  }
+  return rc;
+}
+
+// One solve() call (solve.C:44-933), device-only.
+int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot) {
+  int rc = 0;
+  int total = c->nn + c->ng;
+  c->citer = ts;
+  k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 1);
+  rc |= launch_check(c);
+  StepArgs a = make_args(p, ts);
+  for (int mi = 1; mi <= p->iter; mi++) {
+    int jac = ((mi - 1) % p->jufreq == 0) || mi == 1;
+    if (mi > 1) {
+      // phi <- 1 at every Newton iteration (solve.C:344-348)
+      k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 0);
+      rc |= launch_check(c);
+    }
+    rc |= launch_node_prepare(c, a);
+    rc |= launch_residuals(c, a, jac);
+    rc |= launch_linear_solve(c, p, false);
+    k_finish_step<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->m, c->s, mi == p->iter);
+    rc |= launch_check(c);
+    bool last = mi == p->iter;
+    k_finalize_step<<<1, kRedThreads, 0, c->stream>>>(
+        c->s, last && hist_slot >= 0 ? c->d_hist : nullptr,
+        last && hist_slot >= 0 ? c->d_hist + c->hist_cap : nullptr, hist_slot < 0 ? 0 : hist_slot);
+    rc |= launch_check(c);
+  }
+  return rc;
+}
+
+int read_status(flow_ctx* c) {
+  int st = 0;
+  if (cudaMemcpyAsync(&st, c->s.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream) !=
+      cudaSuccess)
+    return FLOW_ERR_CUDA;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error(cudaGetErrorString(cudaGetLastError()));
+    return FLOW_ERR_CUDA;
+  }
+  return st;
+}
+
+int ensure_hist(flow_ctx* c, int n) {
+  if (n <= c->hist_cap) return 0;
+  if (c->d_hist) cudaFree(c->d_hist);
+  c->d_hist = nullptr;
+  if (cudaMalloc(&c->d_hist, sizeof(double) * 2 * n) != cudaSuccess) return FLOW_ERR_CUDA;
+  c->hist_cap = n;
+  return 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char* flow_last_error(void) { return g_last_error.c_str(); }
+
+flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device, int* status) {
+  auto fail = [&](flow_ctx* c, int code, const char* msg) -> flow_ctx* {
+    set_error(msg);
+    if (status) *status = code;
+    if (c) flow_destroy(c);
+    return nullptr;
+  };
+  if (!g || !p) return fail(nullptr, FLOW_ERR_ARG, "null grid or params");
+  if (p->order != 1 && p->order != 3) return fail(nullptr, FLOW_ERR_ARG, "order must be 1 or 3");
+  const int nn = g->nn, ng = g->nn_ghost, ne = g->nedges, ns = g->nsubedges, nbe = g->nbedges;
+  if (nn < 1 || ne < 1 || ns < 1 || !g->edges || !g->subedges || !g->ia || !g->ja || !g->iau ||
+      !g->x || !g->cv_area || !g->xn_subedges || !g->bedges || !g->bbc || !g->node_order)
+    return fail(nullptr, FLOW_ERR_ARG, "incomplete grid view");
+  if (p->order == 1 && !g->edge_weight) return fail(nullptr, FLOW_ERR_ARG, "order 1 needs edge_weight");
+  if (p->order == 3 && (!g->gnsn || !g->gnnsn || !g->gnnsn1 || !g->svd_m || !g->svd_off ||
+                        !g->svd_U || !g->svd_VT || !g->svd_S || !g->moments || !g->xg_subedges))
+    return fail(nullptr, FLOW_ERR_ARG, "order 3 needs stencils, SVD factors, moments, Gauss points");
+  for (int i = 1; i <= nn; i++)
+    if (g->node_order[i] != p->order)
+      return fail(nullptr, FLOW_ERR_ARG, "mixed node_order is not supported");
+
+  flow_ctx* c = new flow_ctx();
+  c->device = device;
+  c->order = p->order;
+  c->nn = nn; c->ng = ng; c->ns = ns; c->nbe = nbe;
+  c->nnz = g->ia[nn + 1];
+  if (cudaSetDevice(device) != cudaSuccess) return fail(c, FLOW_ERR_CUDA, "cudaSetDevice failed");
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(c, FLOW_ERR_CUDA, "stream creation failed");
+  cudaEventCreate(&c->ev0);
+  cudaEventCreate(&c->ev1);
+
+  // ---- host-side re-layout ----
+  std::vector<std::pair<int, int>> items;
+  Csr nsub, nbed, nedg;
+  items.reserve(2 * ns);
+  std::vector<int2> sub_lr(ns + 1);
+  std::vector<double4> sub_geo(ns + 1), sub_dx(ns + 1);
+  for (int s = 1; s <= ns; s++) {
+    int e = g->subedges[2 * s];
+    int L = g->edges[2 * e], R = g->edges[2 * e + 1];
+    sub_lr[s] = make_int2(L, R);
+    sub_geo[s] = make_double4(g->xn_subedges[3 * s], g->xn_subedges[3 * s + 1],
+                              g->xn_subedges[3 * s + 2], 0.);
+    // face point of Reconstruct (reconstruct.C:183-197)
+    int gel = g->subedges[2 * s + 1];
+    double fc0 = (g->el_cent[2 * gel] + g->xm_subedges[2 * s]) * 0.5;
+    double fc1 = (g->el_cent[2 * gel + 1] + g->xm_subedges[2 * s + 1]) * 0.5;
+    sub_dx[s] = make_double4(fc0 - g->x[2 * L], fc1 - g->x[2 * L + 1], fc0 - g->x[2 * R],
+                             fc1 - g->x[2 * R + 1]);
+    items.push_back({L, s << 1});
+    items.push_back({R, (s << 1) | 1});
+  }
+  nsub.build(nn, items);
+  items.clear();
+  for (int b = 1; b <= nbe; b++) items.push_back({g->bedges[5 * b], b});
+  nbed.build(nn, items);
+  items.clear();
+  std::vector<int2> edge_lr(ne + 1);
+  std::vector<double4> edge_w(ne + 1, make_double4(0, 0, 0, 0));
+  for (int e = 1; e <= ne; e++) {
+    int L = g->edges[2 * e], R = g->edges[2 * e + 1];
+    edge_lr[e] = make_int2(L, R);
+    if (g->edge_weight)
+      edge_w[e] = make_double4(g->edge_weight[4 * e], g->edge_weight[4 * e + 1],
+                               g->edge_weight[4 * e + 2], g->edge_weight[4 * e + 3]);
+    items.push_back({L, e << 1});
+    items.push_back({R, (e << 1) | 1});
+  }
+  nedg.build(nn, items);
+  // subedges of each edge, ascending
+  std::vector<int2> edge_sub(ne + 1, make_int2(-1, -1));
+  for (int s = 1; s <= ns; s++) {
+    int e = g->subedges[2 * s];
+    if (edge_sub[e].x < 0) edge_sub[e].x = s;
+    else if (edge_sub[e].y < 0) edge_sub[e].y = s;
+    else return fail(c, FLOW_ERR_ARG, "an edge has more than two subedges");
+  }
+  // per CSR block: the edge's subedges and the row's role
+  const int nnz = c->nnz;
+  std::vector<int4> csr_sub(nnz, make_int4(-1, -1, 0, 0));
+  for (int n = 1; n <= nn; n++) {
+    for (int k = g->ia[n]; k < g->ia[n + 1]; k++) {
+      int col = g->ja[k];
+      if (col == n) continue;
+      int found = -1, role = 0;
+      for (int q = nedg.ptr[n]; q < nedg.ptr[n + 1]; q++) {
+        int e = nedg.idx[q] >> 1, side = nedg.idx[q] & 1;
+        int other = side ? edge_lr[e].x : edge_lr[e].y;
+        if (other == col) { found = e; role = side; break; }
+      }
+      if (found < 0) return fail(c, FLOW_ERR_ARG, "CSR block without an edge");
+      csr_sub[k] = make_int4(edge_sub[found].x, edge_sub[found].y, role, 0);
+    }
+  }
+  std::vector<int4> bed_info(nbe + 1, make_int4(0, 0, 0, 0));
+  std::vector<double2> bed_cnrm(nbe + 1, make_double2(0., 0.));
+  for (int b = 1; b <= nbe; b++) {
+    int rn = g->bedges[5 * b], gn = g->bedges[5 * b + 1] + nn;
+    int bc = g->bbc[g->bedges[5 * b + 3]];
+    int wall = !(bc == 0 || (bc % 2 == 0));
+    bed_info[b] = make_int4(rn, gn, bc, wall);
+    if (bc > 10) {
+      double nx, ny;
+      flow_curved_normal(bc, &g->x[2 * rn], &nx, &ny);
+      bed_cnrm[b] = make_double2(nx, ny);
+    }
+  }
+  // k=2 stencils: node i uses gnsn[gnnsn[gnnsn1[i]+1] .. gnnsn[gnnsn1[i+1]])
+  std::vector<int> st_ptr(nn + 2, 0), st_idx;
+  std::vector<double> st_w, U1, VT((size_t)(nn + 1) * 25, 0.), S((size_t)(nn + 1) * 5, 1.);
+  int stencil_max = 0;
+  if (p->order == 3) {
+    for (int i = 1; i <= nn; i++) {
+      int a0 = g->gnnsn[g->gnnsn1[i] + 1], a1 = g->gnnsn[g->gnnsn1[i + 1]];
+      int mrows = a1 - a0;
+      if (mrows != g->svd_m[i]) return fail(c, FLOW_ERR_ARG, "stencil size differs from svd_m");
+      if (mrows < 5 || mrows > 64) return fail(c, FLOW_ERR_ARG, "stencil size out of range");
+      stencil_max = std::max(stencil_max, mrows);
+      st_ptr[i] = (int)st_idx.size();
+      for (int j = a0; j < a1; j++) {
+        int nb = g->gnsn[j];
+        double dx0 = g->x[2 * nb] - g->x[2 * i];
+        double dx1 = g->x[2 * nb + 1] - g->x[2 * i + 1];
+        double dist = sqrt(dx0 * dx0 + dx1 * dx1);
+        st_idx.push_back(nb);
+        st_w.push_back(1.0 / pow(dist, 1.0));  // compute_derivatives.C:1470 (GEOM_WEIGHT 1)
+      }
+      const double* Ui = g->svd_U + g->svd_off[i];
+      for (int q = 0; q < 5 * mrows; q++) U1.push_back(Ui[q]);
+      for (int q = 0; q < 25; q++) VT[(size_t)i * 25 + q] = g->svd_VT[(size_t)i * 25 + q];
+      for (int q = 0; q < 5; q++) S[(size_t)i * 5 + q] = g->svd_S[(size_t)i * 5 + q];
+    }
+    st_ptr[nn + 1] = (int)st_idx.size();
+  }
+
+  // ---- device mesh ----
+  DevMesh& m = c->m;
+  m.nn = nn; m.ng = ng; m.ne = ne; m.ns = ns; m.nbe = nbe; m.nnz = nnz; m.order = p->order;
+  m.stencil_max = stencil_max;
+  bool okk = true;
+#define UP(field, vec) do { auto* d = upload_vec(c, vec); okk = okk && d; m.field = d; } while (0)
+  UP(nsub_ptr, nsub.ptr); UP(nsub, nsub.idx);
+  UP(nbed_ptr, nbed.ptr); UP(nbed, nbed.idx);
+  UP(nedg_ptr, nedg.ptr); UP(nedg, nedg.idx);
+  UP(sub_lr, sub_lr); UP(sub_geo, sub_geo); UP(sub_dx, sub_dx);
+  UP(edge_lr, edge_lr); UP(edge_w, edge_w);
+  UP(csr_sub, csr_sub);
+  UP(bed_info, bed_info); UP(bed_cnrm, bed_cnrm);
+  {
+    std::vector<int> ia(g->ia, g->ia + nn + 2), iau(g->iau, g->iau + nn + 1), ja(g->ja, g->ja + nnz);
+    UP(ia, ia); UP(iau, iau); UP(ja, ja);
+    std::vector<double> x(g->x, g->x + (size_t)(nn + ng + 1) * 2), cv(g->cv_area, g->cv_area + nn + 1);
+    UP(x, x); UP(cv_area, cv);
+    std::vector<int> no(g->node_order, g->node_order + nn + ng + 1);
+    UP(node_order, no);
+    std::vector<double> xg((size_t)(ns + 1) * 6, 0.);
+    if (g->xg_subedges) std::copy(g->xg_subedges, g->xg_subedges + xg.size(), xg.begin());
+    UP(sub_xg, xg);
+    std::vector<double> xgb((size_t)(nbe + 1) * 6, 0.), xgnb((size_t)(nbe + 1) * 9, 0.);
+    if (g->xg_bedges) std::copy(g->xg_bedges, g->xg_bedges + xgb.size(), xgb.begin());
+    if (g->xgn_bedges) std::copy(g->xgn_bedges, g->xgn_bedges + xgnb.size(), xgnb.begin());
+    UP(xg_bedges, xgb); UP(xgn_bedges, xgnb);
+    std::vector<double> mo((size_t)(nn + 1) * 9, 0.);
+    if (g->moments) std::copy(g->moments, g->moments + mo.size(), mo.begin());
+    UP(moments, mo);
+  }
+  if (p->order == 3) {
+    UP(st_ptr, st_ptr); UP(st_idx, st_idx); UP(st_w, st_w);
+    UP(svd_U1, U1); UP(svd_VT, VT); UP(svd_S, S);
+  }
+#undef UP
+  if (!okk) return fail(c, FLOW_ERR_CUDA, "device allocation or upload failed");
+
+  // ---- device state ----
+  DevState& s = c->s;
+  size_t nq = (size_t)(nn + ng + 1) * 4;
+  s.Q = c->buf.alloc<double>(nq);
+  s.nQ = c->buf.alloc<double>(nq);
+  s.pQ = c->buf.alloc<double>(nq);
+  s.dQ = c->buf.alloc<double>((size_t)(nn + 1) * 4);
+  s.R = c->buf.alloc<double>((size_t)(nn + 1) * 4);
+  s.RHS = c->buf.alloc<double>((size_t)(nn + 1) * 4);
+  s.grad = c->buf.alloc<double>((size_t)(nn + 1) * 8);
+  s.phi = c->buf.alloc<double>((size_t)(nn + 1) * 8);
+  s.hess5 = c->buf.alloc<double>((size_t)(nn + 1) * 20);
+  s.pv = c->buf.alloc<double>((size_t)(nn + 1) * 4);
+  s.dt = c->buf.alloc<double>((size_t)(nn + 1));
+  s.LHS = c->buf.alloc<double>((size_t)nnz * 16);
+  s.LUd = c->buf.alloc<double>((size_t)(nn + 1) * 16);
+  s.xn_bedges = c->buf.alloc<double>((size_t)(nbe + 1) * 3);
+  s.F = c->buf.alloc<double>((size_t)(ns + 1) * 4);
+  s.JL = c->buf.alloc<double>((size_t)(ns + 1) * 16);
+  s.JR = c->buf.alloc<double>((size_t)(ns + 1) * 16);
+  s.Fb = c->buf.alloc<double>((size_t)(nbe + 1) * 4);
+  s.Jb = c->buf.alloc<double>((size_t)(nbe + 1) * 16);
+  s.bforce = c->buf.alloc<double>((size_t)(nbe + 1) * 4);
+  s.done = c->buf.alloc<int>((size_t)(nn + 1));
+  s.counter = c->buf.alloc<unsigned>(4);
+  s.status = c->buf.alloc<int>(1);
+  s.skip = c->buf.alloc<int>(1);
+  s.partial = c->buf.alloc<double>(2 * kRedBlocks);
+  s.scalars = c->buf.alloc<double>(8);
+  if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
+      !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
+      !s.Jb || !s.bforce || !s.done || !s.counter || !s.status || !s.skip || !s.partial ||
+      !s.scalars)
+    return fail(c, FLOW_ERR_CUDA, "device state allocation failed");
+  cudaMemset(s.Q, 0, nq * 8);
+  cudaMemset(s.nQ, 0, nq * 8);
+  cudaMemset(s.pQ, 0, nq * 8);
+  cudaMemset(s.dQ, 0, (size_t)(nn + 1) * 32);
+  cudaMemset(s.R, 0, (size_t)(nn + 1) * 32);
+  cudaMemset(s.RHS, 0, (size_t)(nn + 1) * 32);
+  cudaMemset(s.grad, 0, (size_t)(nn + 1) * 64);
+  cudaMemset(s.phi, 0, (size_t)(nn + 1) * 64);
+  cudaMemset(s.hess5, 0, (size_t)(nn + 1) * 160);
+  cudaMemset(s.pv, 0, (size_t)(nn + 1) * 32);
+  cudaMemset(s.dt, 0, (size_t)(nn + 1) * 8);
+  cudaMemset(s.LHS, 0, (size_t)nnz * 128);
+  cudaMemset(s.done, 0, (size_t)(nn + 1) * 4);
+  cudaMemset(s.status, 0, 4);
+  cudaMemset(s.skip, 0, 4);
+  cudaMemset(s.scalars, 0, 64);
+  std::vector<double> xnb((size_t)(nbe + 1) * 3, 0.);
+  std::copy(g->xn_bedges, g->xn_bedges + xnb.size(), xnb.begin());
+  if (!upload(c, s.xn_bedges, xnb.data(), xnb.size() * 8))
+    return fail(c, FLOW_ERR_CUDA, "upload failed");
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(c, FLOW_ERR_CUDA, "device error at set-up");
+  c->ok = true;
+  if (status) *status = 0;
+  return c;
+}
+
+void flow_destroy(flow_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->buf.release();
+  if (c->d_hist) cudaFree(c->d_hist);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int flow_set_state(flow_ctx* c, const double* Q) {
+  if (!c || !c->ok || !Q) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  size_t bytes = sizeof(double) * 4 * (size_t)(c->nn + c->ng + 1);
+  if (cudaMemcpyAsync(c->s.Q, Q, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(c->s.nQ, Q, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return FLOW_ERR_CUDA;
+  return 0;
+}
+
+int flow_set_sweep_mode(flow_ctx* c, int mode) {
+  if (!c || mode != 0) return FLOW_ERR_ARG;
+  c->sweep_mode = mode;
+  return 0;
+}
+
+int flow_solve(flow_ctx* c, const flow_params* p, int ts, double* dq_norm, double* r_rho) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if ((rc = ensure_hist(c, 1))) return rc;
+  cudaEventRecord(c->ev0, c->stream);
+  rc = enqueue_step(c, p, ts, 0);
+  cudaEventRecord(c->ev1, c->stream);
+  if (rc) return rc;
+  int st = read_status(c);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_ms = ms;
+  double h[2] = {0., 0.};
+  cudaMemcpy(&h[0], c->d_hist, sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&h[1], c->d_hist + c->hist_cap, sizeof(double), cudaMemcpyDeviceToHost);
+  if (dq_norm) *dq_norm = h[0];
+  if (r_rho) *r_rho = h[1];
+  return st;
+}
+
+int flow_run(flow_ctx* c, const flow_params* p, int ts0, int nsteps, double* r_hist,
+             double* dq_hist) {
+  if (!c || !c->ok || nsteps < 0) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if ((rc = ensure_hist(c, std::max(nsteps, 1)))) return rc;
+  cudaEventRecord(c->ev0, c->stream);
+  for (int i = 0; i < nsteps && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, i);
+  cudaEventRecord(c->ev1, c->stream);
+  if (rc) return rc;
+  int st = read_status(c);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_ms = ms;
+  if (dq_hist) cudaMemcpy(dq_hist, c->d_hist, sizeof(double) * nsteps, cudaMemcpyDeviceToHost);
+  if (r_hist)
+    cudaMemcpy(r_hist, c->d_hist + c->hist_cap, sizeof(double) * nsteps, cudaMemcpyDeviceToHost);
+  return st;
+}
+
+int flow_build_matrix(flow_ctx* c, const flow_params* p, int citer) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  StepArgs a = make_args(p, citer);
+  a.do_grad = a.do_derivs = a.do_lim = 0;
+  c->citer = citer;
+  rc = launch_node_prepare(c, a);
+  k_diag_only<<<grid_blocks(c->nn, 128), 128, 0, c->stream>>>(c->m, c->s);
+  rc |= launch_check(c);
+  if (rc) return rc;
+  return read_status(c);
+}
+
+int flow_reconstruct(flow_ctx* c, const flow_params* p, int ts) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  StepArgs a = make_args(p, ts);
+  c->citer = ts;
+  // grad, hess <- 0 and phi <- 1 (solve.C:298-348), keeping the current nQ
+  k_begin_step<<<grid_blocks(c->nn + c->ng, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 0);
+  rc |= launch_check(c);
+  rc |= launch_node_prepare(c, a);
+  if (rc) return rc;
+  return read_status(c);
+}
+
+int flow_residuals(flow_ctx* c, const flow_params* p, int jupdate, int ts) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  StepArgs a = make_args(p, ts);
+  c->citer = ts;
+  rc = launch_residuals(c, a, jupdate);
+  if (rc) return rc;
+  return read_status(c);
+}
+
+int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  rc = launch_linear_solve(c, p, true);
+  if (rc) return rc;
+  int st = read_status(c);
+  if (rms) {
+    double v = 10.;
+    if (p->subits > 0) cudaMemcpy(&v, c->s.scalars, sizeof(double), cudaMemcpyDeviceToHost);
+    *rms = v;
+  }
+  return st;
+}
+
+int flow_body_forces(flow_ctx* c, const flow_params* p, double* forces) {
+  if (!c || !c->ok || !forces) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  StepArgs a = make_args(p, 1);
+  // Reconstruct_Gauss_Boundary's order at the current step (reconstruct.C:1725-1760)
+  int citer = c->citer;
+  int ro = 0;
+  if (p->order == 1) ro = citer > p->foits ? 1 : 0;
+  if (p->order == 3) ro = citer > p->foits + p->soits ? 3 : (citer > p->foits ? 1 : 0);
+  int rc = 0;
+  if (c->nbe > 0) {
+    k_body_forces<<<grid_blocks(c->nbe, 128), 128, 0, c->stream>>>(c->m, c->s, a, ro);
+    rc |= launch_check(c);
+  }
+  k_body_forces_sum<<<1, 32, 0, c->stream>>>(c->m, c->s);
+  rc |= launch_check(c);
+  if (rc) return rc;
+  double f[2];
+  cudaMemcpyAsync(f, c->s.scalars + 4, sizeof(f), cudaMemcpyDeviceToHost, c->stream);
+  int st = read_status(c);
+  forces[0] = f[0];
+  forces[1] = f[1];
+  return st;
+}
+
+long flow_size(flow_ctx* c, const char* name) {
+  if (!c || !name) return -1;
+  long nn = c->nn, ng = c->ng;
+  std::string n(name);
+  if (n == "Q" || n == "nQ" || n == "pQ") return (nn + ng + 1) * 4;
+  if (n == "dQ" || n == "R" || n == "RHS" || n == "point_value") return (nn + 1) * 4;
+  if (n == "grad" || n == "phi") return (nn + 1) * 8;
+  if (n == "hess") return (nn + 1) * 36;
+  if (n == "dt") return nn + 1;
+  if (n == "LHS") return (long)c->nnz * 16;
+  if (n == "xn_bedges") return (long)(c->nbe + 1) * 3;
+  return -1;
+}
+
+int flow_get(flow_ctx* c, const char* name, double* out, long n) {
+  if (!c || !c->ok || !name || !out) return FLOW_ERR_ARG;
+  long need = flow_size(c, name);
+  if (need < 0) return FLOW_ERR_NOT_FOUND;
+  if (n < need) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
+  std::string nm(name);
+  const double* src = nullptr;
+  if (nm == "Q") src = c->s.Q;
+  else if (nm == "nQ") src = c->s.nQ;
+  else if (nm == "pQ") src = c->s.pQ;
+  else if (nm == "dQ") src = c->s.dQ;
+  else if (nm == "R") src = c->s.R;
+  else if (nm == "RHS") src = c->s.RHS;
+  else if (nm == "grad") src = c->s.grad;
+  else if (nm == "phi") src = c->s.phi;
+  else if (nm == "dt") src = c->s.dt;
+  else if (nm == "LHS") src = c->s.LHS;
+  else if (nm == "xn_bedges") src = c->s.xn_bedges;
+  else if (nm == "point_value") src = c->s.pv;
+  if (src) {
+    if (cudaMemcpy(out, src, sizeof(double) * need, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return FLOW_ERR_CUDA;
+    return 0;
+  }
+  if (nm == "hess") {
+    std::vector<double> h((size_t)(c->nn + 1) * 20);
+    if (cudaMemcpy(h.data(), c->s.hess5, h.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return FLOW_ERR_CUDA;
+    std::fill(out, out + need, 0.);
+    for (long i = 0; i <= c->nn; i++)
+      for (int v = 0; v < 4; v++)
+        for (int k = 0; k < 5; k++) out[i * 36 + v * 9 + k] = h[i * 20 + v * 5 + k];
+    return 0;
+  }
+  return FLOW_ERR_NOT_FOUND;
+}
+
+int flow_status(flow_ctx* c) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  return read_status(c);
+}
+
+void flow_clear_status(flow_ctx* c) {
+  if (!c || !c->ok) return;
+  cudaSetDevice(c->device);
+  cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream);
+  cudaStreamSynchronize(c->stream);
+}
+
+long flow_launch_count(flow_ctx* c) { return c ? c->launches : 0; }
+
+double flow_last_device_ms(flow_ctx* c) { return c ? c->last_ms : 0.; }
+
+}  // extern "C"

@@ -1,0 +1,815 @@
+// flow_kernels.cuh - CUDA kernels of one nonlinear iteration (solve.C:44-933).
+//
+// One pseudo-time step is a fixed sequence of launches on the context's
+// stream:
+//   k_begin_step      nQ <- Q, grad/hess <- 0, phi <- 1        (solve.C:298-348)
+//   k_node_prepare    per node: wave-speed sum, dt and V/dt    (build_matrix)
+//                     + LSQ gradient or k=2 derivatives + Venkatakrishnan phi
+//   k_subedge_flux    per subedge: reconstructed Roe flux and the 8-flux
+//                     forward-difference Jacobian               (residual.C, jacobian.C)
+//   k_boundary        per boundary edge: ghost state, boundary flux and
+//                     approximate Jacobian                      (cvbc.C, residual.C)
+//   k_assemble        per node: R, RHS, the node's LHS row, LU of the diagonal
+//   k_sweep_ordered   block Gauss-Seidel sweeps in reference row order
+//   k_lin_residual    b - Ax RMS after a sweep                  (linear_algebra.C:348-387)
+//   k_finish_step     nQ += dQ, pQ <- Q, Q <- nQ, norms         (solve.C:883-928)
+// Face results are written once per face and gathered per node in ascending
+// face order, which reproduces the reference's sequential scatter sums
+// exactly without atomics.
+#pragma once
+#include <cuda/atomic>
+#include "flow_device.cuh"
+#include "flow_state.h"
+
+namespace flow {
+
+enum : int {
+  ERR_EIGEN = 4,
+  ERR_DT = 8,
+  ERR_LIMITER = 16,
+  ERR_BC = 32,
+  ERR_SWEEP_TIMEOUT = 64,
+};
+
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs; fixed so reductions are deterministic
+constexpr int kRedThreads = 256;
+
+struct StepArgs {
+  double gamma;
+  double cfl;
+  double uinf, vinf, pinf;  // far-field state (cvbc.C:70-74)
+  double cos_a, sin_a;      // angle of attack (grid_io.C:1432)
+  int do_grad;              // k=1 gradient
+  int do_derivs;            // k=2 derivatives
+  int do_lim;               // Venkatakrishnan limiter
+  int recon;                // interior reconstruction order: 0, 1 or 3
+  int gauss;                // k=2 Gauss pass active (curved-boundary side effects)
+  int jac;                  // Jacobian update
+  int steady_diag;          // V/dt diagonal (steady runs)
+};
+
+// ---------------------------------------------------------------------------
+__global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
+  int total = m.nn + m.ng;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= total;
+       i += gridDim.x * blockDim.x) {
+    if (copy_q) {
+      const double4* q = reinterpret_cast<const double4*>(s.Q) + i;
+      reinterpret_cast<double4*>(s.nQ)[i] = *q;
+    }
+    if (i <= m.nn) {
+      double4 z = make_double4(0., 0., 0., 0.);
+      double4* g = reinterpret_cast<double4*>(s.grad) + 2 * i;
+      g[0] = z;
+      g[1] = z;
+      if (m.order == 3) {
+        double* h = s.hess5 + 20 * i;
+#pragma unroll
+        for (int k = 0; k < 20; k++) h[k] = 0.;
+      }
+      if (reset_phi) {
+        double4 o = make_double4(1., 1., 1., 1.);
+        double4* p = reinterpret_cast<double4*>(s.phi) + 2 * i;
+        p[0] = o;
+        p[1] = o;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per node: cv_calc_eigenvalue_contribution (cv_calc.C:819-953) and the dt /
+// V/dt of build_matrix (init_memory.C:200-290); then the LSQ gradient
+// (gradient.C:382-403) or the k=2 derivatives (compute_derivatives.C:
+// 1438-1521); then the Venkatakrishnan limiter (limiter.C:594-906).
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_node_prepare(DevMesh m, DevState s, StepArgs a) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > m.nn) return;
+  const double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
+  const double q0[4] = {q4.x, q4.y, q4.z, q4.w};
+
+  // ---- wave-speed sum over the node's subedges, then boundary edges ----
+  double ev = 0.;
+  int bad = 0;
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int k = s0; k < s1; k++) {
+    int sd = m.nsub[k];
+    double4 g = m.sub_geo[sd >> 1];
+    double w = max_wave(q0, g.x, g.y, a.gamma);
+    if (!isfinite(w)) bad = 1;
+    ev += (w * g.z);
+  }
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  for (int k = b0; k < b1; k++) {
+    int b = m.nbed[k];
+    const double* xn = s.xn_bedges + 3 * b;
+    double w = max_wave(q0, xn[0], xn[1], a.gamma);
+    if (!isfinite(w)) bad = 1;
+    ev += (w * xn[2]);
+  }
+  double V = m.cv_area[n];
+  double dt = a.cfl * (V / ev);
+  s.dt[n] = dt;
+  if (bad) atomicOr(s.status, ERR_EIGEN);
+  if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
+  if (!a.do_grad && !a.do_derivs && !a.do_lim) return;
+
+  // ---- 1-ring min/max and the k=1 LSQ gradient over incident edges ----
+  double qmin[4], qmax[4], gr[8];
+#pragma unroll
+  for (int j = 0; j < 4; j++) { qmin[j] = q0[j]; qmax[j] = q0[j]; }
+#pragma unroll
+  for (int j = 0; j < 8; j++) gr[j] = 0.;
+  const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
+  for (int k = e0; k < e1; k++) {
+    int ed = m.nedg[k];
+    int e = ed >> 1, side = ed & 1;
+    int2 lr = m.edge_lr[e];
+    int other = side ? lr.x : lr.y;
+    double4 qo4 = reinterpret_cast<const double4*>(s.nQ)[other];
+    double qo[4] = {qo4.x, qo4.y, qo4.z, qo4.w};
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      qmin[j] = qmin[j] <= qo[j] ? qmin[j] : qo[j];
+      qmax[j] = qmax[j] >= qo[j] ? qmax[j] : qo[j];
+    }
+    if (ORDER == 1 && a.do_grad) {
+      double4 w = m.edge_w[e];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        // dQ = nQ[R] - nQ[L] (gradient.C:391)
+        double dq = side ? (q0[j] - qo[j]) : (qo[j] - q0[j]);
+        if (side == 0) {
+          gr[2 * j] += w.x * dq;
+          gr[2 * j + 1] += w.y * dq;
+        } else {
+          gr[2 * j] -= w.z * dq;
+          gr[2 * j + 1] -= w.w * dq;
+        }
+      }
+    }
+  }
+  if (ORDER == 1 && a.do_grad) {
+    double4* g = reinterpret_cast<double4*>(s.grad) + 2 * n;
+    g[0] = make_double4(gr[0], gr[1], gr[2], gr[3]);
+    g[1] = make_double4(gr[4], gr[5], gr[6], gr[7]);
+  }
+
+  // ---- k=2: x = V S^-1 U^T b over the two-ring stencil ----
+  double h[20], pv[4];
+  if (ORDER == 3 && a.do_derivs) {
+    const int t0 = m.st_ptr[n], t1 = m.st_ptr[n + 1];
+    const int mrows = t1 - t0;
+    const double* U = m.svd_U1 + 5 * (long)t0;
+    const double* VT = m.svd_VT + 25 * (long)n;
+    const double* S = m.svd_S + 5 * (long)n;
+    const double* mo = m.moments + 9 * (long)n;
+    double acc[4][5];
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+      for (int c = 0; c < 5; c++) acc[v][c] = 0.;
+    for (int k = 0; k < mrows; k++) {
+      int nb = m.st_idx[t0 + k];
+      double w = m.st_w[t0 + k];
+      double4 qb4 = reinterpret_cast<const double4*>(s.nQ)[nb];
+      double bv[4] = {w * (qb4.x - q0[0]), w * (qb4.y - q0[1]), w * (qb4.z - q0[2]),
+                      w * (qb4.w - q0[3])};
+#pragma unroll
+      for (int c = 0; c < 5; c++) {
+        double u = U[c * mrows + k];
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[v][c] += bv[v] * u;
+      }
+    }
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+      double t1v[5], sol[5];
+#pragma unroll
+      for (int c = 0; c < 5; c++) t1v[c] = acc[v][c] / S[c];
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        double sum = 0.;
+#pragma unroll
+        for (int c = 0; c < 5; c++) sum += VT[j * 5 + c] * t1v[c];
+        sol[j] = sum;
+      }
+#pragma unroll
+      for (int c = 0; c < 5; c++) h[v * 5 + c] = sol[c];
+      pv[v] = q0[v] - mo[0] * sol[0] - mo[1] * sol[1] - mo[2] * sol[2] * 0.5 -
+              mo[3] * sol[3] * 0.5 - mo[4] * sol[4];
+    }
+    double* hd = s.hess5 + 20 * (long)n;
+#pragma unroll
+    for (int c = 0; c < 20; c++) hd[c] = h[c];
+    reinterpret_cast<double4*>(s.pv)[n] = make_double4(pv[0], pv[1], pv[2], pv[3]);
+  }
+
+  if (!a.do_lim) return;
+  // ---- Venkatakrishnan: unlimited reconstruction to every face point ----
+  double ph[4] = {1.0, 1.0, 1.0, 1.0};
+  for (int k = s0; k < s1; k++) {
+    int sd = m.nsub[k];
+    int sub = sd >> 1, side = sd & 1;
+    if (ORDER == 1) {
+      double4 d = m.sub_dx[sub];
+      double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        double qr = q0[j] + (gr[2 * j] * dx0 + gr[2 * j + 1] * dx1);
+        ph[j] = venkat_fold(ph[j], qr, q0[j], qmin[j], qmax[j]);
+      }
+    } else {
+      const double* xg = m.sub_xg + 6 * (long)sub;
+      double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
+#pragma unroll
+      for (int gpt = 0; gpt < 3; gpt++) {
+        double dx0 = xg[2 * gpt] - xn0, dx1 = xg[2 * gpt + 1] - xn1;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const double* hh = h + 5 * j;
+          double qr = pv[j];
+          qr += (hh[0] * dx0 + hh[1] * dx1 + hh[2] * dx0 * dx0 * 0.5 + hh[3] * dx1 * dx1 * 0.5 +
+                 hh[4] * dx0 * dx1);
+          ph[j] = venkat_fold(ph[j], qr, q0[j], qmin[j], qmax[j]);
+        }
+      }
+    }
+  }
+  double pmin = ph[0];
+#pragma unroll
+  for (int j = 1; j < 4; j++) pmin = pmin <= ph[j] ? pmin : ph[j];
+  double4* pp = reinterpret_cast<double4*>(s.phi) + 2 * n;
+  pp[0] = make_double4(pmin, pmin, ph[1], ph[1]);
+  pp[1] = make_double4(ph[2], ph[2], ph[3], ph[3]);
+  if (pmin < 0.0 || pmin > 1.0 || ph[1] < 0.0 || ph[1] > 1.0 || ph[2] < 0.0 || ph[2] > 1.0 ||
+      ph[3] < 0.0 || ph[3] > 1.0)
+    atomicOr(s.status, ERR_LIMITER);
+}
+
+// ---------------------------------------------------------------------------
+// Per subedge: face states, Roe flux, forward-difference Jacobian
+// (residual.C:112-333, reconstruct.C:181-203, jacobian.C:45-110).
+template <int RECON, bool JAC>
+__global__ void __launch_bounds__(128) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
+  int sub = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (sub > m.ns) return;
+  int2 lr = m.sub_lr[sub];
+  double4 g = m.sub_geo[sub];
+  double4 qa = reinterpret_cast<const double4*>(s.nQ)[lr.x];
+  double4 qb = reinterpret_cast<const double4*>(s.nQ)[lr.y];
+  double qL[4] = {qa.x, qa.y, qa.z, qa.w};
+  double qR[4] = {qb.x, qb.y, qb.z, qb.w};
+  if (RECON == 1) {
+    double4 d = m.sub_dx[sub];
+    const double* gL = s.grad + 8 * (long)lr.x;
+    const double* gR = s.grad + 8 * (long)lr.y;
+    double phL = s.phi[8 * (long)lr.x], phR = s.phi[8 * (long)lr.y];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      qL[j] += (phL * gL[2 * j] * d.x + phL * gL[2 * j + 1] * d.y);
+      qR[j] += (phR * gR[2 * j] * d.z + phR * gR[2 * j + 1] * d.w);
+    }
+  }
+  double flux[4];
+  roe_flux(g.x, g.y, g.z, a.gamma, qL, qR, flux);
+  reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
+  if (!JAC) return;
+  const double eps = 1.0e-08;
+  double* JLo = s.JL + 16 * (long)sub;
+  double* JRo = s.JR + 16 * (long)sub;
+#pragma unroll 1
+  for (int side = 0; side < 2; side++) {
+    double* Jo = side ? JRo : JLo;
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+      double qp[4], fp[4];
+      const double* base = side ? qR : qL;
+#pragma unroll
+      for (int j = 0; j < 4; j++) qp[j] = base[j];
+      qp[i] += eps;
+      if (side == 0)
+        roe_flux(g.x, g.y, g.z, a.gamma, qp, qR, fp);
+      else
+        roe_flux(g.x, g.y, g.z, a.gamma, qL, qp, fp);
+#pragma unroll
+      for (int j = 0; j < 4; j++) Jo[j * 4 + i] = (fp[j] - flux[j]) / eps;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per boundary edge: Set_Boundary_Values (cvbc.C:78-471) for its ghost, the
+// low-order boundary flux (residual.C:1147-1167) and the approximate
+// Jacobian (jacobian.C:681-962).  On the k=2 Gauss pass a curved bedge uses
+// the node normal and the arc length and writes the normal back into
+// xn_bedges (residual.C:1103-1143), as the reference does.
+template <bool JAC>
+__global__ void __launch_bounds__(128) k_boundary(DevMesh m, DevState s, StepArgs a) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (b > m.nbe) return;
+  int4 info = m.bed_info[b];
+  const int rn = info.x, gn = info.y, bc = info.z;
+  double* xnb = s.xn_bedges + 3 * (long)b;
+  double nx = xnb[0], ny = xnb[1];
+  const double gamma = a.gamma;
+  double4 qi4 = reinterpret_cast<const double4*>(s.nQ)[rn];
+  double4 qg4 = reinterpret_cast<const double4*>(s.nQ)[gn];
+  double rhoi = qi4.x, ui = qi4.y / rhoi, vi = qi4.z / rhoi;
+  double pi = (gamma - 1.) * (qi4.w - 0.5 * rhoi * (ui * ui + vi * vi));
+  double ci = sqrt((gamma * pi) / rhoi);
+  double rhob = qg4.x, ub = qg4.y / rhob, vb = qg4.z / rhob;
+  double pb = (gamma - 1.) * (qg4.w - 0.5 * rhob * (ub * ub + vb * vb));
+  double cb = sqrt((gamma * pb) / rhob);
+  double rho0 = 0.5 * (rhoi + rhob);
+  double c0 = 0.5 * (ci + cb);
+  double theta = ui * nx + vi * ny;
+  double ev1 = theta, ev3 = theta + ci, ev4 = theta - ci;
+  bool ok = true;
+  if (bc == 0 || (bc % 2 == 0)) {
+    if (ev1 <= 0.0 && ev4 <= 0.0) {
+      if (ev3 >= 0.0) {
+        pb = 0.5 * (a.pinf + pi - rho0 * c0 * ((a.uinf - ui) * nx + (a.vinf - vi) * ny));
+        rhob = 1.0 + (pb - a.pinf) / (c0 * c0);
+        ub = a.uinf + (pb - a.pinf) / (rho0 * c0) * nx;
+        vb = a.vinf + (pb - a.pinf) / (rho0 * c0) * ny;
+      } else if (ev3 < 0.0) {
+        rhob = 1.0; ub = a.uinf; vb = a.vinf; pb = a.pinf;
+      } else {
+        ok = false;
+      }
+    } else if (ev1 >= 0.0 && ev3 >= 0.0) {
+      if (ev4 <= 0.0) {
+        pb = a.pinf;
+        rhob = rhoi + (pb - pi) / (c0 * c0);
+        ub = ui - (pb - pi) / (rho0 * c0) * nx;
+        vb = vi - (pb - pi) / (rho0 * c0) * ny;
+      } else if (ev4 > 0.0) {
+        rhob = rhoi; ub = ui; vb = vi; pb = pi;
+      } else {
+        ok = false;
+      }
+    } else {
+      ok = false;
+    }
+  } else {
+    pb = pi + rho0 * c0 * theta;
+    rhob = rhoi + (pb - pi) / (c0 * c0);
+    ub = ui - (pb - pi) / (rho0 * c0) * nx;
+    vb = vi - (pb - pi) / (rho0 * c0) * ny;
+  }
+  if (!ok) {
+    atomicOr(s.status, ERR_BC);
+    return;
+  }
+  double qg[4];
+  qg[0] = rhob;
+  qg[1] = rhob * ub;
+  qg[2] = rhob * vb;
+  qg[3] = pb / (gamma - 1.0) + 0.5 * rhob * (ub * ub + vb * vb);
+  if (rhob < 0.0) {  // cvbc.C:447-470
+    rhob = rhoi;
+    ub = (1. - 2. * nx * nx) * ui - 2. * nx * ny * vi;
+    vb = (1. - 2. * ny * ny) * vi - 2. * nx * ny * ui;
+    pb = pi;
+    qg[0] = rhob;
+    qg[1] = rhob * ub;
+    qg[2] = rhob * vb;
+    qg[3] = pb / (gamma - 1.0) + 0.5 * rhob * (ub * ub + vb * vb);
+  }
+  reinterpret_cast<double4*>(s.nQ)[gn] = make_double4(qg[0], qg[1], qg[2], qg[3]);
+
+  double len = xnb[2];
+  if (a.gauss && bc > 10) {
+    double2 cn = m.bed_cnrm[b];
+    nx = cn.x;
+    ny = cn.y;
+    len = m.xgn_bedges[9 * (long)b + 2];
+    xnb[0] = nx;
+    xnb[1] = ny;
+  }
+  double qL[4] = {qi4.x, qi4.y, qi4.z, qi4.w};
+  double flux[4];
+  roe_flux(nx, ny, len, gamma, qL, qg, flux);
+  reinterpret_cast<double4*>(s.Fb)[b] = make_double4(flux[0], flux[1], flux[2], flux[3]);
+  if (!JAC) return;
+  double Rm[16];
+  roe_matrix(nx, ny, gamma, qL, qg, Rm);
+  double rhoL = qL[0], uL = qL[1] / qL[0], vL = qL[2] / qL[0], EL = qL[3];
+  double th = uL * nx + vL * ny;
+  double ph = 0.5 * (gamma - 1.) * (uL * uL + vL * vL);
+  double d[16];
+  d[0] = 0.;
+  d[1] = nx;
+  d[2] = ny;
+  d[3] = 0.;
+  d[4] = ph * nx - uL * th;
+  d[5] = (2. - gamma) * uL * nx + th;
+  d[6] = uL * ny - (gamma - 1.) * vL * nx;
+  d[7] = (gamma - 1.) * nx;
+  d[8] = ph * ny - vL * th;
+  d[9] = vL * nx - (gamma - 1.) * uL * ny;
+  d[10] = th + (2. - gamma) * vL * ny;
+  d[11] = (gamma - 1.) * ny;
+  double ger = gamma * EL / rhoL;
+  d[12] = (2. * ph - ger) * th;
+  d[13] = (1. - gamma) * uL * th + nx * (ger - ph);
+  d[14] = (1. - gamma) * vL * th + ny * (ger - ph);
+  d[15] = gamma * th;
+  double* Jo = s.Jb + 16 * (long)b;
+#pragma unroll
+  for (int k = 0; k < 16; k++) Jo[k] = 0.5 * (d[k] + Rm[k]) * len;
+}
+
+// ---------------------------------------------------------------------------
+// Per node: R and RHS = -R, the diagonal block (V/dt plus the face Jacobians
+// in face order), the off-diagonal blocks of the node's LHS row, and the LU
+// factors of the diagonal block for the sweeps (linear_algebra.C:226-246).
+template <bool JAC>
+__global__ void __launch_bounds__(128) k_assemble(DevMesh m, DevState s, StepArgs a) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > m.nn) return;
+  double r[4] = {0., 0., 0., 0.};
+  double D[16];
+  double V = m.cv_area[n];
+  double diag = V / (s.dt[n]);
+#pragma unroll
+  for (int k = 0; k < 16; k++) D[k] = 0.;
+  if (a.steady_diag) {
+    D[0] = diag;
+    D[5] = diag;
+    D[10] = diag;
+    D[15] = diag;
+  }
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int k = s0; k < s1; k++) {
+    int sd = m.nsub[k];
+    int sub = sd >> 1, side = sd & 1;
+    double4 f = reinterpret_cast<const double4*>(s.F)[sub];
+    if (side == 0) {
+      r[0] += f.x; r[1] += f.y; r[2] += f.z; r[3] += f.w;
+    } else {
+      r[0] -= f.x; r[1] -= f.y; r[2] -= f.z; r[3] -= f.w;
+    }
+    if (JAC) {
+      const double4* J = reinterpret_cast<const double4*>((side ? s.JR : s.JL) + 16 * (long)sub);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        double4 v = J[q];
+        if (side == 0) {
+          D[4 * q] += v.x; D[4 * q + 1] += v.y; D[4 * q + 2] += v.z; D[4 * q + 3] += v.w;
+        } else {
+          D[4 * q] -= v.x; D[4 * q + 1] -= v.y; D[4 * q + 2] -= v.z; D[4 * q + 3] -= v.w;
+        }
+      }
+    }
+  }
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  for (int k = b0; k < b1; k++) {
+    int b = m.nbed[k];
+    double4 f = reinterpret_cast<const double4*>(s.Fb)[b];
+    r[0] += f.x; r[1] += f.y; r[2] += f.z; r[3] += f.w;
+    if (JAC) {
+      const double4* J = reinterpret_cast<const double4*>(s.Jb + 16 * (long)b);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        double4 v = J[q];
+        D[4 * q] += v.x; D[4 * q + 1] += v.y; D[4 * q + 2] += v.z; D[4 * q + 3] += v.w;
+      }
+    }
+  }
+  reinterpret_cast<double4*>(s.R)[n] = make_double4(r[0], r[1], r[2], r[3]);
+  reinterpret_cast<double4*>(s.RHS)[n] = make_double4(-(r[0]), -(r[1]), -(r[2]), -(r[3]));
+  // the row of the block matrix
+  const int k0 = m.ia[n], k1 = m.ia[n + 1];
+  for (int k = k0; k < k1; k++) {
+    double4* out = reinterpret_cast<double4*>(s.LHS + 16 * (long)k);
+    if (m.ja[k] == n) {
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        out[q] = make_double4(D[4 * q], D[4 * q + 1], D[4 * q + 2], D[4 * q + 3]);
+      continue;
+    }
+    double B[16];
+#pragma unroll
+    for (int q = 0; q < 16; q++) B[q] = 0.;
+    if (JAC) {
+      int4 cs = m.csr_sub[k];
+      // row is the edge's L: += dF/dqR of each subedge; row is R: -= dF/dqL
+      const double* src = cs.z == 0 ? s.JR : s.JL;
+      for (int t = 0; t < 2; t++) {
+        int sub = t == 0 ? cs.x : cs.y;
+        if (sub < 0) break;
+        const double4* J = reinterpret_cast<const double4*>(src + 16 * (long)sub);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          double4 v = J[q];
+          if (cs.z == 0) {
+            B[4 * q] += v.x; B[4 * q + 1] += v.y; B[4 * q + 2] += v.z; B[4 * q + 3] += v.w;
+          } else {
+            B[4 * q] -= v.x; B[4 * q + 1] -= v.y; B[4 * q + 2] -= v.z; B[4 * q + 3] -= v.w;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      out[q] = make_double4(B[4 * q], B[4 * q + 1], B[4 * q + 2], B[4 * q + 3]);
+  }
+  lu4(D);
+  double4* lo = reinterpret_cast<double4*>(s.LUd + 16 * (long)n);
+#pragma unroll
+  for (int q = 0; q < 4; q++) lo[q] = make_double4(D[4 * q], D[4 * q + 1], D[4 * q + 2], D[4 * q + 3]);
+}
+
+// LHS = 0 with V/dt on the diagonal blocks (init_memory.C:189-290).
+__global__ void __launch_bounds__(128) k_diag_only(DevMesh m, DevState s) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > m.nn) return;
+  double d = m.cv_area[n] / (s.dt[n]);
+  for (int k = m.ia[n]; k < m.ia[n + 1]; k++) {
+    double4* out = reinterpret_cast<double4*>(s.LHS + 16 * (long)k);
+    bool dg = m.ja[k] == n;
+    out[0] = make_double4(dg ? d : 0., 0., 0., 0.);
+    out[1] = make_double4(0., dg ? d : 0., 0., 0.);
+    out[2] = make_double4(0., 0., dg ? d : 0., 0.);
+    out[3] = make_double4(0., 0., 0., dg ? d : 0.);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ordered block Gauss-Seidel sweep (linear_algebra.C:178-344).  Rows are
+// handed out in the reference's order (ascending forward, descending
+// backward) by an atomic dispenser; one warp per row.  A row waits only for
+// the rows it reads that the reference updates earlier in the same sweep
+// (its lower, resp. upper, neighbours): each finished row publishes its dQ
+// and then a release flag.  Since a row is only claimed by a running warp
+// and every dependency was claimed earlier, the earliest unfinished row can
+// always proceed; every wait is nevertheless bounded and reports
+// ERR_SWEEP_TIMEOUT instead of spinning forever.
+// Lanes: 8 block slots x 4 matrix rows.
+template <bool FWD>
+__global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, int epoch,
+                                                       long max_spin) {
+  if (*s.skip) return;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int slot = lane >> 2, r = lane & 3;
+  const int nn = m.nn;
+  for (;;) {
+    unsigned t = 0;
+    if (lane == 0) t = atomicAdd(s.counter, 1u);
+    t = __shfl_sync(FULL, t, 0);
+    if (t >= (unsigned)nn) break;
+    const int j = FWD ? (int)(1 + t) : (int)(nn - t);
+    const int k0 = m.ia[j], k1 = m.ia[j + 1];
+    double acc = s.RHS[4 * (long)j + r];
+    for (int base = k0; base < k1; base += 8) {
+      const int k = base + slot;
+      double term = 0.;
+      bool use = false;
+      if (k < k1) {
+        const int c = m.ja[k];
+        if (c != j) {
+          use = true;
+          const bool dep = FWD ? (c < j) : (c > j);
+          if (dep) {
+            cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[c]);
+            long spins = 0;
+            while (f.load(cuda::memory_order_acquire) != epoch) {
+              if (++spins > max_spin) {
+                atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+                break;
+              }
+              // once any wait has timed out, every other wait gives up too
+              if ((spins & 1023) == 0 &&
+                  (*(volatile int*)s.status & ERR_SWEEP_TIMEOUT))
+                break;
+              __nanosleep(32);
+            }
+          }
+          const double* dq = s.dQ + 4 * (long)c;
+          double d[4] = {__ldcg(dq), __ldcg(dq + 1), __ldcg(dq + 2), __ldcg(dq + 3)};
+          term = row_dot(s.LHS + 16 * (long)k, r, d);
+        }
+      }
+      const unsigned used = __ballot_sync(FULL, use);
+#pragma unroll
+      for (int sl = 0; sl < 8; sl++) {
+        double tv = __shfl_sync(FULL, term, sl * 4 + r);
+        if (used & (1u << (sl * 4))) acc -= tv;
+      }
+    }
+    double b[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) b[q] = __shfl_sync(FULL, acc, q);
+    if (lane == 0) {
+      double X[4];
+      double M[16];
+      const double4* lu = reinterpret_cast<const double4*>(s.LUd + 16 * (long)j);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        double4 v = lu[q];
+        M[4 * q] = v.x; M[4 * q + 1] = v.y; M[4 * q + 2] = v.z; M[4 * q + 3] = v.w;
+      }
+      lu_solve4(M, b, X);
+      double* dq = s.dQ + 4 * (long)j;
+      double o[4] = {__ldcg(dq), __ldcg(dq + 1), __ldcg(dq + 2), __ldcg(dq + 3)};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        double dx = X[q] - o[q];
+        o[q] += dx;
+      }
+      __stcg(reinterpret_cast<double2*>(dq), make_double2(o[0], o[1]));
+      __stcg(reinterpret_cast<double2*>(dq) + 1, make_double2(o[2], o[3]));
+      cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[j]);
+      f.store(epoch, cuda::memory_order_release);
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic block reduction helper: fixed tree over kRedThreads lanes.
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  const int tid = threadIdx.x;
+  sh[tid] = v;
+  __syncthreads();
+#pragma unroll
+  for (int w = kRedThreads / 2; w > 0; w >>= 1) {
+    if (tid < w) sh[tid] += sh[tid + w];
+    __syncthreads();
+  }
+  double out = sh[0];
+  __syncthreads();
+  return out;
+}
+
+// b - Ax of every row (linear_algebra.C:348-387), squared, partial sums.
+__global__ void __launch_bounds__(kRedThreads) k_lin_residual(DevMesh m, DevState s) {
+  __shared__ double sh[kRedThreads];
+  double acc = 0.;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x + 1; j <= m.nn;
+       j += gridDim.x * blockDim.x) {
+    double r[4];
+    const double4 rh = reinterpret_cast<const double4*>(s.RHS)[j];
+    r[0] = rh.x; r[1] = rh.y; r[2] = rh.z; r[3] = rh.w;
+    for (int k = m.ia[j]; k < m.ia[j + 1]; k++) {
+      const double4 d4 = reinterpret_cast<const double4*>(s.dQ)[m.ja[k]];
+      const double d[4] = {d4.x, d4.y, d4.z, d4.w};
+      const double* A = s.LHS + 16 * (long)k;
+#pragma unroll
+      for (int q = 0; q < 4; q++) r[q] -= row_dot(A, q, d);
+    }
+    acc += (r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+  }
+  double tot = block_sum(acc, sh);
+  if (threadIdx.x == 0) s.partial[blockIdx.x] = tot;
+}
+
+// Sum the partials in a fixed order; slot 0 = RMS (sets skip below 1e-15).
+__global__ void k_finalize_rms(DevState s, int nparts, int nn) {
+  __shared__ double sh[kRedThreads];
+  double v = 0.;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) v += s.partial[i];
+  double tot = block_sum(v, sh);
+  if (threadIdx.x == 0) {
+    double rms = tot / (1. * nn);
+    rms = sqrt(rms);
+    s.scalars[0] = rms;
+    if (rms < 1.0E-15) *s.skip = 1;
+  }
+}
+
+// nQ += dQ, pQ <- Q, Q <- nQ (solve.C:901-928) and partial sums of |dQ|^2
+// and |R_rho|^2.
+__global__ void __launch_bounds__(kRedThreads) k_finish_step(DevMesh m, DevState s, int last) {
+  __shared__ double sh[kRedThreads];
+  double dq2 = 0., r2 = 0.;
+  const int total = m.nn + m.ng;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= total;
+       i += gridDim.x * blockDim.x) {
+    double4 nq = reinterpret_cast<const double4*>(s.nQ)[i];
+    if (i <= m.nn) {
+      double4 d = reinterpret_cast<const double4*>(s.dQ)[i];
+      dq2 += (d.x * d.x + d.y * d.y + d.z * d.z + d.w * d.w);
+      double rr = s.R[4 * (long)i];
+      r2 += rr * rr;
+      nq.x += d.x; nq.y += d.y; nq.z += d.z; nq.w += d.w;
+      reinterpret_cast<double4*>(s.nQ)[i] = nq;
+    }
+    if (last) {
+      reinterpret_cast<double4*>(s.pQ)[i] = reinterpret_cast<const double4*>(s.Q)[i];
+      reinterpret_cast<double4*>(s.Q)[i] = nq;
+    }
+  }
+  double a = block_sum(dq2, sh);
+  double b = block_sum(r2, sh);
+  if (threadIdx.x == 0) {
+    s.partial[blockIdx.x] = a;
+    s.partial[kRedBlocks + blockIdx.x] = b;
+  }
+}
+
+__global__ void k_finalize_step(DevState s, double* hist_dq, double* hist_r, int slot) {
+  __shared__ double sh[kRedThreads];
+  double a = 0., b = 0.;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) {
+    a += s.partial[i];
+    b += s.partial[kRedBlocks + i];
+  }
+  double ta = block_sum(a, sh);
+  double tb = block_sum(b, sh);
+  if (threadIdx.x == 0) {
+    s.scalars[1] = ta;
+    s.scalars[2] = tb;
+    if (hist_dq) hist_dq[slot] = sqrt(ta);
+    if (hist_r) hist_r[slot] = sqrt(tb);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Compute_Body_Forces (grid_io.C:1430-1694): per wall bedge the 3-point
+// pressure integral, then the reference's sequential sum over bedges.
+__device__ __forceinline__ void recon_boundary_point(const DevMesh& m, const DevState& s, int n,
+                                                     int order, const double* gp, double* q) {
+  double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
+  q[0] = q4.x; q[1] = q4.y; q[2] = q4.z; q[3] = q4.w;
+  if (order == 0) return;
+  double phi = s.phi[8 * (long)n], sig = s.phi[8 * (long)n + 1];
+  double dx0 = gp[0] - m.x[2 * n], dx1 = gp[1] - m.x[2 * n + 1];
+  if (order == 1) {
+    const double* g = s.grad + 8 * (long)n;
+#pragma unroll
+    for (int j = 0; j < 4; j++) q[j] += (phi * g[2 * j] * dx0 + phi * g[2 * j + 1] * dx1);
+  } else {
+    const double* h = s.hess5 + 20 * (long)n;
+#pragma unroll
+    for (int j = 0; j < 4; j++) q[j] = s.pv[4 * (long)n + j];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double* hh = h + 5 * j;
+      q[j] += (phi * hh[0] * dx0 + phi * hh[1] * dx1 + sig * hh[2] * dx0 * dx0 * 0.5 +
+               sig * hh[3] * dx1 * dx1 * 0.5 + sig * hh[4] * dx0 * dx1);
+    }
+  }
+}
+
+__global__ void k_body_forces(DevMesh m, DevState s, StepArgs a, int recon_order) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (b > m.nbe) return;
+  int4 info = m.bed_info[b];
+  double* out = s.bforce + 4 * (long)b;
+  if (!info.w) {
+    out[0] = 0.;
+    out[1] = 0.;
+    out[2] = 0.;
+    return;
+  }
+  const int rn = info.x, bc = info.z;
+  double t1 = 0., t2 = 0., len, q[4];
+  if (bc <= 10) {
+    const double* xnb = s.xn_bedges + 3 * (long)b;
+    double nx = -xnb[0], ny = -xnb[1];
+    len = xnb[2];
+    const double w[3] = {5. / 9., 8. / 9., 5. / 9.};
+    for (int k = 0; k < 3; k++) {
+      recon_boundary_point(m, s, rn, recon_order, m.xg_bedges + 6 * (long)b + 2 * k, q);
+      double rr = q[0], u = q[1] / rr, v = q[2] / rr, e = q[3];
+      double P = (a.gamma - 1.) * (e - 0.5 * rr * (u * u + v * v));
+      t1 += (w[k] * (P * ny * a.cos_a - P * nx * a.sin_a));
+      t2 += (w[k] * (P * nx * a.cos_a + P * ny * a.sin_a));
+    }
+  } else {
+    len = m.xgn_bedges[9 * (long)b + 2];
+    const double w[3] = {8. / 9., 5. / 9., 5. / 9.};
+    for (int k = 0; k < 3; k++) {
+      double nx = -m.xgn_bedges[9 * (long)b + 3 * k], ny = -m.xgn_bedges[9 * (long)b + 3 * k + 1];
+      recon_boundary_point(m, s, rn, recon_order, m.xg_bedges + 6 * (long)b + 2 * k, q);
+      double rr = q[0], u = q[1] / rr, v = q[2] / rr, e = q[3];
+      double P = (a.gamma - 1.) * (e - 0.5 * rr * (u * u + v * v));
+      t1 += (w[k] * (P * ny * a.cos_a - P * nx * a.sin_a));
+      t2 += (w[k] * (P * nx * a.cos_a + P * ny * a.sin_a));
+    }
+  }
+  out[0] = t1 * len * 0.5;
+  out[1] = t2 * len * 0.5;
+  out[2] = 1.;
+}
+
+__global__ void k_body_forces_sum(DevMesh m, DevState s) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double f0 = 0., f1 = 0.;
+  for (int b = 1; b <= m.nbe; b++) {
+    const double* o = s.bforce + 4 * (long)b;
+    if (o[2] != 0.) {
+      f0 += o[0];
+      f1 += o[1];
+    }
+  }
+  s.scalars[4] = f0;
+  s.scalars[5] = f1;
+}
+
+}  // namespace flow

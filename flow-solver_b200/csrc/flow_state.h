@@ -1,0 +1,93 @@
+// flow_state.h - device-resident mesh and solver state of one flow context.
+//
+// Node arrays keep the reference's 1-based array-of-structs layout (a node's
+// 4 conserved variables are one aligned 32-byte sector, its gradient one
+// 64-byte line), because every face kernel gathers whole node records by
+// index.  Face data is re-laid out per face as small aligned structs so each
+// face is read with one or two vector loads.  All incidence lists are sorted
+// by face index, which is what makes the per-node gathers reproduce the
+// reference's sequential scatter order bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace flow {
+
+struct DevMesh {
+  int nn;        // real nodes (1..nn)
+  int ng;        // ghost nodes (nn+1..nn+ng)
+  int ne;        // edges (1..ne)
+  int ns;        // subedges (1..ns)
+  int nbe;       // boundary edges (1..nbe)
+  int nnz;       // CSR blocks
+  int order;     // reconstruction order of the run (1 or 3)
+  int stencil_max;
+  // node -> incident subedges, (s << 1) | side, side 0 = node is the edge's L
+  const int* nsub_ptr;
+  const int* nsub;
+  // node -> incident boundary edges (ascending)
+  const int* nbed_ptr;
+  const int* nbed;
+  // node -> incident edges, (e << 1) | side
+  const int* nedg_ptr;
+  const int* nedg;
+  // block CSR (reference Build_CRS layout: diagonal block last in each row)
+  const int* ia;
+  const int* iau;
+  const int* ja;
+  const int4* csr_sub;   // per block: {first subedge, second subedge or -1, role, 0}
+  // faces
+  const int2* sub_lr;
+  const double4* sub_geo;  // nx, ny, len, 0
+  const double4* sub_dx;   // face point - x[L], face point - x[R]
+  const double* sub_xg;    // 3 Gauss points, 6 doubles
+  const int2* edge_lr;
+  const double4* edge_w;   // LSQ weights wL (2), wR (2)
+  const int4* bed_info;    // real node, ghost node (absolute), bc, is_wall
+  const double2* bed_cnrm; // curved-boundary normal at the real node
+  const double* xg_bedges; // 6 per bedge
+  const double* xgn_bedges;// 9 per bedge
+  // nodes
+  const double* x;
+  const double* cv_area;
+  const int* node_order;
+  const double* moments;   // 9 per node
+  // k=2 stencil and factors
+  const int* st_ptr;
+  const int* st_idx;
+  const double* st_w;
+  const double* svd_U1;    // per node: 5 columns of U, column-major, offset 5*st_ptr[i]
+  const double* svd_VT;    // 25 per node
+  const double* svd_S;     // 5 per node
+};
+
+struct DevState {
+  double* Q;
+  double* nQ;
+  double* pQ;
+  double* dQ;
+  double* R;
+  double* RHS;
+  double* grad;     // 8 per node
+  double* phi;      // 8 per node
+  double* hess5;    // 20 per node (var-major, 5 derivatives)
+  double* pv;       // 4 per node (point values)
+  double* dt;
+  double* LHS;      // nnz * 16
+  double* LUd;      // 16 per node: LU factors of the diagonal block
+  double* xn_bedges;// 3 per bedge (mutated by the k=2 boundary pass)
+  double* F;        // 4 per subedge
+  double* JL;       // 16 per subedge
+  double* JR;       // 16 per subedge
+  double* Fb;       // 4 per bedge
+  double* Jb;       // 16 per bedge
+  double* bforce;   // 4 per bedge: lift, drag, is-wall (body-force scratch)
+  int* done;        // per row epoch flags for the ordered sweeps
+  unsigned int* counter;  // row dispenser for the ordered sweeps
+  int* status;      // sticky error bits (FLOW_ERR_*)
+  int* skip;        // set when the linear residual dropped below 1e-15
+  double* partial;  // reduction partials
+  double* scalars;  // [0] rms, [1] dq^2, [2] R_rho^2, [3] cfl, [4] F_lift, [5] F_drag
+};
+
+}  // namespace flow

@@ -1,0 +1,235 @@
+"""ctypes binding of libflowgpu.so (include/flow_gpu.h).
+
+The solver only runs through the CUDA library: importing works without a
+GPU, but constructing a ``Solver`` fails loudly when the library or a CUDA
+device is missing.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libflowgpu.so")
+
+IP = C.POINTER(C.c_int)
+DP = C.POINTER(C.c_double)
+LP = C.POINTER(C.c_long)
+
+ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
+          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND"}
+
+# exported symbols, in include/flow_gpu.h order
+SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
+           "flow_build_matrix", "flow_reconstruct", "flow_residuals", "flow_linear_solve",
+           "flow_body_forces", "flow_get", "flow_size", "flow_set_sweep_mode", "flow_status",
+           "flow_clear_status", "flow_last_error", "flow_launch_count", "flow_last_device_ms")
+
+
+class FlowParamsC(C.Structure):
+    """struct flow_params (mirrors the reference's PARAMS)."""
+    _fields_ = [("nsteps", C.c_int), ("iter", C.c_int), ("jufreq", C.c_int),
+                ("CFL", C.c_double), ("ramp", C.c_int), ("gamma", C.c_double),
+                ("alpha", C.c_double), ("mach", C.c_double), ("subits", C.c_int),
+                ("unsteady", C.c_int), ("tacc", C.c_int), ("mintime", C.c_double),
+                ("method", C.c_int), ("order", C.c_int), ("foits", C.c_int), ("soits", C.c_int),
+                ("toits", C.c_int), ("isrestart", C.c_int), ("limit", C.c_int),
+                ("reorder", C.c_int), ("ic", C.c_int), ("p_or_cv", C.c_int),
+                ("start_post_pro", C.c_int), ("post_pro_freq", C.c_int)]
+
+
+_VIEW_INTS = ("nn", "nn_ghost", "nedges", "nsubedges", "nbedges", "nb", "nelem")
+_VIEW_IPTR = ("edges", "subedges", "bedges", "bedge_seg", "bbc", "node_order", "ia", "iau", "ja")
+_VIEW_DPTR = ("x", "cv_area", "el_cent", "xn_subedges", "xm_subedges", "xg_subedges",
+              "xn_bedges", "xg_bedges", "xgn_bedges", "edge_weight", "moments")
+_VIEW_IPTR2 = ("gnsn", "gnnsn", "gnnsn1", "svd_m")
+
+
+class FlowGridView(C.Structure):
+    _fields_ = ([(n, C.c_int) for n in _VIEW_INTS]
+                + [(n, IP) for n in _VIEW_IPTR]
+                + [(n, DP) for n in _VIEW_DPTR]
+                + [(n, IP) for n in _VIEW_IPTR2[:3]]
+                + [("svd_m", IP), ("svd_off", LP), ("svd_U", DP), ("svd_VT", DP),
+                   ("svd_S", DP)])
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load():
+    """Load libflowgpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with flow-solver_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    PP = C.POINTER(FlowParamsC)
+    L.flow_create.restype = vp
+    L.flow_create.argtypes = [C.POINTER(FlowGridView), PP, C.c_int, IP]
+    L.flow_destroy.argtypes = [vp]
+    L.flow_set_state.argtypes = [vp, DP]
+    L.flow_solve.argtypes = [vp, PP, C.c_int, DP, DP]
+    L.flow_run.argtypes = [vp, PP, C.c_int, C.c_int, DP, DP]
+    L.flow_build_matrix.argtypes = [vp, PP, C.c_int]
+    L.flow_reconstruct.argtypes = [vp, PP, C.c_int]
+    L.flow_residuals.argtypes = [vp, PP, C.c_int, C.c_int]
+    L.flow_linear_solve.argtypes = [vp, PP, DP]
+    L.flow_body_forces.argtypes = [vp, PP, DP]
+    L.flow_get.argtypes = [vp, C.c_char_p, DP, C.c_long]
+    L.flow_size.restype = C.c_long
+    L.flow_size.argtypes = [vp, C.c_char_p]
+    L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
+    L.flow_status.argtypes = [vp]
+    L.flow_clear_status.argtypes = [vp]
+    L.flow_last_error.restype = C.c_char_p
+    L.flow_launch_count.restype = C.c_long
+    L.flow_launch_count.argtypes = [vp]
+    L.flow_last_device_ms.restype = C.c_double
+    L.flow_last_device_ms.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def params_struct(fp) -> FlowParamsC:
+    """fp: flowgpu.meshgen.FlowParams (or any object with the PARAMS fields)."""
+    p = FlowParamsC()
+    for name, ct in FlowParamsC._fields_:
+        v = getattr(fp, name)
+        setattr(p, name, float(v) if ct is C.c_double else int(v))
+    return p
+
+
+class FlowError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        names = [n for b, n in ERRORS.items() if code & b]
+        msg = f"flow_gpu error {code} ({'|'.join(names) or '?'})"
+        if what:
+            msg += f": {what}"
+        super().__init__(msg)
+        self.code = code
+
+
+def _check(rc: int, what: str = ""):
+    if rc:
+        err = load().flow_last_error()
+        raise FlowError(rc, (what + " " + (err.decode() if err else "")).strip())
+
+
+class Solver:
+    """One device-resident mesh + state (a flow_ctx).
+
+    ``arrays`` holds the grid in the reference's layout (see
+    ``FlowGridView``); ``sizes`` its counts.
+    """
+
+    def __init__(self, sizes: dict, arrays: dict, params, device: int = 0):
+        self.L = load()
+        self._keep = {}
+        v = FlowGridView()
+        for n in _VIEW_INTS:
+            setattr(v, n, int(sizes[n]))
+        for n in _VIEW_IPTR + _VIEW_IPTR2:
+            a = arrays.get(n)
+            if a is not None:
+                a = np.ascontiguousarray(a, dtype=np.int32)
+                self._keep[n] = a
+                setattr(v, n, a.ctypes.data_as(IP))
+        for n in _VIEW_DPTR + ("svd_U", "svd_VT", "svd_S"):
+            a = arrays.get(n)
+            if a is not None:
+                a = np.ascontiguousarray(a, dtype=np.float64)
+                self._keep[n] = a
+                setattr(v, n, a.ctypes.data_as(DP))
+        off = arrays.get("svd_off")
+        if off is not None:
+            off = np.ascontiguousarray(off, dtype=np.int64)
+            self._keep["svd_off"] = off
+            v.svd_off = off.ctypes.data_as(LP)
+        self.params = params
+        self.p = params_struct(params)
+        st = C.c_int(0)
+        self.ctx = self.L.flow_create(C.byref(v), C.byref(self.p), int(device), C.byref(st))
+        self._keep = None  # the library copied everything it needs
+        if not self.ctx:
+            _check(st.value or 1, "flow_create")
+        self.sizes = dict(sizes)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.L.flow_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_params(self, params):
+        self.params = params
+        self.p = params_struct(params)
+
+    def set_state(self, Q: np.ndarray):
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        _check(self.L.flow_set_state(self.ctx, Q.ctypes.data_as(DP)), "flow_set_state")
+
+    def solve(self, ts: int):
+        dq, rr = C.c_double(), C.c_double()
+        _check(self.L.flow_solve(self.ctx, C.byref(self.p), ts, C.byref(dq), C.byref(rr)),
+               f"flow_solve ts={ts}")
+        return dq.value, rr.value
+
+    def run(self, ts0: int, nsteps: int):
+        rh = np.zeros(max(nsteps, 1))
+        dh = np.zeros(max(nsteps, 1))
+        _check(self.L.flow_run(self.ctx, C.byref(self.p), ts0, nsteps, rh.ctypes.data_as(DP),
+                               dh.ctypes.data_as(DP)), "flow_run")
+        return rh[:nsteps], dh[:nsteps]
+
+    def build_matrix(self, citer: int):
+        _check(self.L.flow_build_matrix(self.ctx, C.byref(self.p), citer), "flow_build_matrix")
+
+    def reconstruct(self, ts: int):
+        _check(self.L.flow_reconstruct(self.ctx, C.byref(self.p), ts), "flow_reconstruct")
+
+    def residuals(self, jupdate: int, ts: int):
+        _check(self.L.flow_residuals(self.ctx, C.byref(self.p), jupdate, ts), "flow_residuals")
+
+    def linear_solve(self) -> float:
+        r = C.c_double()
+        _check(self.L.flow_linear_solve(self.ctx, C.byref(self.p), C.byref(r)), "flow_linear_solve")
+        return r.value
+
+    def body_forces(self):
+        f = (C.c_double * 2)()
+        _check(self.L.flow_body_forces(self.ctx, C.byref(self.p), f), "flow_body_forces")
+        return f[0], f[1]
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.L.flow_size(self.ctx, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        _check(self.L.flow_get(self.ctx, name.encode(), out.ctypes.data_as(DP), n), f"get {name}")
+        return out
+
+    def set_sweep_mode(self, mode: int):
+        _check(self.L.flow_set_sweep_mode(self.ctx, int(mode)), "flow_set_sweep_mode")
+
+    def status(self) -> int:
+        return self.L.flow_status(self.ctx)
+
+    def launch_count(self) -> int:
+        return self.L.flow_launch_count(self.ctx)
+
+    def last_device_ms(self) -> float:
+        return self.L.flow_last_device_ms(self.ctx)

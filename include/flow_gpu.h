@@ -1,0 +1,186 @@
+/*
+ * flow_gpu.h - C ABI of the B200 implementation of the flow solver's
+ * nonlinear iteration (libflowgpu.so).
+ *
+ * The reference solver (shedsaw/flow-solver) exposes this path as C++
+ * functions over its GRID / SYS_MEM / PARAMS objects.  Every entry point
+ * below replaces one of them and takes the same data as plain pointers in the
+ * reference's own array layout (1-based, array-of-structs), so a C++ shim
+ * with the reference's signatures can forward GRID fields directly (see
+ * INTEGRATION.md).  No torch or CUDA types appear in the signatures.
+ *
+ * Error behaviour: where the reference prints and calls exit() (cvbc.C:330,
+ * init_memory.C:257-268, limiter.C:965-977, cv_calc.C:868-875), these entry
+ * points return a nonzero FLOW_ERR_* bit set instead and leave the context
+ * usable.  All functions are synchronous with respect to the host buffers
+ * they take; the device work of one context runs on its own CUDA stream.
+ */
+#ifndef FLOW_GPU_H
+#define FLOW_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Error bits (sticky per context until flow_clear_status). */
+#define FLOW_OK 0
+#define FLOW_ERR_ARG 1          /* bad argument or unsupported option */
+#define FLOW_ERR_CUDA 2         /* CUDA runtime error */
+#define FLOW_ERR_EIGEN 4        /* non-finite wave speed (cv_calc.C:868-875) */
+#define FLOW_ERR_DT 8           /* dt <= 0 or non-finite (init_memory.C:257-268) */
+#define FLOW_ERR_LIMITER 16     /* phi outside [0,1] (limiter.C:965-977) */
+#define FLOW_ERR_BC 32          /* invalid far-field state (cvbc.C:330-382) */
+#define FLOW_ERR_SWEEP_TIMEOUT 64 /* an ordered sweep waited past its bound */
+#define FLOW_ERR_NOT_FOUND 128  /* unknown array name */
+
+/* Mirrors PARAMS (include/params.h:19-76 of the reference), same field
+ * order and meaning as euler.params (params.C:44-217). */
+typedef struct flow_params {
+  int nsteps;
+  int iter;
+  int jufreq;
+  double CFL;
+  int ramp;
+  double gamma;
+  double alpha;
+  double mach;
+  int subits;
+  int unsteady;
+  int tacc;
+  double mintime;
+  int method;
+  int order;
+  int foits;
+  int soits;
+  int toits;
+  int isrestart;
+  int limit;
+  int reorder;
+  int ic;
+  int p_or_cv;
+  int start_post_pro;
+  int post_pro_freq;
+} flow_params;
+
+/* Read-only view of a pre-processed grid in the reference's layout
+ * (include/grid.h:223-307 and include/sys_mem.h:43-49).  Array lengths are
+ * those the reference allocates (index 0 unused unless noted). */
+typedef struct flow_grid_view {
+  int nn;          /* GRID::nn */
+  int nn_ghost;    /* GRID::nn_ghost */
+  int nedges;      /* GRID::nedges */
+  int nsubedges;   /* GRID::nsubedges */
+  int nbedges;     /* GRID::nbedges */
+  int nb;          /* GRID::nb */
+  int nelem;       /* triangles + quads */
+  const int *edges;       /* (nedges+1)*2 */
+  const int *subedges;    /* (nsubedges+1)*2 */
+  const int *bedges;      /* (nbedges+1)*5 */
+  const int *bedge_seg;   /* (nbedges+1)*2: GRID::bs[b][s][0..1] of each bedge */
+  const int *bbc;         /* nb+1 */
+  const int *node_order;  /* nn+nn_ghost+1 */
+  const int *ia;          /* nn+2   (SYS_MEM::ia) */
+  const int *iau;         /* nn+1   (SYS_MEM::iau) */
+  const int *ja;          /* ia[nn+1] (SYS_MEM::ja) */
+  const double *x;            /* (nn+nn_ghost+1)*2 */
+  const double *cv_area;      /* nn+1 */
+  const double *el_cent;      /* (nelem+1)*2 */
+  const double *xn_subedges;  /* (nsubedges+1)*3 */
+  const double *xm_subedges;  /* (nsubedges+1)*2 */
+  const double *xg_subedges;  /* (nsubedges+1)*6 */
+  const double *xn_bedges;    /* (nbedges+1)*3, initial values */
+  const double *xg_bedges;    /* (nbedges+1)*6 */
+  const double *xgn_bedges;   /* (nbedges+1)*9 */
+  const double *edge_weight;  /* (nedges+1)*4 (gradient.C:923-1121); NULL if order != 1 */
+  const double *moments;      /* (nn+1)*9 (GRID::Moments); NULL if order != 3 */
+  /* k=2 two-ring stencils after the growth of solve.C:57-114 (GRID::gnsn,
+   * gnnsn, gnnsn1) and the SVD factors of compute_derivatives.C:845-940
+   * (GRID::SVD_U / SVD_V / SVD_S); NULL if order != 3. */
+  const int *gnsn;
+  const int *gnnsn;
+  const int *gnnsn1;
+  const int *svd_m;           /* nn+1: rows m of node i's system */
+  const long *svd_off;        /* nn+1: offset of node i's m*m U in svd_U */
+  const double *svd_U;        /* concatenated column-major m x m */
+  const double *svd_VT;       /* (nn+1)*25 */
+  const double *svd_S;        /* (nn+1)*5 */
+} flow_grid_view;
+
+typedef struct flow_ctx flow_ctx;
+
+/* Upload a grid (and the CSR pattern of Build_CRS, init_memory.C:36-138) to
+ * device `device`.  Replaces the lazily built device mirror the reference's
+ * solve() would need; returns NULL and sets *status on failure. */
+flow_ctx *flow_create(const flow_grid_view *grid, const flow_params *p, int device,
+                      int *status);
+void flow_destroy(flow_ctx *ctx);
+
+/* Set GRID::Q (and nQ = Q), (nn+nn_ghost+1)*4 doubles (ic.C:36-99 output). */
+int flow_set_state(flow_ctx *ctx, const double *Q);
+
+/* double solve(GRID*, SYS_MEM*, PARAMS, int ts)  (include/solve.h:21,
+ * solve.C:44-933): one pseudo-time step at time step ts (GRID::citer = ts).
+ * *dq_norm receives the return value ||dQ||_2 and *r_rho the density
+ * residual norm ||R[:,0]||_2 of the last Newton iteration (either may be
+ * NULL). */
+int flow_solve(flow_ctx *ctx, const flow_params *p, int ts, double *dq_norm, double *r_rho);
+
+/* Run `nsteps` steps ts = ts0 .. ts0+nsteps-1 without host round trips
+ * (the driver loop of main.C:789-815); stops early on error.  r_rho_hist and
+ * dq_hist (optional, nsteps entries) receive the per-step norms. */
+int flow_run(flow_ctx *ctx, const flow_params *p, int ts0, int nsteps, double *r_rho_hist,
+             double *dq_hist);
+
+/* void build_matrix(GRID*, PARAMS, SYS_MEM*)  (include/init_memory.h:24,
+ * init_memory.C:159-310) with GRID::citer = citer; writes dt and the V/dt
+ * diagonal (LHS otherwise zero). */
+int flow_build_matrix(flow_ctx *ctx, const flow_params *p, int citer);
+
+/* Compute_Gradient_LeastSquares (gradient.C:245-403) or, for order 3,
+ * Compute_Derivatives(grid, p, 3) (compute_derivatives.C:1438-1534),
+ * followed by compute_limiter_venkatakrishnan (limiter.C:511-983) when
+ * p->limit == 2.  Uses the current nQ. */
+int flow_reconstruct(flow_ctx *ctx, const flow_params *p, int ts);
+
+/* void build_interior_residuals(GRID*, SYS_MEM*, PARAMS, int jupdate, int ts)
+ * (include/residual.h:21, residual.C:40-342) together with
+ * void build_boundary_residuals(GRID*, SYS_MEM*, PARAMS, int jupdate)
+ * (include/residual.h:23, residual.C:359-1230) and the Jacobian callbacks of
+ * include/jacobian.h:21-33; assembles R, RHS = -R and the LHS blocks on top
+ * of the diagonal written by flow_build_matrix. */
+int flow_residuals(flow_ctx *ctx, const flow_params *p, int jupdate, int ts);
+
+/* double linear_solve(GRID*, SYS_MEM*, PARAMS)  (include/linear_algebra.h:23,
+ * linear_algebra.C:122-401): p->subits alternating ordered block Gauss-Seidel
+ * sweeps from dQ = 0; *rms receives the returned b-Ax RMS. */
+int flow_linear_solve(flow_ctx *ctx, const flow_params *p, double *rms);
+
+/* void Compute_Body_Forces(GRID*, PARAMS, double*)  (include/grid_io.h:36,
+ * grid_io.C:1390-1697): raw pressure lift and drag on the wall boundaries. */
+int flow_body_forces(flow_ctx *ctx, const flow_params *p, double *forces);
+
+/* Copy a named array back in the reference layout: "Q", "nQ", "pQ", "dQ",
+ * "R", "RHS", "LHS", "grad", "phi", "hess" ((nn+1)*36), "point_value",
+ * "dt", "xn_bedges".  n is the number of doubles the caller provides. */
+int flow_get(flow_ctx *ctx, const char *name, double *out, long n);
+/* Number of doubles flow_get(name) writes, or -1. */
+long flow_size(flow_ctx *ctx, const char *name);
+
+/* Execution mode: 0 = ordered Gauss-Seidel sweeps that reproduce the
+ * reference's sequential sweeps exactly (default); 1 = multicolour sweeps
+ * (a different, fully parallel preconditioner). */
+int flow_set_sweep_mode(flow_ctx *ctx, int mode);
+
+int flow_status(flow_ctx *ctx);
+void flow_clear_status(flow_ctx *ctx);
+const char *flow_last_error(void);
+/* Number of kernel launches issued by this context so far. */
+long flow_launch_count(flow_ctx *ctx);
+/* Device time (ms) of the last flow_run / flow_solve call, CUDA events. */
+double flow_last_device_ms(flow_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
