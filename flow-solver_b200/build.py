@@ -24,7 +24,7 @@ LIB = os.path.join(LIBDIR, "libflowgpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xptxas", "-v"]
-HOST_SOURCES = ["host/quadrature.c", "host/svd.c", "host/curved.c"]
+HOST_SOURCES = ["host/quadrature.c", "host/svd.c", "host/curved.c", "host/prep.cpp"]
 CUDA_SOURCES = ["flow_gpu.cu"]
 
 
@@ -50,9 +50,13 @@ def build(verbose: bool = False) -> str:
     inc = ["-I", os.path.join(ROOT, "include"), "-I", CSRC, "-I", os.path.join(CSRC, "host")]
     objs = []
     for src in HOST_SOURCES:
-        obj = os.path.join(OBJDIR, os.path.basename(src).replace(".c", ".o"))
-        _run(["gcc", "-O2", "-fPIC", "-ffp-contract=off", "-std=c99", "-D_DEFAULT_SOURCE",
-              "-Wall", *inc, "-c", os.path.join(CSRC, src), "-o", obj], verbose)
+        obj = os.path.join(OBJDIR, os.path.splitext(os.path.basename(src))[0] + ".o")
+        if src.endswith(".cpp"):
+            cmd = ["g++", "-O2", "-fPIC", "-ffp-contract=off", "-std=c++17", "-Wall"]
+        else:
+            cmd = ["gcc", "-O2", "-fPIC", "-ffp-contract=off", "-std=c99", "-D_DEFAULT_SOURCE",
+                   "-Wall"]
+        _run([*cmd, *inc, "-c", os.path.join(CSRC, src), "-o", obj], verbose)
         objs.append(obj)
     log = []
     for src in CUDA_SOURCES:

@@ -564,35 +564,44 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, in
     if (t >= (unsigned)nn) break;
     const int j = FWD ? (int)(1 + t) : (int)(nn - t);
     const int k0 = m.ia[j], k1 = m.ia[j + 1];
+    // Everything that does not depend on this sweep's results is loaded before
+    // any wait: RHS, the LU factors of the diagonal block, the old dQ of the
+    // row and the row's off-diagonal blocks.
     double acc = s.RHS[4 * (long)j + r];
+    const double lu_v = (lane < 16) ? s.LUd[16 * (long)j + lane] : 0.;
+    const double old_v = (lane < 4) ? __ldcg(s.dQ + 4 * (long)j + lane) : 0.;
     for (int base = k0; base < k1; base += 8) {
       const int k = base + slot;
-      double term = 0.;
+      int c = 0;
       bool use = false;
+      double a0 = 0., a1 = 0., a2 = 0., a3 = 0.;
       if (k < k1) {
-        const int c = m.ja[k];
-        if (c != j) {
-          use = true;
-          const bool dep = FWD ? (c < j) : (c > j);
-          if (dep) {
-            cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[c]);
-            long spins = 0;
-            while (f.load(cuda::memory_order_acquire) != epoch) {
-              if (++spins > max_spin) {
-                atomicOr(s.status, ERR_SWEEP_TIMEOUT);
-                break;
-              }
-              // once any wait has timed out, every other wait gives up too
-              if ((spins & 1023) == 0 &&
-                  (*(volatile int*)s.status & ERR_SWEEP_TIMEOUT))
-                break;
-              __nanosleep(32);
-            }
-          }
-          const double* dq = s.dQ + 4 * (long)c;
-          double d[4] = {__ldcg(dq), __ldcg(dq + 1), __ldcg(dq + 2), __ldcg(dq + 3)};
-          term = row_dot(s.LHS + 16 * (long)k, r, d);
+        c = m.ja[k];
+        use = c != j;
+        if (use) {
+          const double4 av = reinterpret_cast<const double4*>(s.LHS + 16 * (long)k)[r];
+          a0 = av.x; a1 = av.y; a2 = av.z; a3 = av.w;
         }
+      }
+      double term = 0.;
+      if (use) {
+        const bool dep = FWD ? (c < j) : (c > j);
+        if (dep) {
+          cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[c]);
+          long spins = 0;
+          while (f.load(cuda::memory_order_acquire) != epoch) {
+            if (++spins > max_spin) {
+              atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+              break;
+            }
+            // once any wait has timed out, every other wait gives up too
+            if ((spins & 1023) == 0 && (*(volatile int*)s.status & ERR_SWEEP_TIMEOUT)) break;
+            if (spins > 64) __nanosleep(20);
+          }
+        }
+        const double2* dq = reinterpret_cast<const double2*>(s.dQ + 4 * (long)c);
+        const double2 d01 = __ldcg(dq), d23 = __ldcg(dq + 1);
+        term = (a0 * d01.x + a1 * d01.y + a2 * d23.x + a3 * d23.y);
       }
       const unsigned used = __ballot_sync(FULL, use);
 #pragma unroll
@@ -601,26 +610,22 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, in
         if (used & (1u << (sl * 4))) acc -= tv;
       }
     }
-    double b[4];
+    double b[4], M[16], o[4];
 #pragma unroll
     for (int q = 0; q < 4; q++) b[q] = __shfl_sync(FULL, acc, q);
+#pragma unroll
+    for (int q = 0; q < 16; q++) M[q] = __shfl_sync(FULL, lu_v, q);
+#pragma unroll
+    for (int q = 0; q < 4; q++) o[q] = __shfl_sync(FULL, old_v, q);
     if (lane == 0) {
       double X[4];
-      double M[16];
-      const double4* lu = reinterpret_cast<const double4*>(s.LUd + 16 * (long)j);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        double4 v = lu[q];
-        M[4 * q] = v.x; M[4 * q + 1] = v.y; M[4 * q + 2] = v.z; M[4 * q + 3] = v.w;
-      }
       lu_solve4(M, b, X);
-      double* dq = s.dQ + 4 * (long)j;
-      double o[4] = {__ldcg(dq), __ldcg(dq + 1), __ldcg(dq + 2), __ldcg(dq + 3)};
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         double dx = X[q] - o[q];
         o[q] += dx;
       }
+      double* dq = s.dQ + 4 * (long)j;
       __stcg(reinterpret_cast<double2*>(dq), make_double2(o[0], o[1]));
       __stcg(reinterpret_cast<double2*>(dq) + 1, make_double2(o[2], o[3]));
       cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[j]);

@@ -34,8 +34,10 @@ def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps):
         case.ref_step()
         dq, rr = gpu.solve(ts)
         ref = case.ref
-        for name in ("Q", "nQ", "pQ", "LHS", "xn_bedges"):
+        for name in ("LHS", "xn_bedges"):
             assert ndiff(ref.array(name), gpu.get(name)) == 0, (name, ts)
+        for name in ("Q", "nQ", "pQ"):  # entry 0 is unused (and uninitialised) in the reference
+            assert ndiff(ref.array(name)[4:], gpu.get(name)[4:]) == 0, (name, ts)
         for name in ("R", "dQ", "phi", "grad"):
             a, b = ref.array(name), gpu.get(name)
             w = a.size // (nn + 1)
