@@ -19,6 +19,7 @@
 
 #include "flow_gpu.h"
 #include "flow_kernels.cuh"
+#include "flow_sweep_cta.cuh"
 #include "host/curved.h"
 
 using namespace flow;
@@ -64,6 +65,21 @@ struct flow_ctx {
   bool ok = false;
   // host copies needed to answer flow_get in the reference layout
   int nn = 0, ng = 0, ns = 0, nbe = 0, nnz = 0;
+  double drop_target = 0.;   // host copy of the pending target (read by reset_run)
+  // optional per-kernel event timing
+  int timing = 0;
+  std::vector<cudaEvent_t> event_pool;
+  struct Pending { int cls; cudaEvent_t a, b; };
+  std::vector<Pending> pending;
+  long kcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double kms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // device snapshot of the solution state
+  double *snapQ = nullptr, *snapnQ = nullptr, *snappQ = nullptr, *snapXnb = nullptr;
+  double* xnb0 = nullptr;  // boundary normals as created (restored by flow_set_state)
+  // one-CTA ordered sweep: stage tables (null when the matrix bandwidth is too
+  // large for its dQ window, then the multi-CTA sweep is used)
+  SweepTables sweep_tb{};
+  bool sweep_cta_ok = false;
   double* d_hist = nullptr;  // 2 x hist_cap device history of (dq, r_rho)
   int hist_cap = 0;
 };
@@ -151,7 +167,53 @@ int check_params(flow_ctx* c, const flow_params* p) {
 
 int grid_blocks(int n, int t) { return (n + t - 1) / t; }
 
+cudaEvent_t get_event(flow_ctx* c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets the launches of one kernel class with events when timing is on.
+struct Timed {
+  flow_ctx* c;
+  int cls;
+  cudaEvent_t a = nullptr;
+  Timed(flow_ctx* ctx, int k) : c(ctx), cls(k) {
+    if (c->timing) {
+      a = get_event(c);
+      cudaEventRecord(a, c->stream);
+    }
+  }
+  ~Timed() {
+    if (c->timing) {
+      cudaEvent_t b = get_event(c);
+      cudaEventRecord(b, c->stream);
+      c->pending.push_back({cls, a, b});
+    }
+  }
+};
+
+// Accumulate finished event pairs (call after the stream was synchronised).
+void harvest(flow_ctx* c) {
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+      c->kms[p.cls] += ms;
+      c->kcount[p.cls] += 1;
+    }
+    c->event_pool.push_back(p.a);
+    c->event_pool.push_back(p.b);
+  }
+  c->pending.clear();
+}
+
 int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
+  Timed tm(c, 0);
   int nb = grid_blocks(c->nn, 128);
   if (c->order == 1)
     k_node_prepare<1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
@@ -162,25 +224,32 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
 
 int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   int rc = 0;
-  int nbs = grid_blocks(c->ns, 128);
-  if (a.recon == 1) {
-    if (jac) k_subedge_flux<1, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
-    else k_subedge_flux<1, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
-  } else {
-    if (jac) k_subedge_flux<0, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
-    else k_subedge_flux<0, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+  {
+    Timed t(c, 1);
+    int nbs = grid_blocks(c->ns, 128);
+    if (a.recon == 1) {
+      if (jac) k_subedge_flux<1, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+      else k_subedge_flux<1, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+    } else {
+      if (jac) k_subedge_flux<0, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+      else k_subedge_flux<0, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+    }
+    rc |= launch_check(c);
   }
-  rc |= launch_check(c);
   int nbb = grid_blocks(c->nbe, 128);
   if (nbb > 0) {
+    Timed t(c, 2);
     if (jac) k_boundary<true><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
     else k_boundary<false><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
     rc |= launch_check(c);
   }
-  int nbn = grid_blocks(c->nn, 128);
-  if (jac) k_assemble<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
-  else k_assemble<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
-  rc |= launch_check(c);
+  {
+    Timed t(c, 3);
+    int nbn = grid_blocks(c->nn, 128);
+    if (jac) k_assemble<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+    else k_assemble<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+    rc |= launch_check(c);
+  }
   return rc;
 }
 
@@ -194,13 +263,25 @@ int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
   for (int it = 0; it < p->subits; it++) {
     cudaMemsetAsync(c->s.counter, 0, sizeof(unsigned), c->stream);
     int ep = ++c->epoch;
-    int blocks = c->nsm * 4;
-    if (it % 2 == 0)
-      k_sweep_ordered<true><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
-    else
-      k_sweep_ordered<false><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
-    rc |= launch_check(c);
+    {
+      Timed t(c, 4);
+      if (c->sweep_cta_ok && c->sweep_mode == 0) {
+        const size_t sm = sizeof(SweepSmem);
+        if (it % 2 == 0)
+          k_sweep_cta<true><<<1, kSweepThreads, sm, c->stream>>>(c->m, c->s, c->sweep_tb, max_spin);
+        else
+          k_sweep_cta<false><<<1, kSweepThreads, sm, c->stream>>>(c->m, c->s, c->sweep_tb, max_spin);
+      } else {
+        int blocks = c->nsm * 4;
+        if (it % 2 == 0)
+          k_sweep_ordered<true><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
+        else
+          k_sweep_ordered<false><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
+      }
+      rc |= launch_check(c);
+    }
     if (it < p->subits - 1 || final_rms) {
+      Timed t(c, 5);
       k_lin_residual<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->m, c->s);
       rc |= launch_check(c);
       k_finalize_rms<<<1, kRedThreads, 0, c->stream>>>(c->s, kRedBlocks, c->nn);
@@ -211,7 +292,7 @@ int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
 }
 
 // One solve() call (solve.C:44-933), device-only.
-int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot) {
+int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int first) {
   int rc = 0;
   int total = c->nn + c->ng;
   c->citer = ts;
@@ -233,10 +314,20 @@ int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot) {
     bool last = mi == p->iter;
     k_finalize_step<<<1, kRedThreads, 0, c->stream>>>(
         c->s, last && hist_slot >= 0 ? c->d_hist : nullptr,
-        last && hist_slot >= 0 ? c->d_hist + c->hist_cap : nullptr, hist_slot < 0 ? 0 : hist_slot);
+        last && hist_slot >= 0 ? c->d_hist + c->hist_cap : nullptr, hist_slot < 0 ? 0 : hist_slot,
+        last && first);
     rc |= launch_check(c);
   }
   return rc;
+}
+
+// Clear the convergence stop and set the run's target drop (0 = none).
+void reset_run(flow_ctx* c, double drop) {
+  c->drop_target = drop;
+  cudaMemsetAsync(c->s.stop, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(c->s.steps_done, 0, sizeof(int), c->stream);
+  cudaMemcpyAsync(c->s.scalars + 7, &c->drop_target, sizeof(double), cudaMemcpyHostToDevice,
+                  c->stream);
 }
 
 int read_status(flow_ctx* c) {
@@ -248,6 +339,7 @@ int read_status(flow_ctx* c) {
     set_error(cudaGetErrorString(cudaGetLastError()));
     return FLOW_ERR_CUDA;
   }
+  harvest(c);
   return st;
 }
 
@@ -442,6 +534,49 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
 #undef UP
   if (!okk) return fail(c, FLOW_ERR_CUDA, "device allocation or upload failed");
 
+  // ---- stage tables of the one-CTA ordered sweep ----
+  {
+    int bw = 0;
+    for (int n = 1; n <= nn; n++)
+      for (int k = g->ia[n]; k < g->ia[n + 1]; k++) bw = std::max(bw, std::abs(g->ja[k] - n));
+    std::vector<int> rs, row_stage(nn + 1, 0);
+    bool fits = bw <= kWindow - kStages * kStageRows - 1;
+    rs.push_back(1);
+    int rows = 0, blocks = 0;
+    for (int n = 1; n <= nn && fits; n++) {
+      int nb = g->ia[n + 1] - g->ia[n];
+      if (nb > kStageBlocks) { fits = false; break; }
+      if (rows + 1 > kStageRows || blocks + nb > kStageBlocks) {
+        rs.push_back(n);
+        rows = 0;
+        blocks = 0;
+      }
+      rows++;
+      blocks += nb;
+      row_stage[n] = (int)rs.size() - 1;
+    }
+    rs.push_back(nn + 1);
+    if (fits) {
+      std::vector<int> japad(g->ja, g->ja + nnz);
+      japad.resize((size_t)nnz + 16, 0);
+      int* d_rs = upload_vec(c, rs);
+      int* d_row = upload_vec(c, row_stage);
+      int* d_ja = upload_vec(c, japad);
+      if (!d_rs || !d_row || !d_ja) return fail(c, FLOW_ERR_CUDA, "sweep table upload failed");
+      c->sweep_tb.stage_row0 = d_rs;
+      c->sweep_tb.row_stage = d_row;
+      c->sweep_tb.ja_pad = d_ja;
+      c->sweep_tb.nstages = (int)rs.size() - 1;
+      const int smem = (int)sizeof(SweepSmem);
+      if (cudaFuncSetAttribute(k_sweep_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem) != cudaSuccess ||
+          cudaFuncSetAttribute(k_sweep_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               smem) != cudaSuccess)
+        return fail(c, FLOW_ERR_CUDA, "cannot reserve shared memory for the sweep");
+      c->sweep_cta_ok = true;
+    }
+  }
+
   // ---- device state ----
   DevState& s = c->s;
   size_t nq = (size_t)(nn + ng + 1) * 4;
@@ -469,12 +604,14 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   s.counter = c->buf.alloc<unsigned>(4);
   s.status = c->buf.alloc<int>(1);
   s.skip = c->buf.alloc<int>(1);
+  s.stop = c->buf.alloc<int>(1);
+  s.steps_done = c->buf.alloc<int>(1);
   s.partial = c->buf.alloc<double>(2 * kRedBlocks);
   s.scalars = c->buf.alloc<double>(8);
   if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
       !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
       !s.Jb || !s.bforce || !s.done || !s.counter || !s.status || !s.skip || !s.partial ||
-      !s.scalars)
+      !s.scalars || !s.stop || !s.steps_done)
     return fail(c, FLOW_ERR_CUDA, "device state allocation failed");
   cudaMemset(s.Q, 0, nq * 8);
   cudaMemset(s.nQ, 0, nq * 8);
@@ -491,10 +628,14 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   cudaMemset(s.done, 0, (size_t)(nn + 1) * 4);
   cudaMemset(s.status, 0, 4);
   cudaMemset(s.skip, 0, 4);
+  cudaMemset(s.stop, 0, 4);
+  cudaMemset(s.steps_done, 0, 4);
   cudaMemset(s.scalars, 0, 64);
   std::vector<double> xnb((size_t)(nbe + 1) * 3, 0.);
   std::copy(g->xn_bedges, g->xn_bedges + xnb.size(), xnb.begin());
-  if (!upload(c, s.xn_bedges, xnb.data(), xnb.size() * 8))
+  c->xnb0 = c->buf.alloc<double>(xnb.size());
+  if (!c->xnb0 || !upload(c, s.xn_bedges, xnb.data(), xnb.size() * 8) ||
+      !upload(c, c->xnb0, xnb.data(), xnb.size() * 8))
     return fail(c, FLOW_ERR_CUDA, "upload failed");
   if (cudaDeviceSynchronize() != cudaSuccess) return fail(c, FLOW_ERR_CUDA, "device error at set-up");
   c->ok = true;
@@ -506,6 +647,8 @@ void flow_destroy(flow_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  harvest(c);
+  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   c->buf.release();
   if (c->d_hist) cudaFree(c->d_hist);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -518,15 +661,19 @@ int flow_set_state(flow_ctx* c, const double* Q) {
   if (!c || !c->ok || !Q) return FLOW_ERR_ARG;
   cudaSetDevice(c->device);
   size_t bytes = sizeof(double) * 4 * (size_t)(c->nn + c->ng + 1);
+  size_t xbytes = sizeof(double) * 3 * (size_t)(c->nbe + 1);
   if (cudaMemcpyAsync(c->s.Q, Q, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
-      cudaMemcpyAsync(c->s.nQ, Q, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+      cudaMemcpyAsync(c->s.nQ, c->s.Q, bytes, cudaMemcpyDeviceToDevice, c->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(c->s.xn_bedges, c->xnb0, xbytes, cudaMemcpyDeviceToDevice, c->stream) !=
+          cudaSuccess ||
       cudaStreamSynchronize(c->stream) != cudaSuccess)
     return FLOW_ERR_CUDA;
   return 0;
 }
 
 int flow_set_sweep_mode(flow_ctx* c, int mode) {
-  if (!c || mode != 0) return FLOW_ERR_ARG;
+  if (!c || mode < 0 || mode > 2) return FLOW_ERR_ARG;
   c->sweep_mode = mode;
   return 0;
 }
@@ -538,7 +685,8 @@ int flow_solve(flow_ctx* c, const flow_params* p, int ts, double* dq_norm, doubl
   cudaSetDevice(c->device);
   if ((rc = ensure_hist(c, 1))) return rc;
   cudaEventRecord(c->ev0, c->stream);
-  rc = enqueue_step(c, p, ts, 0);
+  reset_run(c, 0.);
+  rc = enqueue_step(c, p, ts, 0, 1);
   cudaEventRecord(c->ev1, c->stream);
   if (rc) return rc;
   int st = read_status(c);
@@ -561,7 +709,8 @@ int flow_run(flow_ctx* c, const flow_params* p, int ts0, int nsteps, double* r_h
   cudaSetDevice(c->device);
   if ((rc = ensure_hist(c, std::max(nsteps, 1)))) return rc;
   cudaEventRecord(c->ev0, c->stream);
-  for (int i = 0; i < nsteps && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, i);
+  reset_run(c, 0.);
+  for (int i = 0; i < nsteps && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, i, i == 0);
   cudaEventRecord(c->ev1, c->stream);
   if (rc) return rc;
   int st = read_status(c);
@@ -574,11 +723,56 @@ int flow_run(flow_ctx* c, const flow_params* p, int ts0, int nsteps, double* r_h
   return st;
 }
 
+int flow_converge(flow_ctx* c, const flow_params* p, int ts0, int max_steps, double drop,
+                  int chunk, int* steps, double* r_first, double* r_last) {
+  if (!c || !c->ok || max_steps < 1 || !(drop > 0.)) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if (chunk < 1) chunk = 64;
+  if ((rc = ensure_hist(c, 1))) return rc;
+  reset_run(c, drop);
+  cudaEventRecord(c->ev0, c->stream);
+  int done = 0, stop = 0, issued = 0;
+  while (!rc && issued < max_steps) {
+    int n = std::min(chunk, max_steps - issued);
+    for (int i = 0; i < n && !rc; i++, issued++) rc |= enqueue_step(c, p, ts0 + issued, -1, issued == 0);
+    if (rc) break;
+    cudaMemcpyAsync(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaMemcpyAsync(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
+    harvest(c);
+    if (stop) break;
+    int st = 0;
+    cudaMemcpy(&st, c->s.status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (st) break;
+  }
+  cudaEventRecord(c->ev1, c->stream);
+  if (rc) return rc;
+  int st = read_status(c);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+  c->last_ms = ms;
+  double sc[8];
+  cudaMemcpy(sc, c->s.scalars, sizeof(sc), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaMemcpy(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost);
+  // leave the device in the no-target state for later calls
+  reset_run(c, 0.);
+  cudaStreamSynchronize(c->stream);
+  if (steps) *steps = done;
+  if (r_first) *r_first = sc[6];
+  if (r_last) *r_last = sqrt(sc[2]);
+  if (st) return st;
+  return stop ? 0 : FLOW_ERR_NOT_CONVERGED;
+}
+
 int flow_build_matrix(flow_ctx* c, const flow_params* p, int citer) {
   if (!c || !c->ok) return FLOW_ERR_ARG;
   int rc = check_params(c, p);
   if (rc) return rc;
   cudaSetDevice(c->device);
+  reset_run(c, 0.);
   StepArgs a = make_args(p, citer);
   a.do_grad = a.do_derivs = a.do_lim = 0;
   c->citer = citer;
@@ -594,6 +788,7 @@ int flow_reconstruct(flow_ctx* c, const flow_params* p, int ts) {
   int rc = check_params(c, p);
   if (rc) return rc;
   cudaSetDevice(c->device);
+  reset_run(c, 0.);
   StepArgs a = make_args(p, ts);
   c->citer = ts;
   // grad, hess <- 0 and phi <- 1 (solve.C:298-348), keeping the current nQ
@@ -609,6 +804,7 @@ int flow_residuals(flow_ctx* c, const flow_params* p, int jupdate, int ts) {
   int rc = check_params(c, p);
   if (rc) return rc;
   cudaSetDevice(c->device);
+  reset_run(c, 0.);
   StepArgs a = make_args(p, ts);
   c->citer = ts;
   rc = launch_residuals(c, a, jupdate);
@@ -621,6 +817,7 @@ int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
   int rc = check_params(c, p);
   if (rc) return rc;
   cudaSetDevice(c->device);
+  reset_run(c, 0.);
   rc = launch_linear_solve(c, p, true);
   if (rc) return rc;
   int st = read_status(c);
@@ -693,7 +890,9 @@ int flow_get(flow_ctx* c, const char* name, double* out, long n) {
   else if (nm == "xn_bedges") src = c->s.xn_bedges;
   else if (nm == "point_value") src = c->s.pv;
   if (src) {
-    if (cudaMemcpy(out, src, sizeof(double) * need, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpyAsync(out, src, sizeof(double) * need, cudaMemcpyDeviceToHost, c->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
       return FLOW_ERR_CUDA;
     return 0;
   }
@@ -709,6 +908,57 @@ int flow_get(flow_ctx* c, const char* name, double* out, long n) {
   }
   return FLOW_ERR_NOT_FOUND;
 }
+
+int flow_save_state(flow_ctx* c) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  size_t nq = (size_t)(c->nn + c->ng + 1) * 4, nx = (size_t)(c->nbe + 1) * 3;
+  if (!c->snapQ) {
+    c->snapQ = c->buf.alloc<double>(nq);
+    c->snapnQ = c->buf.alloc<double>(nq);
+    c->snappQ = c->buf.alloc<double>(nq);
+    c->snapXnb = c->buf.alloc<double>(nx);
+    if (!c->snapQ || !c->snapnQ || !c->snappQ || !c->snapXnb) return FLOW_ERR_CUDA;
+  }
+  cudaMemcpyAsync(c->snapQ, c->s.Q, nq * 8, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->snapnQ, c->s.nQ, nq * 8, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->snappQ, c->s.pQ, nq * 8, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->snapXnb, c->s.xn_bedges, nx * 8, cudaMemcpyDeviceToDevice, c->stream);
+  return read_status(c);
+}
+
+int flow_restore_state(flow_ctx* c) {
+  if (!c || !c->ok || !c->snapQ) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  size_t nq = (size_t)(c->nn + c->ng + 1) * 4, nx = (size_t)(c->nbe + 1) * 3;
+  cudaMemcpyAsync(c->s.Q, c->snapQ, nq * 8, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->s.nQ, c->snapnQ, nq * 8, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->s.pQ, c->snappQ, nq * 8, cudaMemcpyDeviceToDevice, c->stream);
+  cudaMemcpyAsync(c->s.xn_bedges, c->snapXnb, nx * 8, cudaMemcpyDeviceToDevice, c->stream);
+  return read_status(c);
+}
+
+int flow_set_timing(flow_ctx* c, int on) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  harvest(c);
+  c->timing = on ? 1 : 0;
+  for (int i = 0; i < 8; i++) { c->kcount[i] = 0; c->kms[i] = 0.; }
+  return 0;
+}
+
+int flow_kernel_times(flow_ctx* c, long* launches, double* ms, int nclasses) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  harvest(c);
+  for (int i = 0; i < nclasses && i < 8; i++) {
+    if (launches) launches[i] = c->kcount[i];
+    if (ms) ms[i] = c->kms[i];
+  }
+  return 0;
+}
+
+void* flow_stream(flow_ctx* c) { return c ? (void*)c->stream : nullptr; }
 
 int flow_status(flow_ctx* c) {
   if (!c || !c->ok) return FLOW_ERR_ARG;

@@ -50,6 +50,7 @@ struct StepArgs {
 
 // ---------------------------------------------------------------------------
 __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
+  if (*s.stop) return;  // the run has converged
   int total = m.nn + m.ng;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= total;
        i += gridDim.x * blockDim.x) {
@@ -84,6 +85,7 @@ __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
 // 1438-1521); then the Venkatakrishnan limiter (limiter.C:594-906).
 template <int ORDER>
 __global__ void __launch_bounds__(128) k_node_prepare(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
   int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (n > m.nn) return;
   const double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
@@ -253,6 +255,7 @@ __global__ void __launch_bounds__(128) k_node_prepare(DevMesh m, DevState s, Ste
 // (residual.C:112-333, reconstruct.C:181-203, jacobian.C:45-110).
 template <int RECON, bool JAC>
 __global__ void __launch_bounds__(128) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
   int sub = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (sub > m.ns) return;
   int2 lr = m.sub_lr[sub];
@@ -307,6 +310,7 @@ __global__ void __launch_bounds__(128) k_subedge_flux(DevMesh m, DevState s, Ste
 // xn_bedges (residual.C:1103-1143), as the reference does.
 template <bool JAC>
 __global__ void __launch_bounds__(128) k_boundary(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
   int b = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (b > m.nbe) return;
   int4 info = m.bed_info[b];
@@ -428,6 +432,7 @@ __global__ void __launch_bounds__(128) k_boundary(DevMesh m, DevState s, StepArg
 // factors of the diagonal block for the sweeps (linear_algebra.C:226-246).
 template <bool JAC>
 __global__ void __launch_bounds__(128) k_assemble(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
   int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (n > m.nn) return;
   double r[4] = {0., 0., 0., 0.};
@@ -552,6 +557,7 @@ __global__ void __launch_bounds__(128) k_diag_only(DevMesh m, DevState s) {
 template <bool FWD>
 __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, int epoch,
                                                        long max_spin) {
+  if (*s.stop) return;  // the run has converged
   if (*s.skip) return;
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
@@ -653,6 +659,7 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
 
 // b - Ax of every row (linear_algebra.C:348-387), squared, partial sums.
 __global__ void __launch_bounds__(kRedThreads) k_lin_residual(DevMesh m, DevState s) {
+  if (*s.stop) return;  // the run has converged
   __shared__ double sh[kRedThreads];
   double acc = 0.;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x + 1; j <= m.nn;
@@ -675,6 +682,7 @@ __global__ void __launch_bounds__(kRedThreads) k_lin_residual(DevMesh m, DevStat
 
 // Sum the partials in a fixed order; slot 0 = RMS (sets skip below 1e-15).
 __global__ void k_finalize_rms(DevState s, int nparts, int nn) {
+  if (*s.stop) return;  // the run has converged
   __shared__ double sh[kRedThreads];
   double v = 0.;
   for (int i = threadIdx.x; i < nparts; i += blockDim.x) v += s.partial[i];
@@ -690,6 +698,7 @@ __global__ void k_finalize_rms(DevState s, int nparts, int nn) {
 // nQ += dQ, pQ <- Q, Q <- nQ (solve.C:901-928) and partial sums of |dQ|^2
 // and |R_rho|^2.
 __global__ void __launch_bounds__(kRedThreads) k_finish_step(DevMesh m, DevState s, int last) {
+  if (*s.stop) return;  // the run has converged
   __shared__ double sh[kRedThreads];
   double dq2 = 0., r2 = 0.;
   const int total = m.nn + m.ng;
@@ -717,7 +726,9 @@ __global__ void __launch_bounds__(kRedThreads) k_finish_step(DevMesh m, DevState
   }
 }
 
-__global__ void k_finalize_step(DevState s, double* hist_dq, double* hist_r, int slot) {
+__global__ void k_finalize_step(DevState s, double* hist_dq, double* hist_r, int slot,
+                                int first) {
+  if (*s.stop) return;  // the run has converged
   __shared__ double sh[kRedThreads];
   double a = 0., b = 0.;
   for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) {
@@ -729,8 +740,13 @@ __global__ void k_finalize_step(DevState s, double* hist_dq, double* hist_r, int
   if (threadIdx.x == 0) {
     s.scalars[1] = ta;
     s.scalars[2] = tb;
+    double r = sqrt(tb);
     if (hist_dq) hist_dq[slot] = sqrt(ta);
-    if (hist_r) hist_r[slot] = sqrt(tb);
+    if (hist_r) hist_r[slot] = r;
+    if (first) s.scalars[6] = r;
+    *s.steps_done += 1;
+    // stop once ||R_rho|| < drop * ||R_rho|| of the first step
+    if (s.scalars[7] > 0. && r < s.scalars[7] * s.scalars[6]) *s.stop = 1;
   }
 }
 

@@ -86,8 +86,11 @@ struct DevState {
   unsigned int* counter;  // row dispenser for the ordered sweeps
   int* status;      // sticky error bits (FLOW_ERR_*)
   int* skip;        // set when the linear residual dropped below 1e-15
+  int* stop;        // set once the run's density residual dropped below its target
+  int* steps_done;  // pseudo-time steps completed since the last reset
   double* partial;  // reduction partials
-  double* scalars;  // [0] rms, [1] dq^2, [2] R_rho^2, [3] cfl, [4] F_lift, [5] F_drag
+  double* scalars;  // [0] rms, [1] dq^2, [2] R_rho^2, [3] cfl, [4] F_lift, [5] F_drag,
+                    // [6] R_rho of the run's first step, [7] target drop (0 = none)
 };
 
 }  // namespace flow

@@ -19,12 +19,14 @@ DP = C.POINTER(C.c_double)
 LP = C.POINTER(C.c_long)
 
 ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
-          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND"}
+          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND", 256: "NOT_CONVERGED"}
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
-           "flow_build_matrix", "flow_reconstruct", "flow_residuals", "flow_linear_solve",
-           "flow_body_forces", "flow_get", "flow_size", "flow_set_sweep_mode", "flow_status",
+           "flow_converge", "flow_build_matrix", "flow_reconstruct", "flow_residuals", "flow_linear_solve",
+           "flow_body_forces", "flow_get", "flow_size", "flow_set_sweep_mode", "flow_save_state",
+           "flow_restore_state", "flow_set_timing", "flow_kernel_times", "flow_stream",
+           "flow_status",
            "flow_clear_status", "flow_last_error", "flow_launch_count", "flow_last_device_ms")
 
 
@@ -79,6 +81,7 @@ def load():
     L.flow_set_state.argtypes = [vp, DP]
     L.flow_solve.argtypes = [vp, PP, C.c_int, DP, DP]
     L.flow_run.argtypes = [vp, PP, C.c_int, C.c_int, DP, DP]
+    L.flow_converge.argtypes = [vp, PP, C.c_int, C.c_int, C.c_double, C.c_int, IP, DP, DP]
     L.flow_build_matrix.argtypes = [vp, PP, C.c_int]
     L.flow_reconstruct.argtypes = [vp, PP, C.c_int]
     L.flow_residuals.argtypes = [vp, PP, C.c_int, C.c_int]
@@ -88,6 +91,12 @@ def load():
     L.flow_size.restype = C.c_long
     L.flow_size.argtypes = [vp, C.c_char_p]
     L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
+    L.flow_save_state.argtypes = [vp]
+    L.flow_restore_state.argtypes = [vp]
+    L.flow_set_timing.argtypes = [vp, C.c_int]
+    L.flow_kernel_times.argtypes = [vp, LP, DP, C.c_int]
+    L.flow_stream.restype = vp
+    L.flow_stream.argtypes = [vp]
     L.flow_status.argtypes = [vp]
     L.flow_clear_status.argtypes = [vp]
     L.flow_last_error.restype = C.c_char_p
@@ -163,6 +172,21 @@ class Solver:
             _check(st.value or 1, "flow_create")
         self.sizes = dict(sizes)
 
+    @classmethod
+    def from_mesh(cls, mesh, params, device: int = 0):
+        """Build from a flowgpu.prep.Mesh (the library's own preprocessing)."""
+        self = cls.__new__(cls)
+        self.L = load()
+        self._keep = None
+        self.params = params
+        self.p = params_struct(params)
+        st = C.c_int(0)
+        self.ctx = self.L.flow_create(C.byref(mesh.view), C.byref(self.p), int(device), C.byref(st))
+        if not self.ctx:
+            _check(st.value or 1, "flow_create")
+        self.sizes = mesh.sizes
+        return self
+
     def close(self):
         if getattr(self, "ctx", None):
             self.L.flow_destroy(self.ctx)
@@ -173,6 +197,13 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+    def get_into(self, name: str, out: np.ndarray):
+        """flow_get into a caller-owned float64 buffer (e.g. pinned memory)."""
+        n = self.L.flow_size(self.ctx, name.encode())
+        if n < 0 or out.dtype != np.float64 or out.size < n or not out.flags.c_contiguous:
+            raise ValueError(f"bad output buffer for {name}")
+        _check(self.L.flow_get(self.ctx, name.encode(), out.ctypes.data_as(DP), n), f"get {name}")
 
     def set_params(self, params):
         self.params = params
@@ -194,6 +225,16 @@ class Solver:
         _check(self.L.flow_run(self.ctx, C.byref(self.p), ts0, nsteps, rh.ctypes.data_as(DP),
                                dh.ctypes.data_as(DP)), "flow_run")
         return rh[:nsteps], dh[:nsteps]
+
+    def converge(self, ts0: int = 1, max_steps: int = 20000, drop: float = 1e-10,
+                 chunk: int = 64, check: bool = True):
+        """Steps until ||R_rho|| drops by `drop`; returns (steps, r_first, r_last)."""
+        n, r0, r1 = C.c_int(), C.c_double(), C.c_double()
+        rc = self.L.flow_converge(self.ctx, C.byref(self.p), ts0, max_steps, drop, chunk,
+                                  C.byref(n), C.byref(r0), C.byref(r1))
+        if check:
+            _check(rc, "flow_converge")
+        return n.value, r0.value, r1.value
 
     def build_matrix(self, citer: int):
         _check(self.L.flow_build_matrix(self.ctx, C.byref(self.p), citer), "flow_build_matrix")
@@ -224,6 +265,28 @@ class Solver:
 
     def set_sweep_mode(self, mode: int):
         _check(self.L.flow_set_sweep_mode(self.ctx, int(mode)), "flow_set_sweep_mode")
+
+    def save_state(self):
+        _check(self.L.flow_save_state(self.ctx), "flow_save_state")
+
+    def restore_state(self):
+        _check(self.L.flow_restore_state(self.ctx), "flow_restore_state")
+
+    def set_timing(self, on: bool):
+        _check(self.L.flow_set_timing(self.ctx, int(bool(on))), "flow_set_timing")
+
+    KERNEL_CLASSES = ("node_prepare", "subedge_flux", "boundary", "assemble", "sweep",
+                      "lin_residual", "other")
+
+    def kernel_times(self) -> dict:
+        n = len(self.KERNEL_CLASSES)
+        cnt = (C.c_long * n)()
+        ms = (C.c_double * n)()
+        _check(self.L.flow_kernel_times(self.ctx, cnt, ms, n), "flow_kernel_times")
+        return {k: (cnt[i], ms[i]) for i, k in enumerate(self.KERNEL_CLASSES)}
+
+    def stream(self) -> int:
+        return self.L.flow_stream(self.ctx)
 
     def status(self) -> int:
         return self.L.flow_status(self.ctx)

@@ -32,6 +32,7 @@ extern "C" {
 #define FLOW_ERR_BC 32          /* invalid far-field state (cvbc.C:330-382) */
 #define FLOW_ERR_SWEEP_TIMEOUT 64 /* an ordered sweep waited past its bound */
 #define FLOW_ERR_NOT_FOUND 128  /* unknown array name */
+#define FLOW_ERR_NOT_CONVERGED 256 /* flow_converge reached max_steps */
 
 /* Mirrors PARAMS (include/params.h:19-76 of the reference), same field
  * order and meaning as euler.params (params.C:44-217). */
@@ -100,8 +101,9 @@ typedef struct flow_grid_view {
   const int *gnnsn;
   const int *gnnsn1;
   const int *svd_m;           /* nn+1: rows m of node i's system */
-  const long *svd_off;        /* nn+1: offset of node i's m*m U in svd_U */
-  const double *svd_U;        /* concatenated column-major m x m */
+  const long *svd_off;        /* nn+1: offset of node i's U block in svd_U */
+  const double *svd_U;        /* per node, column-major with leading dimension m;
+                                 only the first 5 columns are read */
   const double *svd_VT;       /* (nn+1)*25 */
   const double *svd_S;        /* (nn+1)*5 */
 } flow_grid_view;
@@ -115,7 +117,9 @@ flow_ctx *flow_create(const flow_grid_view *grid, const flow_params *p, int devi
                       int *status);
 void flow_destroy(flow_ctx *ctx);
 
-/* Set GRID::Q (and nQ = Q), (nn+nn_ghost+1)*4 doubles (ic.C:36-99 output). */
+/* Start a solve from GRID::Q = Q (and nQ = Q), (nn+nn_ghost+1)*4 doubles
+ * (ic.C:36-99 output).  The boundary normals that the k=2 boundary pass
+ * rewrites (residual.C:1103-1143) go back to their initial values. */
 int flow_set_state(flow_ctx *ctx, const double *Q);
 
 /* double solve(GRID*, SYS_MEM*, PARAMS, int ts)  (include/solve.h:21,
@@ -130,6 +134,18 @@ int flow_solve(flow_ctx *ctx, const flow_params *p, int ts, double *dq_norm, dou
  * dq_hist (optional, nsteps entries) receive the per-step norms. */
 int flow_run(flow_ctx *ctx, const flow_params *p, int ts0, int nsteps, double *r_rho_hist,
              double *dq_hist);
+
+/* The driver loop of main.C:789-815 run to convergence: steps
+ * ts = ts0, ts0+1, ... until ||R[:,0]||_2 < drop * (its value at step ts0)
+ * or max_steps steps.  The test runs on the device; the host looks at it
+ * every `chunk` steps, and steps enqueued after convergence do no work.
+ * *steps receives the steps taken (the step that met the target included),
+ * *r_first / *r_last the density residual norms of the first / last step.
+ * Returns FLOW_ERR_NOT_CONVERGED when max_steps ran out.  The reference's
+ * driver has no convergence test (it runs nsteps steps); this is the
+ * 1e-10-drop criterion the solves/s metric is quoted on. */
+int flow_converge(flow_ctx *ctx, const flow_params *p, int ts0, int max_steps, double drop,
+                  int chunk, int *steps, double *r_first, double *r_last);
 
 /* void build_matrix(GRID*, PARAMS, SYS_MEM*)  (include/init_memory.h:24,
  * init_memory.C:159-310) with GRID::citer = citer; writes dt and the V/dt
@@ -166,10 +182,33 @@ int flow_get(flow_ctx *ctx, const char *name, double *out, long n);
 /* Number of doubles flow_get(name) writes, or -1. */
 long flow_size(flow_ctx *ctx, const char *name);
 
-/* Execution mode: 0 = ordered Gauss-Seidel sweeps that reproduce the
- * reference's sequential sweeps exactly (default); 1 = multicolour sweeps
- * (a different, fully parallel preconditioner). */
+/* Sweep kernel: 0 = ordered Gauss-Seidel sweeps that reproduce the
+ * reference's sequential sweeps exactly, one CTA per mesh with the matrix
+ * streamed through shared memory (default; falls back to 2 when the matrix
+ * bandwidth exceeds its window); 2 = the same ordered sweeps spread over
+ * the whole GPU with global-memory ready flags.  Both give identical
+ * results. */
 int flow_set_sweep_mode(flow_ctx *ctx, int mode);
+
+/* Device snapshot of the solution state (Q, nQ, pQ and the boundary normals
+ * the k=2 pass rewrites): flow_save_state keeps a copy on the device,
+ * flow_restore_state puts it back (pre-emption / restart without host
+ * round trips; the reference's restart goes through the mesh file,
+ * mesh_io.C:218-277). */
+int flow_save_state(flow_ctx *ctx);
+int flow_restore_state(flow_ctx *ctx);
+
+/* Per-kernel device timing with CUDA events on the context's stream
+ * (off by default).  flow_kernel_times fills, per kernel class
+ * (0 node_prepare, 1 subedge_flux, 2 boundary, 3 assemble, 4 sweep,
+ * 5 lin_residual, 6 other), the number of launches and total milliseconds
+ * since timing was switched on. */
+int flow_set_timing(flow_ctx *ctx, int on);
+int flow_kernel_times(flow_ctx *ctx, long *launches, double *ms, int nclasses);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events against it. */
+void *flow_stream(flow_ctx *ctx);
 
 int flow_status(flow_ctx *ctx);
 void flow_clear_status(flow_ctx *ctx);

@@ -13,22 +13,26 @@ from cases import ParityCase, ndiff
 pytestmark = pytest.mark.gpu
 
 
-def _solver(case):
+def _solver(case, sweep_mode=0):
     from flowgpu.capi import Solver
     s = Solver(case.sizes, case.arrays, case.fp, device=0)
+    s.set_sweep_mode(sweep_mode)
     s.set_state(case.Q0)
     return s
 
 
-@pytest.mark.parametrize("nc,nr,curved,order,steps", [
-    (32, 8, False, 1, 6),
-    (128, 32, False, 1, 4),
-    (32, 8, True, 3, 6),
-    (128, 32, True, 3, 4),
+@pytest.mark.parametrize("nc,nr,curved,order,steps,mode", [
+    (32, 8, False, 1, 6, 0),
+    (128, 32, False, 1, 4, 0),
+    (32, 8, True, 3, 6, 0),
+    (128, 32, True, 3, 4, 0),
+    (128, 32, True, 3, 3, 2),
+    (64, 16, False, 1, 3, 2),
 ])
-def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps):
+def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode):
+    """mode 0: one-CTA ordered sweep; mode 2: grid-wide ordered sweep."""
     case = ParityCase(nc, nr, curved, order)
-    gpu = _solver(case)
+    gpu = _solver(case, mode)
     nn = case.sizes["nn"]
     for ts in range(1, steps + 1):
         case.ref_step()
