@@ -6,10 +6,12 @@
 //   * warp 0 streams the matrix in "stages" (consecutive rows whose blocks
 //     fit in one buffer) into a shared-memory ring with cp.async.bulk,
 //     completion tracked by one mbarrier per ring slot;
-//   * warps 1..31 take the rows in the reference's order (row position
-//     p -> warp 1 + p % 31) and publish each finished dQ in a shared-memory
-//     window slot tagged with its row number; a row waits only for the
-//     window tags of the neighbours the reference updates before it;
+//   * warps 1..31 each run 8 rows at a time, 4 lanes per row (one per
+//     matrix row of the 4x4 blocks); row positions are dealt round-robin to
+//     the 248 lane groups in the reference's order, and each finished dQ is
+//     published in a shared-memory window slot tagged with its row number;
+//     a row waits only for the window tags of the neighbours the reference
+//     updates before it;
 //   * a ring slot is refilled once every row of its previous stage is done.
 // Progress: rows only wait for earlier rows, stage t+NS is loaded only after
 // stage t finished, and the window is larger than the matrix bandwidth plus
@@ -21,9 +23,9 @@
 
 namespace flow {
 
-constexpr int kStageBlocks = 128;   // 16 KB of 4x4 FP64 blocks per stage
+constexpr int kStageBlocks = 192;   // 24 KB of 4x4 FP64 blocks per stage
 constexpr int kStageRows = 32;      // at most 32 rows per stage
-constexpr int kStages = 5;          // ring depth
+constexpr int kStages = 6;          // ring depth
 constexpr int kWindow = 1024;       // dQ window rows (power of two)
 constexpr int kSweepThreads = 1024; // 1 producer warp + 31 row warps
 
@@ -145,9 +147,11 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     return;
   }
 
-  // ---------------- row warps ----------------
-  const int slotl = lane >> 2, r = lane & 3;
-  for (int p = warp - 1; p < nn; p += 31) {
+  // ---------------- row groups: 4 lanes per row ----------------
+  const int g = lane >> 2, r = lane & 3;
+  const unsigned gmask = 0xFu << (4 * g);
+  const int ngroups = 31 * 8;
+  for (int p = (warp - 1) * 8 + g; p < nn; p += ngroups) {
     const int j = FWD ? (1 + p) : (nn - p);
     const int t = tb.row_stage[j];
     const int u = FWD ? t : (T - 1 - t);
@@ -157,90 +161,73 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     const int k0 = m.ia[j], k1 = m.ia[j + 1];
     const int b0 = m.ia[r0];
     const int j0 = b0 & ~3;
-    // old dQ of this row and of the neighbours the sweep does not update first
-    const double old_v = (lane < 4) ? __ldcg(s.dQ + 4 * (long)j + lane) : 0.;
+    const double old_r = __ldcg(s.dQ + 4 * (long)j + r);
+    bool bad = false;
     {
       long spins = 0;
       while (!mbar_try_wait(&sm.full[slot], parity)) {
         if (++spins > (max_spin >> 4) || *(volatile int*)&sm.abort) {
           atomicOr(s.status, ERR_SWEEP_TIMEOUT);
           sm.abort = 1;
+          bad = true;
           break;
         }
       }
     }
-    if (*(volatile int*)&sm.abort) return;
+    if (__any_sync(gmask, bad)) return;
     const StageSlot& st = sm.slot[slot];
     double acc = st.rhs[4 * (j - r0) + r];
-    const double lu_v = (lane < 16) ? st.lud[16 * (j - r0) + lane] : 0.;
-    bool bad = false;
-    for (int base = k0; base < k1; base += 8) {
-      const int k = base + slotl;
-      bool use = false;
-      double term = 0.;
-      if (k < k1) {
-        const int c = st.ja[k - j0];
-        use = c != j;
-        if (use) {
-          const double* A = st.lhs + 16 * (k - b0) + 4 * r;
-          double d0, d1, d2, d3;
-          const bool dep = FWD ? (c < j) : (c > j);
-          if (dep) {
-            const int w = c & (kWindow - 1);
-            long spins = 0;
-            while (*(volatile int*)&sm.tag[w] != c) {
-              if (++spins > max_spin || *(volatile int*)&sm.abort) {
-                atomicOr(s.status, ERR_SWEEP_TIMEOUT);
-                sm.abort = 1;
-                bad = true;
-                break;
-              }
-            }
-            __threadfence_block();
-            const volatile double* wv = sm.win + 4 * w;
-            d0 = wv[0]; d1 = wv[1]; d2 = wv[2]; d3 = wv[3];
-          } else {
-            const double2* dq = reinterpret_cast<const double2*>(s.dQ + 4 * (long)c);
-            const double2 a = __ldcg(dq), b = __ldcg(dq + 1);
-            d0 = a.x; d1 = a.y; d2 = b.x; d3 = b.y;
+    for (int k = k0; k < k1 && !bad; k++) {
+      const int c = st.ja[k - j0];
+      if (c == j) continue;
+      const double* A = st.lhs + 16 * (k - b0) + 4 * r;
+      double d0, d1, d2, d3;
+      const bool dep = FWD ? (c < j) : (c > j);
+      if (dep) {
+        const int w = c & (kWindow - 1);
+        long spins = 0;
+        while (*(volatile int*)&sm.tag[w] != c) {
+          if (++spins > max_spin || *(volatile int*)&sm.abort) {
+            atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+            sm.abort = 1;
+            bad = true;
+            break;
           }
-          term = (A[0] * d0 + A[1] * d1 + A[2] * d2 + A[3] * d3);
         }
+        __threadfence_block();
+        const volatile double* wv = sm.win + 4 * w;
+        d0 = wv[0]; d1 = wv[1]; d2 = wv[2]; d3 = wv[3];
+      } else {
+        const double2* dq = reinterpret_cast<const double2*>(s.dQ + 4 * (long)c);
+        const double2 a = __ldcg(dq), b = __ldcg(dq + 1);
+        d0 = a.x; d1 = a.y; d2 = b.x; d3 = b.y;
       }
-      const unsigned used = __ballot_sync(FULL, use);
-#pragma unroll
-      for (int sl = 0; sl < 8; sl++) {
-        const double tv = __shfl_sync(FULL, term, sl * 4 + r);
-        if (used & (1u << (sl * 4))) acc -= tv;
-      }
+      acc -= (A[0] * d0 + A[1] * d1 + A[2] * d2 + A[3] * d3);
     }
-    if (__any_sync(FULL, bad)) return;
-    double b[4], M[16], o[4];
+    if (__any_sync(gmask, bad)) return;
+    double b[4], o[4], X[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) b[q] = __shfl_sync(FULL, acc, q);
+    for (int q = 0; q < 4; q++) {
+      b[q] = __shfl_sync(gmask, acc, 4 * g + q);
+      o[q] = __shfl_sync(gmask, old_r, 4 * g + q);
+    }
+    lu_solve4(st.lud + 16 * (j - r0), b, X);
+    double xr = X[0], orr = o[0];
 #pragma unroll
-    for (int q = 0; q < 16; q++) M[q] = __shfl_sync(FULL, lu_v, q);
-#pragma unroll
-    for (int q = 0; q < 4; q++) o[q] = __shfl_sync(FULL, old_v, q);
-    if (lane == 0) {
-      double X[4];
-      lu_solve4(M, b, X);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const double dx = X[q] - o[q];
-        o[q] += dx;
-      }
-      const int w = j & (kWindow - 1);
-      volatile double* wv = sm.win + 4 * w;
-      wv[0] = o[0]; wv[1] = o[1]; wv[2] = o[2]; wv[3] = o[3];
+    for (int q = 1; q < 4; q++)
+      if (r == q) { xr = X[q]; orr = o[q]; }
+    const double dx = xr - orr;
+    const double val = orr + dx;
+    const int w = j & (kWindow - 1);
+    ((volatile double*)sm.win)[4 * w + r] = val;
+    s.dQ[4 * (long)j + r] = val;
+    __syncwarp(gmask);
+    if (r == 0) {
       __threadfence_block();
       *(volatile int*)&sm.tag[w] = j;
-      double* dq = s.dQ + 4 * (long)j;
-      reinterpret_cast<double2*>(dq)[0] = make_double2(o[0], o[1]);
-      reinterpret_cast<double2*>(dq)[1] = make_double2(o[2], o[3]);
       atomicAdd(&sm.rows_done[slot], 1);
     }
-    __syncwarp();
+    __syncwarp(gmask);
   }
 }
 
