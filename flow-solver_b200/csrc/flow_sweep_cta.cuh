@@ -48,6 +48,7 @@ struct SweepSmem {
   double win[kWindow * 4];
   int tag[kWindow];
   int rows_done[kStages];
+  int armed[kStages];      // stage index the slot was last armed for
   unsigned long long full[kStages];
   int abort;
 };
@@ -104,6 +105,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
   if (threadIdx.x < kStages) {
     mbar_init(&sm.full[threadIdx.x], 1);
     sm.rows_done[threadIdx.x] = 0;
+    sm.armed[threadIdx.x] = -1;
   }
   if (threadIdx.x == 0) sm.abort = 0;
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -142,6 +144,10 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         bulk_copy(st.lud, s.LUd + 16 * (long)r0, bu, &sm.full[slot]);
         bulk_copy(st.rhs, s.RHS + 4 * (long)r0, br, &sm.full[slot]);
         bulk_copy(st.ja, tb.ja_pad + j0, bj, &sm.full[slot]);
+        // publish which stage the slot now holds: a consumer must see this
+        // before its parity wait, or it could match the slot's previous phase
+        __threadfence_block();
+        *(volatile int*)&sm.armed[slot] = u;
       }
     }
     return;
@@ -165,6 +171,18 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     bool bad = false;
     {
       long spins = 0;
+      while (*(volatile int*)&sm.armed[slot] != u) {
+        if (++spins > max_spin || *(volatile int*)&sm.abort) {
+          atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+          sm.abort = 1;
+          bad = true;
+          break;
+        }
+      }
+    }
+    if (__any_sync(gmask, bad)) return;
+    {
+      long spins = 0;
       while (!mbar_try_wait(&sm.full[slot], parity)) {
         if (++spins > (max_spin >> 4) || *(volatile int*)&sm.abort) {
           atomicOr(s.status, ERR_SWEEP_TIMEOUT);
@@ -180,6 +198,12 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     for (int k = k0; k < k1 && !bad; k++) {
       const int c = st.ja[k - j0];
       if (c == j) continue;
+      if (c < 1 || c > nn) {  // a corrupt stage: report, never dereference
+        atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+        sm.abort = 1;
+        bad = true;
+        break;
+      }
       const double* A = st.lhs + 16 * (k - b0) + 4 * r;
       double d0, d1, d2, d3;
       const bool dep = FWD ? (c < j) : (c > j);

@@ -232,8 +232,10 @@ void orc_derivatives_k2(orc_grid *g)
         double w = 1.0 / pow(dist, 1.0);
         b[j - s0] = w * (g->nQ[node * NV + var] - g->nQ[i * NV + var]);
       }
-      /* linear_algebra.C dotProductGeneral: sequential sum from 0 */
-      for (int j = 0; j < m; j++) {
+      /* linear_algebra.C dotProductGeneral: sequential sum from 0.  The
+       * reference forms all m entries of U^T b but reads only the first 5
+       * (compute_derivatives.C:1479-1491). */
+      for (int j = 0; j < 5; j++) {
         double s = 0.;
         for (int k = 0; k < m; k++) s += b[k] * U[j * m + k];
         t2[j] = s;
