@@ -171,6 +171,7 @@ def run_flow(args):
     mesh = Mesh.from_case(casedir, order=wl.order)
     prep_s = time.time() - t0
     solver = capi.Solver.from_mesh(mesh, params, device=local)
+    solver.set_sweep_mode(args.sweep_mode)
     sizes = mesh.sizes
     nnz = int(mesh.array("ia")[sizes["nn"] + 1])
     Q0 = mesh.initial_state(params)
@@ -296,6 +297,24 @@ def cpu_baseline(casedir: str, steps_conv: int) -> dict:
                       f"the same solve, {dt:.3f} s/step, x {steps_conv} steps per solve"}
 
 
+def run_profile(args):
+    """A few pseudo-time steps of one solve of the workload, nothing else:
+    the command the ncu launch lists and kernel captures in profiles/ run."""
+    from flowgpu import capi, workloads
+    from flowgpu.prep import Mesh
+    wl = workloads.get(args.workload)
+    mesh = Mesh.from_case(wl.write(), order=wl.order)
+    solver = capi.Solver.from_mesh(mesh, wl.params(), device=0)
+    solver.set_sweep_mode(args.sweep_mode)
+    solver.set_state(mesh.initial_state(wl.params()))
+    rh, dh = solver.run(1, args.profile_steps)
+    print(json.dumps({"workload": wl.name, "steps": args.profile_steps,
+                      "ms_per_step": solver.last_device_ms() / args.profile_steps,
+                      "r_rho_last": rh[-1], "launches": solver.launch_count(),
+                      "status": solver.status()}), flush=True)
+    solver.close()
+
+
 # ---------------------------------------------------------------------------
 def _ref_worker(args_tuple):
     casedir, warmup, steps = args_tuple
@@ -364,11 +383,16 @@ def main():
     ap.add_argument("--impl", default="flow", choices=("flow", "reference"))
     ap.add_argument("--workload", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="only run this many pseudo-time steps of one solve (for ncu captures)")
+    ap.add_argument("--sweep-mode", type=int, default=0, help="0 grid-wide, 1 one-CTA ordered sweep")
     args = ap.parse_args()
     from flowgpu import workloads
     args.workload = args.workload or workloads.DEFAULT
     if args.impl == "reference":
         run_reference(args)
+    elif args.profile_steps > 0:
+        run_profile(args)
     else:
         run_flow(args)
 

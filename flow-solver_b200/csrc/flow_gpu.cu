@@ -59,13 +59,15 @@ struct flow_ctx {
   int nsm = 148;
   int epoch = 0;
   int citer = 0;
-  int sweep_mode = 0;
+  int sweep_mode = 0;  // 0 grid-wide ordered sweep, 1 one-CTA ordered sweep
   long launches = 0;
   double last_ms = 0.;
   bool ok = false;
   // host copies needed to answer flow_get in the reference layout
   int nn = 0, ng = 0, ns = 0, nbe = 0, nnz = 0;
   double drop_target = 0.;   // host copy of the pending target (read by reset_run)
+  int* h_flags = nullptr;      // pinned: stop flag and status read back by flow_converge_batch
+  cudaEvent_t ev_flag = nullptr;
   // optional per-kernel event timing
   int timing = 0;
   std::vector<cudaEvent_t> event_pool;
@@ -262,23 +264,30 @@ int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
   const long max_spin = 1L << 21;  // ~0.1-0.2 s per wait at most
   for (int it = 0; it < p->subits; it++) {
     cudaMemsetAsync(c->s.counter, 0, sizeof(unsigned), c->stream);
-    int ep = ++c->epoch;
     {
       Timed t(c, 4);
-      if (c->sweep_cta_ok && c->sweep_mode == 0) {
+      if (c->sweep_cta_ok && c->sweep_mode == 1) {
         const size_t sm = sizeof(SweepSmem);
         if (it % 2 == 0)
           k_sweep_cta<true><<<1, kSweepThreads, sm, c->stream>>>(c->m, c->s, c->sweep_tb, max_spin);
         else
           k_sweep_cta<false><<<1, kSweepThreads, sm, c->stream>>>(c->m, c->s, c->sweep_tb, max_spin);
+        rc |= launch_check(c);
       } else {
+        // results go to the other dQ buffer, pre-filled with the not-ready
+        // pattern; the buffers swap roles afterwards
+        double* dq_new = c->s.dQ2;
+        k_prepare_sweep<<<grid_blocks(4 * (c->nn + 1), 256), 256, 0, c->stream>>>(
+            c->s, c->s.dQ, dq_new, 4 * (c->nn + 1));
+        rc |= launch_check(c);
         int blocks = c->nsm * 4;
         if (it % 2 == 0)
-          k_sweep_ordered<true><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
+          k_sweep_ordered<true><<<blocks, 128, 0, c->stream>>>(c->m, c->s, c->s.dQ, dq_new, max_spin);
         else
-          k_sweep_ordered<false><<<blocks, 128, 0, c->stream>>>(c->m, c->s, ep, max_spin);
+          k_sweep_ordered<false><<<blocks, 128, 0, c->stream>>>(c->m, c->s, c->s.dQ, dq_new, max_spin);
+        rc |= launch_check(c);
+        std::swap(c->s.dQ, c->s.dQ2);
       }
-      rc |= launch_check(c);
     }
     if (it < p->subits - 1 || final_rms) {
       Timed t(c, 5);
@@ -584,6 +593,7 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   s.nQ = c->buf.alloc<double>(nq);
   s.pQ = c->buf.alloc<double>(nq);
   s.dQ = c->buf.alloc<double>((size_t)(nn + 1) * 4);
+  s.dQ2 = c->buf.alloc<double>((size_t)(nn + 1) * 4);
   s.R = c->buf.alloc<double>((size_t)(nn + 1) * 4);
   s.RHS = c->buf.alloc<double>((size_t)(nn + 1) * 4);
   s.grad = c->buf.alloc<double>((size_t)(nn + 1) * 8);
@@ -608,7 +618,7 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   s.steps_done = c->buf.alloc<int>(1);
   s.partial = c->buf.alloc<double>(2 * kRedBlocks);
   s.scalars = c->buf.alloc<double>(8);
-  if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
+  if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.dQ2 || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
       !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
       !s.Jb || !s.bforce || !s.done || !s.counter || !s.status || !s.skip || !s.partial ||
       !s.scalars || !s.stop || !s.steps_done)
@@ -617,6 +627,7 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   cudaMemset(s.nQ, 0, nq * 8);
   cudaMemset(s.pQ, 0, nq * 8);
   cudaMemset(s.dQ, 0, (size_t)(nn + 1) * 32);
+  cudaMemset(s.dQ2, 0, (size_t)(nn + 1) * 32);
   cudaMemset(s.R, 0, (size_t)(nn + 1) * 32);
   cudaMemset(s.RHS, 0, (size_t)(nn + 1) * 32);
   cudaMemset(s.grad, 0, (size_t)(nn + 1) * 64);
@@ -649,6 +660,8 @@ void flow_destroy(flow_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   harvest(c);
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+  if (c->ev_flag) cudaEventDestroy(c->ev_flag);
+  if (c->h_flags) cudaFreeHost(c->h_flags);
   c->buf.release();
   if (c->d_hist) cudaFree(c->d_hist);
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -673,7 +686,11 @@ int flow_set_state(flow_ctx* c, const double* Q) {
 }
 
 int flow_set_sweep_mode(flow_ctx* c, int mode) {
-  if (!c || mode < 0 || mode > 2) return FLOW_ERR_ARG;
+  if (!c || mode < 0 || mode > 1) return FLOW_ERR_ARG;
+  if (mode == 1 && !c->sweep_cta_ok) {
+    set_error("matrix bandwidth too large for the one-CTA sweep window");
+    return FLOW_ERR_ARG;
+  }
   c->sweep_mode = mode;
   return 0;
 }
@@ -765,6 +782,80 @@ int flow_converge(flow_ctx* c, const flow_params* p, int ts0, int max_steps, dou
   if (r_last) *r_last = sqrt(sc[2]);
   if (st) return st;
   return stop ? 0 : FLOW_ERR_NOT_CONVERGED;
+}
+
+int flow_converge_batch(flow_ctx** ctxs, int n, const flow_params* p, int ts0, int max_steps,
+                        double drop, int chunk, int* steps, int* status) {
+  if (!ctxs || n < 1 || max_steps < 1 || !(drop > 0.)) return FLOW_ERR_ARG;
+  if (chunk < 1) chunk = 64;
+  int rc_all = 0;
+  for (int i = 0; i < n; i++) {
+    flow_ctx* c = ctxs[i];
+    if (!c || !c->ok) return FLOW_ERR_ARG;
+    int rc = check_params(c, p);
+    if (rc) return rc;
+    cudaSetDevice(c->device);
+    if ((rc = ensure_hist(c, 1))) return rc;
+    if (!c->h_flags) {
+      if (cudaHostAlloc(&c->h_flags, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
+        return FLOW_ERR_CUDA;
+    }
+    if (!c->ev_flag) cudaEventCreateWithFlags(&c->ev_flag, cudaEventDisableTiming);
+    c->h_flags[0] = 0;
+    c->h_flags[1] = 0;
+    reset_run(c, drop);
+    cudaEventRecord(c->ev0, c->stream);
+  }
+  std::vector<int> issued(n, 0), active(n, 1), pending(n, 0);
+  int nactive = n;
+  while (nactive > 0) {
+    // issue one chunk per active context, then read back the previous round
+    for (int i = 0; i < n; i++) {
+      if (!active[i]) continue;
+      flow_ctx* c = ctxs[i];
+      cudaSetDevice(c->device);
+      int k = std::min(chunk, max_steps - issued[i]);
+      int rc = 0;
+      for (int q = 0; q < k && !rc; q++, issued[i]++)
+        rc |= enqueue_step(c, p, ts0 + issued[i], -1, issued[i] == 0);
+      if (rc) { rc_all |= rc; active[i] = 0; nactive--; continue; }
+      if (pending[i]) {
+        // the flags of the previous round are ready once its event completed
+        if (cudaEventSynchronize(c->ev_flag) != cudaSuccess) {
+          rc_all |= FLOW_ERR_CUDA;
+          active[i] = 0;
+          nactive--;
+          continue;
+        }
+        harvest(c);
+        if (c->h_flags[0] || c->h_flags[1]) { active[i] = 0; nactive--; continue; }
+      }
+      cudaMemcpyAsync(&c->h_flags[0], c->s.stop, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+      cudaMemcpyAsync(&c->h_flags[1], c->s.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+      cudaEventRecord(c->ev_flag, c->stream);
+      pending[i] = 1;
+      if (issued[i] >= max_steps) { active[i] = 0; nactive--; }
+    }
+  }
+  for (int i = 0; i < n; i++) {
+    flow_ctx* c = ctxs[i];
+    cudaSetDevice(c->device);
+    cudaEventRecord(c->ev1, c->stream);
+    int st = read_status(c);
+    int done = 0, stop = 0;
+    cudaMemcpy(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    c->last_ms = ms;
+    reset_run(c, 0.);
+    cudaStreamSynchronize(c->stream);
+    if (steps) steps[i] = done;
+    if (!stop && !st) st = FLOW_ERR_NOT_CONVERGED;
+    if (status) status[i] = st;
+    rc_all |= st;
+  }
+  return rc_all;
 }
 
 int flow_build_matrix(flow_ctx* c, const flow_params* p, int citer) {

@@ -546,17 +546,33 @@ __global__ void __launch_bounds__(128) k_diag_only(DevMesh m, DevState s) {
 // ---------------------------------------------------------------------------
 // Ordered block Gauss-Seidel sweep (linear_algebra.C:178-344).  Rows are
 // handed out in the reference's order (ascending forward, descending
-// backward) by an atomic dispenser; one warp per row.  A row waits only for
-// the rows it reads that the reference updates earlier in the same sweep
-// (its lower, resp. upper, neighbours): each finished row publishes its dQ
-// and then a release flag.  Since a row is only claimed by a running warp
-// and every dependency was claimed earlier, the earliest unfinished row can
-// always proceed; every wait is nevertheless bounded and reports
-// ERR_SWEEP_TIMEOUT instead of spinning forever.
+// backward) by an atomic dispenser; one warp per row.  The sweep writes its
+// results into dq_new, which is filled with an all-ones bit pattern (a NaN
+// no arithmetic produces) before the sweep: a row that needs a neighbour the
+// reference updates earlier in the same sweep polls that neighbour's four
+// values until none is the pattern any more (each 8-byte store is
+// single-copy atomic), so the value itself is the ready signal.  Other
+// neighbours and the row's own previous value come from dq_old.  Rows are
+// only claimed by running warps and every dependency was claimed earlier,
+// so the earliest unfinished row always proceeds; every wait is nevertheless
+// bounded and reports ERR_SWEEP_TIMEOUT instead of spinning forever.
 // Lanes: 8 block slots x 4 matrix rows.
+constexpr unsigned long long kNotReady = 0xFFFFFFFFFFFFFFFFull;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const double* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void st_relaxed_f64(double* p, double v) {
+  asm volatile("st.relaxed.gpu.global.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
 template <bool FWD>
-__global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, int epoch,
-                                                       long max_spin) {
+__global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s,
+                                                       const double* __restrict__ dq_old,
+                                                       double* dq_new, long max_spin) {
   if (*s.stop) return;  // the run has converged
   if (*s.skip) return;
   const unsigned FULL = 0xffffffffu;
@@ -570,12 +586,11 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, in
     if (t >= (unsigned)nn) break;
     const int j = FWD ? (int)(1 + t) : (int)(nn - t);
     const int k0 = m.ia[j], k1 = m.ia[j + 1];
-    // Everything that does not depend on this sweep's results is loaded before
-    // any wait: RHS, the LU factors of the diagonal block, the old dQ of the
-    // row and the row's off-diagonal blocks.
+    // everything that does not depend on this sweep's results first
     double acc = s.RHS[4 * (long)j + r];
     const double lu_v = (lane < 16) ? s.LUd[16 * (long)j + lane] : 0.;
-    const double old_v = (lane < 4) ? __ldcg(s.dQ + 4 * (long)j + lane) : 0.;
+    const double old_v = (lane < 4) ? dq_old[4 * (long)j + lane] : 0.;
+    bool timeout = false;
     for (int base = k0; base < k1; base += 8) {
       const int k = base + slot;
       int c = 0;
@@ -592,22 +607,39 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, in
       double term = 0.;
       if (use) {
         const bool dep = FWD ? (c < j) : (c > j);
+        double d0, d1, d2, d3;
         if (dep) {
-          cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[c]);
+          const double* src = dq_new + 4 * (long)c;
+          unsigned long long u0, u1, u2, u3;
           long spins = 0;
-          while (f.load(cuda::memory_order_acquire) != epoch) {
+          for (;;) {
+            u0 = ld_relaxed_u64(src);
+            u1 = ld_relaxed_u64(src + 1);
+            u2 = ld_relaxed_u64(src + 2);
+            u3 = ld_relaxed_u64(src + 3);
+            if (u0 != kNotReady && u1 != kNotReady && u2 != kNotReady && u3 != kNotReady) break;
             if (++spins > max_spin) {
               atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+              timeout = true;
               break;
             }
             // once any wait has timed out, every other wait gives up too
-            if ((spins & 1023) == 0 && (*(volatile int*)s.status & ERR_SWEEP_TIMEOUT)) break;
-            if (spins > 64) __nanosleep(20);
+            if ((spins & 1023) == 0 && (*(volatile int*)s.status & ERR_SWEEP_TIMEOUT)) {
+              timeout = true;
+              break;
+            }
+            if (spins > 256) __nanosleep(32);
           }
+          d0 = __longlong_as_double((long long)u0);
+          d1 = __longlong_as_double((long long)u1);
+          d2 = __longlong_as_double((long long)u2);
+          d3 = __longlong_as_double((long long)u3);
+        } else {
+          const double2* dq = reinterpret_cast<const double2*>(dq_old + 4 * (long)c);
+          const double2 x01 = __ldcg(dq), x23 = __ldcg(dq + 1);
+          d0 = x01.x; d1 = x01.y; d2 = x23.x; d3 = x23.y;
         }
-        const double2* dq = reinterpret_cast<const double2*>(s.dQ + 4 * (long)c);
-        const double2 d01 = __ldcg(dq), d23 = __ldcg(dq + 1);
-        term = (a0 * d01.x + a1 * d01.y + a2 * d23.x + a3 * d23.y);
+        term = (a0 * d0 + a1 * d1 + a2 * d2 + a3 * d3);
       }
       const unsigned used = __ballot_sync(FULL, use);
 #pragma unroll
@@ -623,22 +655,36 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s, in
     for (int q = 0; q < 16; q++) M[q] = __shfl_sync(FULL, lu_v, q);
 #pragma unroll
     for (int q = 0; q < 4; q++) o[q] = __shfl_sync(FULL, old_v, q);
-    if (lane == 0) {
-      double X[4];
-      lu_solve4(M, b, X);
+    double X[4];
+    lu_solve4(M, b, X);
+    double mine = X[0], own = o[0];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        double dx = X[q] - o[q];
-        o[q] += dx;
-      }
-      double* dq = s.dQ + 4 * (long)j;
-      __stcg(reinterpret_cast<double2*>(dq), make_double2(o[0], o[1]));
-      __stcg(reinterpret_cast<double2*>(dq) + 1, make_double2(o[2], o[3]));
-      cuda::atomic_ref<int, cuda::thread_scope_device> f(s.done[j]);
-      f.store(epoch, cuda::memory_order_release);
+    for (int q = 1; q < 4; q++)
+      if (lane == q) { mine = X[q]; own = o[q]; }
+    if (__any_sync(FULL, timeout)) {
+      // a timed-out row publishes something so that nothing waits on it
+      mine = 0.;
+      own = 0.;
+    }
+    if (lane < 4) {
+      const double dx = mine - own;
+      st_relaxed_f64(dq_new + 4 * (long)j + lane, own + dx);
     }
     __syncwarp();
   }
+}
+
+// Before an ordered sweep: fill its result buffer with the not-ready
+// pattern.  When the sweep will not run (the run converged, or the linear
+// residual already dropped below 1e-15, linear_algebra.C:389) carry the
+// current dQ over instead, so that the buffer swap after the sweep keeps it.
+__global__ void k_prepare_sweep(DevState s, const double* cur, double* next, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (*s.stop || *s.skip)
+    next[i] = cur[i];
+  else
+    next[i] = __longlong_as_double((long long)0xFFFFFFFFFFFFFFFFull);
 }
 
 // ---------------------------------------------------------------------------

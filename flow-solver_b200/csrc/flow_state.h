@@ -65,7 +65,8 @@ struct DevState {
   double* Q;
   double* nQ;
   double* pQ;
-  double* dQ;
+  double* dQ;       // current dQ (the host swaps it with dQ2 after each ordered sweep)
+  double* dQ2;
   double* R;
   double* RHS;
   double* grad;     // 8 per node

@@ -23,7 +23,7 @@ ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
-           "flow_converge", "flow_build_matrix", "flow_reconstruct", "flow_residuals", "flow_linear_solve",
+           "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct", "flow_residuals", "flow_linear_solve",
            "flow_body_forces", "flow_get", "flow_size", "flow_set_sweep_mode", "flow_save_state",
            "flow_restore_state", "flow_set_timing", "flow_kernel_times", "flow_stream",
            "flow_status",
@@ -82,6 +82,8 @@ def load():
     L.flow_solve.argtypes = [vp, PP, C.c_int, DP, DP]
     L.flow_run.argtypes = [vp, PP, C.c_int, C.c_int, DP, DP]
     L.flow_converge.argtypes = [vp, PP, C.c_int, C.c_int, C.c_double, C.c_int, IP, DP, DP]
+    L.flow_converge_batch.argtypes = [C.POINTER(vp), C.c_int, PP, C.c_int, C.c_int, C.c_double,
+                                      C.c_int, IP, IP]
     L.flow_build_matrix.argtypes = [vp, PP, C.c_int]
     L.flow_reconstruct.argtypes = [vp, PP, C.c_int]
     L.flow_residuals.argtypes = [vp, PP, C.c_int, C.c_int]
@@ -125,6 +127,21 @@ class FlowError(RuntimeError):
             msg += f": {what}"
         super().__init__(msg)
         self.code = code
+
+
+def converge_batch(solvers, ts0: int = 1, max_steps: int = 20000, drop: float = 1e-10,
+                   chunk: int = 64, check: bool = True):
+    """flow_converge_batch over several Solver objects; returns (steps, status) lists."""
+    L = load()
+    n = len(solvers)
+    arr = (C.c_void_p * n)(*[s.ctx for s in solvers])
+    steps = (C.c_int * n)()
+    st = (C.c_int * n)()
+    rc = L.flow_converge_batch(arr, n, C.byref(solvers[0].p), ts0, max_steps, drop, chunk,
+                               steps, st)
+    if check:
+        _check(rc, "flow_converge_batch")
+    return list(steps), list(st)
 
 
 def _check(rc: int, what: str = ""):

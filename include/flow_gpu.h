@@ -147,6 +147,15 @@ int flow_run(flow_ctx *ctx, const flow_params *p, int ts0, int nsteps, double *r
 int flow_converge(flow_ctx *ctx, const flow_params *p, int ts0, int max_steps, double drop,
                   int chunk, int *steps, double *r_first, double *r_last);
 
+/* flow_converge for n independent contexts at once (a batch of solves):
+ * each context's steps run on its own stream so the solves overlap on the
+ * device; the host issues `chunk` steps per context per round and reads each
+ * context's stop flag one round later.  steps[i] / status[i] (optional)
+ * receive each solve's step count and status; the return value ORs the
+ * statuses.  Use flow_last_device_ms per context for its device span. */
+int flow_converge_batch(flow_ctx **ctxs, int n, const flow_params *p, int ts0, int max_steps,
+                        double drop, int chunk, int *steps, int *status);
+
 /* void build_matrix(GRID*, PARAMS, SYS_MEM*)  (include/init_memory.h:24,
  * init_memory.C:159-310) with GRID::citer = citer; writes dt and the V/dt
  * diagonal (LHS otherwise zero). */
@@ -182,12 +191,11 @@ int flow_get(flow_ctx *ctx, const char *name, double *out, long n);
 /* Number of doubles flow_get(name) writes, or -1. */
 long flow_size(flow_ctx *ctx, const char *name);
 
-/* Sweep kernel: 0 = ordered Gauss-Seidel sweeps that reproduce the
- * reference's sequential sweeps exactly, one CTA per mesh with the matrix
- * streamed through shared memory (default; falls back to 2 when the matrix
- * bandwidth exceeds its window); 2 = the same ordered sweeps spread over
- * the whole GPU with global-memory ready flags.  Both give identical
- * results. */
+/* Sweep kernel; both reproduce the reference's sequential block
+ * Gauss-Seidel sweeps exactly: 0 = rows dispensed in order to warps across
+ * the whole GPU (default); 1 = one CTA per mesh, matrix streamed through a
+ * shared-memory ring (uses one SM; for many concurrent meshes; refused when
+ * the matrix bandwidth exceeds its dQ window). */
 int flow_set_sweep_mode(flow_ctx *ctx, int mode);
 
 /* Device snapshot of the solution state (Q, nQ, pQ and the boundary normals

@@ -26,11 +26,11 @@ def _solver(case, sweep_mode=0):
     (128, 32, False, 1, 4, 0),
     (32, 8, True, 3, 6, 0),
     (128, 32, True, 3, 4, 0),
-    (128, 32, True, 3, 3, 2),
-    (64, 16, False, 1, 3, 2),
+    (128, 32, True, 3, 3, 1),
+    (64, 16, False, 1, 3, 1),
 ])
 def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode):
-    """mode 0: one-CTA ordered sweep; mode 2: grid-wide ordered sweep."""
+    """mode 0: grid-wide ordered sweep; mode 1: one-CTA ordered sweep."""
     case = ParityCase(nc, nr, curved, order)
     gpu = _solver(case, mode)
     nn = case.sizes["nn"]
