@@ -308,10 +308,19 @@ def run_profile(args):
     solver.set_sweep_mode(args.sweep_mode)
     solver.set_state(mesh.initial_state(wl.params()))
     rh, dh = solver.run(1, args.profile_steps)
-    print(json.dumps({"workload": wl.name, "steps": args.profile_steps,
-                      "ms_per_step": solver.last_device_ms() / args.profile_steps,
-                      "r_rho_last": rh[-1], "launches": solver.launch_count(),
-                      "status": solver.status()}), flush=True)
+    out = {"workload": wl.name, "steps": args.profile_steps,
+           "ms_per_step": solver.last_device_ms() / args.profile_steps,
+           "r_rho_last": rh[-1], "launches": solver.launch_count(),
+           "status": solver.status()}
+    if args.kernel_times:
+        # the same steps again with per-kernel events (continues the solve)
+        solver.set_timing(True)
+        solver.run(1 + args.profile_steps, args.profile_steps)
+        out["kernels_ms_per_launch"] = {
+            k: (round(ms / cnt, 4) if cnt else 0.0) for k, (cnt, ms) in
+            solver.kernel_times().items()}
+        solver.set_timing(False)
+    print(json.dumps(out), flush=True)
     solver.close()
 
 
@@ -383,6 +392,8 @@ def main():
     ap.add_argument("--impl", default="flow", choices=("flow", "reference"))
     ap.add_argument("--workload", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="with --profile-steps: also print per-kernel device times")
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many pseudo-time steps of one solve (for ncu captures)")
     ap.add_argument("--sweep-mode", type=int, default=0, help="0 grid-wide, 1 one-CTA ordered sweep")

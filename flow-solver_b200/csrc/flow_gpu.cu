@@ -216,11 +216,11 @@ void harvest(flow_ctx* c) {
 
 int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   Timed tm(c, 0);
-  int nb = grid_blocks(c->nn, 128);
+  int nb = grid_blocks(4 * c->nn, 128);
   if (c->order == 1)
-    k_node_prepare<1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+    k_node_prepare4<1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
   else
-    k_node_prepare<3><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+    k_node_prepare4<3><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
   return launch_check(c);
 }
 
@@ -247,9 +247,9 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   }
   {
     Timed t(c, 3);
-    int nbn = grid_blocks(c->nn, 128);
-    if (jac) k_assemble<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
-    else k_assemble<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+    int nbn = grid_blocks(4 * c->nn, 128);
+    if (jac) k_assemble4<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+    else k_assemble4<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
     rc |= launch_check(c);
   }
   return rc;

@@ -251,6 +251,245 @@ __global__ void __launch_bounds__(128) k_node_prepare(DevMesh m, DevState s, Ste
 }
 
 // ---------------------------------------------------------------------------
+// k_node_prepare with four lanes per node, lane v owning conserved variable
+// v: the gradient, the k=2 derivatives and point value, and the limiter
+// value of variable v only involve variable v, and each lane accumulates
+// its sums in the same face / stencil order as the reference, so the
+// results are those of k_node_prepare.  The wave-speed sum (all variables)
+// is formed by every lane of the quad from node constants computed once.
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = (tid >> 2) + 1, v = tid & 3;
+  const int qbase = threadIdx.x & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (n > m.nn) return;  // whole quads leave together
+  const double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
+  const double q0v = v == 0 ? q4.x : v == 1 ? q4.y : v == 2 ? q4.z : q4.w;
+
+  // ---- wave-speed sum (cv_calc.C:819-953): node constants first ----
+  const double rho = q4.x, uu = q4.y / rho, vv = q4.z / rho;
+  const double P = (a.gamma - 1.0) * (q4.w - 0.5 * rho * (uu * uu + vv * vv));
+  const double cs = sqrt((a.gamma * P) / rho);
+  double ev = 0.;
+  int bad = 0;
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int k = s0; k < s1; k++) {
+    const double4 g = m.sub_geo[m.nsub[k] >> 1];
+    const double theta = uu * g.x + vv * g.y;
+    const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+    const double w = tpc >= tmc ? tpc : tmc;
+    if (!isfinite(w)) bad = 1;
+    ev += (w * g.z);
+  }
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  for (int k = b0; k < b1; k++) {
+    const double* xn = s.xn_bedges + 3 * m.nbed[k];
+    const double theta = uu * xn[0] + vv * xn[1];
+    const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+    const double w = tpc >= tmc ? tpc : tmc;
+    if (!isfinite(w)) bad = 1;
+    ev += (w * xn[2]);
+  }
+  if (v == 0) {
+    const double dt = a.cfl * (m.cv_area[n] / ev);
+    s.dt[n] = dt;
+    if (bad) atomicOr(s.status, ERR_EIGEN);
+    if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
+  }
+  if (!a.do_grad && !a.do_derivs && !a.do_lim) return;
+
+  // ---- 1-ring min/max and the k=1 LSQ gradient of variable v ----
+  double qmin = q0v, qmax = q0v, g0 = 0., g1 = 0.;
+  const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
+  for (int k = e0; k < e1; k++) {
+    const int ed = m.nedg[k];
+    const int e = ed >> 1, side = ed & 1;
+    const int2 lr = m.edge_lr[e];
+    const int other = side ? lr.x : lr.y;
+    const double qo = s.nQ[4 * (long)other + v];
+    qmin = qmin <= qo ? qmin : qo;
+    qmax = qmax >= qo ? qmax : qo;
+    if (ORDER == 1 && a.do_grad) {
+      const double4 w = m.edge_w[e];
+      const double dq = side ? (q0v - qo) : (qo - q0v);  // nQ[R] - nQ[L]
+      if (side == 0) {
+        g0 += w.x * dq;
+        g1 += w.y * dq;
+      } else {
+        g0 -= w.z * dq;
+        g1 -= w.w * dq;
+      }
+    }
+  }
+  if (ORDER == 1 && a.do_grad)
+    reinterpret_cast<double2*>(s.grad + 8 * (long)n)[v] = make_double2(g0, g1);
+
+  // ---- k=2: x = V S^-1 U^T b of variable v ----
+  double h[5], pv = 0.;
+  if (ORDER == 3 && a.do_derivs) {
+    const int t0 = m.st_ptr[n], t1 = m.st_ptr[n + 1];
+    const int mrows = t1 - t0;
+    const double* U = m.svd_U1 + 5 * (long)t0;
+    double acc[5] = {0., 0., 0., 0., 0.};
+    for (int k = 0; k < mrows; k++) {
+      const int nb = m.st_idx[t0 + k];
+      const double bv = m.st_w[t0 + k] * (s.nQ[4 * (long)nb + v] - q0v);
+#pragma unroll
+      for (int c = 0; c < 5; c++) acc[c] += bv * U[c * mrows + k];
+    }
+    const double* VT = m.svd_VT + 25 * (long)n;
+    const double* S = m.svd_S + 5 * (long)n;
+    double t1v[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) t1v[c] = acc[c] / S[c];
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      double sum = 0.;
+#pragma unroll
+      for (int c = 0; c < 5; c++) sum += VT[j * 5 + c] * t1v[c];
+      h[j] = sum;
+    }
+    const double* mo = m.moments + 9 * (long)n;
+    pv = q0v - mo[0] * h[0] - mo[1] * h[1] - mo[2] * h[2] * 0.5 - mo[3] * h[3] * 0.5 -
+         mo[4] * h[4];
+    double* hd = s.hess5 + 20 * (long)n + 5 * v;
+#pragma unroll
+    for (int c = 0; c < 5; c++) hd[c] = h[c];
+    s.pv[4 * (long)n + v] = pv;
+  }
+
+  if (!a.do_lim) return;
+  // ---- Venkatakrishnan bound of variable v over every face point ----
+  double ph = 1.0;
+  const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
+  for (int k = s0; k < s1; k++) {
+    const int sd = m.nsub[k];
+    const int sub = sd >> 1, side = sd & 1;
+    if (ORDER == 1) {
+      const double4 d = m.sub_dx[sub];
+      const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
+      const double qr = q0v + (g0 * dx0 + g1 * dx1);
+      ph = venkat_fold(ph, qr, q0v, qmin, qmax);
+    } else {
+      const double* xg = m.sub_xg + 6 * (long)sub;
+#pragma unroll
+      for (int gpt = 0; gpt < 3; gpt++) {
+        const double dx0 = xg[2 * gpt] - xn0, dx1 = xg[2 * gpt + 1] - xn1;
+        double qr = pv;
+        qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
+               h[4] * dx0 * dx1);
+        ph = venkat_fold(ph, qr, q0v, qmin, qmax);
+      }
+    }
+  }
+  // min over the variables in order 0..3 (limiter.C:895-906)
+  const double p1 = __shfl_sync(qmask, ph, qbase + 1);
+  const double p2 = __shfl_sync(qmask, ph, qbase + 2);
+  const double p3 = __shfl_sync(qmask, ph, qbase + 3);
+  double pmin = ph;
+  pmin = pmin <= p1 ? pmin : p1;
+  pmin = pmin <= p2 ? pmin : p2;
+  pmin = pmin <= p3 ? pmin : p3;
+  const double out = v == 0 ? pmin : ph;
+  reinterpret_cast<double2*>(s.phi + 8 * (long)n)[v] = make_double2(out, out);
+  if (out < 0.0 || out > 1.0) atomicOr(s.status, ERR_LIMITER);
+}
+
+// ---------------------------------------------------------------------------
+// k_assemble with four lanes per node, lane q owning row q of every 4x4
+// block and component q of R: each lane sums its row in the reference's
+// face order, so the results are those of k_assemble.
+template <bool JAC>
+__global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = (tid >> 2) + 1, q = tid & 3;
+  const int qbase = threadIdx.x & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (n > m.nn) return;
+  double r = 0.;
+  double D0 = 0., D1 = 0., D2 = 0., D3 = 0.;
+  const double diag = m.cv_area[n] / (s.dt[n]);
+  if (a.steady_diag) {
+    if (q == 0) D0 = diag;
+    if (q == 1) D1 = diag;
+    if (q == 2) D2 = diag;
+    if (q == 3) D3 = diag;
+  }
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int k = s0; k < s1; k++) {
+    const int sd = m.nsub[k];
+    const int sub = sd >> 1, side = sd & 1;
+    const double f = s.F[4 * (long)sub + q];
+    if (side == 0) r += f;
+    else r -= f;
+    if (JAC) {
+      const double4 J =
+          reinterpret_cast<const double4*>((side ? s.JR : s.JL) + 16 * (long)sub)[q];
+      if (side == 0) {
+        D0 += J.x; D1 += J.y; D2 += J.z; D3 += J.w;
+      } else {
+        D0 -= J.x; D1 -= J.y; D2 -= J.z; D3 -= J.w;
+      }
+    }
+  }
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  for (int k = b0; k < b1; k++) {
+    const int b = m.nbed[k];
+    r += s.Fb[4 * (long)b + q];
+    if (JAC) {
+      const double4 J = reinterpret_cast<const double4*>(s.Jb + 16 * (long)b)[q];
+      D0 += J.x; D1 += J.y; D2 += J.z; D3 += J.w;
+    }
+  }
+  s.R[4 * (long)n + q] = r;
+  s.RHS[4 * (long)n + q] = -(r);
+  const int k0 = m.ia[n], k1 = m.ia[n + 1];
+  for (int k = k0; k < k1; k++) {
+    double4* out = reinterpret_cast<double4*>(s.LHS + 16 * (long)k) + q;
+    if (m.ja[k] == n) {
+      *out = make_double4(D0, D1, D2, D3);
+      continue;
+    }
+    double B0 = 0., B1 = 0., B2 = 0., B3 = 0.;
+    if (JAC) {
+      const int4 cs = m.csr_sub[k];
+      const double* src = cs.z == 0 ? s.JR : s.JL;
+      for (int t = 0; t < 2; t++) {
+        const int sub = t == 0 ? cs.x : cs.y;
+        if (sub < 0) break;
+        const double4 J = reinterpret_cast<const double4*>(src + 16 * (long)sub)[q];
+        if (cs.z == 0) {
+          B0 += J.x; B1 += J.y; B2 += J.z; B3 += J.w;
+        } else {
+          B0 -= J.x; B1 -= J.y; B2 -= J.z; B3 -= J.w;
+        }
+      }
+    }
+    *out = make_double4(B0, B1, B2, B3);
+  }
+  // LU of the diagonal block: every lane factors the whole block
+  double M[16];
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    M[4 * row + 0] = __shfl_sync(qmask, D0, qbase + row);
+    M[4 * row + 1] = __shfl_sync(qmask, D1, qbase + row);
+    M[4 * row + 2] = __shfl_sync(qmask, D2, qbase + row);
+    M[4 * row + 3] = __shfl_sync(qmask, D3, qbase + row);
+  }
+  lu4(M);
+  double o0 = M[0], o1 = M[1], o2 = M[2], o3 = M[3];
+#pragma unroll
+  for (int row = 1; row < 4; row++)
+    if (q == row) {
+      o0 = M[4 * row]; o1 = M[4 * row + 1]; o2 = M[4 * row + 2]; o3 = M[4 * row + 3];
+    }
+  reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] = make_double4(o0, o1, o2, o3);
+}
+
+// ---------------------------------------------------------------------------
 // Per subedge: face states, Roe flux, forward-difference Jacobian
 // (residual.C:112-333, reconstruct.C:181-203, jacobian.C:45-110).
 template <int RECON, bool JAC>

@@ -53,13 +53,13 @@ class Workload:
 
 
 WORKLOADS = {
-    # 512 x 128 O-grid, M 0.8, AoA 1.25, k=2, curved NACA 0012, FP64
+    # the headline workload: 512 x 128 O-grid, M 0.8, AoA 1.25, k=2, curved NACA 0012, FP64
     "ogrid512x128_k2_m080": Workload("ogrid512x128_k2_m080", 512, 128, True, 3, 0.8,
                                      steps_to_converge=4826),
     # a 16x smaller member of the same family, for quick runs
     "ogrid128x32_k2_m080": Workload("ogrid128x32_k2_m080", 128, 32, True, 3, 0.8,
                                     steps_to_converge=691),
-    # 128 x 32 O-grid, M 0.5, k=1, straight walls (a parity case:
+    # the small k=1 case: 128 x 32 O-grid, M 0.5, straight walls (a parity case:
     # with the reference's limiter 2 it settles into a limit cycle)
     "ogrid128x32_k1_m050": Workload("ogrid128x32_k1_m050", 128, 32, False, 1, 0.5),
 }
