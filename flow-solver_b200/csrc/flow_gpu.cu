@@ -13,7 +13,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <stdint.h>
+
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1069,3 +1072,188 @@ long flow_launch_count(flow_ctx* c) { return c ? c->launches : 0; }
 double flow_last_device_ms(flow_ctx* c) { return c ? c->last_ms : 0.; }
 
 }  // extern "C"
+
+// ===========================================================================
+// b - A x RMS of a caller-held BCSR system, with no device allocation.
+//
+// For callers that cannot allocate device memory: host applications that
+// hand all of a GPU's memory to their own arena or caching allocator at
+// start-up (a cudaMalloc behind the arena's back fails once it holds the
+// GPU, or fragments it), and time-step loops that must not take the implicit
+// device-wide synchronisation that cudaMalloc and cudaFree can cause.  The
+// kernels below are the per-sweep residual of flow_linear_solve
+// (k_lin_residual + k_finalize_rms) with their scratch moved into one
+// file-scope __device__ array: the squared residual of each row, the block
+// partial sums, the RMS and an error word.  The partial sums follow
+// k_lin_residual's order, so the RMS is the one flow_linear_solve returns for
+// the same matrix, right-hand side and dQ.
+// ===========================================================================
+namespace flow {
+namespace noalloc {
+constexpr long kRowOff = 0;                                 // [1, nn]: |r_j|^2
+constexpr long kPartOff = (long)FLOW_NOALLOC_MAX_ROWS + 1;  // kRedBlocks block sums
+constexpr long kOutOff = kPartOff + kRedBlocks;             // RMS, then the error word
+constexpr long kWords = ((kOutOff + 2 + 31) / 32) * 32;
+constexpr int kMaxDevices = 64;
+constexpr unsigned long long kBadRowPtr = 1ull, kBadColumn = 2ull;
+}  // namespace noalloc
+}  // namespace flow
+
+// The scratch of flow_linear_residual_noalloc: about 2 MB per device, shared
+// by every call on that device.
+static __device__ __align__(256) double g_noalloc_scratch[flow::noalloc::kWords];
+
+namespace flow {
+namespace noalloc {
+
+// Squared residual of every row; the residual itself is formed exactly as in
+// k_lin_residual.  Row pointers and columns outside the system are reported
+// in the error word and never dereferenced.
+__global__ void __launch_bounds__(kRedThreads)
+    k_rows(const int* ia, const int* ja, const double* lhs, const double* rhs, const double* x,
+           int nn, long nnz, double* scratch) {
+  unsigned long long* err = reinterpret_cast<unsigned long long*>(scratch + kOutOff + 1);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x + 1; j <= nn;
+       j += gridDim.x * blockDim.x) {
+    double r[4] = {rhs[4 * (long)j], rhs[4 * (long)j + 1], rhs[4 * (long)j + 2],
+                   rhs[4 * (long)j + 3]};
+    const int k0 = ia[j], k1 = ia[j + 1];
+    if (k0 < 0 || k1 < k0 || (long)k1 > nnz) {
+      atomicOr(err, kBadRowPtr);
+      scratch[kRowOff + j] = 0.;
+      continue;
+    }
+    for (int k = k0; k < k1; k++) {
+      const int c = ja[k];
+      if (c < 1 || c > nn) {
+        atomicOr(err, kBadColumn);
+        continue;
+      }
+      const double d[4] = {x[4 * (long)c], x[4 * (long)c + 1], x[4 * (long)c + 2],
+                           x[4 * (long)c + 3]};
+      const double* A = lhs + 16 * (long)k;
+#pragma unroll
+      for (int q = 0; q < 4; q++) r[q] -= row_dot(A, q, d);
+    }
+    scratch[kRowOff + j] = (r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+  }
+}
+
+// Block partial sums over the same rows, in the same order, as k_lin_residual.
+__global__ void __launch_bounds__(kRedThreads) k_partials(int nn, double* scratch) {
+  __shared__ double sh[kRedThreads];
+  double acc = 0.;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x + 1; j <= nn;
+       j += gridDim.x * blockDim.x)
+    acc += scratch[kRowOff + j];
+  double tot = block_sum(acc, sh);
+  if (threadIdx.x == 0) scratch[kPartOff + blockIdx.x] = tot;
+}
+
+// The RMS from the partials, as k_finalize_rms forms it.
+__global__ void __launch_bounds__(kRedThreads) k_rms(int nn, double* scratch) {
+  __shared__ double sh[kRedThreads];
+  double v = 0.;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) v += scratch[kPartOff + i];
+  double tot = block_sum(v, sh);
+  if (threadIdx.x == 0) {
+    double rms = tot / (1. * nn);
+    rms = sqrt(rms);
+    scratch[kOutOff] = rms;
+  }
+}
+
+std::mutex g_mu;
+double* g_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on device `dev` (the current device),
+// looked up on the first call for that device.
+double* scratch_for(int dev, int* rc) {
+  std::lock_guard<std::mutex> lock(g_mu);
+  if (dev < 0 || dev >= kMaxDevices) {
+    set_error("flow_linear_residual_noalloc: device ordinal outside 0..63");
+    *rc = FLOW_ERR_ARG;
+    return nullptr;
+  }
+  if (!g_ptr[dev]) {
+    double* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess || !ptr) {
+      set_error((std::string("flow_linear_residual_noalloc: cudaGetSymbolAddress failed: ") +
+                 cudaGetErrorString(e)).c_str());
+      *rc = FLOW_ERR_CUDA;
+      return nullptr;
+    }
+    g_ptr[dev] = ptr;
+  }
+  return g_ptr[dev];
+}
+
+}  // namespace noalloc
+}  // namespace flow
+
+extern "C" int flow_linear_residual_noalloc(const int* ia, const int* ja, const double* lhs,
+                                            const double* rhs, const double* x, int nn,
+                                            long nnz, void* stream, double* rms) {
+  using namespace flow::noalloc;
+  if (!ia || !ja || !lhs || !rhs || !x || !rms) {
+    set_error("flow_linear_residual_noalloc: null argument");
+    return FLOW_ERR_ARG;
+  }
+  if (nn < 1 || nn > FLOW_NOALLOC_MAX_ROWS) {
+    char msg[160];
+    snprintf(msg, sizeof msg,
+             "flow_linear_residual_noalloc: nn = %d rows is outside 1..%d, the rows its static "
+             "scratch holds",
+             nn, FLOW_NOALLOC_MAX_ROWS);
+    set_error(msg);
+    return FLOW_ERR_ARG;
+  }
+  if (nnz < 0 || nnz > 0x7fffffffL) {
+    set_error("flow_linear_residual_noalloc: nnz outside 0..2^31-1");
+    return FLOW_ERR_ARG;
+  }
+  if (((uintptr_t)ia | (uintptr_t)ja) % sizeof(int) ||
+      ((uintptr_t)lhs | (uintptr_t)rhs | (uintptr_t)x) % sizeof(double)) {
+    set_error("flow_linear_residual_noalloc: misaligned device pointer");
+    return FLOW_ERR_ARG;
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return FLOW_ERR_CUDA;
+  }
+  int rc = 0;
+  double* scratch = scratch_for(dev, &rc);
+  if (!scratch) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The error word must start at zero; every other word this call reads, it
+  // writes first.
+  e = cudaMemsetAsync(scratch + kOutOff + 1, 0, sizeof(double), st);
+  if (e == cudaSuccess) {
+    k_rows<<<flow::kRedBlocks, flow::kRedThreads, 0, st>>>(ia, ja, lhs, rhs, x, nn, nnz,
+                                                           scratch);
+    k_partials<<<flow::kRedBlocks, flow::kRedThreads, 0, st>>>(nn, scratch);
+    k_rms<<<1, flow::kRedThreads, 0, st>>>(nn, scratch);
+    e = cudaGetLastError();
+  }
+  double out[2] = {0., 0.};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, scratch + kOutOff, sizeof out,
+                                            cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    set_error((std::string("flow_linear_residual_noalloc: ") + cudaGetErrorString(e)).c_str());
+    return FLOW_ERR_CUDA;
+  }
+  unsigned long long err = 0;
+  memcpy(&err, &out[1], sizeof err);
+  if (err) {
+    set_error(err & kBadRowPtr
+                  ? "flow_linear_residual_noalloc: a row pointer ia[j] lies outside 0..nnz"
+                  : "flow_linear_residual_noalloc: a column index ja[k] lies outside 1..nn");
+    return FLOW_ERR_ARG;
+  }
+  *rms = out[0];
+  return FLOW_OK;
+}

@@ -23,11 +23,12 @@ ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
-           "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct", "flow_residuals", "flow_linear_solve",
-           "flow_body_forces", "flow_get", "flow_size", "flow_set_sweep_mode", "flow_save_state",
-           "flow_restore_state", "flow_set_timing", "flow_kernel_times", "flow_stream",
-           "flow_status",
-           "flow_clear_status", "flow_last_error", "flow_launch_count", "flow_last_device_ms")
+           "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
+           "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
+           "flow_set_sweep_mode", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
+           "flow_last_error", "flow_launch_count", "flow_last_device_ms",
+           "flow_linear_residual_noalloc")
 
 
 class FlowParamsC(C.Structure):
@@ -106,8 +107,24 @@ def load():
     L.flow_launch_count.argtypes = [vp]
     L.flow_last_device_ms.restype = C.c_double
     L.flow_last_device_ms.argtypes = [vp]
+    L.flow_linear_residual_noalloc.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_long, vp, DP]
     _lib = L
     return L
+
+
+def linear_residual_noalloc(ia: int, ja: int, lhs: int, rhs: int, x: int, nn: int, nnz: int,
+                            stream: int | None = None) -> float:
+    """b - A x RMS of a BCSR system in caller-held device memory (device
+    pointers as ints), through flow_linear_residual_noalloc: no device
+    allocation, static scratch of FLOW_NOALLOC_MAX_ROWS rows."""
+    L = load()
+    r = C.c_double()
+    _check(L.flow_linear_residual_noalloc(ia, ja, lhs, rhs, x, int(nn), int(nnz), stream,
+                                          C.byref(r)), "flow_linear_residual_noalloc")
+    return r.value
+
+
+NOALLOC_MAX_ROWS = 262144
 
 
 def params_struct(fp) -> FlowParamsC:

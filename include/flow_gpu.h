@@ -226,6 +226,40 @@ long flow_launch_count(flow_ctx *ctx);
 /* Device time (ms) of the last flow_run / flow_solve call, CUDA events. */
 double flow_last_device_ms(flow_ctx *ctx);
 
+/* ---- b - A x RMS with no device allocation ------------------------------
+ * No counterpart in the reference.  It computes the b - A x RMS that
+ * flow_linear_solve returns (linear_algebra.C:348-387) for a 4x4-block BCSR
+ * system that sits in the caller's own device memory, and allocates
+ * nothing: no cudaMalloc or cudaFree, no allocating library routine.  It is
+ * for callers that cannot allocate device memory: host applications that
+ * hand all of a GPU's memory to their own arena or caching allocator at
+ * start-up (a cudaMalloc behind the arena's back fails once the arena holds
+ * the GPU, or fragments it), and time-step loops that must not take the
+ * implicit device-wide synchronisation cudaMalloc and cudaFree can cause.
+ *
+ * Layout (the reference's SYS_MEM): row j = 1..nn owns blocks
+ * ia[j] .. ia[j+1]-1, ja[k] is the 1-based column of block k, lhs holds 16
+ * doubles per block (row-major 4x4), rhs and x hold (nn+1)*4 doubles with
+ * row 0 unused.  All five are device pointers on the current device.  The
+ * work runs on `stream` (NULL: the legacy default stream); the call waits
+ * for it and stores the RMS in the host double *rms.  A row pointer or
+ * column outside the system is reported as FLOW_ERR_ARG.
+ *
+ * Scratch: one file-scope __device__ array per device (about 2 MB), sized
+ * for FLOW_NOALLOC_MAX_ROWS rows; a larger nn is rejected with FLOW_ERR_ARG
+ * and a message in flow_last_error().  The first call on each device does a
+ * one-time set-up (it looks up the array's device address, which also loads
+ * this library's device code on that device): make that first call before
+ * any stream capture starts.  Every call on a device shares the array, which
+ * keeps the last call's contents; each call clears the one word that must
+ * start at zero.  Calls whose GPU work overlaps (several host threads on
+ * different streams) race on the array and return wrong results: serialise
+ * them. */
+#define FLOW_NOALLOC_MAX_ROWS 262144
+int flow_linear_residual_noalloc(const int *ia, const int *ja, const double *lhs,
+                                 const double *rhs, const double *x, int nn, long nnz,
+                                 void *stream, double *rms);
+
 #ifdef __cplusplus
 }
 #endif
