@@ -30,6 +30,7 @@ pseudo-time steps), rank 0 only.
 """
 from __future__ import annotations
 
+import dataclasses
 import argparse
 import json
 import os
@@ -303,9 +304,12 @@ def run_profile(args):
     from flowgpu import capi, workloads
     from flowgpu.prep import Mesh
     wl = workloads.get(args.workload)
+    if args.subits:
+        wl = dataclasses.replace(wl, subits=args.subits)
     mesh = Mesh.from_case(wl.write(), order=wl.order)
     solver = capi.Solver.from_mesh(mesh, wl.params(), device=0)
     solver.set_sweep_mode(args.sweep_mode)
+    solver.set_precision(args.precision)
     solver.set_state(mesh.initial_state(wl.params()))
     rh, dh = solver.run(1, args.profile_steps)
     out = {"workload": wl.name, "steps": args.profile_steps,
@@ -397,6 +401,10 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many pseudo-time steps of one solve (for ncu captures)")
     ap.add_argument("--sweep-mode", type=int, default=0, help="0 grid-wide, 1 one-CTA ordered sweep")
+    ap.add_argument("--precision", type=int, default=0,
+                    help="with --profile-steps: 0 FP64 drop-in, 1 FP32 multicolour sweeps")
+    ap.add_argument("--subits", type=int, default=0,
+                    help="with --profile-steps: Gauss-Seidel sweeps per step (0: the workload's)")
     args = ap.parse_args()
     from flowgpu import workloads
     args.workload = args.workload or workloads.DEFAULT

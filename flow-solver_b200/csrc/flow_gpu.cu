@@ -87,6 +87,12 @@ struct flow_ctx {
   bool sweep_cta_ok = false;
   double* d_hist = nullptr;  // 2 x hist_cap device history of (dq, r_rho)
   int hist_cap = 0;
+  // precision form (flow_set_precision): 0 FP64 reference order, 1 FP32
+  // blocks with multicolour sweeps; tables built on first use
+  int precision = 0;
+  MixedTables mt{};
+  std::vector<int> h_color_ptr;
+  std::vector<int> h_ia, h_ja;  // host copy of the block pattern
 };
 
 namespace {
@@ -251,8 +257,13 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   {
     Timed t(c, 3);
     int nbn = grid_blocks(4 * c->nn, 128);
-    if (jac) k_assemble4<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
-    else k_assemble4<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a);
+    if (c->precision == 1) {
+      if (jac) k_assemble4<true, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
+      else k_assemble4<false, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
+    } else {
+      if (jac) k_assemble4<true, false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
+      else k_assemble4<false, false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
+    }
     rc |= launch_check(c);
   }
   return rc;
@@ -260,7 +271,31 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
 
 // linear_solve (linear_algebra.C:122-401): subits sweeps, alternating
 // forward/backward, each followed by the b-Ax RMS that may stop the loop.
+// Precision form: p->subits multicolour FP32 sweeps from dQ = 0, colours
+// ascending on forward sweeps and descending on backward ones; no b-Ax RMS.
+int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
+  int rc = 0;
+  cudaMemsetAsync(c->s.dQ, 0, sizeof(double) * 4 * (c->nn + 1), c->stream);
+  cudaMemsetAsync(c->mt.dq32, 0, sizeof(float) * 4 * (c->nn + 1), c->stream);
+  const int nc = c->mt.ncolors;
+  for (int it = 0; it < p->subits; it++) {
+    Timed t(c, 4);
+    const bool last = it == p->subits - 1;
+    for (int ci = 0; ci < nc; ci++) {
+      const int col = (it % 2 == 0) ? ci : nc - 1 - ci;
+      const int p0 = c->h_color_ptr[col], p1 = c->h_color_ptr[col + 1];
+      const int nb = grid_blocks(4 * (p1 - p0), 128);
+      if (nb == 0) continue;
+      if (last) k_sweep_color32<true><<<nb, 128, 0, c->stream>>>(c->s, c->mt, p0, p1);
+      else k_sweep_color32<false><<<nb, 128, 0, c->stream>>>(c->s, c->mt, p0, p1);
+      rc |= launch_check(c);
+    }
+  }
+  return rc;
+}
+
 int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
+  if (c->precision == 1) return launch_linear_solve_mixed(c, p);
   int rc = 0;
   cudaMemsetAsync(c->s.dQ, 0, sizeof(double) * 4 * (c->nn + 1), c->stream);
   cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream);
@@ -353,6 +388,67 @@ int read_status(flow_ctx* c) {
   }
   harvest(c);
   return st;
+}
+
+// Colour the block pattern greedily in row order (each row takes the
+// smallest colour none of its earlier neighbours holds) and lay out the FP32
+// tables of the precision form in colour order.
+int build_mixed_tables(flow_ctx* c) {
+  if (c->mt.lhs32) return 0;
+  const int nn = c->nn;
+  const std::vector<int>& ia = c->h_ia;
+  const std::vector<int>& ja = c->h_ja;
+  std::vector<int> color(nn + 1, 0);
+  int ncol = 0;
+  std::vector<char> used;
+  for (int j = 1; j <= nn; j++) {
+    if (ia[j + 1] <= ia[j] || ja[ia[j + 1] - 1] != j) {
+      set_error("precision form: a row's diagonal block is not its last block");
+      return FLOW_ERR_ARG;
+    }
+    used.assign(ncol + 1, 0);
+    for (int k = ia[j]; k < ia[j + 1]; k++)
+      if (ja[k] < j) used[color[ja[k]]] = 1;
+    int col = 0;
+    while (used[col]) col++;
+    color[j] = col;
+    ncol = std::max(ncol, col + 1);
+  }
+  std::vector<int> cptr(ncol + 1, 0), rows(nn), pos(nn + 1, 0), optr(nn + 1, 0), ocol;
+  for (int j = 1; j <= nn; j++) cptr[color[j] + 1]++;
+  for (int q = 0; q < ncol; q++) cptr[q + 1] += cptr[q];
+  std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+  for (int j = 1; j <= nn; j++) {
+    int pp = fill[color[j]]++;
+    rows[pp] = j;
+    pos[j] = pp;
+  }
+  ocol.reserve(ja.size());
+  for (int pp = 0; pp < nn; pp++) {
+    int j = rows[pp];
+    optr[pp] = (int)ocol.size();
+    for (int k = ia[j]; k < ia[j + 1] - 1; k++) ocol.push_back(ja[k]);
+  }
+  optr[nn] = (int)ocol.size();
+  MixedTables& mt = c->mt;
+  mt.ncolors = ncol;
+  mt.color_ptr = upload_vec(c, cptr);
+  mt.rows = upload_vec(c, rows);
+  mt.pos = upload_vec(c, pos);
+  mt.offd_ptr = upload_vec(c, optr);
+  mt.offd_col = upload_vec(c, ocol);
+  mt.lu32 = c->buf.alloc<float>((size_t)16 * nn);
+  mt.dq32 = c->buf.alloc<float>((size_t)4 * (nn + 1));
+  mt.lhs32 = c->buf.alloc<float>((size_t)16 * std::max<size_t>(ocol.size(), 1));
+  if (!mt.color_ptr || !mt.rows || !mt.pos || !mt.offd_ptr || !mt.offd_col || !mt.lu32 ||
+      !mt.dq32 || !mt.lhs32) {
+    set_error("precision form: device allocation failed");
+    mt.lhs32 = nullptr;
+    return FLOW_ERR_CUDA;
+  }
+  cudaMemset(mt.dq32, 0, sizeof(float) * 4 * (nn + 1));
+  c->h_color_ptr = cptr;
+  return 0;
 }
 
 int ensure_hist(flow_ctx* c, int n) {
@@ -524,6 +620,8 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   {
     std::vector<int> ia(g->ia, g->ia + nn + 2), iau(g->iau, g->iau + nn + 1), ja(g->ja, g->ja + nnz);
     UP(ia, ia); UP(iau, iau); UP(ja, ja);
+    c->h_ia = ia;
+    c->h_ja = ja;
     std::vector<double> x(g->x, g->x + (size_t)(nn + ng + 1) * 2), cv(g->cv_area, g->cv_area + nn + 1);
     UP(x, x); UP(cv_area, cv);
     std::vector<int> no(g->node_order, g->node_order + nn + ng + 1);
@@ -695,6 +793,21 @@ int flow_set_sweep_mode(flow_ctx* c, int mode) {
     return FLOW_ERR_ARG;
   }
   c->sweep_mode = mode;
+  return 0;
+}
+
+int flow_set_precision(flow_ctx* c, int mode) {
+  if (!c || !c->ok || (mode != 0 && mode != 1)) {
+    set_error("flow_set_precision: null context or mode not 0/1");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  if (mode == 1) {
+    cudaStreamSynchronize(c->stream);
+    int rc = build_mixed_tables(c);
+    if (rc) return rc;
+  }
+  c->precision = mode;
   return 0;
 }
 
@@ -917,7 +1030,8 @@ int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
   int st = read_status(c);
   if (rms) {
     double v = 10.;
-    if (p->subits > 0) cudaMemcpy(&v, c->s.scalars, sizeof(double), cudaMemcpyDeviceToHost);
+    if (c->precision == 1) v = -1.;  // the precision form forms no b-Ax RMS
+    else if (p->subits > 0) cudaMemcpy(&v, c->s.scalars, sizeof(double), cudaMemcpyDeviceToHost);
     *rms = v;
   }
   return st;

@@ -401,8 +401,9 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
 // k_assemble with four lanes per node, lane q owning row q of every 4x4
 // block and component q of R: each lane sums its row in the reference's
 // face order, so the results are those of k_assemble.
-template <bool JAC>
-__global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a) {
+template <bool JAC, bool MIXED>
+__global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a,
+                                                   MixedTables mt) {
   if (*s.stop) return;  // the run has converged
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (tid >> 2) + 1, q = tid & 3;
@@ -447,10 +448,14 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
   s.R[4 * (long)n + q] = r;
   s.RHS[4 * (long)n + q] = -(r);
   const int k0 = m.ia[n], k1 = m.ia[n + 1];
+  // precision form: this row's off-diagonal blocks in colour order (the
+  // diagonal block is the row's last, so block k is off-diagonal k - k0)
+  const int mpos = MIXED ? mt.pos[n] : 0;
+  const int moff = MIXED ? mt.offd_ptr[mpos] : 0;
   for (int k = k0; k < k1; k++) {
     double4* out = reinterpret_cast<double4*>(s.LHS + 16 * (long)k) + q;
     if (m.ja[k] == n) {
-      *out = make_double4(D0, D1, D2, D3);
+      if (!MIXED) *out = make_double4(D0, D1, D2, D3);
       continue;
     }
     double B0 = 0., B1 = 0., B2 = 0., B3 = 0.;
@@ -468,7 +473,12 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
         }
       }
     }
-    *out = make_double4(B0, B1, B2, B3);
+    if (MIXED)
+      reinterpret_cast<float4*>(mt.lhs32 + 16 * (long)(moff + (k - k0)))[q] =
+          make_float4(__double2float_rn(B0), __double2float_rn(B1), __double2float_rn(B2),
+                      __double2float_rn(B3));
+    else
+      *out = make_double4(B0, B1, B2, B3);
   }
   // LU of the diagonal block: every lane factors the whole block
   double M[16];
@@ -486,7 +496,20 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
     if (q == row) {
       o0 = M[4 * row]; o1 = M[4 * row + 1]; o2 = M[4 * row + 2]; o3 = M[4 * row + 3];
     }
-  reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] = make_double4(o0, o1, o2, o3);
+  if (MIXED) {
+    // FP32 factors with reciprocal pivots (1/u_qq in FP64, then rounded)
+    float f[4] = {__double2float_rn(o0), __double2float_rn(o1), __double2float_rn(o2),
+                  __double2float_rn(o3)};
+    const double piv = q == 0 ? o0 : q == 1 ? o1 : q == 2 ? o2 : o3;
+    const float rp = __double2float_rn(1.0 / piv);
+    if (q == 0) f[0] = rp;
+    if (q == 1) f[1] = rp;
+    if (q == 2) f[2] = rp;
+    if (q == 3) f[3] = rp;
+    reinterpret_cast<float4*>(mt.lu32 + 16 * (long)mpos)[q] = make_float4(f[0], f[1], f[2], f[3]);
+  } else {
+    reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] = make_double4(o0, o1, o2, o3);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -911,6 +934,74 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s,
     }
     __syncwarp();
   }
+}
+
+// Precision form: one colour of a multicolour block Gauss-Seidel sweep in
+// FP32.  Four lanes per row (lane q owns matrix row q): each lane forms
+// b_q - sum_k A_k[q,:] . dQ[col_k] over the row's off-diagonal blocks in
+// block order, with one multiply and three fused multiply-adds per block;
+// lane 0 then solves with the FP32 LU factors (reciprocal pivots).  Rows of
+// one colour share no block, so they run in parallel and in any order.  The
+// last sweep also writes the FP64 dQ the update reads.
+template <bool LAST>
+__global__ void __launch_bounds__(128) k_sweep_color32(DevState s, MixedTables mt, int p0,
+                                                       int p1) {
+  if (*s.stop) return;  // the run has converged
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pp = p0 + (tid >> 2), q = tid & 3;
+  const int qbase = threadIdx.x & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (pp >= p1) return;  // whole quads leave together
+  const int n = mt.rows[pp];
+  float acc = __double2float_rn(s.RHS[4 * (long)n + q]);
+  const int b0 = mt.offd_ptr[pp], b1 = mt.offd_ptr[pp + 1];
+  const float4* A = reinterpret_cast<const float4*>(mt.lhs32);
+  const float4* X = reinterpret_cast<const float4*>(mt.dq32);
+  int b = b0;
+  for (; b + 1 < b1; b += 2) {
+    const int c0 = mt.offd_col[b], c1 = mt.offd_col[b + 1];
+    const float4 a0 = A[4 * (long)b + q], a1 = A[4 * (long)(b + 1) + q];
+    const float4 d0 = X[c0], d1 = X[c1];
+    float t0 = __fmul_rn(a0.x, d0.x);
+    t0 = __fmaf_rn(a0.y, d0.y, t0);
+    t0 = __fmaf_rn(a0.z, d0.z, t0);
+    t0 = __fmaf_rn(a0.w, d0.w, t0);
+    float t1 = __fmul_rn(a1.x, d1.x);
+    t1 = __fmaf_rn(a1.y, d1.y, t1);
+    t1 = __fmaf_rn(a1.z, d1.z, t1);
+    t1 = __fmaf_rn(a1.w, d1.w, t1);
+    acc = __fsub_rn(acc, t0);
+    acc = __fsub_rn(acc, t1);
+  }
+  if (b < b1) {
+    const int c0 = mt.offd_col[b];
+    const float4 a0 = A[4 * (long)b + q];
+    const float4 d0 = X[c0];
+    float t0 = __fmul_rn(a0.x, d0.x);
+    t0 = __fmaf_rn(a0.y, d0.y, t0);
+    t0 = __fmaf_rn(a0.z, d0.z, t0);
+    t0 = __fmaf_rn(a0.w, d0.w, t0);
+    acc = __fsub_rn(acc, t0);
+  }
+  const float r0 = __shfl_sync(qmask, acc, qbase);
+  const float r1 = __shfl_sync(qmask, acc, qbase + 1);
+  const float r2 = __shfl_sync(qmask, acc, qbase + 2);
+  const float r3 = __shfl_sync(qmask, acc, qbase + 3);
+  if (q != 0) return;
+  const float4* L = reinterpret_cast<const float4*>(mt.lu32) + 4 * (long)pp;
+  const float4 M0 = L[0], M1 = L[1], M2 = L[2], M3 = L[3];
+  const float y0 = r0;
+  const float y1 = __fmaf_rn(-M1.x, y0, r1);
+  const float y2 = __fmaf_rn(-M2.y, y1, __fmaf_rn(-M2.x, y0, r2));
+  const float y3 = __fmaf_rn(-M3.z, y2, __fmaf_rn(-M3.y, y1, __fmaf_rn(-M3.x, y0, r3)));
+  const float x3 = __fmul_rn(y3, M3.w);
+  const float x2 = __fmul_rn(__fmaf_rn(-M2.w, x3, y2), M2.z);
+  const float x1 = __fmul_rn(__fmaf_rn(-M1.w, x3, __fmaf_rn(-M1.z, x2, y1)), M1.y);
+  const float x0 =
+      __fmul_rn(__fmaf_rn(-M0.w, x3, __fmaf_rn(-M0.z, x2, __fmaf_rn(-M0.y, x1, y0))), M0.x);
+  reinterpret_cast<float4*>(mt.dq32)[n] = make_float4(x0, x1, x2, x3);
+  if (LAST)
+    reinterpret_cast<double4*>(s.dQ)[n] = make_double4(x0, x1, x2, x3);
 }
 
 // Before an ordered sweep: fill its result buffer with the not-ready

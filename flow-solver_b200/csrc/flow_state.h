@@ -61,6 +61,20 @@ struct DevMesh {
   const double* svd_S;     // 5 per node
 };
 
+// Precision form: FP32 off-diagonal blocks and LU factors laid out in
+// colour order (rows of one colour contiguous), for the multicolour sweeps.
+struct MixedTables {
+  int ncolors;
+  const int* color_ptr;   // ncolors+1: first position of each colour
+  const int* rows;        // nn: row at each position (colour-sorted, ascending)
+  const int* pos;         // nn+1: position of each row
+  const int* offd_ptr;    // nn+1: first off-diagonal block of each position
+  const int* offd_col;    // column (row index) of each off-diagonal block
+  float* lhs32;           // 16 floats per off-diagonal block, row-major
+  float* lu32;            // 16 floats per position: LU factors, reciprocal pivots
+  float* dq32;            // 4 floats per row (1..nn), the sweeps' iterate
+};
+
 struct DevState {
   double* Q;
   double* nQ;

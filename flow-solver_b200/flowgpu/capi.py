@@ -25,7 +25,7 @@ ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
-           "flow_set_sweep_mode", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_set_sweep_mode", "flow_set_precision", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
            "flow_linear_residual_noalloc")
@@ -94,6 +94,7 @@ def load():
     L.flow_size.restype = C.c_long
     L.flow_size.argtypes = [vp, C.c_char_p]
     L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
+    L.flow_set_precision.argtypes = [vp, C.c_int]
     L.flow_save_state.argtypes = [vp]
     L.flow_restore_state.argtypes = [vp]
     L.flow_set_timing.argtypes = [vp, C.c_int]
@@ -296,6 +297,10 @@ class Solver:
         out = np.zeros(n)
         _check(self.L.flow_get(self.ctx, name.encode(), out.ctypes.data_as(DP), n), f"get {name}")
         return out
+
+    def set_precision(self, mode: int):
+        """0: FP64 reference-order drop-in; 1: FP32 blocks, multicolour sweeps."""
+        _check(self.L.flow_set_precision(self.ctx, int(mode)), "flow_set_precision")
 
     def set_sweep_mode(self, mode: int):
         _check(self.L.flow_set_sweep_mode(self.ctx, int(mode)), "flow_set_sweep_mode")

@@ -198,6 +198,19 @@ long flow_size(flow_ctx *ctx, const char *name);
  * the matrix bandwidth exceeds its dQ window). */
 int flow_set_sweep_mode(flow_ctx *ctx, int mode);
 
+/* Precision form (no counterpart in the reference; its defect-correction
+ * preconditioner): mode 0 (default) is the FP64 drop-in, bit-identical to
+ * the reference.  Mode 1 keeps the residual, geometry, limiter, fluxes,
+ * face Jacobians and the update in FP64, but rounds the assembled
+ * off-diagonal blocks and the LU factors of the diagonal blocks to FP32
+ * and runs p->subits multicolour block Gauss-Seidel sweeps in FP32 (greedy
+ * colouring of the block pattern in row order; forward sweeps take the
+ * colours ascending, backward sweeps descending).  The converged state is
+ * that of mode 0 (same residual); the iterates differ.  In mode 1 the FP64
+ * LHS is not formed (flow_get "LHS" is stale) and flow_linear_solve reports
+ * rms = -1.  The first switch to mode 1 builds the colour tables. */
+int flow_set_precision(flow_ctx *ctx, int mode);
+
 /* Device snapshot of the solution state (Q, nQ, pQ and the boundary normals
  * the k=2 pass rewrites): flow_save_state keeps a copy on the device,
  * flow_restore_state puts it back (pre-emption / restart without host

@@ -814,7 +814,106 @@ void orc_body_forces(orc_grid *g, const orc_params *p, double *F)
 /* ------------------------------------------------------------------ */
 /* solve.C:44-933 (steady implicit, orders 1 and 3, limiter 2)          */
 /* ------------------------------------------------------------------ */
+/* ------------------------------------------------------------------ */
+/* Precision form: multicolour FP32 block Gauss-Seidel (no reference     */
+/* counterpart; the FP64 sweep it replaces is linear_algebra.C:178-344)  */
+/* ------------------------------------------------------------------ */
+int orc_greedy_colors(const orc_grid *g, int *color)
+{
+  int nn = g->nn, ncol = 0;
+  unsigned char used[256];
+  for (int j = 1; j <= nn; j++) {
+    memset(used, 0, sizeof(used));
+    for (int k = g->ia[j]; k < g->ia[j + 1]; k++) {
+      int c = g->ja[k];
+      if (c < j) used[color[c]] = 1;
+    }
+    int col = 0;
+    while (col < 255 && used[col]) col++;
+    color[j] = col;
+    if (col + 1 > ncol) ncol = col + 1;
+  }
+  return ncol;
+}
+
+static void gs_row_mixed(const orc_grid *g, const float *A32, const float *lu32, float *dq32,
+                         int j)
+{
+  float b[4];
+  for (int r = 0; r < 4; r++) b[r] = (float)g->RHS[j * NV + r];
+  for (int k = g->ia[j]; k < g->ia[j + 1]; k++) {
+    int c = g->ja[k];
+    if (c == j) continue;
+    const float *a = &A32[(long)k * 16];
+    const float *d = &dq32[c * NV];
+    for (int r = 0; r < 4; r++) {
+      float t = a[r * 4] * d[0];
+      t = fmaf(a[r * 4 + 1], d[1], t);
+      t = fmaf(a[r * 4 + 2], d[2], t);
+      t = fmaf(a[r * 4 + 3], d[3], t);
+      b[r] = b[r] - t;
+    }
+  }
+  const float *M = &lu32[j * 16];  /* LU factors, reciprocal pivots on the diagonal */
+  float y0 = b[0];
+  float y1 = fmaf(-M[4], y0, b[1]);
+  float y2 = fmaf(-M[9], y1, fmaf(-M[8], y0, b[2]));
+  float y3 = fmaf(-M[14], y2, fmaf(-M[13], y1, fmaf(-M[12], y0, b[3])));
+  float x3 = y3 * M[15];
+  float x2 = fmaf(-M[11], x3, y2) * M[10];
+  float x1 = fmaf(-M[7], x3, fmaf(-M[6], x2, y1)) * M[5];
+  float x0 = fmaf(-M[3], x3, fmaf(-M[2], x2, fmaf(-M[1], x1, y0))) * M[0];
+  dq32[j * NV] = x0;
+  dq32[j * NV + 1] = x1;
+  dq32[j * NV + 2] = x2;
+  dq32[j * NV + 3] = x3;
+}
+
+void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, int ncolors)
+{
+  int nn = g->nn;
+  long nnz = g->ia[nn + 1];
+  float *A32 = (float *)malloc(sizeof(float) * 16 * (nnz > 0 ? nnz : 1));
+  float *lu32 = (float *)malloc(sizeof(float) * 16 * (nn + 1));
+  float *dq32 = (float *)calloc((size_t)(nn + 1) * NV, sizeof(float));
+  for (long k = 0; k < 16 * nnz; k++) A32[k] = (float)g->LHS[k];
+  for (int j = 1; j <= nn; j++) {
+    double M[16];
+    memcpy(M, &g->LHS[(long)g->iau[j] * 16], sizeof(M));
+    lu4(M);
+    for (int q = 0; q < 16; q++) lu32[j * 16 + q] = (float)M[q];
+    for (int q = 0; q < 4; q++) lu32[j * 16 + 5 * q] = (float)(1.0 / M[5 * q]);
+  }
+  for (int it = 0; it < p->subits; it++) {
+    for (int ci = 0; ci < ncolors; ci++) {
+      int col = (it % 2 == 0) ? ci : ncolors - 1 - ci;
+      for (int j = 1; j <= nn; j++)
+        if (color[j] == col) gs_row_mixed(g, A32, lu32, dq32, j);
+    }
+  }
+  for (int j = 1; j <= nn; j++)
+    for (int r = 0; r < NV; r++) g->dQ[j * NV + r] = (double)dq32[j * NV + r];
+  free(A32);
+  free(lu32);
+  free(dq32);
+}
+
+static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm,
+                      const int *color, int ncolors);
+
 int orc_solve(orc_grid *g, const orc_params *p, int ts, double *dqnorm)
+{
+  return solve_impl(g, p, ts, dqnorm, NULL, 0);
+}
+
+int orc_solve_mixed(orc_grid *g, const orc_params *p, int ts, double *dqnorm, const int *color,
+                    int ncolors)
+{
+  return solve_impl(g, p, ts, dqnorm, color, ncolors);
+}
+
+static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm,
+                      const int *color, int ncolors)
 {
   int nn = g->nn, rc;
   double dql2 = 0.;
@@ -850,7 +949,10 @@ int orc_solve(orc_grid *g, const orc_params *p, int ts, double *dqnorm)
     if (p->tacc != 0 || p->unsteady != 0) return 40;
     for (int i = 1; i <= nn; i++)
       for (int j = 0; j < NV; j++) g->RHS[i * NV + j] = -(g->R[i * NV + j]);
-    orc_linear_solve(g, p);
+    if (color)
+      orc_linear_solve_mixed(g, p, color, ncolors);
+    else
+      orc_linear_solve(g, p);
     dql2 = 0.;
     for (int i = 1; i <= nn; i++)
       for (int j = 0; j < NV; j++) dql2 += (g->dQ[i * NV + j] * g->dQ[i * NV + j]);

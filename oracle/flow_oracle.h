@@ -76,6 +76,25 @@ void orc_body_forces(orc_grid *g, const orc_params *p, double *forces);
  * Returns ||dQ||_2 in *dq, 0 on success. */
 int orc_solve(orc_grid *g, const orc_params *p, int ts, double *dq);
 
+/* ---- precision form: FP32 Jacobian blocks, multicolour block GS ----
+ * Not in the reference: the defect-correction preconditioner of the
+ * precision form.  The residual, geometry and update stay FP64; the linear
+ * solve rounds the off-diagonal blocks and the LU factors of each diagonal
+ * block (factored in FP64 with the reference's lu, linear_algebra.C:571-590)
+ * to FP32, keeps reciprocal pivots, and runs p->subits sweeps of block
+ * Gauss-Seidel in colour order (forward: colours ascending, backward:
+ * descending) with FP32 arithmetic in a fixed fused-multiply-add order.
+ * Rows of one colour share no block, so their order inside a colour does not
+ * matter and the result is unique. */
+/* Greedy distance-1 colouring of the block pattern in row order 1..nn:
+ * each row takes the smallest colour no earlier neighbour holds.
+ * color[1..nn] receives the colours; returns the number of colours. */
+int orc_greedy_colors(const orc_grid *g, int *color);
+void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, int ncolors);
+/* orc_solve with orc_linear_solve_mixed in place of orc_linear_solve. */
+int orc_solve_mixed(orc_grid *g, const orc_params *p, int ts, double *dq, const int *color,
+                    int ncolors);
+
 /* Building blocks, exposed for unit checks. */
 int orc_roe_flux(double nx, double ny, double len, double gamma, const double *ql,
                  const double *qr, double *flux);

@@ -64,6 +64,9 @@ def lib():
         L.orc_linear_solve.restype = C.c_double
         L.orc_body_forces.argtypes = [gp, pp, DP]
         L.orc_solve.argtypes = [gp, pp, C.c_int, DP]
+        L.orc_greedy_colors.argtypes = [gp, IP]
+        L.orc_linear_solve_mixed.argtypes = [gp, pp, IP, C.c_int]
+        L.orc_solve_mixed.argtypes = [gp, pp, C.c_int, DP, IP, C.c_int]
         L.orc_roe_flux.argtypes = [C.c_double] * 4 + [DP, DP, DP]
         L.orc_curved_normal.argtypes = [C.c_int, DP, DP, DP]
         _lib = L
@@ -174,6 +177,29 @@ class OracleGrid:
 
     def linear_solve(self, p):
         return self.L.orc_linear_solve(C.byref(self.g), C.byref(p))
+
+    # ---- precision form (FP32 blocks, multicolour sweeps) ----
+    def colors(self):
+        """Greedy colouring of the block pattern: (color[0..nn], ncolors)."""
+        if getattr(self, "_colors", None) is None:
+            col = np.zeros(self.sizes["nn"] + 1, dtype=np.int32)
+            nc = self.L.orc_greedy_colors(C.byref(self.g), col.ctypes.data_as(IP))
+            self._colors = (col, nc)
+        return self._colors
+
+    def linear_solve_mixed(self, p):
+        col, nc = self.colors()
+        self.L.orc_linear_solve_mixed(C.byref(self.g), C.byref(p), col.ctypes.data_as(IP), nc)
+
+    def solve_mixed(self, p: OrcParams, ts: int) -> float:
+        col, nc = self.colors()
+        self.g.citer = ts
+        dq = C.c_double()
+        rc = self.L.orc_solve_mixed(C.byref(self.g), C.byref(p), ts, C.byref(dq),
+                                    col.ctypes.data_as(IP), nc)
+        if rc:
+            raise RuntimeError(f"oracle solve failed with code {rc}")
+        return dq.value
 
 
 def roe_flux(nx, ny, length, gamma, ql, qr):
