@@ -115,6 +115,107 @@ __device__ __forceinline__ void roe_flux(double nx, double ny, double len, doubl
   for (int i = 0; i < 4; i++) flux[i] = 0.5 * (FL[i] + FR[i] - diss[i]);
 }
 
+// roe_flux split for the forward-difference Jacobian: the quantities of one
+// face state (primitive variables, h = (E+p)/rho, its physical flux) and of
+// the Roe average's density weight are formed once and reused by the
+// evaluations that do not perturb them.  Each piece is the same expression
+// on the same operands as in euler_flux / roe_matrix / roe_flux, so
+// roe_core(...) returns the bits roe_flux(...) returns.
+struct RoeSide {
+  double rho, u, v, E, p, h;
+  double F[4];
+};
+
+__device__ __forceinline__ void roe_side(const double* q, double nx, double ny, double len,
+                                         double gamma, RoeSide& S) {
+  S.rho = q[0];
+  S.u = q[1] / q[0];
+  S.v = q[2] / q[0];
+  S.E = q[3];
+  S.p = (gamma - 1.0) * (S.E - 0.5 * S.rho * (S.u * S.u + S.v * S.v));
+  const double H = S.E + S.p;
+  S.h = H / S.rho;
+  const double theta = S.u * nx + S.v * ny;
+  S.F[0] = S.rho * theta * len;
+  S.F[1] = S.rho * S.u * theta * len + S.p * nx * len;
+  S.F[2] = S.rho * S.v * theta * len + S.p * ny * len;
+  S.F[3] = theta * (S.E + S.p) * len;
+}
+
+// bg = rhobar / (rhoL + rhobar), rhobar = sqrt(rhoL * rhoR)  (flux.C:371-372)
+__device__ __forceinline__ double roe_weight(double rhoL, double rhoR) {
+  const double rhobar = sqrt(rhoL * rhoR);
+  return rhobar / (rhoL + rhobar);
+}
+
+// ogm1 = 1 / (gamma - 1), a per-run constant of the eigenvector matrix.
+__device__ __forceinline__ void roe_core(double nx, double ny, double len, double gamma,
+                                         double ogm1, const double* ql, const double* qr,
+                                         const RoeSide& L, const RoeSide& R, double bg,
+                                         double* flux) {
+  const double ubar = L.u + bg * (R.u - L.u);
+  const double vbar = L.v + bg * (R.v - L.v);
+  const double hbar = L.h + bg * (R.h - L.h);
+  const double thetabar = ubar * nx + vbar * ny;
+  const double V2bar = (ubar * ubar + vbar * vbar);
+  const double cbar = sqrt((gamma - 1.0) * (hbar - 0.5 * V2bar));
+  double lam[4], T[16], Ti[16];
+  lam[0] = fabs(thetabar);
+  lam[1] = fabs(thetabar);
+  lam[2] = fabs(thetabar + cbar);
+  lam[3] = fabs(thetabar - cbar);
+  const double c2 = cbar * cbar;
+  T[0] = 1.0;
+  T[1] = 0.0;
+  T[2] = 1.0 / c2;
+  T[3] = 1.0 / c2;
+  T[4] = ubar;
+  T[5] = -ny;
+  T[6] = ubar / c2 + nx / cbar;
+  T[7] = ubar / c2 - nx / cbar;
+  T[8] = vbar;
+  T[9] = nx;
+  T[10] = vbar / c2 + ny / cbar;
+  T[11] = vbar / c2 - ny / cbar;
+  T[12] = 0.5 * V2bar;
+  T[13] = ubar * (-ny) + vbar * nx;
+  const double tc = thetabar / cbar, hv = (0.5 * V2bar) / c2;
+  T[14] = ogm1 + tc + hv;
+  T[15] = ogm1 - tc + hv;
+  Ti[0] = 1.0 - (gamma - 1.0) * (0.5 * V2bar) / c2;
+  Ti[1] = (gamma - 1.0) * ubar / c2;
+  Ti[2] = (gamma - 1.0) * vbar / c2;
+  Ti[3] = -1.0 * (gamma - 1.0) / c2;
+  Ti[4] = -1.0 * (ubar * (-ny) + vbar * nx);
+  Ti[5] = -ny;
+  Ti[6] = nx;
+  Ti[7] = 0.;
+  Ti[8] = 0.5 * (-cbar * thetabar + (gamma - 1.0) * 0.5 * V2bar);
+  Ti[9] = 0.5 * (cbar * nx - (gamma - 1.0) * ubar);
+  Ti[10] = 0.5 * (cbar * ny - (gamma - 1.0) * vbar);
+  Ti[11] = 0.5 * (gamma - 1.0);
+  Ti[12] = 0.5 * (cbar * thetabar + (gamma - 1.0) * 0.5 * V2bar);
+  Ti[13] = -0.5 * (cbar * nx + (gamma - 1.0) * ubar);
+  Ti[14] = -0.5 * (cbar * ny + (gamma - 1.0) * vbar);
+  Ti[15] = 0.5 * (gamma - 1.0);
+  double dq[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) dq[i] = qr[i] - ql[i];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    double sd = 0.;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      double rm = 0.;
+#pragma unroll
+      for (int k = 0; k < 4; k++) rm += T[i * 4 + k] * (lam[k] * Ti[k * 4 + j]);
+      sd += rm * dq[j];
+    }
+    const double diss = sd * len;
+    flux[i] = 0.5 * (L.F[i] + R.F[i] - diss);
+  }
+}
+
 // cv_calc.C:840-866: max(|theta+c|, |theta-c|) for one node state.
 __device__ __forceinline__ double max_wave(const double* q, double nx, double ny, double gamma) {
   double rho = q[0];

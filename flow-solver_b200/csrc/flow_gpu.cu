@@ -16,11 +16,13 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "flow_gpu.h"
+#include "flow_internal.h"
 #include "flow_kernels.cuh"
 #include "flow_sweep_cta.cuh"
 #include "host/curved.h"
@@ -33,19 +35,91 @@ thread_local std::string g_last_error;
 
 void set_error(const char* msg) { g_last_error = msg; }
 
+}  // namespace
+
+// One device allocation carved into the buffers of many contexts
+// (offset-indexed, 256-byte aligned first fit with coalescing free list).
+struct flow_arena {
+  int device = 0;
+  char* base = nullptr;
+  size_t size = 0, used = 0;
+  std::map<size_t, size_t> free_blocks;  // offset -> bytes
+  std::mutex mu;
+
+  void* alloc(size_t bytes) {
+    bytes = (bytes + 255) & ~size_t(255);
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto it = free_blocks.begin(); it != free_blocks.end(); ++it) {
+      if (it->second < bytes) continue;
+      size_t off = it->first, rest = it->second - bytes;
+      free_blocks.erase(it);
+      if (rest) free_blocks[off + bytes] = rest;
+      used += bytes;
+      sizes[off] = bytes;
+      return base + off;
+    }
+    return nullptr;
+  }
+  void release(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t off = (size_t)((char*)p - base);
+    auto sz = sizes.find(off);
+    if (sz == sizes.end()) return;
+    size_t bytes = sz->second;
+    sizes.erase(sz);
+    used -= bytes;
+    auto next = free_blocks.lower_bound(off);
+    if (next != free_blocks.end() && off + bytes == next->first) {
+      bytes += next->second;
+      next = free_blocks.erase(next);
+    }
+    if (next != free_blocks.begin()) {
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += bytes;
+        return;
+      }
+    }
+    free_blocks[off] = bytes;
+  }
+  size_t largest_free() {
+    std::lock_guard<std::mutex> lock(mu);
+    size_t m = 0;
+    for (auto& f : free_blocks) m = std::max(m, f.second);
+    return m;
+  }
+  std::map<size_t, size_t> sizes;  // offset -> bytes of live blocks
+};
+
+namespace {
+
+// Device buffers of one context: cudaMalloc'ed, or carved from an arena.
 struct Buffers {
+  flow_arena* arena = nullptr;
   std::vector<void*> ptrs;
+  size_t bytes = 0;
   template <class T>
   T* alloc(size_t n) {
     if (n == 0) n = 1;
     void* p = nullptr;
-    if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+    if (arena) {
+      p = arena->alloc(n * sizeof(T));
+      if (!p) return nullptr;
+    } else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+      return nullptr;
+    }
     ptrs.push_back(p);
+    bytes += (n * sizeof(T) + 255) & ~size_t(255);
     return static_cast<T*>(p);
   }
   void release() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) {
+      if (arena) arena->release(p);
+      else cudaFree(p);
+    }
     ptrs.clear();
+    bytes = 0;
   }
 };
 
@@ -71,6 +145,8 @@ struct flow_ctx {
   double drop_target = 0.;   // host copy of the pending target (read by reset_run)
   int* h_flags = nullptr;      // pinned: stop flag and status read back by flow_converge_batch
   cudaEvent_t ev_flag = nullptr;
+  int* h_run = nullptr;        // pinned: 2 slots of {stop, status, steps done} for a served run
+  cudaEvent_t ev_run[2] = {nullptr, nullptr};
   // optional per-kernel event timing
   int timing = 0;
   std::vector<cudaEvent_t> event_pool;
@@ -93,6 +169,16 @@ struct flow_ctx {
   MixedTables mt{};
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
+  // CUDA graphs of chunks of K steps with the step index advancing on the
+  // device, one per chunk length (flow_set_graphs; on by default)
+  int use_graphs = 1;
+  struct ChunkGraph {
+    cudaGraphExec_t exec = nullptr;
+    int K = 0, precision = -1, sweep_mode = -1, phase = -1;
+    flow_params p{};
+    long launches = 0;
+  };
+  std::vector<ChunkGraph> graphs;
 };
 
 namespace {
@@ -133,20 +219,9 @@ int launch_check(flow_ctx* c) {
   return 0;
 }
 
-double ramp_cfl(const flow_params* p, int citer) {
-  // init_memory.C:200-216
-  if (p->method == 1) {
-    if (citer < p->ramp) return 1. + (1. * (citer - 1)) / (1. * p->ramp) * (p->CFL - 1.);
-    return p->CFL;
-  }
-  if (p->method == 0) return 1.0;
-  return p->CFL;
-}
-
 StepArgs make_args(const flow_params* p, int ts) {
   StepArgs a{};
   a.gamma = p->gamma;
-  a.cfl = ramp_cfl(p, ts);
   double angle = p->alpha * M_PI / 180.;
   a.uinf = p->mach * cos(angle);
   a.vinf = p->mach * sin(angle);
@@ -338,11 +413,24 @@ int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
   return rc;
 }
 
-// One solve() call (solve.C:44-933), device-only.
-int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int first) {
+// Step index and CFL on the device (k_step_args): citer > 0 sets the index,
+// 0 advances the device's own.
+int launch_step_args(flow_ctx* c, const flow_params* p, int citer) {
+  k_step_args<<<1, 1, 0, c->stream>>>(c->s, citer, p->method, p->ramp, p->CFL);
+  return launch_check(c);
+}
+
+// One solve() call (solve.C:44-933), device-only.  device_ts: the step index
+// advances on the device (for captured chunks of steps; ts then only selects
+// the order phase, which must be the same for every step of the chunk) and
+// the run's first step is recognised on the device.
+int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int first,
+                 bool device_ts = false) {
   int rc = 0;
   int total = c->nn + c->ng;
   c->citer = ts;
+  rc |= launch_step_args(c, p, device_ts ? 0 : ts);
+  if (device_ts) first = -1;
   k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 1);
   rc |= launch_check(c);
   StepArgs a = make_args(p, ts);
@@ -362,10 +450,88 @@ int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int f
     k_finalize_step<<<1, kRedThreads, 0, c->stream>>>(
         c->s, last && hist_slot >= 0 ? c->d_hist : nullptr,
         last && hist_slot >= 0 ? c->d_hist + c->hist_cap : nullptr, hist_slot < 0 ? 0 : hist_slot,
-        last && first);
+        last ? (first < 0 ? -1 : first) : 0);
     rc |= launch_check(c);
   }
   return rc;
+}
+
+bool params_equal(const flow_params& a, const flow_params& b) {
+  return a.iter == b.iter && a.jufreq == b.jufreq && a.CFL == b.CFL && a.ramp == b.ramp &&
+         a.gamma == b.gamma && a.alpha == b.alpha && a.mach == b.mach && a.subits == b.subits &&
+         a.method == b.method && a.order == b.order && a.foits == b.foits && a.soits == b.soits &&
+         a.limit == b.limit && a.unsteady == b.unsteady && a.tacc == b.tacc;
+}
+
+// Order-phase signature of step ts (which reconstruction/limiter passes run).
+int phase_of(const flow_params* p, int ts) {
+  StepArgs a = make_args(p, ts);
+  return a.do_grad | (a.do_derivs << 1) | (a.do_lim << 2) | (a.recon << 3) | (a.gauss << 6);
+}
+
+void drop_graphs(flow_ctx* c) {
+  for (auto& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  c->graphs.clear();
+}
+
+// K steps ts0 .. ts0+K-1 with the step index advancing on the device,
+// replayed from a captured CUDA graph when the chunk allows it (one order
+// phase throughout; the FP64 ordered sweep's buffer swaps return to their
+// start; no per-kernel timing), else launched one by one.
+int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
+  int rc = 0;
+  const int ph = phase_of(p, ts0);
+  const bool graphable = c->use_graphs && !c->timing && K > 0 && ph == phase_of(p, ts0 + K - 1) &&
+                         (c->precision == 1 || c->sweep_mode == 1 || p->subits % 2 == 0);
+  if (!graphable) {
+    for (int i = 0; i < K && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
+    return rc;
+  }
+  flow_ctx::ChunkGraph* g = nullptr;
+  for (auto& x : c->graphs)
+    if (x.K == K && x.precision == c->precision && x.sweep_mode == c->sweep_mode &&
+        x.phase == ph && params_equal(x.p, *p))
+      g = &x;
+  if (!g) {
+    if (c->graphs.size() >= 4) drop_graphs(c);
+    flow_ctx::ChunkGraph ng;
+    ng.K = K;
+    ng.precision = c->precision;
+    ng.sweep_mode = c->sweep_mode;
+    ng.phase = ph;
+    ng.p = *p;
+    const long l0 = c->launches;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      set_error("stream capture could not begin");
+      return FLOW_ERR_CUDA;
+    }
+    for (int i = 0; i < K; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc || e != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      set_error("step capture failed");
+      return rc ? rc : FLOW_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(&ng.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      set_error("graph instantiation failed");
+      return FLOW_ERR_CUDA;
+    }
+    ng.launches = c->launches - l0;
+    c->launches = l0;
+    c->graphs.push_back(ng);
+    g = &c->graphs.back();
+  }
+  if (cudaGraphLaunch(g->exec, c->stream) != cudaSuccess) {
+    set_error("graph launch failed");
+    return FLOW_ERR_CUDA;
+  }
+  c->launches += g->launches;
+  c->citer = ts0 + K - 1;
+  return 0;
 }
 
 // Clear the convergence stop and set the run's target drop (0 = none).
@@ -437,10 +603,13 @@ int build_mixed_tables(flow_ctx* c) {
   mt.pos = upload_vec(c, pos);
   mt.offd_ptr = upload_vec(c, optr);
   mt.offd_col = upload_vec(c, ocol);
+  std::vector<int4> rinfo(nn);
+  for (int pp = 0; pp < nn; pp++) rinfo[pp] = make_int4(rows[pp], optr[pp], optr[pp + 1], 0);
+  mt.rowinfo = upload_vec(c, rinfo);
   mt.lu32 = c->buf.alloc<float>((size_t)16 * nn);
   mt.dq32 = c->buf.alloc<float>((size_t)4 * (nn + 1));
   mt.lhs32 = c->buf.alloc<float>((size_t)16 * std::max<size_t>(ocol.size(), 1));
-  if (!mt.color_ptr || !mt.rows || !mt.pos || !mt.offd_ptr || !mt.offd_col || !mt.lu32 ||
+  if (!mt.color_ptr || !mt.rows || !mt.pos || !mt.offd_ptr || !mt.offd_col || !mt.rowinfo || !mt.lu32 ||
       !mt.dq32 || !mt.lhs32) {
     set_error("precision form: device allocation failed");
     mt.lhs32 = nullptr;
@@ -453,9 +622,13 @@ int build_mixed_tables(flow_ctx* c) {
 
 int ensure_hist(flow_ctx* c, int n) {
   if (n <= c->hist_cap) return 0;
-  if (c->d_hist) cudaFree(c->d_hist);
-  c->d_hist = nullptr;
-  if (cudaMalloc(&c->d_hist, sizeof(double) * 2 * n) != cudaSuccess) return FLOW_ERR_CUDA;
+  n = std::max(n, 64);
+  double* h = c->buf.alloc<double>((size_t)2 * n);  // the old block stays with the context
+  if (!h) {
+    set_error("history allocation failed");
+    return FLOW_ERR_CUDA;
+  }
+  c->d_hist = h;
   c->hist_cap = n;
   return 0;
 }
@@ -467,7 +640,25 @@ extern "C" {
 
 const char* flow_last_error(void) { return g_last_error.c_str(); }
 
+static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const flow_params* p,
+                             int device, int* status);
+
 flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device, int* status) {
+  return create_impl(nullptr, g, p, device, status);
+}
+
+flow_ctx* flow_create_in(flow_arena* arena, const flow_grid_view* g, const flow_params* p,
+                         int* status) {
+  if (!arena) {
+    set_error("null arena");
+    if (status) *status = FLOW_ERR_ARG;
+    return nullptr;
+  }
+  return create_impl(arena, g, p, arena->device, status);
+}
+
+static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const flow_params* p,
+                             int device, int* status) {
   auto fail = [&](flow_ctx* c, int code, const char* msg) -> flow_ctx* {
     set_error(msg);
     if (status) *status = code;
@@ -489,6 +680,7 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
       return fail(nullptr, FLOW_ERR_ARG, "mixed node_order is not supported");
 
   flow_ctx* c = new flow_ctx();
+  c->buf.arena = arena;
   c->device = device;
   c->order = p->order;
   c->nn = nn; c->ng = ng; c->ns = ns; c->nbe = nbe;
@@ -597,7 +789,9 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
         st_w.push_back(1.0 / pow(dist, 1.0));  // compute_derivatives.C:1470 (GEOM_WEIGHT 1)
       }
       const double* Ui = g->svd_U + g->svd_off[i];
-      for (int q = 0; q < 5 * mrows; q++) U1.push_back(Ui[q]);
+      // the first 5 columns of U, re-laid row by row (U1[k][c] = U[c*m + k])
+      for (int k = 0; k < mrows; k++)
+        for (int q = 0; q < 5; q++) U1.push_back(Ui[q * mrows + k]);
       for (int q = 0; q < 25; q++) VT[(size_t)i * 25 + q] = g->svd_VT[(size_t)i * 25 + q];
       for (int q = 0; q < 5; q++) S[(size_t)i * 5 + q] = g->svd_S[(size_t)i * 5 + q];
     }
@@ -717,12 +911,13 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   s.skip = c->buf.alloc<int>(1);
   s.stop = c->buf.alloc<int>(1);
   s.steps_done = c->buf.alloc<int>(1);
+  s.citer = c->buf.alloc<int>(1);
   s.partial = c->buf.alloc<double>(2 * kRedBlocks);
   s.scalars = c->buf.alloc<double>(8);
   if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.dQ2 || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
       !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
       !s.Jb || !s.bforce || !s.done || !s.counter || !s.status || !s.skip || !s.partial ||
-      !s.scalars || !s.stop || !s.steps_done)
+      !s.scalars || !s.stop || !s.steps_done || !s.citer)
     return fail(c, FLOW_ERR_CUDA, "device state allocation failed");
   cudaMemset(s.Q, 0, nq * 8);
   cudaMemset(s.nQ, 0, nq * 8);
@@ -742,6 +937,7 @@ flow_ctx* flow_create(const flow_grid_view* g, const flow_params* p, int device,
   cudaMemset(s.skip, 0, 4);
   cudaMemset(s.stop, 0, 4);
   cudaMemset(s.steps_done, 0, 4);
+  cudaMemset(s.citer, 0, 4);
   cudaMemset(s.scalars, 0, 64);
   std::vector<double> xnb((size_t)(nbe + 1) * 3, 0.);
   std::copy(g->xn_bedges, g->xn_bedges + xnb.size(), xnb.begin());
@@ -760,11 +956,14 @@ void flow_destroy(flow_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   harvest(c);
+  drop_graphs(c);
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   if (c->ev_flag) cudaEventDestroy(c->ev_flag);
   if (c->h_flags) cudaFreeHost(c->h_flags);
+  for (cudaEvent_t e : c->ev_run)
+    if (e) cudaEventDestroy(e);
+  if (c->h_run) cudaFreeHost(c->h_run);
   c->buf.release();
-  if (c->d_hist) cudaFree(c->d_hist);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -808,6 +1007,15 @@ int flow_set_precision(flow_ctx* c, int mode) {
     if (rc) return rc;
   }
   c->precision = mode;
+  return 0;
+}
+
+int flow_set_graphs(flow_ctx* c, int on) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  if (!on) drop_graphs(c);
+  c->use_graphs = on ? 1 : 0;
   return 0;
 }
 
@@ -869,7 +1077,13 @@ int flow_converge(flow_ctx* c, const flow_params* p, int ts0, int max_steps, dou
   int done = 0, stop = 0, issued = 0;
   while (!rc && issued < max_steps) {
     int n = std::min(chunk, max_steps - issued);
-    for (int i = 0; i < n && !rc; i++, issued++) rc |= enqueue_step(c, p, ts0 + issued, -1, issued == 0);
+    if (issued == 0 || n < chunk) {
+      for (int i = 0; i < n && !rc; i++, issued++)
+        rc |= enqueue_step(c, p, ts0 + issued, -1, issued == 0);
+    } else {
+      rc |= enqueue_chunk(c, p, ts0 + issued, n);
+      issued += n;
+    }
     if (rc) break;
     cudaMemcpyAsync(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
@@ -932,8 +1146,13 @@ int flow_converge_batch(flow_ctx** ctxs, int n, const flow_params* p, int ts0, i
       cudaSetDevice(c->device);
       int k = std::min(chunk, max_steps - issued[i]);
       int rc = 0;
-      for (int q = 0; q < k && !rc; q++, issued[i]++)
-        rc |= enqueue_step(c, p, ts0 + issued[i], -1, issued[i] == 0);
+      if (issued[i] == 0 || k < chunk) {
+        for (int q = 0; q < k && !rc; q++, issued[i]++)
+          rc |= enqueue_step(c, p, ts0 + issued[i], -1, issued[i] == 0);
+      } else {
+        rc |= enqueue_chunk(c, p, ts0 + issued[i], k);
+        issued[i] += k;
+      }
       if (rc) { rc_all |= rc; active[i] = 0; nactive--; continue; }
       if (pending[i]) {
         // the flags of the previous round are ready once its event completed
@@ -983,7 +1202,8 @@ int flow_build_matrix(flow_ctx* c, const flow_params* p, int citer) {
   StepArgs a = make_args(p, citer);
   a.do_grad = a.do_derivs = a.do_lim = 0;
   c->citer = citer;
-  rc = launch_node_prepare(c, a);
+  rc = launch_step_args(c, p, citer);
+  rc |= launch_node_prepare(c, a);
   k_diag_only<<<grid_blocks(c->nn, 128), 128, 0, c->stream>>>(c->m, c->s);
   rc |= launch_check(c);
   if (rc) return rc;
@@ -998,6 +1218,7 @@ int flow_reconstruct(flow_ctx* c, const flow_params* p, int ts) {
   reset_run(c, 0.);
   StepArgs a = make_args(p, ts);
   c->citer = ts;
+  rc |= launch_step_args(c, p, ts);
   // grad, hess <- 0 and phi <- 1 (solve.C:298-348), keeping the current nQ
   k_begin_step<<<grid_blocks(c->nn + c->ng, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 0);
   rc |= launch_check(c);
@@ -1180,6 +1401,49 @@ void flow_clear_status(flow_ctx* c) {
   cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream);
   cudaStreamSynchronize(c->stream);
 }
+
+flow_arena* flow_arena_create(int device, long long bytes, int* status) {
+  if (bytes <= 0) {
+    set_error("arena size must be positive");
+    if (status) *status = FLOW_ERR_ARG;
+    return nullptr;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    set_error("cudaSetDevice failed");
+    if (status) *status = FLOW_ERR_CUDA;
+    return nullptr;
+  }
+  flow_arena* a = new flow_arena();
+  a->device = device;
+  a->size = ((size_t)bytes + 255) & ~size_t(255);
+  if (cudaMalloc((void**)&a->base, a->size) != cudaSuccess) {
+    cudaGetLastError();
+    delete a;
+    set_error("arena allocation failed (not enough device memory)");
+    if (status) *status = FLOW_ERR_CUDA;
+    return nullptr;
+  }
+  a->free_blocks[0] = a->size;
+  if (status) *status = 0;
+  return a;
+}
+
+void flow_arena_destroy(flow_arena* a) {
+  if (!a) return;
+  cudaSetDevice(a->device);
+  cudaFree(a->base);
+  delete a;
+}
+
+long long flow_arena_free_bytes(flow_arena* a) {
+  if (!a) return -1;
+  std::lock_guard<std::mutex> lock(a->mu);
+  return (long long)(a->size - a->used);
+}
+
+long long flow_arena_largest_free(flow_arena* a) { return a ? (long long)a->largest_free() : -1; }
+
+long long flow_ctx_device_bytes(flow_ctx* c) { return c ? (long long)c->buf.bytes : -1; }
 
 long flow_launch_count(flow_ctx* c) { return c ? c->launches : 0; }
 
@@ -1371,3 +1635,86 @@ extern "C" int flow_linear_residual_noalloc(const int* ia, const int* ja, const 
   *rms = out[0];
   return FLOW_OK;
 }
+
+// ===========================================================================
+// Hooks for the serving engine (flow_internal.h).
+// ===========================================================================
+namespace flow {
+namespace internal {
+
+int begin_run(flow_ctx* c, const flow_params* p, double drop) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if ((rc = ensure_hist(c, 1))) return rc;
+  if (!c->h_run) {
+    if (cudaHostAlloc(&c->h_run, 6 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+      set_error("pinned flag allocation failed");
+      return FLOW_ERR_CUDA;
+    }
+    for (auto& e : c->ev_run)
+      if (cudaEventCreate(&e) != cudaSuccess) return FLOW_ERR_CUDA;
+  }
+  for (int i = 0; i < 6; i++) c->h_run[i] = 0;
+  reset_run(c, drop);
+  if (cudaEventRecord(c->ev0, c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
+  return 0;
+}
+
+int enqueue_steps(flow_ctx* c, const flow_params* p, int ts0, int K) {
+  if (!c || !c->ok || K < 1) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (ts0 == 1) {
+    int rc = 0;
+    for (int i = 0; i < K && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, -1, i == 0);
+    return rc;
+  }
+  return enqueue_chunk(c, p, ts0, K);
+}
+
+int post_flags(flow_ctx* c, int slot) {
+  int* h = c->h_run + 3 * slot;
+  cudaMemcpyAsync(h, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(h + 1, c->s.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(h + 2, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  if (cudaEventRecord(c->ev_run[slot], c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
+  return 0;
+}
+
+int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps) {
+  cudaError_t e = cudaEventQuery(c->ev_run[slot]);
+  if (e == cudaErrorNotReady) return 0;
+  if (e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return -1;
+  }
+  const int* h = c->h_run + 3 * slot;
+  *stop = h[0];
+  *status = h[1];
+  *steps = h[2];
+  return 1;
+}
+
+double run_ms(flow_ctx* c, int slot) {
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, c->ev0, c->ev_run[slot]);
+  return ms;
+}
+
+int run_norms(flow_ctx* c, double* r_first, double* r_last) {
+  double sc[8];
+  if (cudaMemcpyAsync(sc, c->s.scalars, sizeof(sc), cudaMemcpyDeviceToHost, c->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return FLOW_ERR_CUDA;
+  *r_first = sc[6];
+  *r_last = sqrt(sc[2]);
+  return 0;
+}
+
+cudaStream_t stream_of(flow_ctx* c) { return c->stream; }
+int device_of(flow_ctx* c) { return c->device; }
+
+}  // namespace internal
+}  // namespace flow

@@ -1,0 +1,30 @@
+// flow_internal.h - hooks of the context implementation (flow_gpu.cu) used by
+// the serving engine (flow_serve.cu).  Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include "flow_gpu.h"
+
+namespace flow {
+namespace internal {
+
+// Start a run on the context's stream: clear the stop flag and step count,
+// set the target drop of ||R_rho|| and record the run's start event.
+int begin_run(flow_ctx* c, const flow_params* p, double drop);
+// Enqueue steps ts0 .. ts0+K-1 (ts0 == 1 starts the run); full chunks after
+// the first replay the context's CUDA graphs.
+int enqueue_steps(flow_ctx* c, const flow_params* p, int ts0, int K);
+// Queue a read-back of {stop, status, steps done} into flag slot `slot`
+// (0 or 1) of the context's pinned flags, with an event behind it.
+int post_flags(flow_ctx* c, int slot);
+// 1 when flag slot `slot` has arrived (values in *stop, *status, *steps),
+// 0 while it is in flight, -1 on a CUDA error.
+int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps);
+// Device time from the run's start to flag slot `slot` (ms).
+double run_ms(flow_ctx* c, int slot);
+// ||R_rho|| of the run's first step and of its last step.
+int run_norms(flow_ctx* c, double* r_first, double* r_last);
+cudaStream_t stream_of(flow_ctx* c);
+int device_of(flow_ctx* c);
+
+}  // namespace internal
+}  // namespace flow

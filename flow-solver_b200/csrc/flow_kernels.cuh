@@ -36,7 +36,6 @@ constexpr int kRedThreads = 256;
 
 struct StepArgs {
   double gamma;
-  double cfl;
   double uinf, vinf, pinf;  // far-field state (cvbc.C:70-74)
   double cos_a, sin_a;      // angle of attack (grid_io.C:1432)
   int do_grad;              // k=1 gradient
@@ -49,6 +48,23 @@ struct StepArgs {
 };
 
 // ---------------------------------------------------------------------------
+// Step index and CFL of the step about to run (init_memory.C:200-216).
+// citer > 0 sets the index; citer == 0 takes the one after the previous step,
+// which lets a captured sequence of steps replay with an advancing ramp.
+__global__ void k_step_args(DevState s, int citer, int method, int ramp, double CFL) {
+  if (*s.stop) return;  // the run has converged
+  const int ci = citer > 0 ? citer : *s.citer + 1;
+  *s.citer = ci;
+  double cfl;
+  if (method == 1)
+    cfl = ci < ramp ? 1. + (1. * (ci - 1)) / (1. * ramp) * (CFL - 1.) : CFL;
+  else if (method == 0)
+    cfl = 1.0;
+  else
+    cfl = CFL;
+  s.scalars[3] = cfl;
+}
+
 __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
   if (*s.stop) return;  // the run has converged
   int total = m.nn + m.ng;
@@ -83,180 +99,11 @@ __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
 // V/dt of build_matrix (init_memory.C:200-290); then the LSQ gradient
 // (gradient.C:382-403) or the k=2 derivatives (compute_derivatives.C:
 // 1438-1521); then the Venkatakrishnan limiter (limiter.C:594-906).
-template <int ORDER>
-__global__ void __launch_bounds__(128) k_node_prepare(DevMesh m, DevState s, StepArgs a) {
-  if (*s.stop) return;  // the run has converged
-  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (n > m.nn) return;
-  const double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
-  const double q0[4] = {q4.x, q4.y, q4.z, q4.w};
-
-  // ---- wave-speed sum over the node's subedges, then boundary edges ----
-  double ev = 0.;
-  int bad = 0;
-  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
-  for (int k = s0; k < s1; k++) {
-    int sd = m.nsub[k];
-    double4 g = m.sub_geo[sd >> 1];
-    double w = max_wave(q0, g.x, g.y, a.gamma);
-    if (!isfinite(w)) bad = 1;
-    ev += (w * g.z);
-  }
-  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
-  for (int k = b0; k < b1; k++) {
-    int b = m.nbed[k];
-    const double* xn = s.xn_bedges + 3 * b;
-    double w = max_wave(q0, xn[0], xn[1], a.gamma);
-    if (!isfinite(w)) bad = 1;
-    ev += (w * xn[2]);
-  }
-  double V = m.cv_area[n];
-  double dt = a.cfl * (V / ev);
-  s.dt[n] = dt;
-  if (bad) atomicOr(s.status, ERR_EIGEN);
-  if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
-  if (!a.do_grad && !a.do_derivs && !a.do_lim) return;
-
-  // ---- 1-ring min/max and the k=1 LSQ gradient over incident edges ----
-  double qmin[4], qmax[4], gr[8];
-#pragma unroll
-  for (int j = 0; j < 4; j++) { qmin[j] = q0[j]; qmax[j] = q0[j]; }
-#pragma unroll
-  for (int j = 0; j < 8; j++) gr[j] = 0.;
-  const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
-  for (int k = e0; k < e1; k++) {
-    int ed = m.nedg[k];
-    int e = ed >> 1, side = ed & 1;
-    int2 lr = m.edge_lr[e];
-    int other = side ? lr.x : lr.y;
-    double4 qo4 = reinterpret_cast<const double4*>(s.nQ)[other];
-    double qo[4] = {qo4.x, qo4.y, qo4.z, qo4.w};
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      qmin[j] = qmin[j] <= qo[j] ? qmin[j] : qo[j];
-      qmax[j] = qmax[j] >= qo[j] ? qmax[j] : qo[j];
-    }
-    if (ORDER == 1 && a.do_grad) {
-      double4 w = m.edge_w[e];
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        // dQ = nQ[R] - nQ[L] (gradient.C:391)
-        double dq = side ? (q0[j] - qo[j]) : (qo[j] - q0[j]);
-        if (side == 0) {
-          gr[2 * j] += w.x * dq;
-          gr[2 * j + 1] += w.y * dq;
-        } else {
-          gr[2 * j] -= w.z * dq;
-          gr[2 * j + 1] -= w.w * dq;
-        }
-      }
-    }
-  }
-  if (ORDER == 1 && a.do_grad) {
-    double4* g = reinterpret_cast<double4*>(s.grad) + 2 * n;
-    g[0] = make_double4(gr[0], gr[1], gr[2], gr[3]);
-    g[1] = make_double4(gr[4], gr[5], gr[6], gr[7]);
-  }
-
-  // ---- k=2: x = V S^-1 U^T b over the two-ring stencil ----
-  double h[20], pv[4];
-  if (ORDER == 3 && a.do_derivs) {
-    const int t0 = m.st_ptr[n], t1 = m.st_ptr[n + 1];
-    const int mrows = t1 - t0;
-    const double* U = m.svd_U1 + 5 * (long)t0;
-    const double* VT = m.svd_VT + 25 * (long)n;
-    const double* S = m.svd_S + 5 * (long)n;
-    const double* mo = m.moments + 9 * (long)n;
-    double acc[4][5];
-#pragma unroll
-    for (int v = 0; v < 4; v++)
-#pragma unroll
-      for (int c = 0; c < 5; c++) acc[v][c] = 0.;
-    for (int k = 0; k < mrows; k++) {
-      int nb = m.st_idx[t0 + k];
-      double w = m.st_w[t0 + k];
-      double4 qb4 = reinterpret_cast<const double4*>(s.nQ)[nb];
-      double bv[4] = {w * (qb4.x - q0[0]), w * (qb4.y - q0[1]), w * (qb4.z - q0[2]),
-                      w * (qb4.w - q0[3])};
-#pragma unroll
-      for (int c = 0; c < 5; c++) {
-        double u = U[c * mrows + k];
-#pragma unroll
-        for (int v = 0; v < 4; v++) acc[v][c] += bv[v] * u;
-      }
-    }
-#pragma unroll
-    for (int v = 0; v < 4; v++) {
-      double t1v[5], sol[5];
-#pragma unroll
-      for (int c = 0; c < 5; c++) t1v[c] = acc[v][c] / S[c];
-#pragma unroll
-      for (int j = 0; j < 5; j++) {
-        double sum = 0.;
-#pragma unroll
-        for (int c = 0; c < 5; c++) sum += VT[j * 5 + c] * t1v[c];
-        sol[j] = sum;
-      }
-#pragma unroll
-      for (int c = 0; c < 5; c++) h[v * 5 + c] = sol[c];
-      pv[v] = q0[v] - mo[0] * sol[0] - mo[1] * sol[1] - mo[2] * sol[2] * 0.5 -
-              mo[3] * sol[3] * 0.5 - mo[4] * sol[4];
-    }
-    double* hd = s.hess5 + 20 * (long)n;
-#pragma unroll
-    for (int c = 0; c < 20; c++) hd[c] = h[c];
-    reinterpret_cast<double4*>(s.pv)[n] = make_double4(pv[0], pv[1], pv[2], pv[3]);
-  }
-
-  if (!a.do_lim) return;
-  // ---- Venkatakrishnan: unlimited reconstruction to every face point ----
-  double ph[4] = {1.0, 1.0, 1.0, 1.0};
-  for (int k = s0; k < s1; k++) {
-    int sd = m.nsub[k];
-    int sub = sd >> 1, side = sd & 1;
-    if (ORDER == 1) {
-      double4 d = m.sub_dx[sub];
-      double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        double qr = q0[j] + (gr[2 * j] * dx0 + gr[2 * j + 1] * dx1);
-        ph[j] = venkat_fold(ph[j], qr, q0[j], qmin[j], qmax[j]);
-      }
-    } else {
-      const double* xg = m.sub_xg + 6 * (long)sub;
-      double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
-#pragma unroll
-      for (int gpt = 0; gpt < 3; gpt++) {
-        double dx0 = xg[2 * gpt] - xn0, dx1 = xg[2 * gpt + 1] - xn1;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          const double* hh = h + 5 * j;
-          double qr = pv[j];
-          qr += (hh[0] * dx0 + hh[1] * dx1 + hh[2] * dx0 * dx0 * 0.5 + hh[3] * dx1 * dx1 * 0.5 +
-                 hh[4] * dx0 * dx1);
-          ph[j] = venkat_fold(ph[j], qr, q0[j], qmin[j], qmax[j]);
-        }
-      }
-    }
-  }
-  double pmin = ph[0];
-#pragma unroll
-  for (int j = 1; j < 4; j++) pmin = pmin <= ph[j] ? pmin : ph[j];
-  double4* pp = reinterpret_cast<double4*>(s.phi) + 2 * n;
-  pp[0] = make_double4(pmin, pmin, ph[1], ph[1]);
-  pp[1] = make_double4(ph[2], ph[2], ph[3], ph[3]);
-  if (pmin < 0.0 || pmin > 1.0 || ph[1] < 0.0 || ph[1] > 1.0 || ph[2] < 0.0 || ph[2] > 1.0 ||
-      ph[3] < 0.0 || ph[3] > 1.0)
-    atomicOr(s.status, ERR_LIMITER);
-}
-
-// ---------------------------------------------------------------------------
-// k_node_prepare with four lanes per node, lane v owning conserved variable
-// v: the gradient, the k=2 derivatives and point value, and the limiter
-// value of variable v only involve variable v, and each lane accumulates
-// its sums in the same face / stencil order as the reference, so the
-// results are those of k_node_prepare.  The wave-speed sum (all variables)
-// is formed by every lane of the quad from node constants computed once.
+// Four lanes per node, lane v owning conserved variable v: the gradient,
+// the k=2 derivatives and point value, and the limiter value of variable v
+// only involve variable v, and each lane accumulates its sums in the
+// reference's face / stencil order.  The wave-speed sum (all variables) is
+// formed by every lane of the quad from node constants computed once.
 template <int ORDER>
 __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
@@ -275,6 +122,7 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
   double ev = 0.;
   int bad = 0;
   const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  #pragma unroll 4
   for (int k = s0; k < s1; k++) {
     const double4 g = m.sub_geo[m.nsub[k] >> 1];
     const double theta = uu * g.x + vv * g.y;
@@ -293,7 +141,7 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
     ev += (w * xn[2]);
   }
   if (v == 0) {
-    const double dt = a.cfl * (m.cv_area[n] / ev);
+    const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
     s.dt[n] = dt;
     if (bad) atomicOr(s.status, ERR_EIGEN);
     if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
@@ -303,6 +151,7 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
   // ---- 1-ring min/max and the k=1 LSQ gradient of variable v ----
   double qmin = q0v, qmax = q0v, g0 = 0., g1 = 0.;
   const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
+  #pragma unroll 4
   for (int k = e0; k < e1; k++) {
     const int ed = m.nedg[k];
     const int e = ed >> 1, side = ed & 1;
@@ -331,13 +180,14 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
   if (ORDER == 3 && a.do_derivs) {
     const int t0 = m.st_ptr[n], t1 = m.st_ptr[n + 1];
     const int mrows = t1 - t0;
-    const double* U = m.svd_U1 + 5 * (long)t0;
+    const double* U = m.svd_U1 + 5 * (long)t0;  // row k: U[k][0..4], contiguous
     double acc[5] = {0., 0., 0., 0., 0.};
+#pragma unroll 4
     for (int k = 0; k < mrows; k++) {
       const int nb = m.st_idx[t0 + k];
       const double bv = m.st_w[t0 + k] * (s.nQ[4 * (long)nb + v] - q0v);
 #pragma unroll
-      for (int c = 0; c < 5; c++) acc[c] += bv * U[c * mrows + k];
+      for (int c = 0; c < 5; c++) acc[c] += bv * U[5 * k + c];
     }
     const double* VT = m.svd_VT + 25 * (long)n;
     const double* S = m.svd_S + 5 * (long)n;
@@ -364,6 +214,7 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
   // ---- Venkatakrishnan bound of variable v over every face point ----
   double ph = 1.0;
   const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
+  #pragma unroll 4
   for (int k = s0; k < s1; k++) {
     const int sd = m.nsub[k];
     const int sub = sd >> 1, side = sd & 1;
@@ -398,9 +249,13 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
 }
 
 // ---------------------------------------------------------------------------
-// k_assemble with four lanes per node, lane q owning row q of every 4x4
-// block and component q of R: each lane sums its row in the reference's
-// face order, so the results are those of k_assemble.
+// Per node: R and RHS = -R, the diagonal block (V/dt plus the face Jacobians
+// in face order), the off-diagonal blocks of the node's LHS row, and the LU
+// factors of the diagonal block for the sweeps (linear_algebra.C:226-246).
+// Four lanes per node, lane q owning row q of every 4x4 block and component
+// q of R; each lane sums its row in the reference's face order.  MIXED (the
+// precision form) writes FP32 off-diagonal blocks in colour order and FP32
+// LU factors with reciprocal pivots instead of the FP64 row.
 template <bool JAC, bool MIXED>
 __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a,
                                                    MixedTables mt) {
@@ -516,7 +371,7 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
 // Per subedge: face states, Roe flux, forward-difference Jacobian
 // (residual.C:112-333, reconstruct.C:181-203, jacobian.C:45-110).
 template <int RECON, bool JAC>
-__global__ void __launch_bounds__(128) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
+__global__ void __launch_bounds__(128, 4) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
   int sub = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (sub > m.ns) return;
@@ -537,8 +392,16 @@ __global__ void __launch_bounds__(128) k_subedge_flux(DevMesh m, DevState s, Ste
       qR[j] += (phR * gR[2 * j] * d.z + phR * gR[2 * j + 1] * d.w);
     }
   }
+  // Roe_flux_centered and its 8 forward differences (jacobian.C:45-185): the
+  // unperturbed side's quantities and, unless the density is perturbed, the
+  // Roe density weight are reused from the base evaluation
+  const double ogm1 = 1.0 / (a.gamma - 1.0);
+  RoeSide SL, SR;
+  roe_side(qL, g.x, g.y, g.z, a.gamma, SL);
+  roe_side(qR, g.x, g.y, g.z, a.gamma, SR);
+  const double bg = roe_weight(SL.rho, SR.rho);
   double flux[4];
-  roe_flux(g.x, g.y, g.z, a.gamma, qL, qR, flux);
+  roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qR, SL, SR, bg, flux);
   reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
   if (!JAC) return;
   const double eps = 1.0e-08;
@@ -550,14 +413,19 @@ __global__ void __launch_bounds__(128) k_subedge_flux(DevMesh m, DevState s, Ste
 #pragma unroll 1
     for (int i = 0; i < 4; i++) {
       double qp[4], fp[4];
-      const double* base = side ? qR : qL;
 #pragma unroll
-      for (int j = 0; j < 4; j++) qp[j] = base[j];
-      qp[i] += eps;
+      for (int j = 0; j < 4; j++) {
+        const double bj = side ? qR[j] : qL[j];
+        qp[j] = j == i ? bj + eps : bj;
+      }
+      RoeSide SP;
+      roe_side(qp, g.x, g.y, g.z, a.gamma, SP);
+      double bgp = bg;
+      if (i == 0) bgp = side ? roe_weight(SL.rho, SP.rho) : roe_weight(SP.rho, SR.rho);
       if (side == 0)
-        roe_flux(g.x, g.y, g.z, a.gamma, qp, qR, fp);
+        roe_core(g.x, g.y, g.z, a.gamma, ogm1, qp, qR, SP, SR, bgp, fp);
       else
-        roe_flux(g.x, g.y, g.z, a.gamma, qL, qp, fp);
+        roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qp, SL, SP, bgp, fp);
 #pragma unroll
       for (int j = 0; j < 4; j++) Jo[j * 4 + i] = (fp[j] - flux[j]) / eps;
     }
@@ -686,108 +554,6 @@ __global__ void __launch_bounds__(128) k_boundary(DevMesh m, DevState s, StepArg
   double* Jo = s.Jb + 16 * (long)b;
 #pragma unroll
   for (int k = 0; k < 16; k++) Jo[k] = 0.5 * (d[k] + Rm[k]) * len;
-}
-
-// ---------------------------------------------------------------------------
-// Per node: R and RHS = -R, the diagonal block (V/dt plus the face Jacobians
-// in face order), the off-diagonal blocks of the node's LHS row, and the LU
-// factors of the diagonal block for the sweeps (linear_algebra.C:226-246).
-template <bool JAC>
-__global__ void __launch_bounds__(128) k_assemble(DevMesh m, DevState s, StepArgs a) {
-  if (*s.stop) return;  // the run has converged
-  int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (n > m.nn) return;
-  double r[4] = {0., 0., 0., 0.};
-  double D[16];
-  double V = m.cv_area[n];
-  double diag = V / (s.dt[n]);
-#pragma unroll
-  for (int k = 0; k < 16; k++) D[k] = 0.;
-  if (a.steady_diag) {
-    D[0] = diag;
-    D[5] = diag;
-    D[10] = diag;
-    D[15] = diag;
-  }
-  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
-  for (int k = s0; k < s1; k++) {
-    int sd = m.nsub[k];
-    int sub = sd >> 1, side = sd & 1;
-    double4 f = reinterpret_cast<const double4*>(s.F)[sub];
-    if (side == 0) {
-      r[0] += f.x; r[1] += f.y; r[2] += f.z; r[3] += f.w;
-    } else {
-      r[0] -= f.x; r[1] -= f.y; r[2] -= f.z; r[3] -= f.w;
-    }
-    if (JAC) {
-      const double4* J = reinterpret_cast<const double4*>((side ? s.JR : s.JL) + 16 * (long)sub);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        double4 v = J[q];
-        if (side == 0) {
-          D[4 * q] += v.x; D[4 * q + 1] += v.y; D[4 * q + 2] += v.z; D[4 * q + 3] += v.w;
-        } else {
-          D[4 * q] -= v.x; D[4 * q + 1] -= v.y; D[4 * q + 2] -= v.z; D[4 * q + 3] -= v.w;
-        }
-      }
-    }
-  }
-  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
-  for (int k = b0; k < b1; k++) {
-    int b = m.nbed[k];
-    double4 f = reinterpret_cast<const double4*>(s.Fb)[b];
-    r[0] += f.x; r[1] += f.y; r[2] += f.z; r[3] += f.w;
-    if (JAC) {
-      const double4* J = reinterpret_cast<const double4*>(s.Jb + 16 * (long)b);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        double4 v = J[q];
-        D[4 * q] += v.x; D[4 * q + 1] += v.y; D[4 * q + 2] += v.z; D[4 * q + 3] += v.w;
-      }
-    }
-  }
-  reinterpret_cast<double4*>(s.R)[n] = make_double4(r[0], r[1], r[2], r[3]);
-  reinterpret_cast<double4*>(s.RHS)[n] = make_double4(-(r[0]), -(r[1]), -(r[2]), -(r[3]));
-  // the row of the block matrix
-  const int k0 = m.ia[n], k1 = m.ia[n + 1];
-  for (int k = k0; k < k1; k++) {
-    double4* out = reinterpret_cast<double4*>(s.LHS + 16 * (long)k);
-    if (m.ja[k] == n) {
-#pragma unroll
-      for (int q = 0; q < 4; q++)
-        out[q] = make_double4(D[4 * q], D[4 * q + 1], D[4 * q + 2], D[4 * q + 3]);
-      continue;
-    }
-    double B[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) B[q] = 0.;
-    if (JAC) {
-      int4 cs = m.csr_sub[k];
-      // row is the edge's L: += dF/dqR of each subedge; row is R: -= dF/dqL
-      const double* src = cs.z == 0 ? s.JR : s.JL;
-      for (int t = 0; t < 2; t++) {
-        int sub = t == 0 ? cs.x : cs.y;
-        if (sub < 0) break;
-        const double4* J = reinterpret_cast<const double4*>(src + 16 * (long)sub);
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-          double4 v = J[q];
-          if (cs.z == 0) {
-            B[4 * q] += v.x; B[4 * q + 1] += v.y; B[4 * q + 2] += v.z; B[4 * q + 3] += v.w;
-          } else {
-            B[4 * q] -= v.x; B[4 * q + 1] -= v.y; B[4 * q + 2] -= v.z; B[4 * q + 3] -= v.w;
-          }
-        }
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++)
-      out[q] = make_double4(B[4 * q], B[4 * q + 1], B[4 * q + 2], B[4 * q + 3]);
-  }
-  lu4(D);
-  double4* lo = reinterpret_cast<double4*>(s.LUd + 16 * (long)n);
-#pragma unroll
-  for (int q = 0; q < 4; q++) lo[q] = make_double4(D[4 * q], D[4 * q + 1], D[4 * q + 2], D[4 * q + 3]);
 }
 
 // LHS = 0 with V/dt on the diagonal blocks (init_memory.C:189-290).
@@ -941,8 +707,12 @@ __global__ void __launch_bounds__(128) k_sweep_ordered(DevMesh m, DevState s,
 // b_q - sum_k A_k[q,:] . dQ[col_k] over the row's off-diagonal blocks in
 // block order, with one multiply and three fused multiply-adds per block;
 // lane 0 then solves with the FP32 LU factors (reciprocal pivots).  Rows of
-// one colour share no block, so they run in parallel and in any order.  The
-// last sweep also writes the FP64 dQ the update reads.
+// one colour share no block, so they run in parallel and in any order.  All
+// loads that do not depend on the iterate (row record, blocks, columns, LU
+// factors) are issued before the neighbour gathers.  The last sweep also
+// writes the FP64 dQ the update reads.
+constexpr int kMixedMaxB = 12;  // off-diagonal blocks held in registers per row
+
 template <bool LAST>
 __global__ void __launch_bounds__(128) k_sweep_color32(DevState s, MixedTables mt, int p0,
                                                        int p1) {
@@ -952,35 +722,55 @@ __global__ void __launch_bounds__(128) k_sweep_color32(DevState s, MixedTables m
   const int qbase = threadIdx.x & ~3 & 31;
   const unsigned qmask = 0xFu << qbase;
   if (pp >= p1) return;  // whole quads leave together
-  const int n = mt.rows[pp];
-  float acc = __double2float_rn(s.RHS[4 * (long)n + q]);
-  const int b0 = mt.offd_ptr[pp], b1 = mt.offd_ptr[pp + 1];
+  const int4 rw = mt.rowinfo[pp];  // row, first block, end block
+  const int n = rw.x, b0 = rw.y, nb = rw.z - rw.y;
   const float4* A = reinterpret_cast<const float4*>(mt.lhs32);
   const float4* X = reinterpret_cast<const float4*>(mt.dq32);
-  int b = b0;
-  for (; b + 1 < b1; b += 2) {
-    const int c0 = mt.offd_col[b], c1 = mt.offd_col[b + 1];
-    const float4 a0 = A[4 * (long)b + q], a1 = A[4 * (long)(b + 1) + q];
-    const float4 d0 = X[c0], d1 = X[c1];
-    float t0 = __fmul_rn(a0.x, d0.x);
-    t0 = __fmaf_rn(a0.y, d0.y, t0);
-    t0 = __fmaf_rn(a0.z, d0.z, t0);
-    t0 = __fmaf_rn(a0.w, d0.w, t0);
-    float t1 = __fmul_rn(a1.x, d1.x);
-    t1 = __fmaf_rn(a1.y, d1.y, t1);
-    t1 = __fmaf_rn(a1.z, d1.z, t1);
-    t1 = __fmaf_rn(a1.w, d1.w, t1);
-    acc = __fsub_rn(acc, t0);
-    acc = __fsub_rn(acc, t1);
+  float4 M0 = make_float4(0.f, 0.f, 0.f, 0.f), M1 = M0, M2 = M0, M3 = M0;
+  if (q == 0) {
+    const float4* L = reinterpret_cast<const float4*>(mt.lu32) + 4 * (long)pp;
+    M0 = L[0]; M1 = L[1]; M2 = L[2]; M3 = L[3];
   }
-  if (b < b1) {
-    const int c0 = mt.offd_col[b];
-    const float4 a0 = A[4 * (long)b + q];
-    const float4 d0 = X[c0];
-    float t0 = __fmul_rn(a0.x, d0.x);
-    t0 = __fmaf_rn(a0.y, d0.y, t0);
-    t0 = __fmaf_rn(a0.z, d0.z, t0);
-    t0 = __fmaf_rn(a0.w, d0.w, t0);
+  int cols[kMixedMaxB];
+  float4 a[kMixedMaxB];
+#pragma unroll
+  for (int i = 0; i < kMixedMaxB; i++) {
+    if (i < nb) {
+      cols[i] = mt.offd_col[b0 + i];
+      a[i] = A[4 * (long)(b0 + i) + q];
+    }
+  }
+  float acc = __double2float_rn(s.RHS[4 * (long)n + q]);
+#pragma unroll
+  for (int i = 0; i < kMixedMaxB; i += 2) {
+    if (i + 1 < nb) {
+      const float4 d0 = X[cols[i]], d1 = X[cols[i + 1]];
+      float t0 = __fmul_rn(a[i].x, d0.x);
+      t0 = __fmaf_rn(a[i].y, d0.y, t0);
+      t0 = __fmaf_rn(a[i].z, d0.z, t0);
+      t0 = __fmaf_rn(a[i].w, d0.w, t0);
+      float t1 = __fmul_rn(a[i + 1].x, d1.x);
+      t1 = __fmaf_rn(a[i + 1].y, d1.y, t1);
+      t1 = __fmaf_rn(a[i + 1].z, d1.z, t1);
+      t1 = __fmaf_rn(a[i + 1].w, d1.w, t1);
+      acc = __fsub_rn(acc, t0);
+      acc = __fsub_rn(acc, t1);
+    } else if (i < nb) {
+      const float4 d0 = X[cols[i]];
+      float t0 = __fmul_rn(a[i].x, d0.x);
+      t0 = __fmaf_rn(a[i].y, d0.y, t0);
+      t0 = __fmaf_rn(a[i].z, d0.z, t0);
+      t0 = __fmaf_rn(a[i].w, d0.w, t0);
+      acc = __fsub_rn(acc, t0);
+    }
+  }
+  for (int i = kMixedMaxB; i < nb; i++) {  // rows with more blocks than the window
+    const float4 ai = A[4 * (long)(b0 + i) + q];
+    const float4 d0 = X[mt.offd_col[b0 + i]];
+    float t0 = __fmul_rn(ai.x, d0.x);
+    t0 = __fmaf_rn(ai.y, d0.y, t0);
+    t0 = __fmaf_rn(ai.z, d0.z, t0);
+    t0 = __fmaf_rn(ai.w, d0.w, t0);
     acc = __fsub_rn(acc, t0);
   }
   const float r0 = __shfl_sync(qmask, acc, qbase);
@@ -988,8 +778,6 @@ __global__ void __launch_bounds__(128) k_sweep_color32(DevState s, MixedTables m
   const float r2 = __shfl_sync(qmask, acc, qbase + 2);
   const float r3 = __shfl_sync(qmask, acc, qbase + 3);
   if (q != 0) return;
-  const float4* L = reinterpret_cast<const float4*>(mt.lu32) + 4 * (long)pp;
-  const float4 M0 = L[0], M1 = L[1], M2 = L[2], M3 = L[3];
   const float y0 = r0;
   const float y1 = __fmaf_rn(-M1.x, y0, r1);
   const float y2 = __fmaf_rn(-M2.y, y1, __fmaf_rn(-M2.x, y0, r2));
@@ -1010,7 +798,7 @@ __global__ void __launch_bounds__(128) k_sweep_color32(DevState s, MixedTables m
 // current dQ over instead, so that the buffer swap after the sweep keeps it.
 __global__ void k_prepare_sweep(DevState s, const double* cur, double* next, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i < 4 || i >= n) return;  // row 0 is unused (and stays zero)
   if (*s.stop || *s.skip)
     next[i] = cur[i];
   else
@@ -1119,7 +907,8 @@ __global__ void k_finalize_step(DevState s, double* hist_dq, double* hist_r, int
     double r = sqrt(tb);
     if (hist_dq) hist_dq[slot] = sqrt(ta);
     if (hist_r) hist_r[slot] = r;
-    if (first) s.scalars[6] = r;
+    // first < 0: the first step of the run is the one with no step done yet
+    if (first > 0 || (first < 0 && *s.steps_done == 0)) s.scalars[6] = r;
     *s.steps_done += 1;
     // stop once ||R_rho|| < drop * ||R_rho|| of the first step
     if (s.scalars[7] > 0. && r < s.scalars[7] * s.scalars[6]) *s.stop = 1;

@@ -1,0 +1,248 @@
+// flow_serve.cu - continuous-batching engine for steady solves on one GPU.
+//
+// A server owns an arena (one device allocation) and a table of slots.  A
+// submitted solve becomes a context carved from the arena with its own
+// stream; the server keeps up to two chunks of pseudo-time steps in flight
+// per running solve (CUDA-graph replays after the first chunk), reads each
+// chunk's {stop, status, steps} back through pinned memory without blocking,
+// and retires a solve when its density residual dropped by the requested
+// factor (the stop flag is raised on the device, so steps queued behind the
+// converged one do no work), when it reached its step limit, or on an error.
+// Solves of different meshes, orders, flow conditions and precisions run
+// side by side; each one's arithmetic is that of a context run alone, so its
+// result does not depend on what else is admitted.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "flow_gpu.h"
+#include "flow_internal.h"
+
+namespace {
+
+thread_local std::string g_serve_error;
+
+struct Slot {
+  flow_ctx* ctx = nullptr;
+  flow_params p{};
+  double drop = 0.;
+  int max_steps = 0;
+  long long tag = 0;
+  int state = 0;       // 0 free, 1 running, 2 finished (result not yet released)
+  int issued = 0;      // steps enqueued so far
+  int inflight = 0;    // chunks whose flags have not been read (0..2)
+  int next_flag = 0;   // flag slot of the next chunk
+  int oldest_flag = 0; // flag slot of the oldest chunk in flight
+  int status = 0, steps = 0;
+  double r_first = 0., r_last = 0., ms = 0.;
+};
+
+}  // namespace
+
+struct flow_server {
+  flow_arena* arena = nullptr;
+  int device = 0;
+  int chunk = 32;
+  std::vector<Slot> slots;
+  int running = 0;
+};
+
+namespace {
+
+void finish(Slot& sl, int status, int steps, int flag_slot) {
+  sl.state = 2;
+  sl.steps = steps;
+  sl.status = status;
+  sl.ms = flow::internal::run_ms(sl.ctx, flag_slot);
+  flow::internal::run_norms(sl.ctx, &sl.r_first, &sl.r_last);
+}
+
+// Queue one more chunk of steps for a running slot.
+int issue_chunk(flow_server* sv, Slot& sl) {
+  const int K = std::min(sv->chunk, sl.max_steps - sl.issued);
+  if (K <= 0) return 0;
+  int rc = flow::internal::enqueue_steps(sl.ctx, &sl.p, 1 + sl.issued, K);
+  if (rc) return rc;
+  sl.issued += K;
+  rc = flow::internal::post_flags(sl.ctx, sl.next_flag);
+  if (rc) return rc;
+  sl.next_flag ^= 1;
+  sl.inflight++;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* flow_server_last_error(void) { return g_serve_error.c_str(); }
+
+flow_server* flow_server_create(flow_arena* arena, int chunk, int max_slots, int* status) {
+  if (!arena || max_slots < 1) {
+    g_serve_error = "flow_server_create: null arena or max_slots < 1";
+    if (status) *status = FLOW_ERR_ARG;
+    return nullptr;
+  }
+  flow_server* sv = new flow_server();
+  sv->arena = arena;
+  sv->chunk = chunk > 0 ? chunk : 32;
+  sv->slots.resize(max_slots);
+  if (status) *status = 0;
+  return sv;
+}
+
+void flow_server_destroy(flow_server* sv) {
+  if (!sv) return;
+  for (auto& sl : sv->slots)
+    if (sl.ctx) flow_destroy(sl.ctx);
+  delete sv;
+}
+
+int flow_server_submit(flow_server* sv, const flow_grid_view* g, const flow_params* p,
+                       const double* Q0, int precision, double drop, int max_steps,
+                       long long tag, int* slot_out) {
+  if (!sv || !g || !p || !Q0 || !(drop > 0.) || max_steps < 1) {
+    g_serve_error = "flow_server_submit: bad argument";
+    return FLOW_ERR_ARG;
+  }
+  int idx = -1;
+  for (int i = 0; i < (int)sv->slots.size(); i++)
+    if (sv->slots[i].state == 0) { idx = i; break; }
+  if (idx < 0) {
+    g_serve_error = "flow_server_submit: every slot is busy";
+    return FLOW_ERR_BUDGET;
+  }
+  int st = 0;
+  flow_ctx* c = flow_create_in(sv->arena, g, p, &st);
+  if (!c) {
+    // a failed carve from the arena is a budget refusal, not an error
+    g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
+    return st == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : (st ? st : FLOW_ERR_ARG);
+  }
+  int rc = flow_set_precision(c, precision);
+  if (!rc) rc = flow_set_state(c, Q0);
+  if (!rc) rc = flow::internal::begin_run(c, p, drop);
+  if (rc) {
+    g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
+    flow_destroy(c);
+    return rc == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : rc;
+  }
+  Slot& sl = sv->slots[idx];
+  sl = Slot();
+  sl.ctx = c;
+  sl.p = *p;
+  sl.drop = drop;
+  sl.max_steps = max_steps;
+  sl.tag = tag;
+  sl.state = 1;
+  sv->running++;
+  // two chunks in flight from the start
+  rc = issue_chunk(sv, sl);
+  if (!rc) rc = issue_chunk(sv, sl);
+  if (rc) {
+    sl.state = 2;
+    sl.status = rc;
+    sv->running--;
+  }
+  if (slot_out) *slot_out = idx;
+  return 0;
+}
+
+int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int max_out,
+                         int* nout) {
+  if (!sv || (max_out > 0 && !out)) return FLOW_ERR_ARG;
+  int n = 0;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    bool any = false;
+    for (int i = 0; i < (int)sv->slots.size() && n < max_out; i++) {
+      Slot& sl = sv->slots[i];
+      if (sl.state != 1) continue;
+      int stop = 0, status = 0, steps = 0;
+      int r = flow::internal::flags_ready(sl.ctx, sl.oldest_flag, &stop, &status, &steps);
+      if (r == 0) continue;
+      any = true;
+      if (r < 0) status = FLOW_ERR_CUDA;
+      const int fs = sl.oldest_flag;
+      sl.oldest_flag ^= 1;
+      sl.inflight--;
+      bool done = stop || status || (sl.issued >= sl.max_steps && sl.inflight == 0);
+      if (done) {
+        // let the chunk still in flight (no-op steps after the stop) drain
+        if (sl.inflight > 0) cudaStreamSynchronize(flow::internal::stream_of(sl.ctx));
+        sl.inflight = 0;
+        finish(sl, status ? status : (stop ? 0 : FLOW_ERR_NOT_CONVERGED), steps, fs);
+        sv->running--;
+        flow_completion& cpl = out[n++];
+        cpl.tag = sl.tag;
+        cpl.slot = i;
+        cpl.status = sl.status;
+        cpl.steps = sl.steps;
+        cpl.r_first = sl.r_first;
+        cpl.r_last = sl.r_last;
+        cpl.device_ms = sl.ms;
+        continue;
+      }
+      if (sl.issued < sl.max_steps) {
+        int rc = issue_chunk(sv, sl);
+        if (rc) {
+          if (sl.inflight > 0) cudaStreamSynchronize(flow::internal::stream_of(sl.ctx));
+          sl.inflight = 0;
+          finish(sl, rc, steps, fs);
+          sv->running--;
+          flow_completion& cpl = out[n++];
+          cpl.tag = sl.tag;
+          cpl.slot = i;
+          cpl.status = rc;
+          cpl.steps = steps;
+          cpl.r_first = sl.r_first;
+          cpl.r_last = sl.r_last;
+          cpl.device_ms = sl.ms;
+        }
+      }
+    }
+    if (n > 0 || wait_us <= 0 || sv->running == 0) break;
+    const auto dt = std::chrono::duration_cast<std::chrono::microseconds>(
+                        std::chrono::steady_clock::now() - t0)
+                        .count();
+    if (dt >= wait_us) break;
+    if (!any) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  if (nout) *nout = n;
+  return 0;
+}
+
+int flow_server_result(flow_server* sv, int slot, double* Q, long nQ, double* forces) {
+  if (!sv || slot < 0 || slot >= (int)sv->slots.size()) return FLOW_ERR_ARG;
+  Slot& sl = sv->slots[slot];
+  if (sl.state != 2 || !sl.ctx) {
+    g_serve_error = "flow_server_result: slot has no finished solve";
+    return FLOW_ERR_ARG;
+  }
+  int rc = 0;
+  if (Q) rc |= flow_get(sl.ctx, "Q", Q, nQ);
+  if (forces) rc |= flow_body_forces(sl.ctx, &sl.p, forces);
+  return rc;
+}
+
+int flow_server_release(flow_server* sv, int slot) {
+  if (!sv || slot < 0 || slot >= (int)sv->slots.size()) return FLOW_ERR_ARG;
+  Slot& sl = sv->slots[slot];
+  if (sl.state == 1) {
+    g_serve_error = "flow_server_release: the solve is still running";
+    return FLOW_ERR_ARG;
+  }
+  if (sl.ctx) flow_destroy(sl.ctx);
+  sl = Slot();
+  return 0;
+}
+
+int flow_server_running(flow_server* sv) { return sv ? sv->running : -1; }
+
+}  // extern "C"

@@ -56,7 +56,7 @@ struct DevMesh {
   const int* st_ptr;
   const int* st_idx;
   const double* st_w;
-  const double* svd_U1;    // per node: 5 columns of U, column-major, offset 5*st_ptr[i]
+  const double* svd_U1;    // per node: first 5 columns of U, row by row, offset 5*st_ptr[i]
   const double* svd_VT;    // 25 per node
   const double* svd_S;     // 5 per node
 };
@@ -69,6 +69,7 @@ struct MixedTables {
   const int* rows;        // nn: row at each position (colour-sorted, ascending)
   const int* pos;         // nn+1: position of each row
   const int* offd_ptr;    // nn+1: first off-diagonal block of each position
+  const int4* rowinfo;    // nn: {row, first block, end block, 0} of each position
   const int* offd_col;    // column (row index) of each off-diagonal block
   float* lhs32;           // 16 floats per off-diagonal block, row-major
   float* lu32;            // 16 floats per position: LU factors, reciprocal pivots
@@ -103,6 +104,7 @@ struct DevState {
   int* skip;        // set when the linear residual dropped below 1e-15
   int* stop;        // set once the run's density residual dropped below its target
   int* steps_done;  // pseudo-time steps completed since the last reset
+  int* citer;       // pseudo-time step index of the step in flight (drives the CFL ramp)
   double* partial;  // reduction partials
   double* scalars;  // [0] rms, [1] dq^2, [2] R_rho^2, [3] cfl, [4] F_lift, [5] F_drag,
                     // [6] R_rho of the run's first step, [7] target drop (0 = none)

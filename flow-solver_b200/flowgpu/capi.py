@@ -19,16 +19,22 @@ DP = C.POINTER(C.c_double)
 LP = C.POINTER(C.c_long)
 
 ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
-          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND", 256: "NOT_CONVERGED"}
+          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND", 256: "NOT_CONVERGED", 512: "BUDGET"}
+ERR_NOT_CONVERGED = 256
+ERR_BUDGET = 512
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
-           "flow_set_sweep_mode", "flow_set_precision", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_set_sweep_mode", "flow_set_precision", "flow_set_graphs", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
-           "flow_linear_residual_noalloc")
+           "flow_linear_residual_noalloc", "flow_arena_create", "flow_arena_destroy",
+           "flow_arena_free_bytes", "flow_arena_largest_free", "flow_create_in",
+           "flow_ctx_device_bytes", "flow_server_create", "flow_server_destroy",
+           "flow_server_submit", "flow_server_progress", "flow_server_result",
+           "flow_server_release", "flow_server_running", "flow_server_last_error")
 
 
 class FlowParamsC(C.Structure):
@@ -95,6 +101,7 @@ def load():
     L.flow_size.argtypes = [vp, C.c_char_p]
     L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
     L.flow_set_precision.argtypes = [vp, C.c_int]
+    L.flow_set_graphs.argtypes = [vp, C.c_int]
     L.flow_save_state.argtypes = [vp]
     L.flow_restore_state.argtypes = [vp]
     L.flow_set_timing.argtypes = [vp, C.c_int]
@@ -109,6 +116,27 @@ def load():
     L.flow_last_device_ms.restype = C.c_double
     L.flow_last_device_ms.argtypes = [vp]
     L.flow_linear_residual_noalloc.argtypes = [vp, vp, vp, vp, vp, C.c_int, C.c_long, vp, DP]
+    L.flow_arena_create.restype = vp
+    L.flow_arena_create.argtypes = [C.c_int, C.c_longlong, IP]
+    L.flow_arena_destroy.argtypes = [vp]
+    L.flow_arena_free_bytes.restype = C.c_longlong
+    L.flow_arena_free_bytes.argtypes = [vp]
+    L.flow_arena_largest_free.restype = C.c_longlong
+    L.flow_arena_largest_free.argtypes = [vp]
+    L.flow_create_in.restype = vp
+    L.flow_create_in.argtypes = [vp, C.POINTER(FlowGridView), PP, IP]
+    L.flow_ctx_device_bytes.restype = C.c_longlong
+    L.flow_ctx_device_bytes.argtypes = [vp]
+    L.flow_server_create.restype = vp
+    L.flow_server_create.argtypes = [vp, C.c_int, C.c_int, IP]
+    L.flow_server_destroy.argtypes = [vp]
+    L.flow_server_submit.argtypes = [vp, C.POINTER(FlowGridView), PP, DP, C.c_int, C.c_double,
+                                     C.c_int, C.c_longlong, IP]
+    L.flow_server_progress.argtypes = [vp, C.c_int, C.POINTER(FlowCompletion), C.c_int, IP]
+    L.flow_server_result.argtypes = [vp, C.c_int, DP, C.c_long, DP]
+    L.flow_server_release.argtypes = [vp, C.c_int]
+    L.flow_server_running.argtypes = [vp]
+    L.flow_server_last_error.restype = C.c_char_p
     _lib = L
     return L
 
@@ -126,6 +154,96 @@ def linear_residual_noalloc(ia: int, ja: int, lhs: int, rhs: int, x: int, nn: in
 
 
 NOALLOC_MAX_ROWS = 262144
+
+
+class FlowCompletion(C.Structure):
+    _fields_ = [("tag", C.c_longlong), ("slot", C.c_int), ("status", C.c_int),
+                ("steps", C.c_int), ("r_first", C.c_double), ("r_last", C.c_double),
+                ("device_ms", C.c_double)]
+
+
+class Arena:
+    """flow_arena: one device allocation that contexts are carved from."""
+
+    def __init__(self, nbytes: int, device: int = 0):
+        self.L = load()
+        st = C.c_int(0)
+        self.h = self.L.flow_arena_create(int(device), int(nbytes), C.byref(st))
+        if not self.h:
+            raise FlowError(st.value or 2, "flow_arena_create " + self.L.flow_last_error().decode())
+        self.device = device
+
+    def free_bytes(self) -> int:
+        return self.L.flow_arena_free_bytes(self.h)
+
+    def largest_free(self) -> int:
+        return self.L.flow_arena_largest_free(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.flow_arena_destroy(self.h)
+            self.h = None
+
+
+class Server:
+    """flow_server: continuous batching of steady solves in an arena.
+
+    submit() returns a slot or None when the arena / slot table is full
+    (FLOW_ERR_BUDGET); progress() returns retired solves as dicts."""
+
+    def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64):
+        self.L = load()
+        st = C.c_int(0)
+        self.arena = arena
+        self.h = self.L.flow_server_create(arena.h, int(chunk), int(max_slots), C.byref(st))
+        if not self.h:
+            raise FlowError(st.value or 1, "flow_server_create")
+        self._keep = {}
+        self._out = (FlowCompletion * 64)()
+
+    def submit(self, mesh, params, Q0, precision: int = 1, drop: float = 1e-10,
+               max_steps: int = 20000, tag: int = 0):
+        p = params_struct(params)
+        q = np.ascontiguousarray(Q0, dtype=np.float64)
+        slot = C.c_int(-1)
+        rc = self.L.flow_server_submit(self.h, C.byref(mesh.view), C.byref(p),
+                                       q.ctypes.data_as(DP), int(precision), float(drop),
+                                       int(max_steps), int(tag), C.byref(slot))
+        if rc == ERR_BUDGET:
+            return None
+        if rc:
+            raise FlowError(rc, "flow_server_submit " + self.L.flow_server_last_error().decode())
+        self._keep[slot.value] = (mesh, p)
+        return slot.value
+
+    def progress(self, wait_us: int = 0) -> list:
+        n = C.c_int(0)
+        _check(self.L.flow_server_progress(self.h, int(wait_us), self._out, len(self._out),
+                                           C.byref(n)), "flow_server_progress")
+        return [{"tag": c.tag, "slot": c.slot, "status": c.status, "steps": c.steps,
+                 "r_first": c.r_first, "r_last": c.r_last, "device_ms": c.device_ms}
+                for c in self._out[:n.value]]
+
+    def result(self, slot: int, want_q: bool = True):
+        mesh, p = self._keep[slot]
+        v = mesh.view
+        q = np.zeros((v.nn + v.nn_ghost + 1) * 4) if want_q else None
+        f = (C.c_double * 2)()
+        _check(self.L.flow_server_result(self.h, slot, q.ctypes.data_as(DP) if want_q else None,
+                                         q.size if want_q else 0, f), "flow_server_result")
+        return q, (f[0], f[1])
+
+    def release(self, slot: int):
+        _check(self.L.flow_server_release(self.h, slot), "flow_server_release")
+        self._keep.pop(slot, None)
+
+    def running(self) -> int:
+        return self.L.flow_server_running(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.flow_server_destroy(self.h)
+            self.h = None
 
 
 def params_struct(fp) -> FlowParamsC:
@@ -301,6 +419,10 @@ class Solver:
     def set_precision(self, mode: int):
         """0: FP64 reference-order drop-in; 1: FP32 blocks, multicolour sweeps."""
         _check(self.L.flow_set_precision(self.ctx, int(mode)), "flow_set_precision")
+
+    def set_graphs(self, on: bool):
+        """Replay full chunks of flow_converge steps from CUDA graphs (default on)."""
+        _check(self.L.flow_set_graphs(self.ctx, int(bool(on))), "flow_set_graphs")
 
     def set_sweep_mode(self, mode: int):
         _check(self.L.flow_set_sweep_mode(self.ctx, int(mode)), "flow_set_sweep_mode")

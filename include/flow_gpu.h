@@ -33,6 +33,7 @@ extern "C" {
 #define FLOW_ERR_SWEEP_TIMEOUT 64 /* an ordered sweep waited past its bound */
 #define FLOW_ERR_NOT_FOUND 128  /* unknown array name */
 #define FLOW_ERR_NOT_CONVERGED 256 /* flow_converge reached max_steps */
+#define FLOW_ERR_BUDGET 512     /* the arena (or the server's slot table) has no room now */
 
 /* Mirrors PARAMS (include/params.h:19-76 of the reference), same field
  * order and meaning as euler.params (params.C:44-217). */
@@ -211,6 +212,13 @@ int flow_set_sweep_mode(flow_ctx *ctx, int mode);
  * rms = -1.  The first switch to mode 1 builds the colour tables. */
 int flow_set_precision(flow_ctx *ctx, int mode);
 
+/* flow_converge / flow_converge_batch issue steps in chunks; with graphs on
+ * (the default) every full chunk after the first is replayed from a CUDA
+ * graph captured once per chunk length, with the step index and the CFL
+ * ramp advancing on the device.  Results are identical either way; off
+ * launches every kernel from the host. */
+int flow_set_graphs(flow_ctx *ctx, int on);
+
 /* Device snapshot of the solution state (Q, nQ, pQ and the boundary normals
  * the k=2 pass rewrites): flow_save_state keeps a copy on the device,
  * flow_restore_state puts it back (pre-emption / restart without host
@@ -238,6 +246,59 @@ const char *flow_last_error(void);
 long flow_launch_count(flow_ctx *ctx);
 /* Device time (ms) of the last flow_run / flow_solve call, CUDA events. */
 double flow_last_device_ms(flow_ctx *ctx);
+
+/* ---- Device arena (no counterpart in the reference) ----------------------
+ * One cudaMalloc of `bytes` on `device`, carved into the buffers of the
+ * contexts created in it (256-byte aligned, first fit, freed blocks merge).
+ * It is the HBM budget of the serving engine.  Destroy its contexts first. */
+typedef struct flow_arena flow_arena;
+flow_arena *flow_arena_create(int device, long long bytes, int *status);
+void flow_arena_destroy(flow_arena *arena);
+long long flow_arena_free_bytes(flow_arena *arena);
+long long flow_arena_largest_free(flow_arena *arena);
+/* flow_create with every device buffer carved from `arena` (on its device);
+ * NULL with *status = FLOW_ERR_CUDA when the arena has no room. */
+flow_ctx *flow_create_in(flow_arena *arena, const flow_grid_view *g, const flow_params *p,
+                         int *status);
+/* Device bytes a context holds. */
+long long flow_ctx_device_bytes(flow_ctx *ctx);
+
+/* ---- Serving engine (no counterpart in the reference) ---------------------
+ * Continuous batching of steady solves on one GPU: each submitted solve gets
+ * a context in the arena (admission fails with FLOW_ERR_BUDGET while the
+ * arena or the slot table is full) and its own stream; flow_server_progress
+ * keeps two chunks of `chunk` pseudo-time steps in flight per running solve
+ * and retires solves whose ||R_rho|| dropped by `drop` (status 0), that hit
+ * max_steps (FLOW_ERR_NOT_CONVERGED) or failed.  Solves of any mesh, order,
+ * flow condition and precision (flow_set_precision modes) share the GPU; each
+ * one's iterates are those it has when run alone.  Single-threaded: call a
+ * server from one host thread. */
+typedef struct flow_server flow_server;
+typedef struct {
+  long long tag;     /* the submitter's tag */
+  int slot;          /* slot to read with flow_server_result, then release */
+  int status;        /* 0 converged, FLOW_ERR_NOT_CONVERGED, or error bits */
+  int steps;         /* pseudo-time steps taken */
+  double r_first;    /* ||R_rho|| of the first step */
+  double r_last;     /* ||R_rho|| of the last step */
+  double device_ms;  /* device time from submission to retirement */
+} flow_completion;
+flow_server *flow_server_create(flow_arena *arena, int chunk, int max_slots, int *status);
+void flow_server_destroy(flow_server *srv);
+int flow_server_submit(flow_server *srv, const flow_grid_view *g, const flow_params *p,
+                       const double *Q0, int precision, double drop, int max_steps,
+                       long long tag, int *slot);
+/* Launch further chunks and collect retired solves (at most max_out); waits
+ * up to wait_us microseconds for at least one when none is ready. */
+int flow_server_progress(flow_server *srv, int wait_us, flow_completion *out, int max_out,
+                         int *nout);
+/* Converged state Q ((nn+nn_ghost+1)*4 doubles, may be NULL) and the raw
+ * lift/drag forces (may be NULL) of a retired solve. */
+int flow_server_result(flow_server *srv, int slot, double *Q, long nQ, double *forces);
+/* Free a retired solve's context (its arena memory returns to the pool). */
+int flow_server_release(flow_server *srv, int slot);
+int flow_server_running(flow_server *srv);
+const char *flow_server_last_error(void);
 
 /* ---- b - A x RMS with no device allocation ------------------------------
  * No counterpart in the reference.  It computes the b - A x RMS that

@@ -1,0 +1,88 @@
+"""The serving engine (flow_server over a flow_arena): solves of different
+meshes, orders, flow conditions and precisions admitted together give, each,
+the result the same solve gives alone (bit for bit: same steps, state and
+forces), and admission respects the arena's budget."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MIX = [  # nc, nr, curved, order, mach, alpha, precision, subits
+    (64, 16, True, 3, 0.8, 1.25, 1, 4),
+    (32, 8, False, 1, 0.5, 1.25, 0, 2),
+    (48, 12, True, 3, 0.6, -2.0, 0, 2),
+    (96, 24, True, 3, 0.75, 3.0, 1, 3),
+    (40, 10, False, 1, 0.4, 4.0, 1, 3),
+]
+
+
+def _case(nc, nr, curved, order, mach, alpha, subits):
+    from flowgpu import workloads
+    from flowgpu.prep import Mesh
+    wl = workloads.Workload(f"srv{nc}x{nr}", nc, nr, curved, order, mach, alpha=alpha,
+                            subits=subits, max_steps=400)
+    mesh = Mesh.from_case(wl.write(), order=order)
+    return wl, mesh
+
+
+def test_mixed_admission_matches_solves_run_alone():
+    from flowgpu import capi
+    cases = [(_case(nc, nr, cv, o, m, a, sub), prec)
+             for (nc, nr, cv, o, m, a, prec, sub) in MIX]
+    alone = []
+    for (wl, mesh), prec in cases:
+        fp = wl.params()
+        s = capi.Solver.from_mesh(mesh, fp, device=0)
+        s.set_precision(prec)
+        s.set_state(mesh.initial_state(fp))
+        steps, r0, r1 = s.converge(1, wl.max_steps, 1e-10, chunk=32, check=False)
+        assert s.status() == 0
+        alone.append((steps, s.get("Q"), s.body_forces(), r1 < 1e-10 * r0))
+        s.close()
+    arena = capi.Arena(2 << 30)
+    srv = capi.Server(arena, chunk=16, max_slots=8)
+    for i, ((wl, mesh), prec) in enumerate(cases):
+        fp = wl.params()
+        slot = srv.submit(mesh, fp, mesh.initial_state(fp), precision=prec, drop=1e-10,
+                          max_steps=wl.max_steps, tag=i)
+        assert slot is not None
+    got = {}
+    while srv.running() > 0 or len(got) < len(cases):
+        for c in srv.progress(wait_us=2000):
+            q, f = srv.result(c["slot"])
+            got[c["tag"]] = (c, q, f)
+            srv.release(c["slot"])
+    for i, (steps, q, f, converged) in enumerate(alone):
+        c, q2, f2 = got[i]
+        assert c["steps"] == steps, (i, c["steps"], steps)
+        assert c["status"] == (0 if converged else capi.ERR_NOT_CONVERGED)
+        assert np.array_equal(q[4:], q2[4:]), i
+        assert f == f2, i
+    srv.close()
+    arena.close()
+
+
+def test_admission_waits_for_arena_room():
+    from flowgpu import capi
+    (wl, mesh) = _case(64, 16, True, 3, 0.8, 1.25, 4)
+    fp = wl.params()
+    probe = capi.Solver.from_mesh(mesh, fp, device=0)
+    probe.set_precision(1)
+    need = probe.L.flow_ctx_device_bytes(probe.ctx)
+    probe.close()
+    arena = capi.Arena(int(need * 1.5))  # room for one context, not two
+    srv = capi.Server(arena, chunk=16, max_slots=4)
+    s0 = srv.submit(mesh, fp, mesh.initial_state(fp), precision=1, max_steps=64)
+    assert s0 is not None
+    assert srv.submit(mesh, fp, mesh.initial_state(fp), precision=1, max_steps=64) is None
+    done = []
+    while not done:
+        done = srv.progress(wait_us=5000)
+    srv.release(done[0]["slot"])
+    s1 = srv.submit(mesh, fp, mesh.initial_state(fp), precision=1, max_steps=64)
+    assert s1 is not None
+    while srv.running():
+        for c in srv.progress(wait_us=5000):
+            srv.release(c["slot"])
+    srv.close()
+    arena.close()
