@@ -4,29 +4,39 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl flow|reference]
                     [--workload NAME]
 
-A "step" is one complete steady solve of the workload: pseudo-time steps of
-the reference's solve() (residual, Jacobian, two ordered block Gauss-Seidel
-sweeps, update) until the density residual norm has dropped by 1e-10.
+Default workload: the batching form ``batch16`` -- 16 independent steady
+solves per GPU from the seeded request stream (meshes of 2k..200k nodes,
+Mach 0.3..0.85, angle of attack -4..6 degrees, k=1 or k=2), admitted
+together to the serving engine (one device arena, one stream per solve,
+CUDA-graph chunks of pseudo-time steps) in the precision form (FP32 blocks,
+multicolour Gauss-Seidel), each retired at a 1e-10 drop of ||R_rho|| or at
+its step limit.  A "step" of this benchmark is one pass over the batch.
 
-* value: solves/s with the initial state already on the device (restored
-  from a device snapshot), timed with CUDA events on the library's stream.
-* e2e: the same through the C ABI with host buffers: the initial state is
-  copied from pinned host memory, the converged solution and the lift/drag
-  forces are copied back, inside the timed region.
-* roofline: the ordered sweep kernel (the largest share of a step) against
-  the measured HBM copy bandwidth, with the compulsory bytes of one sweep
-  (132 B per matrix block + 96 B per node).
-* cpu_baseline: the reference solver (oracle/_ref, built from its own
-  sources) on this host, a bounded sample of pseudo-time steps extrapolated
-  with the workload's converged step count.
+* value: converged solves / device time of the passes (CUDA events), with
+  every mesh and initial state already on the device (staged).
+* e2e: the same through the C ABI from host buffers: staging (mesh arrays
+  and state copied to the device) and the read-back of every converged
+  state and of the lift/drag forces inside the timed region.
+* latency: p50/p95/p99 of the per-solve device time from start to retirement.
+* plain_fp64: the same requests solved one at a time by the FP64 drop-in
+  (bit-identical to the reference): the recorded FP64 step count of each
+  request x its measured FP64 ms/step.
+* roofline: k_node_prepare4 (the largest kernel of a step) on the batch's
+  largest mesh, compulsory bytes over its measured duration against the
+  measured HBM copy bandwidth.
+* cpu_baseline: the reference (oracle/_ref, built from its own sources) on
+  one host core, timed on the smallest meshes of the batch and scaled by node
+  count to every request's recorded step count.
 
-Multi-GPU (torchrun, one process per GPU): every rank runs its own replica of
-the solve (the path does not shard), value = all ranks' solves / the slowest
-rank's time ("scaling": "weak").
+Single-mesh workloads (``--workload ogrid512x128_k2_m080`` ...) time the
+plain FP64 drop-in: one solve per step, value = solves/s.
 
---impl reference times the reference's own CPU solver on all host cores
-(one process per core, each timing a bounded sample of the workload's
-pseudo-time steps), rank 0 only.
+Multi-GPU (torchrun, one process per GPU): each rank serves its own requests
+(the batch's next 16 of the stream), value = all ranks' converged solves /
+the slowest rank's time ("scaling": "weak"); no device collective.
+
+--impl reference times the reference's own CPU solver on all host cores,
+rank 0 only.
 """
 from __future__ import annotations
 
@@ -40,12 +50,14 @@ import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# many solves share the GPU, one stream each: let their kernels overlap
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 PKG = os.path.join(ROOT, "flow-solver_b200")
 for p in (ROOT, PKG):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-METRIC = "converged solves/s (1e-10 drop of ||R_rho||), steady k=2 Euler, FP64"
+METRIC = "converged solves/s (1e-10 drop) served vs plain FP64 GPU; p50/p99 latency"
 UNIT = "solves/s"
 REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
 CPU_BASELINE_STEPS = 6      # pseudo-time steps timed for cpu_baseline
@@ -148,6 +160,15 @@ def allreduce_max(pg, v: float) -> float:
     import torch
     t = torch.tensor([v], dtype=torch.float64)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(pg, v: float) -> float:
+    if pg is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -277,6 +298,237 @@ def run_flow(args):
         pg.destroy_process_group()
 
 
+def ncu_traffic(workload: str, key: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(workload, {}).get(key)
+    except Exception:
+        return None
+
+
+def _view_bytes(mesh) -> int:
+    """Bytes of the grid arrays a caller passes through flow_grid_view."""
+    return int(sum(a.nbytes for a in mesh.arrays().values() if a is not None))
+
+
+def _lpt_makespan(times, workers: int) -> float:
+    """Makespan of independent jobs on `workers` identical workers, longest
+    job first to the least loaded worker."""
+    loads = [0.0] * max(1, workers)
+    for t in sorted(times, reverse=True):
+        k = loads.index(min(loads))
+        loads[k] += t
+    return max(loads)
+
+
+def run_batch(args, bw):
+    import numpy as np
+    import torch
+    from flowgpu import capi, roofline, serve
+
+    world, rank, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    reqs = [serve.sample_request(rank * bw.n + i, seed=bw.seed) for i in range(bw.n)]
+    t0 = time.time()
+    prep = serve.prepare_all(reqs, bw.subits, bw.max_steps, bw.drop)
+    prep_s = time.time() - t0
+    free, _total = torch.cuda.mem_get_info(local)
+    arena = capi.Arena(int(min(free * 0.85, 150e9)), device=local)
+    h2d = sum(_view_bytes(p.mesh) + p.Q0.nbytes for p in prep)
+    d2h = sum(p.Q0.nbytes + 16 for p in prep)
+    log(f"[rank {rank}] {bw.name}: {bw.n} requests, {sum(r.nodes for r in reqs)} nodes, "
+        f"host preprocessing {prep_s:.1f}s")
+
+    def one_pass():
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n)
+        torch.cuda.synchronize()
+        ev[0].record()
+        slots = []
+        for i, pr in enumerate(prep):  # context + mesh arrays + state to the device
+            sl = srv.submit(pr.mesh, pr.params, pr.Q0, precision=bw.precision, drop=bw.drop,
+                            max_steps=bw.max_steps, tag=i, hold=True)
+            if sl is None:
+                raise RuntimeError("the device arena cannot hold the whole batch")
+            slots.append(sl)
+        torch.cuda.synchronize()
+        ev[1].record()
+        for sl in slots:
+            srv.start(sl)
+        recs = {}
+        while len(recs) < len(slots):
+            for c in srv.progress(wait_us=500):
+                recs[c["tag"]] = c
+        torch.cuda.synchronize()
+        ev[2].record()
+        forces = {}
+        for i, c in recs.items():  # converged states and forces back to the host
+            if c["status"] in (0, capi.ERR_NOT_CONVERGED):
+                _q, forces[i] = srv.result(c["slot"], want_q=True)
+            srv.release(c["slot"])
+        ev[3].record()
+        torch.cuda.synchronize()
+        srv.close()
+        return ([recs[i] for i in range(len(slots))], forces,
+                ev[1].elapsed_time(ev[2]), ev[0].elapsed_time(ev[3]))
+
+    first = None
+    for _ in range(args.warmup):
+        recs, _f, _a, _b = one_pass()
+        sig = [(r["status"], r["steps"]) for r in recs]
+        if first is None:
+            first = sig
+        elif sig != first:
+            raise RuntimeError("non-deterministic batch: step counts differ between passes")
+    barrier(pg)
+    dev_ms = e2e_ms = 0.
+    lat, launches, n_conv, n_fail = [], 0, 0, 0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            recs, forces, v_ms, e_ms = one_pass()
+            dev_ms += v_ms
+            e2e_ms += e_ms
+            lat += [r["device_ms"] / 1e3 for r in recs]
+            launches += sum(r["launches"] for r in recs)
+            n_conv += sum(1 for r in recs if r["status"] == 0)
+            n_fail += sum(1 for r in recs if r["status"] not in (0, capi.ERR_NOT_CONVERGED))
+    barrier(pg)
+    dev_ms_max = allreduce_max(pg, dev_ms)
+    e2e_ms_max = allreduce_max(pg, e2e_ms)
+    n_conv_all = allreduce_sum(pg, n_conv)
+    value = n_conv_all / (dev_ms_max / 1e3)
+    e2e = n_conv_all / (e2e_ms_max / 1e3)
+
+    # ---- roofline: k_node_prepare4 on the largest mesh of the batch, served form ----
+    big = max(prep, key=lambda p: p.req.nodes)
+    s = capi.Solver.from_mesh(big.mesh, big.params, device=local)
+    s.set_precision(bw.precision)
+    s.set_state(big.Q0)
+    s.run(1, 8)
+    s.set_timing(True)
+    s.run(9, 24)
+    kt = s.kernel_times()
+    s.close()
+    peaks, peak_kind = measured_peaks()
+    cnt, ms = kt["node_prepare"]
+    np_ms = ms / max(cnt, 1)
+    np_bytes = roofline.node_prepare_bytes(big.mesh)
+    achieved = np_bytes / (np_ms * 1e-3) / 1e9
+    share = ms / max(sum(v[1] for v in kt.values()), 1e-30)
+    roof = {"bound": "hbm", "kernel": "k_node_prepare4", "mesh": f"{big.req.nc}x{big.req.nr}",
+            "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+            "traffic": ncu_traffic(f"{bw.name}:{big.req.nc}x{big.req.nr}", "node_prepare_dram_bytes"),
+            "algorithmic_bytes_per_launch": np_bytes, "avg_launch_ms": round(np_ms, 4),
+            "share_of_step": round(share, 3),
+            "kernels_ms": {k: round(t / max(c, 1), 4) for k, (c, t) in kt.items() if c}}
+
+    # ---- plain FP64 drop-in on the same requests, one at a time ----
+    plain = None
+    if bw.fp64_steps is not None and rank == 0 and world == 1:
+        tot = 0.
+        per = []
+        for i, pr in enumerate(prep):
+            s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params, subits=2),
+                                      device=local)
+            s.set_state(pr.Q0)
+            n = 96
+            s.converge(1, n, 1e-300, chunk=32, check=False)
+            ms_step = s.last_device_ms() / n
+            s.close()
+            per.append(round(ms_step, 4))
+            tot += bw.fp64_steps[i] * ms_step / 1e3
+        conv64 = sum(1 for st in bw.fp64_status if st == 0)
+        plain = {"value": round(conv64 / tot, 5), "unit": UNIT, "converged": conv64,
+                 "seconds": round(tot, 2), "ms_per_step": per,
+                 "how": "recorded FP64 step count of each request (capped at max_steps) x its "
+                        "FP64 drop-in ms/step measured over 96 steps (graph chunks), solved "
+                        "one after the other"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and bw.fp64_steps is not None:
+        cpu = batch_cpu_baseline(prep, bw)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dev_ms_max / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": bw.name, "form": "batching (served, all admitted together)",
+                       "requests_per_gpu": bw.n, "stream_seed": bw.seed,
+                       "nodes": [r.nodes for r in reqs], "orders": [r.order for r in reqs],
+                       "precision": "FP64 residual/geometry/update, FP32 blocks + multicolour "
+                                    "GS" if bw.precision == 1 else f"mode {bw.precision}",
+                       "gs_sweeps": bw.subits, "drop": bw.drop, "max_steps": bw.max_steps,
+                       "converged_per_pass": n_conv // max(args.steps, 1),
+                       "failed_per_pass": n_fail // max(args.steps, 1),
+                       "l2": "working set larger than L2 (batch of meshes, 0.1-0.5 GB each)",
+                       "parallelism": f"requests sharded over {world} GPU(s)"},
+            "latency_s": serve.percentiles(lat),
+            "plain_fp64": plain,
+            "e2e": {"value": round(e2e, 5), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "roofline": roof, "gpu_launches": int(launches),
+            "clocks": clk.summary(), "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    arena.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def batch_cpu_baseline(prep, bw) -> dict:
+    """The reference on one host core: set-up and first step untimed, then
+    CPU_BASELINE_STEPS steps timed on each of the 4 smallest meshes; the cost
+    per node-step of each order scales every request to its recorded step
+    count."""
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "oracle/_ref/libflowref.so not built"}
+    per_node = {}
+    small = sorted(prep, key=lambda p: p.req.nodes)[:4]
+    for pr in small:
+        r = ref.RefSolver(pr.wl.write())
+        r.solve(1)
+        t0 = time.perf_counter()
+        for ts in range(2, 2 + CPU_BASELINE_STEPS):
+            r.solve(ts)
+        dt = (time.perf_counter() - t0) / CPU_BASELINE_STEPS
+        r.close()
+        per_node.setdefault(pr.req.order, []).append(dt / pr.req.nodes)
+    cost = {o: sum(v) / len(v) for o, v in per_node.items()}
+    fallback = sum(cost.values()) / len(cost)
+    total = sum(bw.fp64_steps[i] * pr.req.nodes * cost.get(pr.req.order, fallback)
+                for i, pr in enumerate(prep))
+    conv64 = sum(1 for st in bw.fp64_status if st == 0)
+    return {"value": round(conv64 / total, 8), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{CPU_BASELINE_STEPS} timed steps on each of the {len(small)} smallest "
+                      f"meshes ({', '.join(str(p.req.nodes) for p in small)} nodes); "
+                      f"s per node-step by order {dict((o, f'{c:.3e}') for o, c in cost.items())}"
+                      f" x recorded FP64 steps of all {len(prep)} requests"}
+
+
+def measure_fp64(args, bw):
+    """Record the FP64 drop-in's step count and status on every request of
+    the batch (the reference's own, since the drop-in is bit-identical)."""
+    import torch
+    from flowgpu import capi, serve
+    torch.cuda.set_device(0)
+    reqs = [serve.sample_request(i, seed=bw.seed) for i in range(bw.n)]
+    prep = serve.prepare_all(reqs, 2, bw.max_steps, bw.drop)
+    r = serve.run_sequential(prep, precision=0)
+    steps = tuple(x["steps"] for x in r["records"])
+    status = tuple(x["status"] for x in r["records"])
+    print(json.dumps({"workload": bw.name, "fp64_steps": steps, "fp64_status": status,
+                      "seconds": round(r["total_s"], 2),
+                      "forces": [x["forces"] for x in r["records"]]}), flush=True)
+
+
 def cpu_baseline(casedir: str, steps_conv: int) -> dict:
     """The reference solver on this host: set-up and its first step (which
     grows the k=2 stencils and factors them), then CPU_BASELINE_STEPS timed
@@ -350,6 +602,74 @@ def _ref_worker(args_tuple):
     return dt / (steps * REF_SAMPLE_STEPS)
 
 
+def _ref_batch_worker(args_tuple):
+    casedir, warmup, steps = args_tuple
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+    r = ref.RefSolver(casedir)
+    r.solve(1)
+    ts = 2
+    for _ in range(warmup * REF_SAMPLE_STEPS):
+        r.solve(ts)
+        ts += 1
+    t0 = time.perf_counter()
+    for _ in range(steps * REF_SAMPLE_STEPS):
+        r.solve(ts)
+        ts += 1
+    dt = time.perf_counter() - t0
+    r.close()
+    return dt / (steps * REF_SAMPLE_STEPS)
+
+
+def run_reference_batch(args, bw):
+    """The reference CPU solver on the batch's requests with all host cores:
+    each request's time per pseudo-time step is measured (one process per
+    core), times its recorded step count; the requests are packed on the
+    cores longest first."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from flowgpu import serve
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libflowref.so (the reference built from "
+                                         "its sources) is missing"}))
+        return
+    if bw.fp64_steps is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": f"step counts of {bw.name} are not recorded"}))
+        return
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    reqs = [serve.sample_request(i, seed=bw.seed) for i in range(bw.n)]
+    dirs = [r.workload(2, bw.max_steps, bw.drop).write(tempfile.mkdtemp(prefix="bench_ref_"))
+            for r in reqs]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(min(cores, len(reqs))) as pool:
+        per_step = pool.map(_ref_batch_worker, [(d, args.warmup, args.steps) for d in dirs])
+    times = [bw.fp64_steps[i] * per_step[i] for i in range(len(reqs))]
+    makespan = _lpt_makespan(times, cores)
+    conv64 = sum(1 for st in bw.fp64_status if st == 0)
+    rate = conv64 / makespan
+    sample = (f"{len(reqs)} requests, each timing {args.steps} x {REF_SAMPLE_STEPS} pseudo-time "
+              f"steps after set-up and {args.warmup} x {REF_SAMPLE_STEPS} warm-up steps "
+              f"({min(cores, len(reqs))} processes); recorded steps per request x s/step, "
+              f"packed on {cores} cores longest first: makespan {makespan:.1f} s for "
+              f"{conv64} converged solves")
+    line = {"metric": METRIC, "value": round(rate, 8), "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": bw.name, "nodes": [r.nodes for r in reqs],
+                       "s_per_step": [round(x, 4) for x in per_step]},
+            "cpu_baseline": {"value": round(rate, 8), "unit": UNIT, "cores": cores,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(rate, 8), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -401,17 +721,29 @@ def main():
     ap.add_argument("--profile-steps", type=int, default=0,
                     help="only run this many pseudo-time steps of one solve (for ncu captures)")
     ap.add_argument("--sweep-mode", type=int, default=0, help="0 grid-wide, 1 one-CTA ordered sweep")
+    ap.add_argument("--measure-fp64", action="store_true",
+                    help="batch workloads: record the FP64 drop-in's step counts per request")
     ap.add_argument("--precision", type=int, default=0,
                     help="with --profile-steps: 0 FP64 drop-in, 1 FP32 multicolour sweeps")
     ap.add_argument("--subits", type=int, default=0,
                     help="with --profile-steps: Gauss-Seidel sweeps per step (0: the workload's)")
     args = ap.parse_args()
     from flowgpu import workloads
-    args.workload = args.workload or workloads.DEFAULT
-    if args.impl == "reference":
-        run_reference(args)
-    elif args.profile_steps > 0:
+    args.workload = args.workload or workloads.DEFAULT_BENCH
+    bw = workloads.BATCHES.get(args.workload)
+    if args.profile_steps > 0:
+        if bw is not None:
+            args.workload = workloads.DEFAULT
         run_profile(args)
+    elif bw is not None:
+        if args.impl == "reference":
+            run_reference_batch(args, bw)
+        elif args.measure_fp64:
+            measure_fp64(args, bw)
+        else:
+            run_batch(args, bw)
+    elif args.impl == "reference":
+        run_reference(args)
     else:
         run_flow(args)
 

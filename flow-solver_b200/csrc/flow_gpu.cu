@@ -167,6 +167,7 @@ struct flow_ctx {
   // blocks with multicolour sweeps; tables built on first use
   int precision = 0;
   MixedTables mt{};
+  bool mt_ordered = false;  // tables in reference row order (mode 2) or colour order (mode 1)
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
   // CUDA graphs of chunks of K steps with the step index advancing on the
@@ -332,7 +333,7 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   {
     Timed t(c, 3);
     int nbn = grid_blocks(4 * c->nn, 128);
-    if (c->precision == 1) {
+    if (c->precision != 0) {
       if (jac) k_assemble4<true, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
       else k_assemble4<false, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
     } else {
@@ -352,6 +353,29 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
   int rc = 0;
   cudaMemsetAsync(c->s.dQ, 0, sizeof(double) * 4 * (c->nn + 1), c->stream);
   cudaMemsetAsync(c->mt.dq32, 0, sizeof(float) * 4 * (c->nn + 1), c->stream);
+  if (c->precision == 2) {
+    // reference row order: dispenser sweeps on ping-pong FP32 iterates
+    cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream);
+    const long max_spin = 1L << 21;
+    for (int it = 0; it < p->subits; it++) {
+      Timed t(c, 4);
+      const int last = it == p->subits - 1;
+      cudaMemsetAsync(c->s.counter, 0, sizeof(unsigned), c->stream);
+      k_prepare_sweep32<<<grid_blocks(4 * (c->nn + 1), 256), 256, 0, c->stream>>>(
+          c->s, c->mt.dq32, c->mt.dq32b, 4 * (c->nn + 1));
+      rc |= launch_check(c);
+      const int blocks = c->nsm * 4;
+      if (it % 2 == 0)
+        k_sweep_ordered32<true><<<blocks, 128, 0, c->stream>>>(c->s, c->mt, c->nn, c->mt.dq32,
+                                                               c->mt.dq32b, last, max_spin);
+      else
+        k_sweep_ordered32<false><<<blocks, 128, 0, c->stream>>>(c->s, c->mt, c->nn, c->mt.dq32,
+                                                                c->mt.dq32b, last, max_spin);
+      rc |= launch_check(c);
+      std::swap(c->mt.dq32, c->mt.dq32b);
+    }
+    return rc;
+  }
   const int nc = c->mt.ncolors;
   for (int it = 0; it < p->subits; it++) {
     Timed t(c, 4);
@@ -370,7 +394,7 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
 }
 
 int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
-  if (c->precision == 1) return launch_linear_solve_mixed(c, p);
+  if (c->precision != 0) return launch_linear_solve_mixed(c, p);
   int rc = 0;
   cudaMemsetAsync(c->s.dQ, 0, sizeof(double) * 4 * (c->nn + 1), c->stream);
   cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream);
@@ -483,7 +507,8 @@ int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
   int rc = 0;
   const int ph = phase_of(p, ts0);
   const bool graphable = c->use_graphs && !c->timing && K > 0 && ph == phase_of(p, ts0 + K - 1) &&
-                         (c->precision == 1 || c->sweep_mode == 1 || p->subits % 2 == 0);
+                         (c->precision == 1 || (c->precision == 0 && c->sweep_mode == 1) ||
+                          p->subits % 2 == 0);
   if (!graphable) {
     for (int i = 0; i < K && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
     return rc;
@@ -559,8 +584,8 @@ int read_status(flow_ctx* c) {
 // Colour the block pattern greedily in row order (each row takes the
 // smallest colour none of its earlier neighbours holds) and lay out the FP32
 // tables of the precision form in colour order.
-int build_mixed_tables(flow_ctx* c) {
-  if (c->mt.lhs32) return 0;
+int build_mixed_tables(flow_ctx* c, bool ordered) {
+  if (c->mt.lhs32 && c->mt_ordered == ordered) return 0;
   const int nn = c->nn;
   const std::vector<int>& ia = c->h_ia;
   const std::vector<int>& ja = c->h_ja;
@@ -576,7 +601,7 @@ int build_mixed_tables(flow_ctx* c) {
     for (int k = ia[j]; k < ia[j + 1]; k++)
       if (ja[k] < j) used[color[ja[k]]] = 1;
     int col = 0;
-    while (used[col]) col++;
+    while (!ordered && used[col]) col++;  // ordered: one class, rows in reference order
     color[j] = col;
     ncol = std::max(ncol, col + 1);
   }
@@ -608,15 +633,18 @@ int build_mixed_tables(flow_ctx* c) {
   mt.rowinfo = upload_vec(c, rinfo);
   mt.lu32 = c->buf.alloc<float>((size_t)16 * nn);
   mt.dq32 = c->buf.alloc<float>((size_t)4 * (nn + 1));
+  mt.dq32b = c->buf.alloc<float>((size_t)4 * (nn + 1));
   mt.lhs32 = c->buf.alloc<float>((size_t)16 * std::max<size_t>(ocol.size(), 1));
   if (!mt.color_ptr || !mt.rows || !mt.pos || !mt.offd_ptr || !mt.offd_col || !mt.rowinfo || !mt.lu32 ||
-      !mt.dq32 || !mt.lhs32) {
+      !mt.dq32 || !mt.dq32b || !mt.lhs32) {
     set_error("precision form: device allocation failed");
     mt.lhs32 = nullptr;
     return FLOW_ERR_CUDA;
   }
   cudaMemset(mt.dq32, 0, sizeof(float) * 4 * (nn + 1));
+  cudaMemset(mt.dq32b, 0, sizeof(float) * 4 * (nn + 1));
   c->h_color_ptr = cptr;
+  c->mt_ordered = ordered;
   return 0;
 }
 
@@ -996,14 +1024,15 @@ int flow_set_sweep_mode(flow_ctx* c, int mode) {
 }
 
 int flow_set_precision(flow_ctx* c, int mode) {
-  if (!c || !c->ok || (mode != 0 && mode != 1)) {
-    set_error("flow_set_precision: null context or mode not 0/1");
+  if (!c || !c->ok || mode < 0 || mode > 2) {
+    set_error("flow_set_precision: null context or mode not 0, 1 or 2");
     return FLOW_ERR_ARG;
   }
   cudaSetDevice(c->device);
-  if (mode == 1) {
+  if (mode != 0) {
     cudaStreamSynchronize(c->stream);
-    int rc = build_mixed_tables(c);
+    drop_graphs(c);
+    int rc = build_mixed_tables(c, mode == 2);
     if (rc) return rc;
   }
   c->precision = mode;
@@ -1251,7 +1280,7 @@ int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
   int st = read_status(c);
   if (rms) {
     double v = 10.;
-    if (c->precision == 1) v = -1.;  // the precision form forms no b-Ax RMS
+    if (c->precision != 0) v = -1.;  // the precision form forms no b-Ax RMS
     else if (p->subits > 0) cudaMemcpy(&v, c->s.scalars, sizeof(double), cudaMemcpyDeviceToHost);
     *rms = v;
   }

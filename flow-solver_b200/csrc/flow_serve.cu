@@ -34,7 +34,7 @@ struct Slot {
   double drop = 0.;
   int max_steps = 0;
   long long tag = 0;
-  int state = 0;       // 0 free, 1 running, 2 finished (result not yet released)
+  int state = 0;       // 0 free, 1 running, 2 finished (result not yet released), 3 staged
   int issued = 0;      // steps enqueued so far
   int inflight = 0;    // chunks whose flags have not been read (0..2)
   int next_flag = 0;   // flag slot of the next chunk
@@ -104,9 +104,17 @@ void flow_server_destroy(flow_server* sv) {
   delete sv;
 }
 
+static int start_slot(flow_server* sv, int idx);
+
 int flow_server_submit(flow_server* sv, const flow_grid_view* g, const flow_params* p,
                        const double* Q0, int precision, double drop, int max_steps,
                        long long tag, int* slot_out) {
+  return flow_server_stage(sv, g, p, Q0, precision, drop, max_steps, tag, 0, slot_out);
+}
+
+int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_params* p,
+                      const double* Q0, int precision, double drop, int max_steps,
+                      long long tag, int hold, int* slot_out) {
   if (!sv || !g || !p || !Q0 || !(drop > 0.) || max_steps < 1) {
     g_serve_error = "flow_server_submit: bad argument";
     return FLOW_ERR_ARG;
@@ -127,7 +135,6 @@ int flow_server_submit(flow_server* sv, const flow_grid_view* g, const flow_para
   }
   int rc = flow_set_precision(c, precision);
   if (!rc) rc = flow_set_state(c, Q0);
-  if (!rc) rc = flow::internal::begin_run(c, p, drop);
   if (rc) {
     g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
     flow_destroy(c);
@@ -140,18 +147,41 @@ int flow_server_submit(flow_server* sv, const flow_grid_view* g, const flow_para
   sl.drop = drop;
   sl.max_steps = max_steps;
   sl.tag = tag;
+  sl.state = 3;  // staged: inputs on the device, nothing launched
+  if (slot_out) *slot_out = idx;
+  if (hold) return 0;
+  return start_slot(sv, idx);
+}
+
+static int start_slot(flow_server* sv, int idx) {
+  Slot& sl = sv->slots[idx];
+  if (sl.state != 3) {
+    g_serve_error = "flow_server_start: slot is not staged";
+    return FLOW_ERR_ARG;
+  }
+  // the run's clock starts here
+  int rc = flow::internal::begin_run(sl.ctx, &sl.p, sl.drop);
   sl.state = 1;
   sv->running++;
   // two chunks in flight from the start
-  rc = issue_chunk(sv, sl);
+  if (!rc) rc = issue_chunk(sv, sl);
   if (!rc) rc = issue_chunk(sv, sl);
   if (rc) {
+    // nothing of this solve is in flight: the caller learns of the failure
+    // here (not through progress) and releases the slot
+    if (sl.inflight > 0) cudaStreamSynchronize(flow::internal::stream_of(sl.ctx));
+    sl.inflight = 0;
     sl.state = 2;
     sl.status = rc;
     sv->running--;
+    g_serve_error = std::string("flow_server_start: ") + flow_last_error();
   }
-  if (slot_out) *slot_out = idx;
-  return 0;
+  return rc;
+}
+
+int flow_server_start(flow_server* sv, int slot) {
+  if (!sv || slot < 0 || slot >= (int)sv->slots.size()) return FLOW_ERR_ARG;
+  return start_slot(sv, slot);
 }
 
 int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int max_out,
@@ -187,6 +217,7 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
         cpl.r_first = sl.r_first;
         cpl.r_last = sl.r_last;
         cpl.device_ms = sl.ms;
+        cpl.launches = flow_launch_count(sl.ctx);
         continue;
       }
       if (sl.issued < sl.max_steps) {
@@ -204,6 +235,7 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
           cpl.r_first = sl.r_first;
           cpl.r_last = sl.r_last;
           cpl.device_ms = sl.ms;
+          cpl.launches = flow_launch_count(sl.ctx);
         }
       }
     }

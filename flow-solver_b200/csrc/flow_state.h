@@ -74,6 +74,7 @@ struct MixedTables {
   float* lhs32;           // 16 floats per off-diagonal block, row-major
   float* lu32;            // 16 floats per position: LU factors, reciprocal pivots
   float* dq32;            // 4 floats per row (1..nn), the sweeps' iterate
+  float* dq32b;           // second buffer of the ordered FP32 sweeps (swapped per sweep)
 };
 
 struct DevState {

@@ -7,6 +7,7 @@ device is missing.  There is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import threading
 import os
 
 import numpy as np
@@ -33,7 +34,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_linear_residual_noalloc", "flow_arena_create", "flow_arena_destroy",
            "flow_arena_free_bytes", "flow_arena_largest_free", "flow_create_in",
            "flow_ctx_device_bytes", "flow_server_create", "flow_server_destroy",
-           "flow_server_submit", "flow_server_progress", "flow_server_result",
+           "flow_server_submit", "flow_server_stage", "flow_server_start", "flow_server_progress", "flow_server_result",
            "flow_server_release", "flow_server_running", "flow_server_last_error")
 
 
@@ -72,11 +73,22 @@ def library_path() -> str:
     return LIB_PATH
 
 
+_load_lock = threading.Lock()
+
+
 def load():
-    """Load libflowgpu.so (raises if it has not been built)."""
+    """Load libflowgpu.so (raises if it has not been built).  Thread-safe:
+    every caller gets the one handle, with every prototype set."""
     global _lib
     if _lib is not None:
         return _lib
+    with _load_lock:
+        if _lib is None:
+            _lib = _load_locked()
+    return _lib
+
+
+def _load_locked():
     if not os.path.exists(LIB_PATH):
         raise RuntimeError(f"{LIB_PATH} is missing: build it with flow-solver_b200/build.py")
     L = C.CDLL(LIB_PATH)
@@ -132,12 +144,23 @@ def load():
     L.flow_server_destroy.argtypes = [vp]
     L.flow_server_submit.argtypes = [vp, C.POINTER(FlowGridView), PP, DP, C.c_int, C.c_double,
                                      C.c_int, C.c_longlong, IP]
+    L.flow_server_stage.argtypes = [vp, C.POINTER(FlowGridView), PP, DP, C.c_int, C.c_double,
+                                    C.c_int, C.c_longlong, C.c_int, IP]
+    L.flow_server_start.argtypes = [vp, C.c_int]
     L.flow_server_progress.argtypes = [vp, C.c_int, C.POINTER(FlowCompletion), C.c_int, IP]
     L.flow_server_result.argtypes = [vp, C.c_int, DP, C.c_long, DP]
     L.flow_server_release.argtypes = [vp, C.c_int]
     L.flow_server_running.argtypes = [vp]
     L.flow_server_last_error.restype = C.c_char_p
-    _lib = L
+    # host preprocessing (include/flow_prep.h)
+    L.flow_prep_read.restype = vp
+    L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
+    L.flow_prep_view.argtypes = [vp, C.POINTER(FlowGridView)]
+    L.flow_prep_initial_state.argtypes = [vp, C.POINTER(FlowParamsC), DP]
+    L.flow_prep_node_map.restype = IP
+    L.flow_prep_node_map.argtypes = [vp]
+    L.flow_prep_free.argtypes = [vp]
+    L.flow_prep_last_error.restype = C.c_char_p
     return L
 
 
@@ -159,7 +182,7 @@ NOALLOC_MAX_ROWS = 262144
 class FlowCompletion(C.Structure):
     _fields_ = [("tag", C.c_longlong), ("slot", C.c_int), ("status", C.c_int),
                 ("steps", C.c_int), ("r_first", C.c_double), ("r_last", C.c_double),
-                ("device_ms", C.c_double)]
+                ("device_ms", C.c_double), ("launches", C.c_longlong)]
 
 
 class Arena:
@@ -202,26 +225,34 @@ class Server:
         self._out = (FlowCompletion * 64)()
 
     def submit(self, mesh, params, Q0, precision: int = 1, drop: float = 1e-10,
-               max_steps: int = 20000, tag: int = 0):
+               max_steps: int = 20000, tag: int = 0, hold: bool = False):
+        """hold: stage only (inputs uploaded); start(slot) launches it."""
         p = params_struct(params)
         q = np.ascontiguousarray(Q0, dtype=np.float64)
         slot = C.c_int(-1)
-        rc = self.L.flow_server_submit(self.h, C.byref(mesh.view), C.byref(p),
-                                       q.ctypes.data_as(DP), int(precision), float(drop),
-                                       int(max_steps), int(tag), C.byref(slot))
+        rc = self.L.flow_server_stage(self.h, C.byref(mesh.view), C.byref(p),
+                                      q.ctypes.data_as(DP), int(precision), float(drop),
+                                      int(max_steps), int(tag), int(bool(hold)), C.byref(slot))
         if rc == ERR_BUDGET:
             return None
         if rc:
-            raise FlowError(rc, "flow_server_submit " + self.L.flow_server_last_error().decode())
+            err = self.L.flow_server_last_error().decode()
+            if slot.value >= 0:  # a start that failed leaves a finished slot behind
+                self.L.flow_server_release(self.h, slot.value)
+            raise FlowError(rc, "flow_server_submit " + err)
         self._keep[slot.value] = (mesh, p)
         return slot.value
+
+    def start(self, slot: int):
+        _check(self.L.flow_server_start(self.h, int(slot)), "flow_server_start")
 
     def progress(self, wait_us: int = 0) -> list:
         n = C.c_int(0)
         _check(self.L.flow_server_progress(self.h, int(wait_us), self._out, len(self._out),
                                            C.byref(n)), "flow_server_progress")
         return [{"tag": c.tag, "slot": c.slot, "status": c.status, "steps": c.steps,
-                 "r_first": c.r_first, "r_last": c.r_last, "device_ms": c.device_ms}
+                 "r_first": c.r_first, "r_last": c.r_last, "device_ms": c.device_ms,
+                 "launches": c.launches}
                 for c in self._out[:n.value]]
 
     def result(self, slot: int, want_q: bool = True):
@@ -417,7 +448,8 @@ class Solver:
         return out
 
     def set_precision(self, mode: int):
-        """0: FP64 reference-order drop-in; 1: FP32 blocks, multicolour sweeps."""
+        """0: FP64 reference-order drop-in; 1: FP32 blocks, multicolour sweeps;
+        2: FP32 blocks, sweeps in the reference's row order."""
         _check(self.L.flow_set_precision(self.ctx, int(mode)), "flow_set_precision")
 
     def set_graphs(self, on: bool):

@@ -9,25 +9,9 @@ import numpy as np
 
 from . import capi
 
-_bound = False
-
-
 def _lib():
-    global _bound
-    L = capi.load()
-    if not _bound:
-        vp = C.c_void_p
-        IP = C.POINTER(C.c_int)
-        L.flow_prep_read.restype = vp
-        L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
-        L.flow_prep_view.argtypes = [vp, C.POINTER(capi.FlowGridView)]
-        L.flow_prep_initial_state.argtypes = [vp, C.POINTER(capi.FlowParamsC), capi.DP]
-        L.flow_prep_node_map.restype = IP
-        L.flow_prep_node_map.argtypes = [vp]
-        L.flow_prep_free.argtypes = [vp]
-        L.flow_prep_last_error.restype = C.c_char_p
-        _bound = True
-    return L
+    """The library handle; capi.load() sets the preprocessing prototypes."""
+    return capi.load()
 
 
 def read_bc(path: str) -> list[int]:

@@ -1,0 +1,65 @@
+"""Algorithmic (compulsory) DRAM bytes per launch of the main kernels.
+
+Each figure counts every array element a launch must read or write once:
+per-node records, per-face records, incidence lists, stencils, and the
+outputs.  Neighbour gathers of node states are counted once per node (the
+rest are cache hits by construction).  The achieved bandwidth of a launch is
+these bytes over its measured duration; DRAM traffic measured by ncu well
+above them would mean re-reads.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _sizes(mesh) -> dict:
+    v = mesh.view
+    out = {"nn": v.nn, "ns": v.nsubedges, "ne": v.nedges, "nbe": v.nbedges, "stencil": 0}
+    if mesh.order == 3:
+        m = np.ctypeslib.as_array(v.svd_m, shape=(v.nn + 1,))
+        out["stencil"] = int(m[1:].sum())
+    nnz = int(np.ctypeslib.as_array(v.ia, shape=(v.nn + 2,))[v.nn + 1])
+    out["nnz"] = nnz
+    return out
+
+
+def node_prepare_bytes(mesh) -> int:
+    """k_node_prepare4: wave-speed sum and dt, the k=1 gradient or the k=2
+    derivatives (x = V S^-1 U^T b over the node's stencil) and point value,
+    and the Venkatakrishnan limiter over every face point.
+
+    per node   read  nQ 32, x 16, cv_area 8, three incidence pointers 12
+                     (k=2: moments 72, V^T 200, S 40, stencil pointer 4)
+               write dt 8, phi 64 (k=1: grad 64; k=2: derivatives 160, point values 32)
+    per subedge      two incidence entries 8, normal/length 32,
+                     face point offsets 32 (k=1) or 3 Gauss points 48 (k=2)
+    per edge         two incidence entries 8, end nodes 8 (k=1: LSQ weights 32)
+    per bedge        incidence entry 4, normal/length 24
+    per stencil entry (k=2) index 4, weight 8, the row of U's first 5 columns 40
+    """
+    z = _sizes(mesh)
+    k2 = mesh.order == 3
+    per_node = 32 + 16 + 8 + 12 + 8 + 64 + ((72 + 200 + 40 + 4 + 160 + 32) if k2 else 64)
+    per_sub = 8 + 32 + (48 if k2 else 32)
+    per_edge = 8 + 8 + (0 if k2 else 32)
+    per_bedge = 4 + 24
+    return int(z["nn"] * per_node + z["ns"] * per_sub + z["ne"] * per_edge +
+               z["nbe"] * per_bedge + z["stencil"] * 52)
+
+
+def colour_sweep_bytes(mesh) -> int:
+    """One whole multicolour FP32 sweep (all colour launches): per row the
+    row record 16, right-hand side 32 (FP64), LU factors 64, the iterate
+    written 16; per off-diagonal block its column 4, the block 64 (FP32) and
+    the neighbour iterate 16."""
+    z = _sizes(mesh)
+    offd = z["nnz"] - z["nn"]
+    return int(z["nn"] * (16 + 32 + 64 + 16) + offd * (4 + 64 + 16))
+
+
+def ordered_sweep_bytes(mesh) -> int:
+    """One FP64 ordered sweep (k_sweep_ordered): per block 128 B of LHS and
+    4 B of column index, per row RHS, LU of the diagonal, dQ read and write
+    (132 B per block + 96 B per row, the diagonal block counted as a block)."""
+    z = _sizes(mesh)
+    return int(132 * z["nnz"] + 96 * z["nn"])

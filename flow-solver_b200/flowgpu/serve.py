@@ -75,6 +75,7 @@ def prepare(req: Request, subits: int, max_steps: int, drop: float) -> Prepared:
 
 
 def prepare_all(reqs, subits: int, max_steps: int, drop: float, threads: int = 8):
+    capi.load()  # bind once before the worker threads use it
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
         return list(ex.map(lambda r: prepare(r, subits, max_steps, drop), reqs))
 
@@ -147,6 +148,7 @@ def run_poisson(reqs, rate_per_s: float, arena: capi.Arena, subits: int, max_ste
     rng = np.random.Generator(np.random.PCG64([seed, 7]))
     gaps = rng.exponential(1.0 / rate_per_s, size=len(reqs))
     arrivals = np.cumsum(gaps) - gaps[0]
+    capi.load()
     srv = capi.Server(arena, chunk=chunk, max_slots=max_slots)
     ex = cf.ThreadPoolExecutor(max_workers=prep_threads)
     t0 = time.perf_counter()

@@ -64,7 +64,8 @@ WORKLOADS = {
     "ogrid128x32_k1_m050": Workload("ogrid128x32_k1_m050", 128, 32, False, 1, 0.5),
 }
 
-DEFAULT = "ogrid512x128_k2_m080"
+DEFAULT = "ogrid512x128_k2_m080"   # the single-mesh drop-in workload
+DEFAULT_BENCH = "batch16"           # bench.py's default: the batching form
 
 
 def get(name: str) -> Workload:
@@ -73,3 +74,39 @@ def get(name: str) -> Workload:
 
 def with_steps(w: Workload, n: int) -> Workload:
     return replace(w, steps_to_converge=n)
+
+
+@dataclass(frozen=True)
+class BatchWorkload:
+    """The batching form: ``n`` independent requests per GPU from the seeded
+    request stream (flowgpu.serve.sample_request: node counts log-uniform in
+    [2k, 200k] with a 4:1 circumferential:radial ratio, Mach U[0.3, 0.85],
+    angle of attack U[-4, 6] degrees, k=1 or k=2), all admitted together to
+    one server and each retired at a ``drop`` of ||R_rho|| or after
+    ``max_steps`` pseudo-time steps.  ``precision``/``subits``: the served
+    form (flow_set_precision mode and Gauss-Seidel sweeps per step).
+
+    ``fp64_steps`` / ``fp64_status``: what the FP64 drop-in (bit-identical to
+    the reference, so these are the reference's own counts) does on requests
+    0..n-1 of the stream: steps taken and 0 converged, 256 stopped at
+    max_steps, other values failed (a non-physical state).  Measured with
+    ``bench.py --measure-fp64``."""
+    name: str
+    seed: int
+    n: int
+    max_steps: int
+    drop: float
+    precision: int
+    subits: int
+    chunk: int = 32
+    fp64_steps: tuple | None = None
+    fp64_status: tuple | None = None
+
+
+BATCHES = {
+    "batch16": BatchWorkload(
+        "batch16", 0, 16, 8000, 1e-10, 1, 4,
+        fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065,
+                    1395, 1487, 8000),
+        fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256)),
+}

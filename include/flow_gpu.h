@@ -207,9 +207,12 @@ int flow_set_sweep_mode(flow_ctx *ctx, int mode);
  * and runs p->subits multicolour block Gauss-Seidel sweeps in FP32 (greedy
  * colouring of the block pattern in row order; forward sweeps take the
  * colours ascending, backward sweeps descending).  The converged state is
- * that of mode 0 (same residual); the iterates differ.  In mode 1 the FP64
- * LHS is not formed (flow_get "LHS" is stale) and flow_linear_solve reports
- * rms = -1.  The first switch to mode 1 builds the colour tables. */
+ * that of mode 0 (same residual); the iterates differ.  Mode 2 is mode 1
+ * with the sweeps in the reference's row order (forward rows 1..nn, backward
+ * nn..1, the FP64 drop-in's dependency-ordered sweep on FP32 blocks): steps
+ * to converge as in mode 0, sweeps latency-bound as in mode 0.  In modes 1
+ * and 2 the FP64 LHS is not formed (flow_get "LHS" is stale) and
+ * flow_linear_solve reports rms = -1.  Switching builds the FP32 tables. */
 int flow_set_precision(flow_ctx *ctx, int mode);
 
 /* flow_converge / flow_converge_batch issue steps in chunks; with graphs on
@@ -281,13 +284,23 @@ typedef struct {
   int steps;         /* pseudo-time steps taken */
   double r_first;    /* ||R_rho|| of the first step */
   double r_last;     /* ||R_rho|| of the last step */
-  double device_ms;  /* device time from submission to retirement */
+  double device_ms;  /* device time from the start of the run to retirement */
+  long long launches; /* kernel launches the solve issued (graph replays included) */
 } flow_completion;
 flow_server *flow_server_create(flow_arena *arena, int chunk, int max_slots, int *status);
 void flow_server_destroy(flow_server *srv);
 int flow_server_submit(flow_server *srv, const flow_grid_view *g, const flow_params *p,
                        const double *Q0, int precision, double drop, int max_steps,
                        long long tag, int *slot);
+/* flow_server_submit split in two: flow_server_stage creates the context and
+ * uploads the state (hold = 1: nothing is launched yet) and
+ * flow_server_start launches a staged solve. */
+int flow_server_stage(flow_server *srv, const flow_grid_view *g, const flow_params *p,
+                      const double *Q0, int precision, double drop, int max_steps,
+                      long long tag, int hold, int *slot);
+/* A start that fails returns its error (the slot is then finished with that
+ * status and must be released); progress never reports it. */
+int flow_server_start(flow_server *srv, int slot);
 /* Launch further chunks and collect retired solves (at most max_out); waits
  * up to wait_us microseconds for at least one when none is ready. */
 int flow_server_progress(flow_server *srv, int wait_us, flow_completion *out, int max_out,

@@ -869,6 +869,8 @@ static void gs_row_mixed(const orc_grid *g, const float *A32, const float *lu32,
   dq32[j * NV + 3] = x3;
 }
 
+/* color == NULL: the reference's row order (forward 1..nn, backward nn..1,
+ * in place, so earlier rows of the sweep are already updated). */
 void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, int ncolors)
 {
   int nn = g->nn;
@@ -885,6 +887,13 @@ void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, 
     for (int q = 0; q < 4; q++) lu32[j * 16 + 5 * q] = (float)(1.0 / M[5 * q]);
   }
   for (int it = 0; it < p->subits; it++) {
+    if (!color) {
+      if (it % 2 == 0)
+        for (int j = 1; j <= nn; j++) gs_row_mixed(g, A32, lu32, dq32, j);
+      else
+        for (int j = nn; j >= 1; j--) gs_row_mixed(g, A32, lu32, dq32, j);
+      continue;
+    }
     for (int ci = 0; ci < ncolors; ci++) {
       int col = (it % 2 == 0) ? ci : ncolors - 1 - ci;
       for (int j = 1; j <= nn; j++)
@@ -898,21 +907,21 @@ void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, 
   free(dq32);
 }
 
-static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm,
+static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm, int mixed,
                       const int *color, int ncolors);
 
 int orc_solve(orc_grid *g, const orc_params *p, int ts, double *dqnorm)
 {
-  return solve_impl(g, p, ts, dqnorm, NULL, 0);
+  return solve_impl(g, p, ts, dqnorm, 0, NULL, 0);
 }
 
 int orc_solve_mixed(orc_grid *g, const orc_params *p, int ts, double *dqnorm, const int *color,
                     int ncolors)
 {
-  return solve_impl(g, p, ts, dqnorm, color, ncolors);
+  return solve_impl(g, p, ts, dqnorm, 1, color, ncolors);
 }
 
-static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm,
+static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm, int mixed,
                       const int *color, int ncolors)
 {
   int nn = g->nn, rc;
@@ -949,7 +958,7 @@ static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm,
     if (p->tacc != 0 || p->unsteady != 0) return 40;
     for (int i = 1; i <= nn; i++)
       for (int j = 0; j < NV; j++) g->RHS[i * NV + j] = -(g->R[i * NV + j]);
-    if (color)
+    if (mixed)
       orc_linear_solve_mixed(g, p, color, ncolors);
     else
       orc_linear_solve(g, p);

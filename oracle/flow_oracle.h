@@ -91,7 +91,9 @@ int orc_solve(orc_grid *g, const orc_params *p, int ts, double *dq);
  * color[1..nn] receives the colours; returns the number of colours. */
 int orc_greedy_colors(const orc_grid *g, int *color);
 void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, int ncolors);
-/* orc_solve with orc_linear_solve_mixed in place of orc_linear_solve. */
+/* color == NULL: FP32 blocks with the sweeps in the reference's row order.
+ * orc_solve_mixed: orc_solve with orc_linear_solve_mixed in place of
+ * orc_linear_solve (color == NULL again selects the reference order). */
 int orc_solve_mixed(orc_grid *g, const orc_params *p, int ts, double *dq, const int *color,
                     int ncolors);
 

@@ -187,16 +187,19 @@ class OracleGrid:
             self._colors = (col, nc)
         return self._colors
 
-    def linear_solve_mixed(self, p):
+    def linear_solve_mixed(self, p, ordered: bool = False):
         col, nc = self.colors()
-        self.L.orc_linear_solve_mixed(C.byref(self.g), C.byref(p), col.ctypes.data_as(IP), nc)
+        cp = None if ordered else col.ctypes.data_as(IP)
+        self.L.orc_linear_solve_mixed(C.byref(self.g), C.byref(p), cp, nc)
 
-    def solve_mixed(self, p: OrcParams, ts: int) -> float:
+    def solve_mixed(self, p: OrcParams, ts: int, ordered: bool = False) -> float:
+        """Precision form step: multicolour sweeps, or (ordered) the
+        reference's row order, with FP32 blocks."""
         col, nc = self.colors()
         self.g.citer = ts
         dq = C.c_double()
-        rc = self.L.orc_solve_mixed(C.byref(self.g), C.byref(p), ts, C.byref(dq),
-                                    col.ctypes.data_as(IP), nc)
+        cp = None if ordered else col.ctypes.data_as(IP)
+        rc = self.L.orc_solve_mixed(C.byref(self.g), C.byref(p), ts, C.byref(dq), cp, nc)
         if rc:
             raise RuntimeError(f"oracle solve failed with code {rc}")
         return dq.value

@@ -14,7 +14,7 @@ from cases import ndiff
 pytestmark = pytest.mark.gpu
 
 
-def _setup(nc, nr, curved, order, subits):
+def _setup(nc, nr, curved, order, subits, mode=1):
     from dataclasses import replace
     from flowgpu import capi, workloads
     from flowgpu.prep import Mesh
@@ -27,22 +27,26 @@ def _setup(nc, nr, curved, order, subits):
     og = port.OracleGrid(mesh.sizes, mesh.arrays())
     og.set("Q", Q0)
     gpu = capi.Solver.from_mesh(mesh, fp, device=0)
-    gpu.set_precision(1)
+    gpu.set_precision(mode)
     gpu.set_state(Q0)
     return mesh, fp, og, port.params_from_flow(fp), gpu
 
 
-@pytest.mark.parametrize("nc,nr,curved,order,subits,steps", [
-    (32, 8, False, 1, 2, 6),
-    (32, 8, True, 3, 2, 6),
-    (128, 32, True, 3, 4, 4),
-    (64, 16, False, 1, 3, 4),
+@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,mode", [
+    (32, 8, False, 1, 2, 6, 1),
+    (32, 8, True, 3, 2, 6, 1),
+    (128, 32, True, 3, 4, 4, 1),
+    (64, 16, False, 1, 3, 4, 1),
+    (32, 8, True, 3, 2, 6, 2),
+    (128, 32, True, 3, 2, 4, 2),
+    (64, 16, False, 1, 3, 4, 2),
 ])
-def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps):
-    mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits)
+def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
+    """mode 1: multicolour sweeps; mode 2: sweeps in the reference's row order."""
+    mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits, mode)
     nn = mesh.sizes["nn"]
     for ts in range(1, steps + 1):
-        og.solve_mixed(p, ts)
+        og.solve_mixed(p, ts, ordered=(mode == 2))
         gpu.solve(ts)
         for name in ("Q", "nQ"):
             assert ndiff(og[name][4:], gpu.get(name)[4:]) == 0, (name, ts)
@@ -60,7 +64,7 @@ def test_mixed_converges_to_the_fp64_answer():
     mesh = Mesh.from_case(wl.write(), order=3)
     fp = wl.params()
     out = {}
-    for mode in (0, 1):
+    for mode in (0, 1, 2):
         s = capi.Solver.from_mesh(mesh, fp, device=0)
         s.set_precision(mode)
         s.set_state(mesh.initial_state(fp))
@@ -68,7 +72,9 @@ def test_mixed_converges_to_the_fp64_answer():
         assert r1 < 1e-10 * r0
         out[mode] = (steps, s.body_forces(), s.get("Q"))
         s.close()
-    (n0, f0, q0), (n1, f1, q1) = out[0], out[1]
-    assert abs(f1[0] - f0[0]) <= 1e-8 * max(1.0, abs(f0[0]))
-    assert abs(f1[1] - f0[1]) <= 1e-8 * max(1.0, abs(f0[1]))
-    assert np.max(np.abs(q1 - q0)) < 1e-7
+    n0, f0, q0 = out[0]
+    for mode in (1, 2):
+        n1, f1, q1 = out[mode]
+        assert abs(f1[0] - f0[0]) <= 1e-8 * max(1.0, abs(f0[0]))
+        assert abs(f1[1] - f0[1]) <= 1e-8 * max(1.0, abs(f0[1]))
+        assert np.max(np.abs(q1 - q0)) < 1e-7
