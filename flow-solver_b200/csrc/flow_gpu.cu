@@ -167,7 +167,10 @@ struct flow_ctx {
   // blocks with multicolour sweeps; tables built on first use
   int precision = 0;
   MixedTables mt{};
-  bool mt_ordered = false;  // tables in reference row order (mode 2) or colour order (mode 1)
+  bool mt_ordered = false;  // tables in reference row order (modes 2, 3) or colour order (mode 1)
+  ChunkTables ct{};          // mode 3 tables and sweep records
+  std::vector<int> h_col_ptr, h_chunk_start;
+  int chunk_rows = 0, chunk_levels = 0;  // requested limits (0: defaults)
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
   // CUDA graphs of chunks of K steps with the step index advancing on the
@@ -333,12 +336,17 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   {
     Timed t(c, 3);
     int nbn = grid_blocks(4 * c->nn, 128);
-    if (c->precision != 0) {
-      if (jac) k_assemble4<true, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
-      else k_assemble4<false, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
+    const MixedTables& mt = c->mt;
+    const ChunkTables& ct = c->ct;
+    if (c->precision == 3) {
+      if (jac) k_assemble4<true, 2><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      else k_assemble4<false, 2><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+    } else if (c->precision != 0) {
+      if (jac) k_assemble4<true, 1><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      else k_assemble4<false, 1><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
     } else {
-      if (jac) k_assemble4<true, false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
-      else k_assemble4<false, false><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, c->mt);
+      if (jac) k_assemble4<true, 0><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      else k_assemble4<false, 0><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
     }
     rc |= launch_check(c);
   }
@@ -353,6 +361,26 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
   int rc = 0;
   cudaMemsetAsync(c->s.dQ, 0, sizeof(double) * 4 * (c->nn + 1), c->stream);
   cudaMemsetAsync(c->mt.dq32, 0, sizeof(float) * 4 * (c->nn + 1), c->stream);
+  if (c->precision == 3) {
+    // coloured chunks of the reference order, in-place FP32 iterate
+    const ChunkTables& ct = c->ct;
+    const size_t smem = sizeof(SweepRec) * kRecSlots * kRecRows + sizeof(float4) * ct.maxwin;
+    for (int it = 0; it < p->subits; it++) {
+      Timed t(c, 4);
+      const int last = it == p->subits - 1, dir = it % 2;
+      for (int ci = 0; ci < ct.ncol; ci++) {
+        const int col = dir == 0 ? ci : ct.ncol - 1 - ci;
+        const int nb = c->h_col_ptr[col + 1] - c->h_col_ptr[col];
+        if (nb <= 0) continue;
+        if (dir == 0)
+          k_sweep_chunk<0><<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
+        else
+          k_sweep_chunk<1><<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
+        rc |= launch_check(c);
+      }
+    }
+    return rc;
+  }
   if (c->precision == 2) {
     // reference row order: dispenser sweeps on ping-pong FP32 iterates
     cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream);
@@ -507,7 +535,8 @@ int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
   int rc = 0;
   const int ph = phase_of(p, ts0);
   const bool graphable = c->use_graphs && !c->timing && K > 0 && ph == phase_of(p, ts0 + K - 1) &&
-                         (c->precision == 1 || (c->precision == 0 && c->sweep_mode == 1) ||
+                         (c->precision == 1 || c->precision == 3 ||
+                          (c->precision == 0 && c->sweep_mode == 1) ||
                           p->subits % 2 == 0);
   if (!graphable) {
     for (int i = 0; i < K && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
@@ -645,6 +674,165 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
   cudaMemset(mt.dq32b, 0, sizeof(float) * 4 * (nn + 1));
   c->h_color_ptr = cptr;
   c->mt_ordered = ordered;
+  return 0;
+}
+
+// Mode 3 tables.  Chunks: consecutive rows of the reference order, closed
+// when the next row would exceed the row limit (default twice the matrix
+// bandwidth, at most 2048) or the level limit (default 32; a row's level is
+// one more than that of its latest in-chunk neighbour upstream, and the
+// longest chain is the same in both directions).  Colours: each chunk takes
+// the smallest colour no earlier adjacent chunk holds.  Records: per
+// direction, chunk by chunk, sub-levels of at most kRecRows rows of one
+// level, rows ascending inside a sub-level.
+int build_chunk_tables(flow_ctx* c) {
+  const int nn = c->nn;
+  const std::vector<int>& ia = c->h_ia;
+  const std::vector<int>& ja = c->h_ja;
+  int bw = 1;
+  for (int j = 1; j <= nn; j++) {
+    if (ia[j + 1] - ia[j] - 1 > kRecBlocks) {
+      set_error("precision mode 3: a row has more than 8 off-diagonal blocks");
+      return FLOW_ERR_ARG;
+    }
+    for (int k = ia[j]; k < ia[j + 1]; k++) bw = std::max(bw, std::abs(ja[k] - j));
+  }
+  const int cmax = c->chunk_rows > 0 ? c->chunk_rows
+                                     : std::min(2048, std::max(64, ((2 * bw + 63) / 64) * 64));
+  const int lmax = c->chunk_levels > 0 ? c->chunk_levels : 32;
+  // chunks
+  std::vector<int> start, lev(nn + 1, 0), chunk_of(nn + 1, 0);
+  start.push_back(1);
+  for (int j = 1; j <= nn; j++) {
+    int lo = start.back();
+    int l = 0;
+    for (int k = ia[j]; k < ia[j + 1]; k++)
+      if (ja[k] >= lo && ja[k] < j) l = std::max(l, lev[ja[k]] + 1);
+    if (j - lo + 1 > cmax || l + 1 > lmax) {
+      start.push_back(j);
+      l = 0;
+    }
+    lev[j] = l;
+    chunk_of[j] = (int)start.size() - 1;
+  }
+  const int nch = (int)start.size();
+  start.push_back(nn + 1);
+  // colours
+  std::vector<int> colour(nch, 0);
+  int ncol = 1;
+  std::vector<char> used;
+  for (int q = 0; q < nch; q++) {
+    used.assign(ncol + 1, 0);
+    for (int j = start[q]; j < start[q + 1]; j++)
+      for (int k = ia[j]; k < ia[j + 1]; k++) {
+        const int o = chunk_of[ja[k]];
+        if (o < q) used[colour[o]] = 1;
+      }
+    int col = 0;
+    while (used[col]) col++;
+    colour[q] = col;
+    ncol = std::max(ncol, col + 1);
+  }
+  std::vector<int> cptr(ncol + 1, 0), clist;
+  for (int q = 0; q < nch; q++) cptr[colour[q] + 1]++;
+  for (int k = 0; k < ncol; k++) cptr[k + 1] += cptr[k];
+  clist.assign(nch, 0);
+  {
+    std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+    for (int q = 0; q < nch; q++) clist[fill[colour[q]]++] = q;
+  }
+  // windows
+  std::vector<int2> win(nch);
+  int maxwin = 0;
+  for (int q = 0; q < nch; q++) {
+    int a = start[q], b = start[q + 1] - 1;
+    for (int j = start[q]; j < start[q + 1]; j++)
+      for (int k = ia[j]; k < ia[j + 1]; k++) {
+        a = std::min(a, ja[k]);
+        b = std::max(b, ja[k]);
+      }
+    win[q] = make_int2(a, b);
+    maxwin = std::max(maxwin, b - a + 1);
+  }
+  const size_t smem = sizeof(SweepRec) * kRecSlots * kRecRows + sizeof(float4) * maxwin;
+  if (smem > 227 * 1024) {
+    set_error("precision mode 3: a chunk's window does not fit in shared memory (bandwidth too large)");
+    return FLOW_ERR_ARG;
+  }
+  ChunkTables& ct = c->ct;
+  ct.nchunks = nch;
+  ct.ncol = ncol;
+  ct.maxwin = maxwin;
+  ct.col_ptr = upload_vec(c, cptr);
+  ct.col_chunks = upload_vec(c, clist);
+  ct.window = upload_vec(c, win);
+  // per direction: levels, sub-levels, records (static part)
+  std::vector<int> levd(nn + 1);
+  for (int dir = 0; dir < 2; dir++) {
+    std::vector<int> ss, cs(nch + 1, 0), pos(nn + 1, 0), order;
+    order.reserve(nn);
+    for (int q = 0; q < nch; q++) {
+      const int lo = start[q], hi = start[q + 1] - 1;
+      int nlev = 0;
+      for (int t = 0; t <= hi - lo; t++) {
+        const int j = dir == 0 ? lo + t : hi - t;
+        int l = 0;
+        for (int k = ia[j]; k < ia[j + 1]; k++) {
+          const int o = ja[k];
+          const bool up = dir == 0 ? (o >= lo && o < j) : (o <= hi && o > j);
+          if (up) l = std::max(l, levd[o] + 1);
+        }
+        levd[j] = l;
+        nlev = std::max(nlev, l + 1);
+      }
+      cs[q] = (int)ss.size();
+      for (int l = 0; l < nlev; l++) {
+        int in_sub = kRecRows;
+        for (int j = lo; j <= hi; j++) {
+          if (levd[j] != l) continue;
+          if (in_sub == kRecRows) {
+            ss.push_back((int)order.size());
+            in_sub = 0;
+          }
+          pos[j] = (int)order.size();
+          order.push_back(j);
+          in_sub++;
+        }
+      }
+    }
+    cs[nch] = (int)ss.size();
+    ss.push_back((int)order.size());
+    std::vector<SweepRec> rec(nn);
+    memset(rec.data(), 0, sizeof(SweepRec) * nn);
+    for (int i = 0; i < nn; i++) {
+      const int j = order[i];
+      const int nb = ia[j + 1] - ia[j] - 1;  // the diagonal block is the row's last
+      rec[i].hdr = make_int4(j, nb, 0, 0);
+      int* cols = reinterpret_cast<int*>(rec[i].cols);
+      for (int t = 0; t < nb; t++) cols[t] = ja[ia[j] + t];
+    }
+    ct.rec[dir] = upload_vec(c, rec);
+    ct.sub_start[dir] = upload_vec(c, ss);
+    ct.chunk_sub[dir] = upload_vec(c, cs);
+    ct.pos[dir] = upload_vec(c, pos);
+    if (!ct.rec[dir] || !ct.sub_start[dir] || !ct.chunk_sub[dir] || !ct.pos[dir]) {
+      set_error("precision mode 3: table upload failed");
+      return FLOW_ERR_CUDA;
+    }
+  }
+  if (!ct.col_ptr || !ct.col_chunks || !ct.window) {
+    set_error("precision mode 3: table upload failed");
+    return FLOW_ERR_CUDA;
+  }
+  if (cudaFuncSetAttribute(k_sweep_chunk<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_sweep_chunk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess) {
+    set_error("precision mode 3: cannot reserve shared memory for the sweep");
+    return FLOW_ERR_CUDA;
+  }
+  c->h_col_ptr = cptr;
+  c->h_chunk_start = start;
   return 0;
 }
 
@@ -1024,18 +1212,45 @@ int flow_set_sweep_mode(flow_ctx* c, int mode) {
 }
 
 int flow_set_precision(flow_ctx* c, int mode) {
-  if (!c || !c->ok || mode < 0 || mode > 2) {
-    set_error("flow_set_precision: null context or mode not 0, 1 or 2");
+  if (!c || !c->ok || mode < 0 || mode > 3) {
+    set_error("flow_set_precision: null context or mode not 0..3");
     return FLOW_ERR_ARG;
   }
   cudaSetDevice(c->device);
   if (mode != 0) {
     cudaStreamSynchronize(c->stream);
     drop_graphs(c);
-    int rc = build_mixed_tables(c, mode == 2);
+    int rc = build_mixed_tables(c, mode >= 2);
+    if (!rc && mode == 3) rc = build_chunk_tables(c);
     if (rc) return rc;
   }
   c->precision = mode;
+  return 0;
+}
+
+int flow_set_chunk(flow_ctx* c, int rows, int levels) {
+  if (!c || !c->ok || rows < 0 || rows > 2048 || levels < 0) {
+    set_error("flow_set_chunk: null context, rows outside 0..2048 or negative levels");
+    return FLOW_ERR_ARG;
+  }
+  c->chunk_rows = rows;
+  c->chunk_levels = levels;
+  if (c->precision == 3) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+    return build_chunk_tables(c);
+  }
+  return 0;
+}
+
+int flow_chunk_starts(flow_ctx* c, int* starts, int cap, int* nchunks, int* ncolours) {
+  if (!c || !c->ok || c->h_chunk_start.empty()) return FLOW_ERR_ARG;
+  const int n = (int)c->h_chunk_start.size() - 1;
+  if (nchunks) *nchunks = n;
+  if (ncolours) *ncolours = c->ct.ncol;
+  if (starts)
+    for (int i = 0; i <= n && i < cap; i++) starts[i] = c->h_chunk_start[i];
   return 0;
 }
 

@@ -254,11 +254,12 @@ __global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, St
 // factors of the diagonal block for the sweeps (linear_algebra.C:226-246).
 // Four lanes per node, lane q owning row q of every 4x4 block and component
 // q of R; each lane sums its row in the reference's face order.  MIXED (the
-// precision form) writes FP32 off-diagonal blocks in colour order and FP32
-// LU factors with reciprocal pivots instead of the FP64 row.
-template <bool JAC, bool MIXED>
+// precision form) writes FP32 off-diagonal blocks and FP32 LU factors with
+// reciprocal pivots instead of the FP64 row: into the mode 1/2 tables
+// (MIXED 1) or into the row's forward and backward sweep records (MIXED 2).
+template <bool JAC, int MIXED>
 __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a,
-                                                   MixedTables mt) {
+                                                   MixedTables mt, ChunkTables ct) {
   if (*s.stop) return;  // the run has converged
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (tid >> 2) + 1, q = tid & 3;
@@ -305,8 +306,15 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
   const int k0 = m.ia[n], k1 = m.ia[n + 1];
   // precision form: this row's off-diagonal blocks in colour order (the
   // diagonal block is the row's last, so block k is off-diagonal k - k0)
-  const int mpos = MIXED ? mt.pos[n] : 0;
-  const int moff = MIXED ? mt.offd_ptr[mpos] : 0;
+  const int mpos = MIXED == 1 ? mt.pos[n] : 0;
+  const int moff = MIXED == 1 ? mt.offd_ptr[mpos] : 0;
+  SweepRec* rf = MIXED == 2 ? ct.rec[0] + ct.pos[0][n] : nullptr;
+  SweepRec* rb = MIXED == 2 ? ct.rec[1] + ct.pos[1][n] : nullptr;
+  if (MIXED == 2) {
+    const float rh = __double2float_rn(-(r));
+    reinterpret_cast<float*>(&rf->rhs)[q] = rh;
+    reinterpret_cast<float*>(&rb->rhs)[q] = rh;
+  }
   for (int k = k0; k < k1; k++) {
     double4* out = reinterpret_cast<double4*>(s.LHS + 16 * (long)k) + q;
     if (m.ja[k] == n) {
@@ -328,12 +336,16 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
         }
       }
     }
-    if (MIXED)
-      reinterpret_cast<float4*>(mt.lhs32 + 16 * (long)(moff + (k - k0)))[q] =
-          make_float4(__double2float_rn(B0), __double2float_rn(B1), __double2float_rn(B2),
-                      __double2float_rn(B3));
-    else
+    const float4 b32 = make_float4(__double2float_rn(B0), __double2float_rn(B1),
+                                   __double2float_rn(B2), __double2float_rn(B3));
+    if (MIXED == 1) {
+      reinterpret_cast<float4*>(mt.lhs32 + 16 * (long)(moff + (k - k0)))[q] = b32;
+    } else if (MIXED == 2) {
+      rf->a[4 * (k - k0) + q] = b32;
+      rb->a[4 * (k - k0) + q] = b32;
+    } else {
       *out = make_double4(B0, B1, B2, B3);
+    }
   }
   // LU of the diagonal block: every lane factors the whole block
   double M[16];
@@ -361,7 +373,13 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
     if (q == 1) f[1] = rp;
     if (q == 2) f[2] = rp;
     if (q == 3) f[3] = rp;
-    reinterpret_cast<float4*>(mt.lu32 + 16 * (long)mpos)[q] = make_float4(f[0], f[1], f[2], f[3]);
+    const float4 lu = make_float4(f[0], f[1], f[2], f[3]);
+    if (MIXED == 1) {
+      reinterpret_cast<float4*>(mt.lu32 + 16 * (long)mpos)[q] = lu;
+    } else {
+      rf->lu[q] = lu;
+      rb->lu[q] = lu;
+    }
   } else {
     reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] = make_double4(o0, o1, o2, o3);
   }
@@ -925,6 +943,112 @@ __global__ void k_prepare_sweep32(DevState s, const float* cur, float* next, int
     next[i] = cur[i];
   else
     next[i] = __uint_as_float(kNotReady32);
+}
+
+// Precision form, chunked order (mode 3): one colour of chunks, a CTA per
+// chunk, 64 rows (one per quad of 4 lanes, lane r owning block row r) per
+// pass.  The CTA first copies its window of the FP32 iterate (every row its
+// chunk touches) into shared memory, then walks the chunk's sub-levels in
+// order: the records of sub-level u+2 are copied into a 3-slot ring with
+// cp.async while sub-level u is computed, so the dependency chain only ever
+// reads shared memory.  Rows of one sub-level are independent; a barrier
+// separates sub-levels.  Rows of other chunks in the window are not written
+// by any CTA of this launch (chunks of one colour share no block).  Per row
+// the arithmetic is that of k_sweep_color32.
+constexpr int kRecRows = 64;
+constexpr int kRecSlots = 3;
+constexpr int kRecInts = (int)(sizeof(SweepRec) / 16);  // 16-byte words per record
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int DIR>
+__global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct, float* dq32,
+                                                     int colour, int last) {
+  if (*s.stop) return;  // the run has converged
+  extern __shared__ __align__(16) unsigned char sweep_smem[];
+  SweepRec* slots = reinterpret_cast<SweepRec*>(sweep_smem);
+  float4* win = reinterpret_cast<float4*>(sweep_smem + sizeof(SweepRec) * kRecSlots * kRecRows);
+  const int tid = threadIdx.x;
+  const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
+  const int2 w = ct.window[q];
+  const int nwin = w.y - w.x + 1;
+  float4* X = reinterpret_cast<float4*>(dq32);
+  for (int i = tid; i < nwin; i += blockDim.x) cp_async16(win + i, X + w.x + i);
+  cp_async_commit();
+  const int S0 = ct.chunk_sub[DIR][q], nsub = ct.chunk_sub[DIR][q + 1] - S0;
+  const int* ss = ct.sub_start[DIR] + S0;
+  const int4* recs = reinterpret_cast<const int4*>(ct.rec[DIR]);
+  auto issue = [&](int u) {
+    if (u < nsub) {
+      const int r0 = ss[u], words = (ss[u + 1] - r0) * kRecInts;
+      const int4* src = recs + (long)r0 * kRecInts;
+      int4* dst = reinterpret_cast<int4*>(slots + (u % kRecSlots) * kRecRows);
+      for (int i = tid; i < words; i += blockDim.x) cp_async16(dst + i, src + i);
+    }
+    cp_async_commit();  // one group per sub-level, empty past the end
+  };
+  issue(0);
+  issue(1);
+  const int quad = tid >> 2, r = tid & 3;
+  const int qbase = tid & 31 & ~3;
+  const unsigned qmask = 0xFu << qbase;
+  for (int u = 0; u < nsub; u++) {
+    issue(u + 2);
+    cp_async_wait<2>();  // the window and sub-levels 0..u have landed
+    __syncthreads();
+    if (quad < ss[u + 1] - ss[u]) {
+      const SweepRec& R = slots[(u % kRecSlots) * kRecRows + quad];
+      const int j = R.hdr.x, nb = R.hdr.y;
+      const int* cols = reinterpret_cast<const int*>(R.cols);
+      float acc = reinterpret_cast<const float*>(&R.rhs)[r];
+#pragma unroll
+      for (int t = 0; t < kRecBlocks; t++) {
+        if (t < nb) {
+          const float4 a = R.a[4 * t + r];
+          const float4 d = win[cols[t] - w.x];
+          float tt = __fmul_rn(a.x, d.x);
+          tt = __fmaf_rn(a.y, d.y, tt);
+          tt = __fmaf_rn(a.z, d.z, tt);
+          tt = __fmaf_rn(a.w, d.w, tt);
+          acc = __fsub_rn(acc, tt);
+        }
+      }
+      const float b0 = __shfl_sync(qmask, acc, qbase);
+      const float b1 = __shfl_sync(qmask, acc, qbase + 1);
+      const float b2 = __shfl_sync(qmask, acc, qbase + 2);
+      const float b3 = __shfl_sync(qmask, acc, qbase + 3);
+      if (r == 0) {
+        const float4 M0 = R.lu[0], M1 = R.lu[1], M2 = R.lu[2], M3 = R.lu[3];
+        const float y0 = b0;
+        const float y1 = __fmaf_rn(-M1.x, y0, b1);
+        const float y2 = __fmaf_rn(-M2.y, y1, __fmaf_rn(-M2.x, y0, b2));
+        const float y3 = __fmaf_rn(-M3.z, y2, __fmaf_rn(-M3.y, y1, __fmaf_rn(-M3.x, y0, b3)));
+        const float x3 = __fmul_rn(y3, M3.w);
+        const float x2 = __fmul_rn(__fmaf_rn(-M2.w, x3, y2), M2.z);
+        const float x1 = __fmul_rn(__fmaf_rn(-M1.w, x3, __fmaf_rn(-M1.z, x2, y1)), M1.y);
+        const float x0 = __fmul_rn(
+            __fmaf_rn(-M0.w, x3, __fmaf_rn(-M0.z, x2, __fmaf_rn(-M0.y, x1, y0))), M0.x);
+        const float4 x = make_float4(x0, x1, x2, x3);
+        win[j - w.x] = x;
+        X[j] = x;
+        if (last) reinterpret_cast<double4*>(s.dQ)[j] = make_double4(x0, x1, x2, x3);
+      }
+    }
+    __syncthreads();
+  }
+  cp_async_wait<0>();
 }
 
 // Before an ordered sweep: fill its result buffer with the not-ready

@@ -77,6 +77,35 @@ struct MixedTables {
   float* dq32b;           // second buffer of the ordered FP32 sweeps (swapped per sweep)
 };
 
+// Precision form, chunked order (mode 3).  The reference row order is cut
+// into chunks of consecutive rows (at most a set number of rows and of
+// dependency levels each), coloured greedily so that chunks of one colour
+// share no block; a sweep runs the colours in order, one CTA per chunk, and
+// inside a chunk the rows in the reference's order, level by level.  Each
+// direction keeps one record per row, in chunk / sub-level order, with all
+// the sweep reads of that row; a sub-level is at most kRecRows rows of one
+// level.
+constexpr int kRecBlocks = 8;  // off-diagonal blocks a record holds
+
+struct __align__(16) SweepRec {
+  int4 hdr;                 // row j, off-diagonal block count, 0, 0
+  float4 rhs;               // right-hand side (FP32)
+  float4 lu[4];             // LU factors of the diagonal block, reciprocal pivots
+  int4 cols[2];             // columns of the off-diagonal blocks (0: none)
+  float4 a[4 * kRecBlocks]; // the blocks, row-major, block t row r at a[4t + r]
+};
+
+struct ChunkTables {
+  int nchunks, ncol, maxwin;
+  const int* col_ptr;        // ncol+1: chunks of each colour in col_chunks
+  const int* col_chunks;
+  const int2* window;        // per chunk: first and last row any of its rows touches
+  SweepRec* rec[2];          // per direction (0 forward, 1 backward)
+  const int* sub_start[2];   // record index of each sub-level, plus the end
+  const int* chunk_sub[2];   // first sub-level of each chunk, plus the end
+  const int* pos[2];         // record index of each row (1..nn)
+};
+
 struct DevState {
   double* Q;
   double* nQ;

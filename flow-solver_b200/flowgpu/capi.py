@@ -28,7 +28,7 @@ ERR_BUDGET = 512
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
-           "flow_set_sweep_mode", "flow_set_precision", "flow_set_graphs", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_chunk_starts", "flow_set_graphs", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
            "flow_linear_residual_noalloc", "flow_arena_create", "flow_arena_destroy",
@@ -114,6 +114,8 @@ def _load_locked():
     L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
     L.flow_set_precision.argtypes = [vp, C.c_int]
     L.flow_set_graphs.argtypes = [vp, C.c_int]
+    L.flow_set_chunk.argtypes = [vp, C.c_int, C.c_int]
+    L.flow_chunk_starts.argtypes = [vp, IP, C.c_int, IP, IP]
     L.flow_save_state.argtypes = [vp]
     L.flow_restore_state.argtypes = [vp]
     L.flow_set_timing.argtypes = [vp, C.c_int]
@@ -449,8 +451,23 @@ class Solver:
 
     def set_precision(self, mode: int):
         """0: FP64 reference-order drop-in; 1: FP32 blocks, multicolour sweeps;
-        2: FP32 blocks, sweeps in the reference's row order."""
+        2: FP32 blocks, sweeps in the reference's row order; 3: FP32 blocks,
+        coloured chunks of the reference order."""
         _check(self.L.flow_set_precision(self.ctx, int(mode)), "flow_set_precision")
+
+    def set_chunk(self, rows: int = 0, levels: int = 0):
+        """Chunk limits of precision mode 3 (0: defaults)."""
+        _check(self.L.flow_set_chunk(self.ctx, int(rows), int(levels)), "flow_set_chunk")
+
+    def chunk_starts(self):
+        """(first row of each mode 3 chunk plus nn+1, number of colours)."""
+        n, k = C.c_int(), C.c_int()
+        _check(self.L.flow_chunk_starts(self.ctx, None, 0, C.byref(n), C.byref(k)),
+               "flow_chunk_starts")
+        out = np.zeros(n.value + 1, dtype=np.int32)
+        _check(self.L.flow_chunk_starts(self.ctx, out.ctypes.data_as(IP), out.size, C.byref(n),
+                                        C.byref(k)), "flow_chunk_starts")
+        return out, k.value
 
     def set_graphs(self, on: bool):
         """Replay full chunks of flow_converge steps from CUDA graphs (default on)."""

@@ -212,8 +212,22 @@ int flow_set_sweep_mode(flow_ctx *ctx, int mode);
  * nn..1, the FP64 drop-in's dependency-ordered sweep on FP32 blocks): steps
  * to converge as in mode 0, sweeps latency-bound as in mode 0.  In modes 1
  * and 2 the FP64 LHS is not formed (flow_get "LHS" is stale) and
- * flow_linear_solve reports rms = -1.  Switching builds the FP32 tables. */
+ * flow_linear_solve reports rms = -1.  Switching builds the FP32 tables.
+ * Mode 3 cuts the reference row order into chunks of consecutive rows (at
+ * most `rows` rows and `levels` dependency levels each, flow_set_chunk),
+ * colours the chunks so that chunks of one colour share no block, and sweeps
+ * the colours in order (forward ascending, backward descending), each chunk
+ * by one CTA in the reference's order inside the chunk: close to the
+ * reference order's convergence with a few launches per sweep.  It needs at
+ * most 8 off-diagonal blocks per row and a matrix bandwidth whose chunk
+ * windows fit in shared memory; otherwise switching to it fails. */
 int flow_set_precision(flow_ctx *ctx, int mode);
+/* Chunk limits of precision mode 3 (0: defaults, rows = twice the matrix
+ * bandwidth up to 2048, levels = 32). */
+int flow_set_chunk(flow_ctx *ctx, int rows, int levels);
+/* Mode 3 chunks in use: starts[0..nchunks] (first row of each chunk, then
+ * nn+1; up to cap entries written), their number and the colour count. */
+int flow_chunk_starts(flow_ctx *ctx, int *starts, int cap, int *nchunks, int *ncolours);
 
 /* flow_converge / flow_converge_batch issue steps in chunks; with graphs on
  * (the default) every full chunk after the first is replayed from a CUDA

@@ -907,22 +907,58 @@ void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, 
   free(dq32);
 }
 
+/* FP32 sweeps in an arbitrary row order: forward sweeps visit order[0..nn-1],
+ * backward sweeps the reverse (in place). */
+void orc_linear_solve_mixed_order(orc_grid *g, const orc_params *p, const int *order)
+{
+  int nn = g->nn;
+  long nnz = g->ia[nn + 1];
+  float *A32 = (float *)malloc(sizeof(float) * 16 * (nnz > 0 ? nnz : 1));
+  float *lu32 = (float *)malloc(sizeof(float) * 16 * (nn + 1));
+  float *dq32 = (float *)calloc((size_t)(nn + 1) * NV, sizeof(float));
+  for (long k = 0; k < 16 * nnz; k++) A32[k] = (float)g->LHS[k];
+  for (int j = 1; j <= nn; j++) {
+    double M[16];
+    memcpy(M, &g->LHS[(long)g->iau[j] * 16], sizeof(M));
+    lu4(M);
+    for (int q = 0; q < 16; q++) lu32[j * 16 + q] = (float)M[q];
+    for (int q = 0; q < 4; q++) lu32[j * 16 + 5 * q] = (float)(1.0 / M[5 * q]);
+  }
+  for (int it = 0; it < p->subits; it++) {
+    if (it % 2 == 0)
+      for (int i = 0; i < nn; i++) gs_row_mixed(g, A32, lu32, dq32, order[i]);
+    else
+      for (int i = nn - 1; i >= 0; i--) gs_row_mixed(g, A32, lu32, dq32, order[i]);
+  }
+  for (int j = 1; j <= nn; j++)
+    for (int r = 0; r < NV; r++) g->dQ[j * NV + r] = (double)dq32[j * NV + r];
+  free(A32);
+  free(lu32);
+  free(dq32);
+}
+
 static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm, int mixed,
-                      const int *color, int ncolors);
+                      const int *color, int ncolors, const int *order);
+
+int orc_solve_mixed_order(orc_grid *g, const orc_params *p, int ts, double *dqnorm,
+                          const int *order)
+{
+  return solve_impl(g, p, ts, dqnorm, 2, NULL, 0, order);
+}
 
 int orc_solve(orc_grid *g, const orc_params *p, int ts, double *dqnorm)
 {
-  return solve_impl(g, p, ts, dqnorm, 0, NULL, 0);
+  return solve_impl(g, p, ts, dqnorm, 0, NULL, 0, NULL);
 }
 
 int orc_solve_mixed(orc_grid *g, const orc_params *p, int ts, double *dqnorm, const int *color,
                     int ncolors)
 {
-  return solve_impl(g, p, ts, dqnorm, 1, color, ncolors);
+  return solve_impl(g, p, ts, dqnorm, 1, color, ncolors, NULL);
 }
 
 static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm, int mixed,
-                      const int *color, int ncolors)
+                      const int *color, int ncolors, const int *order)
 {
   int nn = g->nn, rc;
   double dql2 = 0.;
@@ -958,7 +994,9 @@ static int solve_impl(orc_grid *g, const orc_params *p, int ts, double *dqnorm, 
     if (p->tacc != 0 || p->unsteady != 0) return 40;
     for (int i = 1; i <= nn; i++)
       for (int j = 0; j < NV; j++) g->RHS[i * NV + j] = -(g->R[i * NV + j]);
-    if (mixed)
+    if (mixed == 2)
+      orc_linear_solve_mixed_order(g, p, order);
+    else if (mixed)
       orc_linear_solve_mixed(g, p, color, ncolors);
     else
       orc_linear_solve(g, p);

@@ -97,6 +97,13 @@ void orc_linear_solve_mixed(orc_grid *g, const orc_params *p, const int *color, 
 int orc_solve_mixed(orc_grid *g, const orc_params *p, int ts, double *dq, const int *color,
                     int ncolors);
 
+/* FP32 sweeps visiting rows in `order` (a permutation of 1..nn) forward and
+ * in reverse backward (the chunked order of the precision form is one such
+ * permutation); orc_solve_mixed_order is the step around it. */
+void orc_linear_solve_mixed_order(orc_grid *g, const orc_params *p, const int *order);
+int orc_solve_mixed_order(orc_grid *g, const orc_params *p, int ts, double *dq,
+                          const int *order);
+
 /* Building blocks, exposed for unit checks. */
 int orc_roe_flux(double nx, double ny, double len, double gamma, const double *ql,
                  const double *qr, double *flux);

@@ -67,6 +67,7 @@ def lib():
         L.orc_greedy_colors.argtypes = [gp, IP]
         L.orc_linear_solve_mixed.argtypes = [gp, pp, IP, C.c_int]
         L.orc_solve_mixed.argtypes = [gp, pp, C.c_int, DP, IP, C.c_int]
+        L.orc_solve_mixed_order.argtypes = [gp, pp, C.c_int, DP, IP]
         L.orc_roe_flux.argtypes = [C.c_double] * 4 + [DP, DP, DP]
         L.orc_curved_normal.argtypes = [C.c_int, DP, DP, DP]
         _lib = L
@@ -191,6 +192,17 @@ class OracleGrid:
         col, nc = self.colors()
         cp = None if ordered else col.ctypes.data_as(IP)
         self.L.orc_linear_solve_mixed(C.byref(self.g), C.byref(p), cp, nc)
+
+    def solve_mixed_order(self, p: OrcParams, ts: int, order) -> float:
+        """Precision form step with the sweeps visiting rows in `order`."""
+        o = np.ascontiguousarray(order, dtype=np.int32)
+        self.g.citer = ts
+        dq = C.c_double()
+        rc = self.L.orc_solve_mixed_order(C.byref(self.g), C.byref(p), ts, C.byref(dq),
+                                          o.ctypes.data_as(IP))
+        if rc:
+            raise RuntimeError(f"oracle solve failed with code {rc}")
+        return dq.value
 
     def solve_mixed(self, p: OrcParams, ts: int, ordered: bool = False) -> float:
         """Precision form step: multicolour sweeps, or (ordered) the

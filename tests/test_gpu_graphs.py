@@ -8,7 +8,7 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("precision,order,subits", [(0, 3, 2), (1, 3, 4), (0, 1, 2), (1, 1, 3),
-                                                    (2, 3, 2), (2, 1, 3)])
+                                                    (2, 3, 2), (2, 1, 3), (3, 3, 4), (3, 1, 3)])
 def test_graph_chunks_match_eager_steps(precision, order, subits):
     from flowgpu import capi, workloads
     from flowgpu.prep import Mesh

@@ -57,6 +57,55 @@ def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
     gpu.close()
 
 
+def chunk_order(ia, ja, starts):
+    """The row permutation of a mode 3 forward sweep, restated: chunks get
+    the smallest colour no earlier adjacent chunk holds; colours ascending,
+    chunks ascending, rows ascending."""
+    nn = int(starts[-1]) - 1
+    chunk_of = np.zeros(nn + 1, dtype=np.int64)
+    for q in range(len(starts) - 1):
+        chunk_of[starts[q]:starts[q + 1]] = q
+    colour = []
+    for q in range(len(starts) - 1):
+        used = {colour[int(chunk_of[ja[k]])] for j in range(starts[q], starts[q + 1])
+                for k in range(ia[j], ia[j + 1]) if chunk_of[ja[k]] < q}
+        c = 0
+        while c in used:
+            c += 1
+        colour.append(c)
+    order = [j for c in range(max(colour) + 1) for q in range(len(colour)) if colour[q] == c
+             for j in range(starts[q], starts[q + 1])]
+    return np.asarray(order, dtype=np.int32), max(colour) + 1
+
+
+@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,rows,levels", [
+    (32, 8, True, 3, 4, 6, 0, 0),
+    (128, 32, True, 3, 4, 4, 0, 0),
+    (64, 16, False, 1, 3, 4, 64, 0),
+    (128, 32, True, 3, 2, 3, 200, 6),
+])
+def test_chunked_steps_bitwise(nc, nr, curved, order, subits, steps, rows, levels):
+    """mode 3: coloured chunks of the reference order, against the oracle's
+    sweep in the same row permutation."""
+    mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits, 3)
+    gpu.set_chunk(rows, levels)
+    starts, ncol = gpu.chunk_starts()
+    nn = mesh.sizes["nn"]
+    perm, ncol2 = chunk_order(og["ia"], og["ja"], starts)
+    assert ncol2 == ncol and sorted(perm.tolist()) == list(range(1, nn + 1))
+    if rows:
+        assert np.diff(starts).max() <= rows
+    for ts in range(1, steps + 1):
+        og.solve_mixed_order(p, ts, perm)
+        gpu.solve(ts)
+        for name in ("Q", "nQ"):
+            assert ndiff(og[name][4:], gpu.get(name)[4:]) == 0, (name, ts)
+        for name in ("R", "dQ"):
+            assert ndiff(og[name][4:4 * (nn + 1)], gpu.get(name)[4:]) == 0, (name, ts)
+    assert gpu.status() == 0
+    gpu.close()
+
+
 def test_mixed_converges_to_the_fp64_answer():
     from flowgpu import capi, workloads
     from flowgpu.prep import Mesh
@@ -64,7 +113,7 @@ def test_mixed_converges_to_the_fp64_answer():
     mesh = Mesh.from_case(wl.write(), order=3)
     fp = wl.params()
     out = {}
-    for mode in (0, 1, 2):
+    for mode in (0, 1, 2, 3):
         s = capi.Solver.from_mesh(mesh, fp, device=0)
         s.set_precision(mode)
         s.set_state(mesh.initial_state(fp))
@@ -73,7 +122,7 @@ def test_mixed_converges_to_the_fp64_answer():
         out[mode] = (steps, s.body_forces(), s.get("Q"))
         s.close()
     n0, f0, q0 = out[0]
-    for mode in (1, 2):
+    for mode in (1, 2, 3):
         n1, f1, q1 = out[mode]
         assert abs(f1[0] - f0[0]) <= 1e-8 * max(1.0, abs(f0[0]))
         assert abs(f1[1] - f0[1]) <= 1e-8 * max(1.0, abs(f0[1]))
