@@ -60,6 +60,7 @@ for p in (ROOT, PKG):
 METRIC = "converged solves/s (1e-10 drop) served vs plain FP64 GPU; p50/p99 latency"
 UNIT = "solves/s"
 REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
+REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
 CPU_BASELINE_STEPS = 6      # pseudo-time steps timed for cpu_baseline
 
 
@@ -343,7 +344,8 @@ def run_batch(args, bw):
 
     def one_pass():
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n)
+        srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n, autotune=bw.autotune,
+                          stall=bw.stall)
         torch.cuda.synchronize()
         ev[0].record()
         slots = []
@@ -365,7 +367,7 @@ def run_batch(args, bw):
         ev[2].record()
         forces = {}
         for i, c in recs.items():  # converged states and forces back to the host
-            if c["status"] in (0, capi.ERR_NOT_CONVERGED):
+            if c["status"] in (0, capi.ERR_NOT_CONVERGED, capi.ERR_STALLED):
                 _q, forces[i] = srv.result(c["slot"], want_q=True)
             srv.release(c["slot"])
         ev[3].record()
@@ -384,7 +386,7 @@ def run_batch(args, bw):
             raise RuntimeError("non-deterministic batch: step counts differ between passes")
     barrier(pg)
     dev_ms = e2e_ms = 0.
-    lat, launches, n_conv, n_fail = [], 0, 0, 0
+    lat, launches, n_conv, n_fail, n_stall = [], 0, 0, 0, 0
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             recs, forces, v_ms, e_ms = one_pass()
@@ -393,7 +395,9 @@ def run_batch(args, bw):
             lat += [r["device_ms"] / 1e3 for r in recs]
             launches += sum(r["launches"] for r in recs)
             n_conv += sum(1 for r in recs if r["status"] == 0)
-            n_fail += sum(1 for r in recs if r["status"] not in (0, capi.ERR_NOT_CONVERGED))
+            n_fail += sum(1 for r in recs
+                          if r["status"] not in (0, capi.ERR_NOT_CONVERGED, capi.ERR_STALLED))
+            n_stall += sum(1 for r in recs if r["status"] == capi.ERR_STALLED)
     barrier(pg)
     dev_ms_max = allreduce_max(pg, dev_ms)
     e2e_ms_max = allreduce_max(pg, e2e_ms)
@@ -443,9 +447,10 @@ def run_batch(args, bw):
         conv64 = sum(1 for st in bw.fp64_status if st == 0)
         plain = {"value": round(conv64 / tot, 5), "unit": UNIT, "converged": conv64,
                  "seconds": round(tot, 2), "ms_per_step": per,
-                 "how": "recorded FP64 step count of each request (capped at max_steps) x its "
-                        "FP64 drop-in ms/step measured over 96 steps (graph chunks), solved "
-                        "one after the other"}
+                 "how": "recorded FP64 step count of each request (capped at max_steps; the "
+                        "drop-in runs every solve to its drop or max_steps, as the reference's "
+                        "driver does) x its FP64 drop-in ms/step measured over 96 steps (graph "
+                        "chunks), solved one after the other"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and bw.fp64_steps is not None:
@@ -461,10 +466,15 @@ def run_batch(args, bw):
             "config": {"workload": bw.name, "form": "batching (served, all admitted together)",
                        "requests_per_gpu": bw.n, "stream_seed": bw.seed,
                        "nodes": [r.nodes for r in reqs], "orders": [r.order for r in reqs],
-                       "precision": "FP64 residual/geometry/update, FP32 blocks + multicolour "
-                                    "GS" if bw.precision == 1 else f"mode {bw.precision}",
+                       "precision": {1: "FP64 residual/geometry/update, FP32 blocks, "
+                                        "multicolour GS",
+                                     3: "FP64 residual/geometry/update, FP32 blocks, GS in "
+                                        "coloured chunks of the reference order"}.get(
+                                            bw.precision, f"mode {bw.precision}"),
                        "gs_sweeps": bw.subits, "drop": bw.drop, "max_steps": bw.max_steps,
+                       "stall_retire_steps": bw.stall, "autotune_steps": bw.autotune,
                        "converged_per_pass": n_conv // max(args.steps, 1),
+                       "stalled_per_pass": n_stall // max(args.steps, 1),
                        "failed_per_pass": n_fail // max(args.steps, 1),
                        "l2": "working set larger than L2 (batch of meshes, 0.1-0.5 GB each)",
                        "parallelism": f"requests sharded over {world} GPU(s)"},
@@ -625,11 +635,15 @@ def run_reference_batch(args, bw):
     """The reference CPU solver on the batch's requests with all host cores:
     each request's time per pseudo-time step is measured (one process per
     core), times its recorded step count; the requests are packed on the
-    cores longest first."""
+    cores longest first.  A request on which the FP64 drop-in (and so the
+    reference) fails with a non-physical state is not run: the reference does
+    not return from such states (request 9 of the batch hangs from step 3),
+    so its recorded steps are charged at its order's measured cost per node
+    and step."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from flowgpu import serve
+    from flowgpu import capi, serve
     from oracle import ref
     if not ref.available():
         print(json.dumps({"impl": "reference",
@@ -643,26 +657,43 @@ def run_reference_batch(args, bw):
     import multiprocessing as mp
     cores = os.cpu_count() or 1
     reqs = [serve.sample_request(i, seed=bw.seed) for i in range(bw.n)]
-    dirs = [r.workload(2, bw.max_steps, bw.drop).write(tempfile.mkdtemp(prefix="bench_ref_"))
-            for r in reqs]
+    runnable = [i for i in range(bw.n) if bw.fp64_status[i] in (0, capi.ERR_NOT_CONVERGED)]
+    dirs = {i: reqs[i].workload(2, bw.max_steps, bw.drop).write(
+        tempfile.mkdtemp(prefix="bench_ref_")) for i in runnable}
     ctx = mp.get_context("spawn")
-    with ctx.Pool(min(cores, len(reqs))) as pool:
-        per_step = pool.map(_ref_batch_worker, [(d, args.warmup, args.steps) for d in dirs])
-    times = [bw.fp64_steps[i] * per_step[i] for i in range(len(reqs))]
+    per_step = {}
+    with ctx.Pool(min(cores, len(runnable))) as pool:
+        jobs = {i: pool.apply_async(_ref_batch_worker, ((dirs[i], args.warmup, args.steps),))
+                for i in runnable}
+        deadline = time.time() + REF_ARM_TIMEOUT_S
+        for i, job in jobs.items():
+            per_step[i] = job.get(timeout=max(1.0, deadline - time.time()))
+    cost = {}
+    for o in (1, 3):
+        v = [per_step[i] / reqs[i].nodes for i in runnable if reqs[i].order == o]
+        if v:
+            cost[o] = sorted(v)[len(v) // 2]
+    for i in range(bw.n):
+        if i not in per_step:
+            c = cost.get(reqs[i].order, next(iter(cost.values())))
+            per_step[i] = c * reqs[i].nodes
+    times = [bw.fp64_steps[i] * per_step[i] for i in range(bw.n)]
     makespan = _lpt_makespan(times, cores)
     conv64 = sum(1 for st in bw.fp64_status if st == 0)
     rate = conv64 / makespan
-    sample = (f"{len(reqs)} requests, each timing {args.steps} x {REF_SAMPLE_STEPS} pseudo-time "
-              f"steps after set-up and {args.warmup} x {REF_SAMPLE_STEPS} warm-up steps "
-              f"({min(cores, len(reqs))} processes); recorded steps per request x s/step, "
-              f"packed on {cores} cores longest first: makespan {makespan:.1f} s for "
-              f"{conv64} converged solves")
+    sample = (f"{len(runnable)} of {bw.n} requests run, each timing {args.steps} x "
+              f"{REF_SAMPLE_STEPS} pseudo-time steps after set-up and {args.warmup} x "
+              f"{REF_SAMPLE_STEPS} warm-up steps ({min(cores, len(runnable))} processes); the "
+              f"{bw.n - len(runnable)} that fail with a non-physical state charged at their "
+              f"order's median s per node-step; recorded steps x s/step per request, packed "
+              f"on {cores} cores longest first: makespan {makespan:.1f} s for {conv64} "
+              f"converged solves")
     line = {"metric": METRIC, "value": round(rate, 8), "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {"workload": bw.name, "nodes": [r.nodes for r in reqs],
-                       "s_per_step": [round(x, 4) for x in per_step]},
+                       "s_per_step": [round(per_step[i], 4) for i in range(bw.n)]},
             "cpu_baseline": {"value": round(rate, 8), "unit": UNIT, "cores": cores,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": round(rate, 8), "unit": UNIT, "h2d_bytes_per_step": 0,

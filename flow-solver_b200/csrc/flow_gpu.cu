@@ -16,6 +16,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <map>
 #include <mutex>
 #include <string>
@@ -146,6 +147,7 @@ struct flow_ctx {
   int* h_flags = nullptr;      // pinned: stop flag and status read back by flow_converge_batch
   cudaEvent_t ev_flag = nullptr;
   int* h_run = nullptr;        // pinned: 2 slots of {stop, status, steps done} for a served run
+  double* h_runr = nullptr;    // pinned: 2 slots of {R_rho^2 of the last step, R_rho of the first}
   cudaEvent_t ev_run[2] = {nullptr, nullptr};
   // optional per-kernel event timing
   int timing = 0;
@@ -166,6 +168,7 @@ struct flow_ctx {
   // precision form (flow_set_precision): 0 FP64 reference order, 1 FP32
   // blocks with multicolour sweeps; tables built on first use
   int precision = 0;
+  int var[2] = {0, 0};  // kernel variants: k_node_prepare4, k_subedge_flux (autotuner)
   MixedTables mt{};
   bool mt_ordered = false;  // tables in reference row order (modes 2, 3) or colour order (mode 1)
   ChunkTables ct{};          // mode 3 tables and sweep records
@@ -302,13 +305,35 @@ void harvest(flow_ctx* c) {
   c->pending.clear();
 }
 
+// Kernel variants the autotuner chooses between: minimum resident blocks per
+// SM in __launch_bounds__ (which caps the registers per thread).
+// k_node_prepare4: variant 0, 1, 2 -> 0 (compiler's choice), 10, 12 blocks.
+// k_subedge_flux:  variant 0, 1, 2 -> 4, 5, 3 blocks.
+constexpr int kVariants = 3;
+template <class F>
+void launch_variant(int v, F&& f) {
+  if (v == 1) f(std::integral_constant<int, 10>());
+  else if (v == 2) f(std::integral_constant<int, 12>());
+  else f(std::integral_constant<int, 0>());
+}
+template <class F>
+void launch_flux_variant(int v, F&& f) {
+  if (v == 1) f(std::integral_constant<int, 5>());
+  else if (v == 2) f(std::integral_constant<int, 3>());
+  else f(std::integral_constant<int, 4>());
+}
+
 int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   Timed tm(c, 0);
   int nb = grid_blocks(4 * c->nn, 128);
   if (c->order == 1)
-    k_node_prepare4<1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+    launch_variant(c->var[0], [&](auto V) {
+      k_node_prepare4<1, V.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+    });
   else
-    k_node_prepare4<3><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+    launch_variant(c->var[0], [&](auto V) {
+      k_node_prepare4<3, V.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+    });
   return launch_check(c);
 }
 
@@ -318,11 +343,15 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
     Timed t(c, 1);
     int nbs = grid_blocks(c->ns, 128);
     if (a.recon == 1) {
-      if (jac) k_subedge_flux<1, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
-      else k_subedge_flux<1, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+      launch_flux_variant(c->var[1], [&](auto V) {
+        if (jac) k_subedge_flux<1, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        else k_subedge_flux<1, false, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+      });
     } else {
-      if (jac) k_subedge_flux<0, true><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
-      else k_subedge_flux<0, false><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+      launch_flux_variant(c->var[1], [&](auto V) {
+        if (jac) k_subedge_flux<0, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        else k_subedge_flux<0, false, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+      });
     }
     rc |= launch_check(c);
   }
@@ -364,7 +393,7 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
   if (c->precision == 3) {
     // coloured chunks of the reference order, in-place FP32 iterate
     const ChunkTables& ct = c->ct;
-    const size_t smem = sizeof(SweepRec) * kRecSlots * kRecRows + sizeof(float4) * ct.maxwin;
+    const size_t smem = 16 * kRecStride * kRecSlots * kRecRows + sizeof(float4) * ct.maxwin;
     for (int it = 0; it < p->subits; it++) {
       Timed t(c, 4);
       const int last = it == p->subits - 1, dir = it % 2;
@@ -754,7 +783,7 @@ int build_chunk_tables(flow_ctx* c) {
     win[q] = make_int2(a, b);
     maxwin = std::max(maxwin, b - a + 1);
   }
-  const size_t smem = sizeof(SweepRec) * kRecSlots * kRecRows + sizeof(float4) * maxwin;
+  const size_t smem = 16 * kRecStride * kRecSlots * kRecRows + sizeof(float4) * maxwin;
   if (smem > 227 * 1024) {
     set_error("precision mode 3: a chunk's window does not fit in shared memory (bandwidth too large)");
     return FLOW_ERR_ARG;
@@ -824,10 +853,13 @@ int build_chunk_tables(flow_ctx* c) {
     set_error("precision mode 3: table upload failed");
     return FLOW_ERR_CUDA;
   }
+  // the limit is a property of the kernel, shared by every context: allow the
+  // largest window any context may need, not this context's own
+  const int smem_cap = 227 * 1024;
   if (cudaFuncSetAttribute(k_sweep_chunk<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess ||
+                           smem_cap) != cudaSuccess ||
       cudaFuncSetAttribute(k_sweep_chunk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess) {
+                           smem_cap) != cudaSuccess) {
     set_error("precision mode 3: cannot reserve shared memory for the sweep");
     return FLOW_ERR_CUDA;
   }
@@ -1179,6 +1211,7 @@ void flow_destroy(flow_ctx* c) {
   for (cudaEvent_t e : c->ev_run)
     if (e) cudaEventDestroy(e);
   if (c->h_run) cudaFreeHost(c->h_run);
+  if (c->h_runr) cudaFreeHost(c->h_runr);
   c->buf.release();
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1611,6 +1644,78 @@ int flow_restore_state(flow_ctx* c) {
   return read_status(c);
 }
 
+int flow_set_variants(flow_ctx* c, int node_prepare, int flux) {
+  if (!c || !c->ok || node_prepare < 0 || node_prepare >= kVariants || flux < 0 ||
+      flux >= kVariants) {
+    set_error("flow_set_variants: null context or variant outside 0..2");
+    return FLOW_ERR_ARG;
+  }
+  if (c->var[0] != node_prepare || c->var[1] != flux) {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    drop_graphs(c);
+  }
+  c->var[0] = node_prepare;
+  c->var[1] = flux;
+  return 0;
+}
+
+int flow_autotune(flow_ctx* c, const flow_params* p, int ts, int steps, int* variants,
+                  double* ms) {
+  if (!c || !c->ok || ts < 1) return FLOW_ERR_ARG;
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if (steps < 1) steps = 4;
+  if ((rc = flow_save_state(c))) return rc;
+  if ((rc = ensure_hist(c, 1))) return rc;
+  const int saved_timing = c->timing;
+  long kc[8];
+  double km[8];
+  std::copy(c->kcount, c->kcount + 8, kc);
+  std::copy(c->kms, c->kms + 8, km);
+  for (int k = 0; k < 2 && !rc; k++) {  // class 0: k_node_prepare4, class 1: k_subedge_flux
+    int best = c->var[k];
+    double best_ms = 1e30;
+    for (int v = 0; v < kVariants && !rc; v++) {
+      c->var[k] = v;
+      rc |= flow_restore_state(c);
+      reset_run(c, 0.);
+      c->timing = 0;
+      rc |= enqueue_step(c, p, ts, -1, 1);  // warm-up, untimed
+      cudaStreamSynchronize(c->stream);
+      harvest(c);
+      c->kcount[k] = 0;
+      c->kms[k] = 0.;
+      c->timing = 1;
+      for (int i = 0; i < steps && !rc; i++) rc |= enqueue_step(c, p, ts + 1 + i, -1, 0);
+      if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc |= FLOW_ERR_CUDA;
+      harvest(c);
+      const double t = c->kcount[k] ? c->kms[k] / c->kcount[k] : 1e30;
+      if (ms) ms[k * kVariants + v] = t;
+      if (t < best_ms) {
+        best_ms = t;
+        best = v;
+      }
+    }
+    c->var[k] = best;
+  }
+  c->timing = saved_timing;
+  std::copy(kc, kc + 8, c->kcount);
+  std::copy(km, km + 8, c->kms);
+  // the timing steps may have run into a non-physical state; the solve that
+  // follows starts from the restored state with a clear status
+  cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream);
+  rc |= flow_restore_state(c);
+  reset_run(c, 0.);
+  drop_graphs(c);
+  if (variants) {
+    variants[0] = c->var[0];
+    variants[1] = c->var[1];
+  }
+  return rc & FLOW_ERR_CUDA ? rc : read_status(c);
+}
+
 int flow_set_timing(flow_ctx* c, int on) {
   if (!c || !c->ok) return FLOW_ERR_ARG;
   cudaStreamSynchronize(c->stream);
@@ -1893,7 +1998,8 @@ int begin_run(flow_ctx* c, const flow_params* p, double drop) {
   cudaSetDevice(c->device);
   if ((rc = ensure_hist(c, 1))) return rc;
   if (!c->h_run) {
-    if (cudaHostAlloc(&c->h_run, 6 * sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+    if (cudaHostAlloc(&c->h_run, 6 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaHostAlloc(&c->h_runr, 4 * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
       set_error("pinned flag allocation failed");
       return FLOW_ERR_CUDA;
     }
@@ -1922,11 +2028,14 @@ int post_flags(flow_ctx* c, int slot) {
   cudaMemcpyAsync(h, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   cudaMemcpyAsync(h + 1, c->s.status, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
   cudaMemcpyAsync(h + 2, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+  double* hr = c->h_runr + 2 * slot;
+  cudaMemcpyAsync(hr, c->s.scalars + 2, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  cudaMemcpyAsync(hr + 1, c->s.scalars + 6, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (cudaEventRecord(c->ev_run[slot], c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
   return 0;
 }
 
-int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps) {
+int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps, double* r_rel) {
   cudaError_t e = cudaEventQuery(c->ev_run[slot]);
   if (e == cudaErrorNotReady) return 0;
   if (e != cudaSuccess) {
@@ -1937,6 +2046,8 @@ int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps) {
   *stop = h[0];
   *status = h[1];
   *steps = h[2];
+  const double* hr = c->h_runr + 2 * slot;
+  *r_rel = hr[1] > 0. ? sqrt(hr[0]) / hr[1] : 1.;
   return 1;
 }
 

@@ -16,9 +16,10 @@ int enqueue_steps(flow_ctx* c, const flow_params* p, int ts0, int K);
 // Queue a read-back of {stop, status, steps done} into flag slot `slot`
 // (0 or 1) of the context's pinned flags, with an event behind it.
 int post_flags(flow_ctx* c, int slot);
-// 1 when flag slot `slot` has arrived (values in *stop, *status, *steps),
+// 1 when flag slot `slot` has arrived (values in *stop, *status, *steps and
+// *r_rel = ||R_rho|| of the last step over that of the run's first),
 // 0 while it is in flight, -1 on a CUDA error.
-int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps);
+int flags_ready(flow_ctx* c, int slot, int* stop, int* status, int* steps, double* r_rel);
 // Device time from the run's start to flag slot `slot` (ms).
 double run_ms(flow_ctx* c, int slot);
 // ||R_rho|| of the run's first step and of its last step.

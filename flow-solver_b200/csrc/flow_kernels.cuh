@@ -104,8 +104,10 @@ __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
 // only involve variable v, and each lane accumulates its sums in the
 // reference's face / stencil order.  The wave-speed sum (all variables) is
 // formed by every lane of the quad from node constants computed once.
-template <int ORDER>
-__global__ void __launch_bounds__(128) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
+// MINB: resident blocks per SM the compiler must allow (0: its own choice);
+// the autotuner picks the variant that runs fastest on a given mesh.
+template <int ORDER, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (tid >> 2) + 1, v = tid & 3;
@@ -388,8 +390,8 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
 // ---------------------------------------------------------------------------
 // Per subedge: face states, Roe flux, forward-difference Jacobian
 // (residual.C:112-333, reconstruct.C:181-203, jacobian.C:45-110).
-template <int RECON, bool JAC>
-__global__ void __launch_bounds__(128, 4) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
+template <int RECON, bool JAC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
   int sub = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (sub > m.ns) return;
@@ -958,6 +960,9 @@ __global__ void k_prepare_sweep32(DevState s, const float* cur, float* next, int
 constexpr int kRecRows = 64;
 constexpr int kRecSlots = 3;
 constexpr int kRecInts = (int)(sizeof(SweepRec) / 16);  // 16-byte words per record
+// records sit 704 bytes apart in shared memory (640 + 64 of padding), so the
+// two quads of a half-warp read disjoint bank ranges
+constexpr int kRecStride = kRecInts + 4;
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
@@ -978,8 +983,8 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
                                                      int colour, int last) {
   if (*s.stop) return;  // the run has converged
   extern __shared__ __align__(16) unsigned char sweep_smem[];
-  SweepRec* slots = reinterpret_cast<SweepRec*>(sweep_smem);
-  float4* win = reinterpret_cast<float4*>(sweep_smem + sizeof(SweepRec) * kRecSlots * kRecRows);
+  int4* slots = reinterpret_cast<int4*>(sweep_smem);
+  float4* win = reinterpret_cast<float4*>(sweep_smem + 16 * kRecStride * kRecSlots * kRecRows);
   const int tid = threadIdx.x;
   const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
   const int2 w = ct.window[q];
@@ -994,8 +999,11 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
     if (u < nsub) {
       const int r0 = ss[u], words = (ss[u + 1] - r0) * kRecInts;
       const int4* src = recs + (long)r0 * kRecInts;
-      int4* dst = reinterpret_cast<int4*>(slots + (u % kRecSlots) * kRecRows);
-      for (int i = tid; i < words; i += blockDim.x) cp_async16(dst + i, src + i);
+      int4* dst = slots + (u % kRecSlots) * kRecRows * kRecStride;
+      for (int i = tid; i < words; i += blockDim.x) {
+        const int rr = i / kRecInts, ww = i - rr * kRecInts;
+        cp_async16(dst + rr * kRecStride + ww, src + i);
+      }
     }
     cp_async_commit();  // one group per sub-level, empty past the end
   };
@@ -1009,7 +1017,8 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
     cp_async_wait<2>();  // the window and sub-levels 0..u have landed
     __syncthreads();
     if (quad < ss[u + 1] - ss[u]) {
-      const SweepRec& R = slots[(u % kRecSlots) * kRecRows + quad];
+      const SweepRec& R = *reinterpret_cast<const SweepRec*>(
+          slots + ((u % kRecSlots) * kRecRows + quad) * kRecStride);
       const int j = R.hdr.x, nb = R.hdr.y;
       const int* cols = reinterpret_cast<const int*>(R.cols);
       float acc = reinterpret_cast<const float*>(&R.rhs)[r];

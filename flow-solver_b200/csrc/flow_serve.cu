@@ -17,6 +17,9 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <map>
+#include <tuple>
 #include <string>
 #include <thread>
 #include <vector>
@@ -41,6 +44,8 @@ struct Slot {
   int oldest_flag = 0; // flag slot of the oldest chunk in flight
   int status = 0, steps = 0;
   double r_first = 0., r_last = 0., ms = 0.;
+  double best = 1.;     // best ||R_rho|| relative to the first step, kept by factors of 10
+  int best_step = 0;    // step at which it last improved tenfold
 };
 
 }  // namespace
@@ -51,6 +56,10 @@ struct flow_server {
   int chunk = 32;
   std::vector<Slot> slots;
   int running = 0;
+  int autotune_steps = 0;  // 0: no autotuning at admission
+  int stall_steps = 0;     // 0: no stall retirement
+  // autotuned kernel variants by (order, precision, mesh-size bucket)
+  std::map<std::tuple<int, int, int>, std::pair<int, int>> tuned;
 };
 
 namespace {
@@ -135,6 +144,21 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   }
   int rc = flow_set_precision(c, precision);
   if (!rc) rc = flow_set_state(c, Q0);
+  if (!rc && sv->autotune_steps > 0) {
+    // kernel variants: measured once per (order, precision, size bucket)
+    const long nn = flow_size(c, "dt") - 1;
+    const int bucket = (int)std::floor(2.0 * std::log2((double)std::max(nn, 1L)));
+    const auto key = std::make_tuple(p->order, precision, bucket);
+    auto it = sv->tuned.find(key);
+    if (it != sv->tuned.end()) {
+      rc = flow_set_variants(c, it->second.first, it->second.second);
+    } else {
+      int v[2] = {0, 0};
+      const int trc = flow_autotune(c, p, 1, sv->autotune_steps, v, nullptr);
+      if (trc & FLOW_ERR_CUDA) rc = trc;  // other bits: the tuning steps' physics, not fatal
+      else sv->tuned[key] = std::make_pair(v[0], v[1]);
+    }
+  }
   if (rc) {
     g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
     flow_destroy(c);
@@ -195,13 +219,21 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
       Slot& sl = sv->slots[i];
       if (sl.state != 1) continue;
       int stop = 0, status = 0, steps = 0;
-      int r = flow::internal::flags_ready(sl.ctx, sl.oldest_flag, &stop, &status, &steps);
+      double rr = 1.;
+      int r = flow::internal::flags_ready(sl.ctx, sl.oldest_flag, &stop, &status, &steps, &rr);
       if (r == 0) continue;
       any = true;
       if (r < 0) status = FLOW_ERR_CUDA;
       const int fs = sl.oldest_flag;
       sl.oldest_flag ^= 1;
       sl.inflight--;
+      // stall: no tenfold drop of the best residual within stall_steps steps
+      if (rr < sl.best * 0.1) {
+        sl.best = rr;
+        sl.best_step = steps;
+      }
+      if (!stop && !status && sv->stall_steps > 0 && steps - sl.best_step >= sv->stall_steps)
+        status = FLOW_ERR_STALLED;
       bool done = stop || status || (sl.issued >= sl.max_steps && sl.inflight == 0);
       if (done) {
         // let the chunk still in flight (no-op steps after the stop) drain
@@ -276,5 +308,17 @@ int flow_server_release(flow_server* sv, int slot) {
 }
 
 int flow_server_running(flow_server* sv) { return sv ? sv->running : -1; }
+
+int flow_server_set_stall(flow_server* sv, int steps) {
+  if (!sv || steps < 0) return FLOW_ERR_ARG;
+  sv->stall_steps = steps;
+  return 0;
+}
+
+int flow_server_set_autotune(flow_server* sv, int steps) {
+  if (!sv || steps < 0) return FLOW_ERR_ARG;
+  sv->autotune_steps = steps;
+  return 0;
+}
 
 }  // extern "C"

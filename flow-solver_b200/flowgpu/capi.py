@@ -20,22 +20,26 @@ DP = C.POINTER(C.c_double)
 LP = C.POINTER(C.c_long)
 
 ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
-          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND", 256: "NOT_CONVERGED", 512: "BUDGET"}
+          64: "SWEEP_TIMEOUT", 128: "NOT_FOUND", 256: "NOT_CONVERGED", 512: "BUDGET",
+          1024: "STALLED"}
 ERR_NOT_CONVERGED = 256
 ERR_BUDGET = 512
+ERR_STALLED = 1024
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
-           "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_chunk_starts", "flow_set_graphs", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_chunk_starts", "flow_set_graphs",
+           "flow_autotune", "flow_set_variants", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
            "flow_linear_residual_noalloc", "flow_arena_create", "flow_arena_destroy",
            "flow_arena_free_bytes", "flow_arena_largest_free", "flow_create_in",
            "flow_ctx_device_bytes", "flow_server_create", "flow_server_destroy",
            "flow_server_submit", "flow_server_stage", "flow_server_start", "flow_server_progress", "flow_server_result",
-           "flow_server_release", "flow_server_running", "flow_server_last_error")
+           "flow_server_release", "flow_server_running", "flow_server_last_error",
+           "flow_server_set_autotune", "flow_server_set_stall")
 
 
 class FlowParamsC(C.Structure):
@@ -115,6 +119,8 @@ def _load_locked():
     L.flow_set_precision.argtypes = [vp, C.c_int]
     L.flow_set_graphs.argtypes = [vp, C.c_int]
     L.flow_set_chunk.argtypes = [vp, C.c_int, C.c_int]
+    L.flow_autotune.argtypes = [vp, PP, C.c_int, C.c_int, IP, DP]
+    L.flow_set_variants.argtypes = [vp, C.c_int, C.c_int]
     L.flow_chunk_starts.argtypes = [vp, IP, C.c_int, IP, IP]
     L.flow_save_state.argtypes = [vp]
     L.flow_restore_state.argtypes = [vp]
@@ -154,6 +160,8 @@ def _load_locked():
     L.flow_server_release.argtypes = [vp, C.c_int]
     L.flow_server_running.argtypes = [vp]
     L.flow_server_last_error.restype = C.c_char_p
+    L.flow_server_set_autotune.argtypes = [vp, C.c_int]
+    L.flow_server_set_stall.argtypes = [vp, C.c_int]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
     L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
@@ -216,13 +224,18 @@ class Server:
     submit() returns a slot or None when the arena / slot table is full
     (FLOW_ERR_BUDGET); progress() returns retired solves as dicts."""
 
-    def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64):
+    def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64, autotune: int = 0,
+                 stall: int = 0):
         self.L = load()
         st = C.c_int(0)
         self.arena = arena
         self.h = self.L.flow_server_create(arena.h, int(chunk), int(max_slots), C.byref(st))
         if not self.h:
             raise FlowError(st.value or 1, "flow_server_create")
+        if autotune:
+            _check(self.L.flow_server_set_autotune(self.h, int(autotune)), "autotune")
+        if stall:
+            _check(self.L.flow_server_set_stall(self.h, int(stall)), "stall")
         self._keep = {}
         self._out = (FlowCompletion * 64)()
 
@@ -468,6 +481,19 @@ class Solver:
         _check(self.L.flow_chunk_starts(self.ctx, out.ctypes.data_as(IP), out.size, C.byref(n),
                                         C.byref(k)), "flow_chunk_starts")
         return out, k.value
+
+    def autotune(self, ts: int = 2, steps: int = 4):
+        """Pick the fastest kernel variants on this mesh; returns
+        ((node_prepare variant, flux variant), per-variant ms)."""
+        v = (C.c_int * 2)()
+        ms = (C.c_double * 6)()
+        _check(self.L.flow_autotune(self.ctx, C.byref(self.p), int(ts), int(steps), v, ms),
+               "flow_autotune")
+        return (v[0], v[1]), [round(x, 4) for x in ms]
+
+    def set_variants(self, node_prepare: int, flux: int):
+        _check(self.L.flow_set_variants(self.ctx, int(node_prepare), int(flux)),
+               "flow_set_variants")
 
     def set_graphs(self, on: bool):
         """Replay full chunks of flow_converge steps from CUDA graphs (default on)."""

@@ -90,7 +90,12 @@ class BatchWorkload:
     the reference, so these are the reference's own counts) does on requests
     0..n-1 of the stream: steps taken and 0 converged, 256 stopped at
     max_steps, other values failed (a non-physical state).  Measured with
-    ``bench.py --measure-fp64``."""
+    ``bench.py --measure-fp64``.
+
+    ``stall``: the server retires a solve whose best ||R_rho|| has not
+    dropped tenfold for this many steps (on these requests every converging
+    solve drops tenfold within at most 568 steps, FP64 or precision form);
+    ``autotune``: steps per kernel variant timed at admission."""
     name: str
     seed: int
     n: int
@@ -101,11 +106,13 @@ class BatchWorkload:
     chunk: int = 32
     fp64_steps: tuple | None = None
     fp64_status: tuple | None = None
+    stall: int = 0
+    autotune: int = 0
 
 
 BATCHES = {
     "batch16": BatchWorkload(
-        "batch16", 0, 16, 8000, 1e-10, 1, 4,
+        "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=2000, autotune=4,
         fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065,
                     1395, 1487, 8000),
         fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256)),

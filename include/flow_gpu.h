@@ -34,6 +34,7 @@ extern "C" {
 #define FLOW_ERR_NOT_FOUND 128  /* unknown array name */
 #define FLOW_ERR_NOT_CONVERGED 256 /* flow_converge reached max_steps */
 #define FLOW_ERR_BUDGET 512     /* the arena (or the server's slot table) has no room now */
+#define FLOW_ERR_STALLED 1024   /* a served solve's residual stopped falling (flow_server_set_stall) */
 
 /* Mirrors PARAMS (include/params.h:19-76 of the reference), same field
  * order and meaning as euler.params (params.C:44-217). */
@@ -264,6 +265,21 @@ long flow_launch_count(flow_ctx *ctx);
 /* Device time (ms) of the last flow_run / flow_solve call, CUDA events. */
 double flow_last_device_ms(flow_ctx *ctx);
 
+/* ---- Autotuner (no counterpart in the reference) -------------------------
+ * k_node_prepare4 and k_subedge_flux come in three variants each (the
+ * minimum resident blocks per SM the compiler must allow, i.e. how many
+ * registers a thread may hold); the results are bit-identical, the speed
+ * depends on the mesh.  flow_autotune times each variant over `steps`
+ * pseudo-time steps from step index `ts` (CUDA events, after one warm-up
+ * step), keeps the fastest, and puts the solution state back as it was
+ * with a clear status (the returned status still reports what the timing
+ * steps ran into).  variants[2] receives the choice, ms[6] (may be NULL)
+ * the average kernel times per variant.  flow_set_variants sets a choice
+ * directly (0..2). */
+int flow_autotune(flow_ctx *ctx, const flow_params *p, int ts, int steps, int *variants,
+                  double *ms);
+int flow_set_variants(flow_ctx *ctx, int node_prepare, int flux);
+
 /* ---- Device arena (no counterpart in the reference) ----------------------
  * One cudaMalloc of `bytes` on `device`, carved into the buffers of the
  * contexts created in it (256-byte aligned, first fit, freed blocks merge).
@@ -325,6 +341,17 @@ int flow_server_result(flow_server *srv, int slot, double *Q, long nQ, double *f
 /* Free a retired solve's context (its arena memory returns to the pool). */
 int flow_server_release(flow_server *srv, int slot);
 int flow_server_running(flow_server *srv);
+/* Autotune the kernel variants of each admitted solve over `steps` steps
+ * (flow_autotune), once per (order, precision, mesh-size bucket of a factor
+ * sqrt(2) in nodes); later admissions in the bucket reuse the choice.
+ * 0 (default) turns it off. */
+int flow_server_set_autotune(flow_server *srv, int steps);
+/* Retire a running solve with FLOW_ERR_STALLED once its best ||R_rho||
+ * (relative to its first step, tracked in factors of 10 at chunk
+ * boundaries) has not dropped tenfold for `steps` pseudo-time steps -- a
+ * limit cycle or a stalled solve that will not reach its drop.  0 (default)
+ * turns it off: solves then run to their drop or max_steps. */
+int flow_server_set_stall(flow_server *srv, int steps);
 const char *flow_server_last_error(void);
 
 /* ---- b - A x RMS with no device allocation ------------------------------

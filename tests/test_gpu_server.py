@@ -86,3 +86,58 @@ def test_admission_waits_for_arena_room():
             srv.release(c["slot"])
     srv.close()
     arena.close()
+
+
+def test_stalled_solves_are_retired_and_converging_ones_are_not():
+    """A k=1 solve caught in the limiter's limit cycle is retired as stalled
+    long before its step limit; a converging solve served next to it takes
+    exactly the steps it takes alone."""
+    from flowgpu import capi
+    (wl1, m1) = _case(64, 16, False, 1, 0.5, 1.25, 2)
+    (wl2, m2) = _case(32, 8, True, 3, 0.8, 1.25, 4)
+    fp2 = wl2.params()
+    alone = capi.Solver.from_mesh(m2, fp2, device=0)
+    alone.set_precision(3)
+    alone.set_state(m2.initial_state(fp2))
+    steps2, r0, r1 = alone.converge(1, 3000, 1e-10, check=False)
+    alone.close()
+    assert r1 < 1e-10 * r0
+    arena = capi.Arena(1 << 30)
+    srv = capi.Server(arena, chunk=16, max_slots=4, stall=600)
+    fp1 = wl1.params()
+    srv.submit(m1, fp1, m1.initial_state(fp1), precision=3, max_steps=3000, tag=1)
+    srv.submit(m2, fp2, m2.initial_state(fp2), precision=3, max_steps=3000, tag=2)
+    got = {}
+    while len(got) < 2:
+        for c in srv.progress(wait_us=5000):
+            got[c["tag"]] = c
+            srv.release(c["slot"])
+    assert got[1]["status"] == capi.ERR_STALLED and got[1]["steps"] < 2000
+    assert got[2]["status"] == 0 and got[2]["steps"] == steps2
+    srv.close()
+    arena.close()
+
+
+def test_staged_meshes_of_different_sizes_all_start():
+    """Contexts staged first and started afterwards (the largest chunk
+    window not the last one built) all run: kernel launch limits are not a
+    per-context setting."""
+    from flowgpu import capi
+    cases = [_case(128, 32, True, 3, 0.8, 1.25, 4), _case(32, 8, True, 3, 0.8, 1.25, 4)]
+    arena = capi.Arena(1 << 30)
+    srv = capi.Server(arena, chunk=16, max_slots=4)
+    slots = []
+    for wl, m in cases:
+        fp = wl.params()
+        slots.append(srv.submit(m, fp, m.initial_state(fp), precision=3, max_steps=64,
+                                hold=True))
+    for sl in slots:
+        srv.start(sl)
+    done = []
+    while len(done) < 2:
+        done += srv.progress(wait_us=5000)
+    for c in done:
+        assert c["status"] in (0, capi.ERR_NOT_CONVERGED)
+        srv.release(c["slot"])
+    srv.close()
+    arena.close()
