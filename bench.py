@@ -428,6 +428,19 @@ def run_batch(args, bw):
             "algorithmic_bytes_per_launch": np_bytes, "avg_launch_ms": round(np_ms, 4),
             "share_of_step": round(share, 3),
             "kernels_ms": {k: round(t / max(c, 1), 4) for k, (c, t) in kt.items() if c}}
+    scnt, sms = kt["sweep"]
+    if bw.precision == 3 and scnt:
+        sw_bytes = roofline.chunk_sweep_bytes(big.mesh)
+        sw_ms = sms / scnt
+        sw_ach = sw_bytes / (sw_ms * 1e-3) / 1e9
+        roof_sweep = {"bound": "latency (dependency levels inside a chunk)",
+                      "kernel": "k_sweep_chunk (one sweep = one launch per chunk colour)",
+                      "achieved": round(sw_ach, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                      "frac": round(sw_ach / peaks["hbm_gbs"], 4),
+                      "algorithmic_bytes_per_sweep": sw_bytes, "avg_sweep_ms": round(sw_ms, 4),
+                      "share_of_step": round(sms / max(sum(v[1] for v in kt.values()), 1e-30), 3)}
+    else:
+        roof_sweep = None
 
     # ---- plain FP64 drop-in on the same requests, one at a time ----
     plain = None
@@ -482,7 +495,7 @@ def run_batch(args, bw):
             "plain_fp64": plain,
             "e2e": {"value": round(e2e, 5), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "roofline": roof, "gpu_launches": int(launches),
+            "roofline": roof, "roofline_sweep": roof_sweep, "gpu_launches": int(launches),
             "clocks": clk.summary(), "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -63,3 +63,12 @@ def ordered_sweep_bytes(mesh) -> int:
     (132 B per block + 96 B per row, the diagonal block counted as a block)."""
     z = _sizes(mesh)
     return int(132 * z["nnz"] + 96 * z["nn"])
+
+
+def chunk_sweep_bytes(mesh) -> int:
+    """One whole chunked FP32 sweep (precision mode 3, all colour launches):
+    per row its 640-byte sweep record (header, right-hand side, LU factors,
+    8 columns, 8 FP32 blocks) staged once, its iterate read through the
+    chunk's window and written back (16 + 16)."""
+    z = _sizes(mesh)
+    return int(z["nn"] * (640 + 16 + 16))

@@ -59,6 +59,10 @@ WORKLOADS = {
     # a 16x smaller member of the same family, for quick runs
     "ogrid128x32_k2_m080": Workload("ogrid128x32_k2_m080", 128, 32, True, 3, 0.8,
                                     steps_to_converge=691),
+    # the largest mesh of the batch16 requests (request 3 of stream 0): the
+    # roofline mesh of the batching bench
+    "ogrid704x176_k2_m077": Workload("ogrid704x176_k2_m077", 704, 176, True, 3, 0.773228,
+                                     alpha=-0.786252, seed=1003),
     # the small k=1 case: 128 x 32 O-grid, M 0.5, straight walls (a parity case:
     # with the reference's limiter 2 it settles into a limit cycle)
     "ogrid128x32_k1_m050": Workload("ogrid128x32_k1_m050", 128, 32, False, 1, 0.5),
