@@ -752,6 +752,48 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args):
+    """The serving form: an open-loop Poisson stream of requests (node counts
+    log-uniform in [4k, 500k], the batching stream's flow conditions and
+    orders, seed 1), each prepared on arrival, admitted as the arena allows,
+    retired at a 1e-8 drop (or stalled / at max_steps).  One line: converged
+    solves per second of the run's span and p50/p95/p99 latency from arrival
+    to retirement."""
+    import torch
+    from flowgpu import capi, serve
+    torch.cuda.set_device(0)
+    n, rate = args.serve_requests, args.serve_rate
+    reqs = [serve.sample_request(i, seed=1, n_min=4000, n_max=500000) for i in range(n)]
+    free, _ = torch.cuda.mem_get_info(0)
+    budget = int(min(free * 0.85, 150e9))
+    arena = capi.Arena(budget, device=0)
+    with ClockSampler(0) as clk:
+        r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
+                              precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
+                              stall=2000)
+    arena.close()
+    recs = r["records"]
+    conv = [x for x in recs if x.get("status") == 0]
+    line = {"metric": METRIC, "value": round(len(conv) / r["span_s"], 5), "unit": UNIT,
+            "form": "serving (open-loop Poisson arrivals)", "requests": n,
+            "rate_per_s": rate, "span_s": round(r["span_s"], 2), "converged": len(conv),
+            "stalled": sum(1 for x in recs if x.get("status") == capi.ERR_STALLED),
+            "not_converged": sum(1 for x in recs if x.get("status") == capi.ERR_NOT_CONVERGED),
+            "failed": sum(1 for x in recs if x.get("status") not in
+                          (0, capi.ERR_STALLED, capi.ERR_NOT_CONVERGED)),
+            "latency_s_converged": serve.percentiles([x["latency_s"] for x in conv]),
+            "latency_s_all": serve.percentiles([x["latency_s"] for x in recs]),
+            "admission_wait_s": serve.percentiles([x.get("admitted_s", 0.) for x in recs]),
+            "prep_s": serve.percentiles([x.get("prep_s", 0.) for x in recs]),
+            "nodes": [x.get("nodes") for x in recs], "steps": [x.get("steps") for x in recs],
+            "status": [x.get("status") for x in recs],
+            "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
+                       "stall_retire_steps": 2000, "arena_bytes": budget, "stream_seed": 1,
+                       "nodes_range": [4000, 500000]},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -771,7 +813,13 @@ def main():
                     help="with --profile-steps: 0 FP64 drop-in, 1 FP32 multicolour sweeps")
     ap.add_argument("--subits", type=int, default=0,
                     help="with --profile-steps: Gauss-Seidel sweeps per step (0: the workload's)")
+    ap.add_argument("--serve-rate", type=float, default=0.,
+                    help="run the serving form: Poisson arrivals at this rate (requests/s)")
+    ap.add_argument("--serve-requests", type=int, default=16)
     args = ap.parse_args()
+    if args.serve_rate > 0:
+        run_serve(args)
+        return
     from flowgpu import workloads
     args.workload = args.workload or workloads.DEFAULT_BENCH
     bw = workloads.BATCHES.get(args.workload)

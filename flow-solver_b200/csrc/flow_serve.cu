@@ -143,6 +143,9 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     return st == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : (st ? st : FLOW_ERR_ARG);
   }
   int rc = flow_set_precision(c, precision);
+  // mode 3 needs its chunk windows in shared memory; a mesh whose matrix
+  // bandwidth is too large for that is served in mode 1 instead
+  if (rc == FLOW_ERR_ARG && precision == 3) rc = flow_set_precision(c, 1);
   if (!rc) rc = flow_set_state(c, Q0);
   if (!rc && sv->autotune_steps > 0) {
     // kernel variants: measured once per (order, precision, size bucket)

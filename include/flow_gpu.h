@@ -325,6 +325,9 @@ int flow_server_submit(flow_server *srv, const flow_grid_view *g, const flow_par
 /* flow_server_submit split in two: flow_server_stage creates the context and
  * uploads the state (hold = 1: nothing is launched yet) and
  * flow_server_start launches a staged solve. */
+/* precision 3 falls back to precision 1 for a mesh that mode 3 cannot take
+ * (a row with more than 8 off-diagonal blocks, or a bandwidth whose chunk
+ * windows do not fit in shared memory). */
 int flow_server_stage(flow_server *srv, const flow_grid_view *g, const flow_params *p,
                       const double *Q0, int precision, double drop, int max_steps,
                       long long tag, int hold, int *slot);
