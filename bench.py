@@ -387,9 +387,15 @@ def run_batch(args, bw):
     barrier(pg)
     dev_ms = e2e_ms = 0.
     lat, launches, n_conv, n_fail, n_stall = [], 0, 0, 0, 0
+    dforce = []
     with ClockSampler(local) as clk:
         for k in range(args.steps):
             recs, forces, v_ms, e_ms = one_pass()
+            if bw.fp64_forces is not None and rank == 0:
+                for i, r in enumerate(recs):  # converged in both forms
+                    if r["status"] == 0 and bw.fp64_status[i] == 0 and i in forces:
+                        f64 = bw.fp64_forces[i]
+                        dforce.append(max(abs(forces[i][0] - f64[0]), abs(forces[i][1] - f64[1])))
             dev_ms += v_ms
             e2e_ms += e_ms
             lat += [r["device_ms"] / 1e3 for r in recs]
@@ -492,6 +498,10 @@ def run_batch(args, bw):
                        "l2": "working set larger than L2 (batch of meshes, 0.1-0.5 GB each)",
                        "parallelism": f"requests sharded over {world} GPU(s)"},
             "latency_s": serve.percentiles(lat),
+            "forces_vs_fp64": {"max_abs_diff": max(dforce) if dforce else None,
+                               "solves_compared": len(dforce) // max(args.steps, 1),
+                               "what": "raw lift and drag of every request converged in both "
+                                       "the served form and the FP64 drop-in (recorded)"},
             "plain_fp64": plain,
             "e2e": {"value": round(e2e, 5), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
@@ -752,6 +762,54 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_compare_precision(args):
+    """The precision form against the all-FP64 drop-in on one mesh: each run
+    to a 1e-10 drop of ||R_rho|| (or the workload's step limit) from the same
+    initial state; steps, device time, and the lift/drag (and their
+    coefficients, C = F / (0.5 M^2), chord 1) and state differences."""
+    import numpy as np
+    import torch
+    from flowgpu import capi, workloads
+    from flowgpu.prep import Mesh
+    torch.cuda.set_device(0)
+    wl = workloads.get(args.workload)
+    t0 = time.time()
+    mesh = Mesh.from_case(wl.write(), order=wl.order)
+    prep_s = time.time() - t0
+    Q0 = mesh.initial_state(wl.params())
+    out = {}
+    mode = args.precision or 3
+    for prec, sub in ((0, 2), (mode, 4)):
+        fp = dataclasses.replace(wl.params(), subits=sub)
+        s = capi.Solver.from_mesh(mesh, fp, device=0)
+        try:
+            s.set_precision(prec)
+        except capi.FlowError:
+            prec = 1
+            s.set_precision(1)
+        s.set_state(Q0)
+        steps, r0, r1 = s.converge(1, wl.max_steps, wl.drop, chunk=64, check=False)
+        st = s.status()
+        out[prec] = {"steps": steps, "device_s": round(s.last_device_ms() / 1e3, 3),
+                     "r_drop": r1 / r0, "status": st,
+                     "forces": s.body_forces() if st == 0 else None, "Q": s.get("Q")}
+        s.close()
+    a, b = out[0], out[[k for k in out if k != 0][0]]
+    qn = 0.5 * wl.mach * wl.mach
+    line = {"workload": wl.name, "nodes": mesh.sizes["nn"], "host_prep_s": round(prep_s, 1),
+            "fp64": {k: v for k, v in a.items() if k != "Q"},
+            "precision_form": dict({k: v for k, v in b.items() if k != "Q"},
+                                   mode=[k for k in out if k != 0][0], gs_sweeps=4),
+            "speedup": round(a["device_s"] / max(b["device_s"], 1e-9), 3)}
+    if a["forces"] and b["forces"]:
+        line["d_lift"] = abs(a["forces"][0] - b["forces"][0])
+        line["d_drag"] = abs(a["forces"][1] - b["forces"][1])
+        line["d_CL"] = line["d_lift"] / qn
+        line["d_CD"] = line["d_drag"] / qn
+        line["max_abs_dQ"] = float(np.max(np.abs(a["Q"][4:] - b["Q"][4:])))
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """The serving form: an open-loop Poisson stream of requests (node counts
     log-uniform in [4k, 500k], the batching stream's flow conditions and
@@ -816,9 +874,15 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=0.,
                     help="run the serving form: Poisson arrivals at this rate (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=16)
+    ap.add_argument("--compare-precision", action="store_true",
+                    help="one mesh (--workload): the precision form (--precision, default 3) "
+                         "against the FP64 drop-in, each to a 1e-10 drop")
     args = ap.parse_args()
     if args.serve_rate > 0:
         run_serve(args)
+        return
+    if args.compare_precision:
+        run_compare_precision(args)
         return
     from flowgpu import workloads
     args.workload = args.workload or workloads.DEFAULT_BENCH

@@ -714,6 +714,8 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
 // the smallest colour no earlier adjacent chunk holds.  Records: per
 // direction, chunk by chunk, sub-levels of at most kRecRows rows of one
 // level, rows ascending inside a sub-level.
+int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax);
+
 int build_chunk_tables(flow_ctx* c) {
   const int nn = c->nn;
   const std::vector<int>& ia = c->h_ia;
@@ -726,9 +728,22 @@ int build_chunk_tables(flow_ctx* c) {
     }
     for (int k = ia[j]; k < ia[j + 1]; k++) bw = std::max(bw, std::abs(ja[k] - j));
   }
-  const int cmax = c->chunk_rows > 0 ? c->chunk_rows
-                                     : std::min(2048, std::max(64, ((2 * bw + 63) / 64) * 64));
+  int cmax = c->chunk_rows > 0 ? c->chunk_rows
+                               : std::min(2048, std::max(64, ((2 * bw + 63) / 64) * 64));
   const int lmax = c->chunk_levels > 0 ? c->chunk_levels : 32;
+  // an automatic chunk size shrinks (64 rows at a time) until every chunk's
+  // window of the iterate fits in shared memory beside the record ring
+  for (;;) {
+    const int rc = build_chunks_with(c, bw, cmax, lmax);
+    if (rc != FLOW_ERR_ARG || c->chunk_rows > 0 || cmax - 64 < std::max(64, bw / 2)) return rc;
+    cmax -= 64;
+  }
+}
+
+int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
+  const int nn = c->nn;
+  const std::vector<int>& ia = c->h_ia;
+  const std::vector<int>& ja = c->h_ja;
   // chunks
   std::vector<int> start, lev(nn + 1, 0), chunk_of(nn + 1, 0);
   start.push_back(1);
@@ -1055,6 +1070,31 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   UP(nsub_ptr, nsub.ptr); UP(nsub, nsub.idx);
   UP(nbed_ptr, nbed.ptr); UP(nbed, nbed.idx);
   UP(nedg_ptr, nedg.ptr); UP(nedg, nedg.idx);
+  {
+    // node-major copies of the static face data each node reads
+    std::vector<double4> ngeo(nsub.idx.size());
+    std::vector<double2> nfdx(nsub.idx.size());
+    std::vector<double2> ngdx(p->order == 3 ? 3 * nsub.idx.size() : 1);
+    for (int n = 1; n <= nn; n++) {
+      for (int k = nsub.ptr[n]; k < nsub.ptr[n + 1]; k++) {
+        const int sb = nsub.idx[k] >> 1, side = nsub.idx[k] & 1;
+        ngeo[k] = sub_geo[sb];
+        nfdx[k] = side ? make_double2(sub_dx[sb].z, sub_dx[sb].w)
+                       : make_double2(sub_dx[sb].x, sub_dx[sb].y);
+        if (p->order == 3 && g->xg_subedges)
+          for (int gp = 0; gp < 3; gp++)
+            ngdx[3 * (size_t)k + gp] =
+                make_double2(g->xg_subedges[6 * (size_t)sb + 2 * gp] - g->x[2 * n],
+                             g->xg_subedges[6 * (size_t)sb + 2 * gp + 1] - g->x[2 * n + 1]);
+      }
+    }
+    std::vector<int> nother(nedg.idx.size());
+    for (size_t k = 0; k < nedg.idx.size(); k++) {
+      const int e = nedg.idx[k] >> 1, side = nedg.idx[k] & 1;
+      nother[k] = side ? edge_lr[e].x : edge_lr[e].y;
+    }
+    UP(nsub_geo, ngeo); UP(nsub_fdx, nfdx); UP(nsub_gdx, ngdx); UP(nedg_other, nother);
+  }
   UP(sub_lr, sub_lr); UP(sub_geo, sub_geo); UP(sub_dx, sub_dx);
   UP(edge_lr, edge_lr); UP(edge_w, edge_w);
   UP(csr_sub, csr_sub);

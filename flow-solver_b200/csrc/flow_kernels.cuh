@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
   #pragma unroll 4
   for (int k = s0; k < s1; k++) {
-    const double4 g = m.sub_geo[m.nsub[k] >> 1];
+    const double4 g = m.nsub_geo[k];  // the incident subedge's normal and length
     const double theta = uu * g.x + vv * g.y;
     const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
     const double w = tpc >= tmc ? tpc : tmc;
@@ -155,14 +155,13 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
   #pragma unroll 4
   for (int k = e0; k < e1; k++) {
-    const int ed = m.nedg[k];
-    const int e = ed >> 1, side = ed & 1;
-    const int2 lr = m.edge_lr[e];
-    const int other = side ? lr.x : lr.y;
+    const int other = m.nedg_other[k];  // the edge's other end
     const double qo = s.nQ[4 * (long)other + v];
     qmin = qmin <= qo ? qmin : qo;
     qmax = qmax >= qo ? qmax : qo;
     if (ORDER == 1 && a.do_grad) {
+      const int ed = m.nedg[k];
+      const int e = ed >> 1, side = ed & 1;
       const double4 w = m.edge_w[e];
       const double dq = side ? (q0v - qo) : (qo - q0v);  // nQ[R] - nQ[L]
       if (side == 0) {
@@ -215,21 +214,19 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   if (!a.do_lim) return;
   // ---- Venkatakrishnan bound of variable v over every face point ----
   double ph = 1.0;
-  const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
   #pragma unroll 4
   for (int k = s0; k < s1; k++) {
-    const int sd = m.nsub[k];
-    const int sub = sd >> 1, side = sd & 1;
     if (ORDER == 1) {
-      const double4 d = m.sub_dx[sub];
-      const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
+      const double2 d = m.nsub_fdx[k];  // face point - x[n]
+      const double dx0 = d.x, dx1 = d.y;
       const double qr = q0v + (g0 * dx0 + g1 * dx1);
       ph = venkat_fold(ph, qr, q0v, qmin, qmax);
     } else {
-      const double* xg = m.sub_xg + 6 * (long)sub;
+      const double2* gd = m.nsub_gdx + 3 * (long)k;  // Gauss points - x[n]
 #pragma unroll
       for (int gpt = 0; gpt < 3; gpt++) {
-        const double dx0 = xg[2 * gpt] - xn0, dx1 = xg[2 * gpt + 1] - xn1;
+        const double2 d = gd[gpt];
+        const double dx0 = d.x, dx1 = d.y;
         double qr = pv;
         qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
                h[4] * dx0 * dx1);

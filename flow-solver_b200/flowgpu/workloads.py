@@ -59,6 +59,9 @@ WORKLOADS = {
     # a 16x smaller member of the same family, for quick runs
     "ogrid128x32_k2_m080": Workload("ogrid128x32_k2_m080", 128, 32, True, 3, 0.8,
                                     steps_to_converge=691),
+    # the precision form's mesh: 2048 x 512 O-grid (1.05M nodes), k=2, M 0.8
+    "ogrid2048x512_k2_m080": Workload("ogrid2048x512_k2_m080", 2048, 512, True, 3, 0.8,
+                                      max_steps=40000),
     # the largest mesh of the batch16 requests (request 3 of stream 0): the
     # roofline mesh of the batching bench
     "ogrid704x176_k2_m077": Workload("ogrid704x176_k2_m077", 704, 176, True, 3, 0.773228,
@@ -112,6 +115,7 @@ class BatchWorkload:
     fp64_status: tuple | None = None
     stall: int = 0
     autotune: int = 0
+    fp64_forces: tuple | None = None  # raw lift/drag of the FP64 drop-in per request
 
 
 BATCHES = {
@@ -119,5 +123,6 @@ BATCHES = {
         "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=2000, autotune=4,
         fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065,
                     1395, 1487, 8000),
-        fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256)),
+        fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256),
+        fp64_forces=((0.04361406644387807, -0.0012359952118082152), (-0.1077942504305611, -0.0016940082793635751), (-0.025777386029756044, -0.0054055864833447076), (0.04696757004279522, -0.0057328563651535954), (-0.0010171575037174392, -0.001240139392816858), (-0.0023481805252991883, -0.0018965591568374796), (-0.027248649454864958, -0.003062564172084038), (-0.12773519262622307, -0.018852769853473013), (0.10544934901923901, -0.007440799548675984), None, (-0.018041588523432805, -0.002214218243070119), (0.002168299510290521, -0.0016691959198755204), (0.028612422320067932, -0.005656445411432563), (-0.0017219682626121772, -0.0013359229295129356), (-0.03246397561528733, -0.0029672357554528374), (-0.0480551902857968, -0.001438821319776097))),
 }
