@@ -828,7 +828,7 @@ def run_serve(args):
     with ClockSampler(0) as clk:
         r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
                               precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
-                              stall=2000)
+                              stall=2000, ramp_sweeps=2)
     arena.close()
     recs = r["records"]
     conv = [x for x in recs if x.get("status") == 0]
@@ -846,6 +846,7 @@ def run_serve(args):
             "nodes": [x.get("nodes") for x in recs], "steps": [x.get("steps") for x in recs],
             "status": [x.get("status") for x in recs],
             "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
+                       "ramp_sweeps_on_meshes_from_250k_nodes": 2,
                        "stall_retire_steps": 2000, "arena_bytes": budget, "stream_seed": 1,
                        "nodes_range": [4000, 500000]},
             "clocks": clk.summary()}

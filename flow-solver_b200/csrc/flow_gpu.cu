@@ -169,6 +169,7 @@ struct flow_ctx {
   // blocks with multicolour sweeps; tables built on first use
   int precision = 0;
   int var[2] = {0, 0};  // kernel variants: k_node_prepare4, k_subedge_flux (autotuner)
+  int sched_sweeps = 0, sched_until = 0;  // sweep schedule (flow_set_sweep_schedule)
   MixedTables mt{};
   bool mt_ordered = false;  // tables in reference row order (modes 2, 3) or colour order (mode 1)
   ChunkTables ct{};          // mode 3 tables and sweep records
@@ -181,7 +182,7 @@ struct flow_ctx {
   int use_graphs = 1;
   struct ChunkGraph {
     cudaGraphExec_t exec = nullptr;
-    int K = 0, precision = -1, sweep_mode = -1, phase = -1;
+    int K = 0, precision = -1, sweep_mode = -1, phase = -1, sweeps = -1;
     flow_params p{};
     long launches = 0;
   };
@@ -494,6 +495,16 @@ int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
   return rc;
 }
 
+// Gauss-Seidel sweeps of step ts: the schedule's count up to its last step,
+// the parameters' count after.
+int sweeps_at(const flow_ctx* c, const flow_params* p, int ts) {
+  if (c->sched_sweeps > 0) {
+    const int until = c->sched_until > 0 ? c->sched_until : p->ramp;
+    if (ts <= until) return c->sched_sweeps;
+  }
+  return p->subits;
+}
+
 // Step index and CFL on the device (k_step_args): citer > 0 sets the index,
 // 0 advances the device's own.
 int launch_step_args(flow_ctx* c, const flow_params* p, int citer) {
@@ -524,7 +535,9 @@ int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int f
     }
     rc |= launch_node_prepare(c, a);
     rc |= launch_residuals(c, a, jac);
-    rc |= launch_linear_solve(c, p, false);
+    flow_params pe = *p;  // the sweep schedule may lower the sweep count early on
+    pe.subits = sweeps_at(c, p, ts);
+    rc |= launch_linear_solve(c, &pe, false);
     k_finish_step<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->m, c->s, mi == p->iter);
     rc |= launch_check(c);
     bool last = mi == p->iter;
@@ -563,7 +576,9 @@ void drop_graphs(flow_ctx* c) {
 int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
   int rc = 0;
   const int ph = phase_of(p, ts0);
+  const int sw = sweeps_at(c, p, ts0);
   const bool graphable = c->use_graphs && !c->timing && K > 0 && ph == phase_of(p, ts0 + K - 1) &&
+                         sw == sweeps_at(c, p, ts0 + K - 1) &&
                          (c->precision == 1 || c->precision == 3 ||
                           (c->precision == 0 && c->sweep_mode == 1) ||
                           p->subits % 2 == 0);
@@ -574,7 +589,7 @@ int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
   flow_ctx::ChunkGraph* g = nullptr;
   for (auto& x : c->graphs)
     if (x.K == K && x.precision == c->precision && x.sweep_mode == c->sweep_mode &&
-        x.phase == ph && params_equal(x.p, *p))
+        x.phase == ph && x.sweeps == sw && params_equal(x.p, *p))
       g = &x;
   if (!g) {
     if (c->graphs.size() >= 4) drop_graphs(c);
@@ -583,6 +598,7 @@ int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
     ng.precision = c->precision;
     ng.sweep_mode = c->sweep_mode;
     ng.phase = ph;
+    ng.sweeps = sw;
     ng.p = *p;
     const long l0 = c->launches;
     cudaGraph_t graph = nullptr;
@@ -1324,6 +1340,19 @@ int flow_chunk_starts(flow_ctx* c, int* starts, int cap, int* nchunks, int* ncol
   if (ncolours) *ncolours = c->ct.ncol;
   if (starts)
     for (int i = 0; i <= n && i < cap; i++) starts[i] = c->h_chunk_start[i];
+  return 0;
+}
+
+int flow_set_sweep_schedule(flow_ctx* c, int sweeps, int until_step) {
+  if (!c || !c->ok || sweeps < 0 || until_step < 0) {
+    set_error("flow_set_sweep_schedule: null context or negative argument");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  c->sched_sweeps = sweeps;
+  c->sched_until = until_step;
   return 0;
 }
 

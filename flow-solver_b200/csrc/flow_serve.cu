@@ -58,6 +58,8 @@ struct flow_server {
   int running = 0;
   int autotune_steps = 0;  // 0: no autotuning at admission
   int stall_steps = 0;     // 0: no stall retirement
+  int sched_sweeps = 0, sched_until = 0;  // sweep schedule of precision-form solves
+  long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
   // autotuned kernel variants by (order, precision, mesh-size bucket)
   std::map<std::tuple<int, int, int>, std::pair<int, int>> tuned;
 };
@@ -146,6 +148,9 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   // mode 3 needs its chunk windows in shared memory; a mesh whose matrix
   // bandwidth is too large for that is served in mode 1 instead
   if (rc == FLOW_ERR_ARG && precision == 3) rc = flow_set_precision(c, 1);
+  if (!rc && precision != 0 && sv->sched_sweeps > 0 &&
+      flow_size(c, "dt") - 1 >= sv->sched_min_nodes)
+    rc = flow_set_sweep_schedule(c, sv->sched_sweeps, sv->sched_until);
   if (!rc) rc = flow_set_state(c, Q0);
   if (!rc && sv->autotune_steps > 0) {
     // kernel variants: measured once per (order, precision, size bucket)
@@ -311,6 +316,15 @@ int flow_server_release(flow_server* sv, int slot) {
 }
 
 int flow_server_running(flow_server* sv) { return sv ? sv->running : -1; }
+
+int flow_server_set_sweep_schedule(flow_server* sv, int sweeps, int until_step,
+                                   long long min_nodes) {
+  if (!sv || sweeps < 0 || until_step < 0 || min_nodes < 0) return FLOW_ERR_ARG;
+  sv->sched_sweeps = sweeps;
+  sv->sched_until = until_step;
+  sv->sched_min_nodes = (long)min_nodes;
+  return 0;
+}
 
 int flow_server_set_stall(flow_server* sv, int steps) {
   if (!sv || steps < 0) return FLOW_ERR_ARG;

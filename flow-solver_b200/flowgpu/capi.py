@@ -31,7 +31,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
            "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_chunk_starts", "flow_set_graphs",
-           "flow_autotune", "flow_set_variants", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_autotune", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
            "flow_linear_residual_noalloc", "flow_arena_create", "flow_arena_destroy",
@@ -39,7 +39,8 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_ctx_device_bytes", "flow_server_create", "flow_server_destroy",
            "flow_server_submit", "flow_server_stage", "flow_server_start", "flow_server_progress", "flow_server_result",
            "flow_server_release", "flow_server_running", "flow_server_last_error",
-           "flow_server_set_autotune", "flow_server_set_stall")
+           "flow_server_set_autotune", "flow_server_set_stall",
+           "flow_server_set_sweep_schedule")
 
 
 class FlowParamsC(C.Structure):
@@ -121,6 +122,7 @@ def _load_locked():
     L.flow_set_chunk.argtypes = [vp, C.c_int, C.c_int]
     L.flow_autotune.argtypes = [vp, PP, C.c_int, C.c_int, IP, DP]
     L.flow_set_variants.argtypes = [vp, C.c_int, C.c_int]
+    L.flow_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int]
     L.flow_chunk_starts.argtypes = [vp, IP, C.c_int, IP, IP]
     L.flow_save_state.argtypes = [vp]
     L.flow_restore_state.argtypes = [vp]
@@ -162,6 +164,7 @@ def _load_locked():
     L.flow_server_last_error.restype = C.c_char_p
     L.flow_server_set_autotune.argtypes = [vp, C.c_int]
     L.flow_server_set_stall.argtypes = [vp, C.c_int]
+    L.flow_server_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int, C.c_longlong]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
     L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
@@ -225,7 +228,7 @@ class Server:
     (FLOW_ERR_BUDGET); progress() returns retired solves as dicts."""
 
     def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64, autotune: int = 0,
-                 stall: int = 0):
+                 stall: int = 0, ramp_sweeps: int = 0, ramp_min_nodes: int = 250000):
         self.L = load()
         st = C.c_int(0)
         self.arena = arena
@@ -236,6 +239,9 @@ class Server:
             _check(self.L.flow_server_set_autotune(self.h, int(autotune)), "autotune")
         if stall:
             _check(self.L.flow_server_set_stall(self.h, int(stall)), "stall")
+        if ramp_sweeps:
+            _check(self.L.flow_server_set_sweep_schedule(self.h, int(ramp_sweeps), 0,
+                                                         int(ramp_min_nodes)), "sweep schedule")
         self._keep = {}
         self._out = (FlowCompletion * 64)()
 
@@ -490,6 +496,11 @@ class Solver:
         _check(self.L.flow_autotune(self.ctx, C.byref(self.p), int(ts), int(steps), v, ms),
                "flow_autotune")
         return (v[0], v[1]), [round(x, 4) for x in ms]
+
+    def set_sweep_schedule(self, sweeps: int, until_step: int = 0):
+        """`sweeps` Gauss-Seidel sweeps up to `until_step` (0: end of the CFL ramp)."""
+        _check(self.L.flow_set_sweep_schedule(self.ctx, int(sweeps), int(until_step)),
+               "flow_set_sweep_schedule")
 
     def set_variants(self, node_prepare: int, flux: int):
         _check(self.L.flow_set_variants(self.ctx, int(node_prepare), int(flux)),

@@ -89,10 +89,11 @@ def percentiles(xs, ps=(50, 95, 99)) -> dict:
 
 def run_batch(prepared, arena: capi.Arena, precision: int = 1, chunk: int = 32,
               max_slots: int = 64, want_q: bool = False, autotune: int = 0,
-              stall: int = 0) -> dict:
+              stall: int = 0, ramp_sweeps: int = 0) -> dict:
     """Admit every prepared solve (as the arena allows), run all to
     retirement.  Returns per-solve records and the makespan."""
-    srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall)
+    srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall,
+                      ramp_sweeps=ramp_sweeps)
     pending = list(range(len(prepared)))
     recs = {}
     t0 = time.perf_counter()
@@ -143,7 +144,7 @@ def run_sequential(prepared, precision: int = 0, chunk: int = 64, device: int = 
 def run_poisson(reqs, rate_per_s: float, arena: capi.Arena, subits: int, max_steps: int,
                 drop: float, precision: int = 1, chunk: int = 32, max_slots: int = 64,
                 seed: int = 0, prep_threads: int = 8, autotune: int = 0,
-                stall: int = 0) -> dict:
+                stall: int = 0, ramp_sweeps: int = 0) -> dict:
     """Open-loop Poisson arrivals at `rate_per_s`: each request is prepared
     on arrival (thread pool), admitted when prepared and when the arena has
     room, and retired at its drop; latency = retirement - arrival."""
@@ -151,7 +152,8 @@ def run_poisson(reqs, rate_per_s: float, arena: capi.Arena, subits: int, max_ste
     gaps = rng.exponential(1.0 / rate_per_s, size=len(reqs))
     arrivals = np.cumsum(gaps) - gaps[0]
     capi.load()
-    srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall)
+    srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall,
+                      ramp_sweeps=ramp_sweeps)
     ex = cf.ThreadPoolExecutor(max_workers=prep_threads)
     t0 = time.perf_counter()
     futures, ready, recs = {}, [], [dict() for _ in reqs]

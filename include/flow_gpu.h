@@ -223,6 +223,12 @@ int flow_set_sweep_mode(flow_ctx *ctx, int mode);
  * most 8 off-diagonal blocks per row and a matrix bandwidth whose chunk
  * windows fit in shared memory; otherwise switching to it fails. */
 int flow_set_precision(flow_ctx *ctx, int mode);
+/* Sweep schedule (no reference counterpart): steps up to `until_step` (0:
+ * the end of the CFL ramp, p->ramp) run `sweeps` Gauss-Seidel sweeps instead
+ * of p->subits; sweeps = 0 turns the schedule off (default).  Fewer sweeps
+ * while the CFL ramps keep the early, poorly conditioned Newton steps from
+ * overshooting when the precision form solves them too accurately. */
+int flow_set_sweep_schedule(flow_ctx *ctx, int sweeps, int until_step);
 /* Chunk limits of precision mode 3 (0: defaults, rows = twice the matrix
  * bandwidth up to 2048, levels = 32). */
 int flow_set_chunk(flow_ctx *ctx, int rows, int levels);
@@ -355,6 +361,12 @@ int flow_server_set_autotune(flow_server *srv, int steps);
  * limit cycle or a stalled solve that will not reach its drop.  0 (default)
  * turns it off: solves then run to their drop or max_steps. */
 int flow_server_set_stall(flow_server *srv, int steps);
+/* flow_set_sweep_schedule for every precision-form solve admitted later on
+ * a mesh of at least min_nodes nodes (measured: the 1.05M-node O-grid needs
+ * 2 sweeps during the CFL ramp, meshes up to 124k nodes converge faster
+ * without the schedule). */
+int flow_server_set_sweep_schedule(flow_server *srv, int sweeps, int until_step,
+                                   long long min_nodes);
 const char *flow_server_last_error(void);
 
 /* ---- b - A x RMS with no device allocation ------------------------------

@@ -127,3 +127,22 @@ def test_mixed_converges_to_the_fp64_answer():
         assert abs(f1[0] - f0[0]) <= 1e-8 * max(1.0, abs(f0[0]))
         assert abs(f1[1] - f0[1]) <= 1e-8 * max(1.0, abs(f0[1]))
         assert np.max(np.abs(q1 - q0)) < 1e-7
+
+
+def test_sweep_schedule_bitwise():
+    """mode 3 with 2 sweeps up to step 3 and 4 after, against the oracle run
+    with those sweep counts step by step."""
+    import ctypes
+    from oracle import port
+    mesh, fp, og, p, gpu = _setup(64, 16, True, 3, 4, 3)
+    gpu.set_sweep_schedule(2, 3)
+    starts, ncol = gpu.chunk_starts()
+    nn = mesh.sizes["nn"]
+    perm, _ = chunk_order(og["ia"], og["ja"], starts)
+    for ts in range(1, 7):
+        p.subits = 2 if ts <= 3 else 4
+        og.solve_mixed_order(p, ts, perm)
+        gpu.solve(ts)
+        assert ndiff(og["Q"][4:], gpu.get("Q")[4:]) == 0, ts
+        assert ndiff(og["dQ"][4:4 * (nn + 1)], gpu.get("dQ")[4:]) == 0, ts
+    gpu.close()
