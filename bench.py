@@ -345,7 +345,7 @@ def run_batch(args, bw):
     def one_pass():
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n, autotune=bw.autotune,
-                          stall=bw.stall)
+                          stall=bw.stall, priority_policy=bw.priority_policy)
         torch.cuda.synchronize()
         ev[0].record()
         slots = []
@@ -492,6 +492,7 @@ def run_batch(args, bw):
                                             bw.precision, f"mode {bw.precision}"),
                        "gs_sweeps": bw.subits, "drop": bw.drop, "max_steps": bw.max_steps,
                        "stall_retire_steps": bw.stall, "autotune_steps": bw.autotune,
+                       "priority_policy": bw.priority_policy,
                        "converged_per_pass": n_conv // max(args.steps, 1),
                        "stalled_per_pass": n_stall // max(args.steps, 1),
                        "failed_per_pass": n_fail // max(args.steps, 1),

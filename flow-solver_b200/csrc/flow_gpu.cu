@@ -815,7 +815,7 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
     maxwin = std::max(maxwin, b - a + 1);
   }
   const size_t smem = 16 * kRecStride * kRecSlots * kRecRows + sizeof(float4) * maxwin;
-  if (smem > 227 * 1024) {
+  if (smem + kChunkStaticSmem > 227 * 1024) {
     set_error("precision mode 3: a chunk's window does not fit in shared memory (bandwidth too large)");
     return FLOW_ERR_ARG;
   }
@@ -862,6 +862,11 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
     }
     cs[nch] = (int)ss.size();
     ss.push_back((int)order.size());
+    for (int q = 0; q < nch; q++)
+      if (cs[q + 1] - cs[q] > kChunkSubMax) {
+        set_error("precision mode 3: a chunk has more sub-levels than the sweep kernel holds");
+        return FLOW_ERR_ARG;
+      }
     std::vector<SweepRec> rec(nn);
     memset(rec.data(), 0, sizeof(SweepRec) * nn);
     for (int i = 0; i < nn; i++) {
@@ -886,7 +891,7 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
   }
   // the limit is a property of the kernel, shared by every context: allow the
   // largest window any context may need, not this context's own
-  const int smem_cap = 227 * 1024;
+  const int smem_cap = 227 * 1024 - kChunkStaticSmem;
   if (cudaFuncSetAttribute(k_sweep_chunk<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            smem_cap) != cudaSuccess ||
       cudaFuncSetAttribute(k_sweep_chunk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1353,6 +1358,24 @@ int flow_set_sweep_schedule(flow_ctx* c, int sweeps, int until_step) {
   drop_graphs(c);
   c->sched_sweeps = sweeps;
   c->sched_until = until_step;
+  return 0;
+}
+
+int flow_set_stream_priority(flow_ctx* c, int priority) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  int lo = 0, hi = 0;  // hi is the greatest priority (numerically lowest)
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  const int pr = std::max(hi, std::min(lo, priority));
+  cudaStream_t st = nullptr;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, pr) != cudaSuccess) {
+    set_error("flow_set_stream_priority: stream creation failed");
+    return FLOW_ERR_CUDA;
+  }
+  harvest(c);
+  cudaStreamDestroy(c->stream);
+  c->stream = st;
   return 0;
 }
 

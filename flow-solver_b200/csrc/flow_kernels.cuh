@@ -960,6 +960,9 @@ constexpr int kRecInts = (int)(sizeof(SweepRec) / 16);  // 16-byte words per rec
 // records sit 704 bytes apart in shared memory (640 + 64 of padding), so the
 // two quads of a half-warp read disjoint bank ranges
 constexpr int kRecStride = kRecInts + 4;
+constexpr int kChunkSubMax = 256;   // sub-levels per chunk (host-checked)
+// shared memory the chunk sweep declares statically (room left for the rest)
+constexpr int kChunkStaticSmem = 2048;
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
@@ -990,7 +993,12 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
   for (int i = tid; i < nwin; i += blockDim.x) cp_async16(win + i, X + w.x + i);
   cp_async_commit();
   const int S0 = ct.chunk_sub[DIR][q], nsub = ct.chunk_sub[DIR][q + 1] - S0;
-  const int* ss = ct.sub_start[DIR] + S0;
+  // the chunk's sub-level starts, read once into shared memory (they sit on
+  // the loop's critical path); a chunk has at most kChunkSubMax sub-levels
+  __shared__ int ss[kChunkSubMax + 1];
+  for (int i = tid; i <= nsub && i <= kChunkSubMax; i += blockDim.x)
+    ss[i] = ct.sub_start[DIR][S0 + i];
+  __syncthreads();
   const int4* recs = reinterpret_cast<const int4*>(ct.rec[DIR]);
   auto issue = [&](int u) {
     if (u < nsub) {
@@ -1009,10 +1017,10 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
   const int quad = tid >> 2, r = tid & 3;
   const int qbase = tid & 31 & ~3;
   const unsigned qmask = 0xFu << qbase;
+  cp_async_wait<1>();  // the window and sub-level 0 have landed
+  __syncthreads();
   for (int u = 0; u < nsub; u++) {
     issue(u + 2);
-    cp_async_wait<2>();  // the window and sub-levels 0..u have landed
-    __syncthreads();
     if (quad < ss[u + 1] - ss[u]) {
       const SweepRec& R = *reinterpret_cast<const SweepRec*>(
           slots + ((u % kRecSlots) * kRecRows + quad) * kRecStride);
@@ -1052,6 +1060,10 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
         if (last) reinterpret_cast<double4*>(s.dQ)[j] = make_double4(x0, x1, x2, x3);
       }
     }
+    // one barrier per sub-level: this level's results are visible to the
+    // next, and the next level's records (all but the newest copy group)
+    // have landed
+    cp_async_wait<1>();
     __syncthreads();
   }
   cp_async_wait<0>();

@@ -60,6 +60,7 @@ struct flow_server {
   int stall_steps = 0;     // 0: no stall retirement
   int sched_sweeps = 0, sched_until = 0;  // sweep schedule of precision-form solves
   long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
+  int priority_policy = 0;                // 1: larger meshes get greater stream priority
   // autotuned kernel variants by (order, precision, mesh-size bucket)
   std::map<std::tuple<int, int, int>, std::pair<int, int>> tuned;
 };
@@ -151,6 +152,15 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   if (!rc && precision != 0 && sv->sched_sweeps > 0 &&
       flow_size(c, "dt") - 1 >= sv->sched_min_nodes)
     rc = flow_set_sweep_schedule(c, sv->sched_sweeps, sv->sched_until);
+  if (!rc && sv->priority_policy == 1) {
+    // greatest priority from 256k nodes, one step down per halving of the mesh
+    const long nn = flow_size(c, "dt") - 1;
+    int steps_down = 0;
+    for (long t = 262144; nn < t && steps_down < 8; t >>= 1) steps_down++;
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    rc = flow_set_stream_priority(c, std::min(lo, hi + steps_down));
+  }
   if (!rc) rc = flow_set_state(c, Q0);
   if (!rc && sv->autotune_steps > 0) {
     // kernel variants: measured once per (order, precision, size bucket)
@@ -323,6 +333,12 @@ int flow_server_set_sweep_schedule(flow_server* sv, int sweeps, int until_step,
   sv->sched_sweeps = sweeps;
   sv->sched_until = until_step;
   sv->sched_min_nodes = (long)min_nodes;
+  return 0;
+}
+
+int flow_server_set_priority_policy(flow_server* sv, int policy) {
+  if (!sv || policy < 0 || policy > 1) return FLOW_ERR_ARG;
+  sv->priority_policy = policy;
   return 0;
 }
 

@@ -40,7 +40,8 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_server_submit", "flow_server_stage", "flow_server_start", "flow_server_progress", "flow_server_result",
            "flow_server_release", "flow_server_running", "flow_server_last_error",
            "flow_server_set_autotune", "flow_server_set_stall",
-           "flow_server_set_sweep_schedule")
+           "flow_server_set_sweep_schedule", "flow_set_stream_priority",
+           "flow_server_set_priority_policy")
 
 
 class FlowParamsC(C.Structure):
@@ -165,6 +166,8 @@ def _load_locked():
     L.flow_server_set_autotune.argtypes = [vp, C.c_int]
     L.flow_server_set_stall.argtypes = [vp, C.c_int]
     L.flow_server_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int, C.c_longlong]
+    L.flow_set_stream_priority.argtypes = [vp, C.c_int]
+    L.flow_server_set_priority_policy.argtypes = [vp, C.c_int]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
     L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
@@ -228,7 +231,8 @@ class Server:
     (FLOW_ERR_BUDGET); progress() returns retired solves as dicts."""
 
     def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64, autotune: int = 0,
-                 stall: int = 0, ramp_sweeps: int = 0, ramp_min_nodes: int = 250000):
+                 stall: int = 0, ramp_sweeps: int = 0, ramp_min_nodes: int = 250000,
+                 priority_policy: int = 0):
         self.L = load()
         st = C.c_int(0)
         self.arena = arena
@@ -242,6 +246,9 @@ class Server:
         if ramp_sweeps:
             _check(self.L.flow_server_set_sweep_schedule(self.h, int(ramp_sweeps), 0,
                                                          int(ramp_min_nodes)), "sweep schedule")
+        if priority_policy:
+            _check(self.L.flow_server_set_priority_policy(self.h, int(priority_policy)),
+                   "priority policy")
         self._keep = {}
         self._out = (FlowCompletion * 64)()
 

@@ -89,11 +89,11 @@ def percentiles(xs, ps=(50, 95, 99)) -> dict:
 
 def run_batch(prepared, arena: capi.Arena, precision: int = 1, chunk: int = 32,
               max_slots: int = 64, want_q: bool = False, autotune: int = 0,
-              stall: int = 0, ramp_sweeps: int = 0) -> dict:
+              stall: int = 0, ramp_sweeps: int = 0, priority_policy: int = 0) -> dict:
     """Admit every prepared solve (as the arena allows), run all to
     retirement.  Returns per-solve records and the makespan."""
     srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall,
-                      ramp_sweeps=ramp_sweeps)
+                      ramp_sweeps=ramp_sweeps, priority_policy=priority_policy)
     pending = list(range(len(prepared)))
     recs = {}
     t0 = time.perf_counter()

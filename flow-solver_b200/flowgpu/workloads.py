@@ -116,11 +116,12 @@ class BatchWorkload:
     stall: int = 0
     autotune: int = 0
     fp64_forces: tuple | None = None  # raw lift/drag of the FP64 drop-in per request
+    priority_policy: int = 0          # 1: larger meshes on higher-priority streams
 
 
 BATCHES = {
     "batch16": BatchWorkload(
-        "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=2000, autotune=4,
+        "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=2000, autotune=4, priority_policy=1,
         fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065,
                     1395, 1487, 8000),
         fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256),

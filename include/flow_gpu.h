@@ -243,6 +243,11 @@ int flow_chunk_starts(flow_ctx *ctx, int *starts, int cap, int *nchunks, int *nc
  * launches every kernel from the host. */
 int flow_set_graphs(flow_ctx *ctx, int on);
 
+/* Recreate the context's stream with a CUDA stream priority (clamped to the
+ * device's range; numerically lower is served first).  Kernels of
+ * higher-priority streams get free SMs first when solves share the GPU. */
+int flow_set_stream_priority(flow_ctx *ctx, int priority);
+
 /* Device snapshot of the solution state (Q, nQ, pQ and the boundary normals
  * the k=2 pass rewrites): flow_save_state keeps a copy on the device,
  * flow_restore_state puts it back (pre-emption / restart without host
@@ -361,6 +366,10 @@ int flow_server_set_autotune(flow_server *srv, int steps);
  * limit cycle or a stalled solve that will not reach its drop.  0 (default)
  * turns it off: solves then run to their drop or max_steps. */
 int flow_server_set_stall(flow_server *srv, int steps);
+/* Priority policy for later admissions: 0 (default) one priority for all;
+ * 1 the larger the mesh, the greater its stream priority (the longest solves
+ * of a batch keep the GPU first, the small ones fill the gaps). */
+int flow_server_set_priority_policy(flow_server *srv, int policy);
 /* flow_set_sweep_schedule for every precision-form solve admitted later on
  * a mesh of at least min_nodes nodes (measured: the 1.05M-node O-grid needs
  * 2 sweeps during the CFL ramp, meshes up to 124k nodes converge faster

@@ -40,7 +40,8 @@ def test_mixed_admission_matches_solves_run_alone():
         alone.append((steps, s.get("Q"), s.body_forces(), r1 < 1e-10 * r0))
         s.close()
     arena = capi.Arena(2 << 30)
-    srv = capi.Server(arena, chunk=16, max_slots=8)
+    # larger meshes on higher-priority streams: scheduling only, same results
+    srv = capi.Server(arena, chunk=16, max_slots=8, priority_policy=1)
     for i, ((wl, mesh), prec) in enumerate(cases):
         fp = wl.params()
         slot = srv.submit(mesh, fp, mesh.initial_state(fp), precision=prec, drop=1e-10,
