@@ -53,3 +53,24 @@ def bitwise(a, b):
 
 def ndiff(a, b):
     return int(np.count_nonzero(np.asarray(a) != np.asarray(b)))
+
+
+def chunk_order(ia, ja, starts):
+    """The row permutation of a mode 3 forward sweep, restated: chunks get
+    the smallest colour no earlier adjacent chunk holds; colours ascending,
+    chunks ascending, rows ascending."""
+    nn = int(starts[-1]) - 1
+    chunk_of = np.zeros(nn + 1, dtype=np.int64)
+    for q in range(len(starts) - 1):
+        chunk_of[starts[q]:starts[q + 1]] = q
+    colour = []
+    for q in range(len(starts) - 1):
+        used = {colour[int(chunk_of[ja[k]])] for j in range(starts[q], starts[q + 1])
+                for k in range(ia[j], ia[j + 1]) if chunk_of[ja[k]] < q}
+        c = 0
+        while c in used:
+            c += 1
+        colour.append(c)
+    order = [j for c in range(max(colour) + 1) for q in range(len(colour)) if colour[q] == c
+             for j in range(starts[q], starts[q + 1])]
+    return np.asarray(order, dtype=np.int32), max(colour) + 1

@@ -9,7 +9,7 @@ precision form's contract: the converged answer is that of the FP64 form."""
 import numpy as np
 import pytest
 
-from cases import ndiff
+from cases import chunk_order, ndiff
 
 pytestmark = pytest.mark.gpu
 
@@ -55,27 +55,6 @@ def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
         assert gpu.body_forces() == og.body_forces(p)
     assert gpu.status() == 0
     gpu.close()
-
-
-def chunk_order(ia, ja, starts):
-    """The row permutation of a mode 3 forward sweep, restated: chunks get
-    the smallest colour no earlier adjacent chunk holds; colours ascending,
-    chunks ascending, rows ascending."""
-    nn = int(starts[-1]) - 1
-    chunk_of = np.zeros(nn + 1, dtype=np.int64)
-    for q in range(len(starts) - 1):
-        chunk_of[starts[q]:starts[q + 1]] = q
-    colour = []
-    for q in range(len(starts) - 1):
-        used = {colour[int(chunk_of[ja[k]])] for j in range(starts[q], starts[q + 1])
-                for k in range(ia[j], ia[j + 1]) if chunk_of[ja[k]] < q}
-        c = 0
-        while c in used:
-            c += 1
-        colour.append(c)
-    order = [j for c in range(max(colour) + 1) for q in range(len(colour)) if colour[q] == c
-             for j in range(starts[q], starts[q + 1])]
-    return np.asarray(order, dtype=np.int32), max(colour) + 1
 
 
 @pytest.mark.parametrize("nc,nr,curved,order,subits,steps,rows,levels", [
