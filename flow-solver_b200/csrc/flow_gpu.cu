@@ -1627,6 +1627,32 @@ int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
   return st;
 }
 
+int flow_selftest_sweep_timeout(flow_ctx* c, long max_spin, int* status) {
+  if (!c || !c->ok || max_spin < 1 || max_spin > (1L << 21) || !status) {
+    set_error("flow_selftest_sweep_timeout: null context/status or max_spin outside 1..2^21");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  static const unsigned kFirst = 1;  // the dispenser starts at row 2: row 1 never runs
+  reset_run(c, 0.);
+  cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream);
+  cudaMemcpyAsync(c->s.counter, &kFirst, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream);
+  double* dq_new = c->s.dQ2;
+  k_prepare_sweep<<<grid_blocks(4 * (c->nn + 1), 256), 256, 0, c->stream>>>(
+      c->s, c->s.dQ, dq_new, 4 * (c->nn + 1));
+  int rc = launch_check(c);
+  k_sweep_ordered<true><<<c->nsm * 4, 128, 0, c->stream>>>(c->m, c->s, c->s.dQ, dq_new, max_spin);
+  rc |= launch_check(c);
+  if (rc) return rc;
+  *status = read_status(c);
+  // the sweep's output buffer is scratch (the buffers were not swapped); the
+  // context goes on from its state with a clear status
+  cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
+  return 0;
+}
+
 int flow_body_forces(flow_ctx* c, const flow_params* p, double* forces) {
   if (!c || !c->ok || !forces) return FLOW_ERR_ARG;
   cudaSetDevice(c->device);

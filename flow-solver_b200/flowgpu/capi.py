@@ -25,6 +25,7 @@ ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
 ERR_NOT_CONVERGED = 256
 ERR_BUDGET = 512
 ERR_STALLED = 1024
+ERR_SWEEP_TIMEOUT = 64
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
@@ -41,7 +42,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_server_release", "flow_server_running", "flow_server_last_error",
            "flow_server_set_autotune", "flow_server_set_stall",
            "flow_server_set_sweep_schedule", "flow_set_stream_priority",
-           "flow_server_set_priority_policy")
+           "flow_server_set_priority_policy", "flow_selftest_sweep_timeout")
 
 
 class FlowParamsC(C.Structure):
@@ -168,6 +169,7 @@ def _load_locked():
     L.flow_server_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int, C.c_longlong]
     L.flow_set_stream_priority.argtypes = [vp, C.c_int]
     L.flow_server_set_priority_policy.argtypes = [vp, C.c_int]
+    L.flow_selftest_sweep_timeout.argtypes = [vp, C.c_long, IP]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
     L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
@@ -508,6 +510,14 @@ class Solver:
         """`sweeps` Gauss-Seidel sweeps up to `until_step` (0: end of the CFL ramp)."""
         _check(self.L.flow_set_sweep_schedule(self.ctx, int(sweeps), int(until_step)),
                "flow_set_sweep_schedule")
+
+    def selftest_sweep_timeout(self, max_spin: int = 4096) -> int:
+        """Run a sweep whose first row never runs; returns the status bits it
+        left (FLOW_ERR_SWEEP_TIMEOUT when the bounded waits work)."""
+        st = C.c_int(0)
+        _check(self.L.flow_selftest_sweep_timeout(self.ctx, int(max_spin), C.byref(st)),
+               "flow_selftest_sweep_timeout")
+        return st.value
 
     def set_variants(self, node_prepare: int, flux: int):
         _check(self.L.flow_set_variants(self.ctx, int(node_prepare), int(flux)),

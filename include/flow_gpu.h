@@ -271,6 +271,15 @@ void *flow_stream(flow_ctx *ctx);
 int flow_status(flow_ctx *ctx);
 void flow_clear_status(flow_ctx *ctx);
 const char *flow_last_error(void);
+/* Self-test of the sweeps' bounded waits (no counterpart in the reference):
+ * one forward ordered sweep whose dispenser skips row 1, so the rows that
+ * depend on row 1 poll for a value nothing writes until their spin limit
+ * (max_spin polls, at most 2^21), report FLOW_ERR_SWEEP_TIMEOUT, publish a
+ * value so that nothing waits on them, and the kernel ends.  *status
+ * receives the status bits the sweep left (FLOW_ERR_SWEEP_TIMEOUT expected);
+ * the call then clears them.  The solution state is untouched and the
+ * context stays usable.  Call it between steps. */
+int flow_selftest_sweep_timeout(flow_ctx *ctx, long max_spin, int *status);
 /* Number of kernel launches issued by this context so far. */
 long flow_launch_count(flow_ctx *ctx);
 /* Device time (ms) of the last flow_run / flow_solve call, CUDA events. */
