@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
               "-Xptxas", "-v"]
 HOST_SOURCES = ["host/quadrature.c", "host/svd.c", "host/curved.c", "host/prep.cpp"]
-CUDA_SOURCES = ["flow_gpu.cu", "flow_serve.cu"]
+CUDA_SOURCES = ["flow_gpu.cu", "flow_serve.cu", "flow_output.cu"]
 
 
 def nvcc() -> str:

@@ -2188,6 +2188,14 @@ int run_norms(flow_ctx* c, double* r_first, double* r_last) {
 
 cudaStream_t stream_of(flow_ctx* c) { return c->stream; }
 int device_of(flow_ctx* c) { return c->device; }
+int state_of(flow_ctx* c, const double** Q, int* nn, int* ng) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  *Q = c->s.Q;
+  *nn = c->nn;
+  *ng = c->ng;
+  return 0;
+}
+void set_last_error(const char* msg) { set_error(msg); }
 
 }  // namespace internal
 }  // namespace flow

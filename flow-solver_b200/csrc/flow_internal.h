@@ -26,6 +26,11 @@ double run_ms(flow_ctx* c, int slot);
 int run_norms(flow_ctx* c, double* r_first, double* r_last);
 cudaStream_t stream_of(flow_ctx* c);
 int device_of(flow_ctx* c);
+// The context's resident state GRID::Q ((nn+nn_ghost+1)*4 doubles on the
+// device) and its node counts; FLOW_ERR_ARG for a null or failed context.
+int state_of(flow_ctx* c, const double** Q, int* nn, int* ng);
+// Message returned by flow_last_error() on this thread.
+void set_last_error(const char* msg);
 
 }  // namespace internal
 }  // namespace flow

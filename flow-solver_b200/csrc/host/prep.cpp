@@ -36,6 +36,7 @@ struct flow_mesh {
   std::vector<int> tri, quad;         // (n+1)*nv, 1-based rows
   std::vector<int> nbs;               // nb+1
   std::vector<std::vector<std::array<int, 2>>> bs;  // bs[b][s], b,s 1-based
+  std::vector<int> seg_flat;          // bs of every boundary in order, 2 per segment
   std::vector<int> bbc;
   std::vector<int> nn_map;
   std::vector<int> csn, ncsn, nsn, nnsn, esn, edges;
@@ -828,6 +829,12 @@ flow_mesh* finish(flow_mesh* m, int reorder, int order, int* status) {
     if (!build_stencils(*m)) return fail("a node's stencil stays below 6 neighbours");
     if (!factor_stencils(*m)) return fail("SVD of a stencil failed");
   }
+  m->seg_flat.clear();
+  for (int b = 1; b <= m->nb; b++)
+    for (int t = 1; t <= m->nbs[b]; t++) {
+      m->seg_flat.push_back(m->bs[b][t][0]);
+      m->seg_flat.push_back(m->bs[b][t][1]);
+    }
   if (status) *status = 0;
   return m;
 }
@@ -993,6 +1000,26 @@ int flow_prep_initial_state(const flow_mesh* m, const flow_params* p, double* Q)
 }
 
 const int* flow_prep_node_map(const flow_mesh* m) { return m ? m->nn_map.data() : nullptr; }
+
+int flow_prep_elements(const flow_mesh* m, int* ntri, const int** tri, int* nquad,
+                       const int** quad) {
+  if (!m || !ntri || !tri || !nquad || !quad) return FLOW_ERR_ARG;
+  *ntri = m->ntri;
+  *tri = m->tri.data();
+  *nquad = m->nquad;
+  *quad = m->quad.data();
+  return 0;
+}
+
+int flow_prep_segments(const flow_mesh* m, int* nb, const int** bbc, const int** nbs,
+                       const int** seg) {
+  if (!m || !nb || !bbc || !nbs || !seg) return FLOW_ERR_ARG;
+  *nb = m->nb;
+  *bbc = m->bbc.data();
+  *nbs = m->nbs.data();
+  *seg = m->seg_flat.data();
+  return 0;
+}
 
 void flow_prep_free(flow_mesh* m) { delete m; }
 

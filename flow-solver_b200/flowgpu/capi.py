@@ -22,6 +22,7 @@ LP = C.POINTER(C.c_long)
 ERRORS = {1: "ARG", 2: "CUDA", 4: "EIGEN", 8: "DT", 16: "LIMITER", 32: "BC",
           64: "SWEEP_TIMEOUT", 128: "NOT_FOUND", 256: "NOT_CONVERGED", 512: "BUDGET",
           1024: "STALLED"}
+ERR_ARG = 1
 ERR_NOT_CONVERGED = 256
 ERR_BUDGET = 512
 ERR_STALLED = 1024
@@ -30,7 +31,8 @@ ERR_SWEEP_TIMEOUT = 64
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
-           "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_get", "flow_size",
+           "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_surface_cp",
+           "flow_write_surface_cp", "flow_write_tecplot", "flow_get", "flow_size",
            "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_chunk_starts", "flow_set_graphs",
            "flow_autotune", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
@@ -115,6 +117,9 @@ def _load_locked():
     L.flow_residuals.argtypes = [vp, PP, C.c_int, C.c_int]
     L.flow_linear_solve.argtypes = [vp, PP, DP]
     L.flow_body_forces.argtypes = [vp, PP, DP]
+    L.flow_surface_cp.argtypes = [vp, PP, C.c_int, IP, IP, C.c_int, IP, DP, C.c_int, IP]
+    L.flow_write_surface_cp.argtypes = [vp, PP, C.c_char_p, C.c_int, IP, IP, IP, DP]
+    L.flow_write_tecplot.argtypes = [vp, PP, C.c_char_p, C.c_int, DP, C.c_int, IP, C.c_int, IP]
     L.flow_get.argtypes = [vp, C.c_char_p, DP, C.c_long]
     L.flow_size.restype = C.c_long
     L.flow_size.argtypes = [vp, C.c_char_p]
@@ -177,6 +182,8 @@ def _load_locked():
     L.flow_prep_initial_state.argtypes = [vp, C.POINTER(FlowParamsC), DP]
     L.flow_prep_node_map.restype = IP
     L.flow_prep_node_map.argtypes = [vp]
+    L.flow_prep_elements.argtypes = [vp, IP, C.POINTER(IP), IP, C.POINTER(IP)]
+    L.flow_prep_segments.argtypes = [vp, IP, C.POINTER(IP), C.POINTER(IP), C.POINTER(IP)]
     L.flow_prep_free.argtypes = [vp]
     L.flow_prep_last_error.restype = C.c_char_p
     return L
@@ -468,6 +475,40 @@ class Solver:
         f = (C.c_double * 2)()
         _check(self.L.flow_body_forces(self.ctx, C.byref(self.p), f), "flow_body_forces")
         return f[0], f[1]
+
+    def surface_cp(self, mesh, b: int):
+        """Nodes of boundary b in first-appearance order and their pressure
+        coefficients (flow_surface_cp, computed on the device)."""
+        nb, bbc, nbs, seg = mesh.segments()
+        cap = int(nbs[b]) * 2 if 1 <= b <= nb else 0
+        nodes = np.zeros(max(cap, 1), dtype=np.int32)
+        cp = np.zeros(max(cap, 1))
+        cnt = C.c_int(0)
+        _check(self.L.flow_surface_cp(self.ctx, C.byref(self.p), nb, nbs.ctypes.data_as(IP),
+                                      seg.ctypes.data_as(IP), int(b), nodes.ctypes.data_as(IP),
+                                      cp.ctypes.data_as(DP), cap, C.byref(cnt)), "flow_surface_cp")
+        return nodes[:cnt.value].copy(), cp[:cnt.value].copy()
+
+    def write_surface_cp(self, mesh, directory: str):
+        """surface_<b>_pressure.dat of every inviscid boundary into directory
+        (write_surface_cp)."""
+        nb, bbc, nbs, seg = mesh.segments()
+        x = mesh.array("x")
+        _check(self.L.flow_write_surface_cp(self.ctx, C.byref(self.p), directory.encode(), nb,
+                                            bbc.ctypes.data_as(IP), nbs.ctypes.data_as(IP),
+                                            seg.ctypes.data_as(IP), x.ctypes.data_as(DP)),
+               "flow_write_surface_cp")
+
+    def write_tecplot(self, mesh, path: str, primitive: bool = False):
+        """Tecplot solution file of the current state (write_tecplot_solutionC,
+        or write_tecplot_solutionP with primitive=True)."""
+        tri, quad = mesh.elements()
+        x = mesh.array("x")
+        _check(self.L.flow_write_tecplot(self.ctx, C.byref(self.p), path.encode(),
+                                         1 if primitive else 0, x.ctypes.data_as(DP),
+                                         len(tri) // 3 - 1, tri.ctypes.data_as(IP),
+                                         len(quad) // 4 - 1, quad.ctypes.data_as(IP)),
+               "flow_write_tecplot")
 
     def get(self, name: str) -> np.ndarray:
         n = self.L.flow_size(self.ctx, name.encode())

@@ -103,5 +103,28 @@ class Mesh:
             names += ["gnsn", "gnnsn", "gnnsn1", "svd_m", "svd_off", "svd_U", "svd_VT", "svd_S"]
         return {n: self.array(n) for n in names}
 
+    def elements(self):
+        """Renumbered connectivity (GRID::c2n[Tri], c2n[Quad]): 1-based rows,
+        row 0 unused, as flat int32 arrays."""
+        nt, nq = C.c_int(), C.c_int()
+        tp, qp = capi.IP(), capi.IP()
+        self.L.flow_prep_elements(self.h, C.byref(nt), C.byref(tp), C.byref(nq), C.byref(qp))
+        tri = np.ctypeslib.as_array(tp, shape=((nt.value + 1) * 3,)).copy()
+        quad = np.ctypeslib.as_array(qp, shape=((nq.value + 1) * 4,)).copy()
+        return tri, quad
+
+    def segments(self):
+        """nb, bbc and nbs (index 0 unused) and every boundary's renumbered
+        segment node pairs in order, flat int32 (GRID::bs)."""
+        nb = C.c_int()
+        bp, np_, sp = capi.IP(), capi.IP(), capi.IP()
+        self.L.flow_prep_segments(self.h, C.byref(nb), C.byref(bp), C.byref(np_), C.byref(sp))
+        bbc = np.ctypeslib.as_array(bp, shape=(nb.value + 1,)).copy()
+        nbs = np.ctypeslib.as_array(np_, shape=(nb.value + 1,)).copy()
+        n = 2 * int(nbs[1:].sum())
+        seg = (np.ctypeslib.as_array(sp, shape=(n,)).copy() if n
+               else np.zeros(1, dtype=np.int32))
+        return nb.value, bbc, nbs, seg
+
     def node_map(self) -> np.ndarray:
         return np.ctypeslib.as_array(self.L.flow_prep_node_map(self.h), shape=(self.view.nn + 1,)).copy()

@@ -186,6 +186,40 @@ int flow_linear_solve(flow_ctx *ctx, const flow_params *p, double *rms);
  * grid_io.C:1390-1697): raw pressure lift and drag on the wall boundaries. */
 int flow_body_forces(flow_ctx *ctx, const flow_params *p, double *forces);
 
+/* ---- Outputs of a solve (grid_io.C), from the resident state GRID::Q ----
+ * The GRID arrays these writers read besides the state are passed as plain
+ * host pointers: x is GRID::x ((nn+1)*2 or more doubles), tri / quad are
+ * GRID::c2n[Tri] / c2n[Quad] (1-based rows, row 0 unused), bbc and nbs are
+ * GRID::bbc and GRID::nbs (nb+1 ints, index 0 unused) and seg is every
+ * boundary's GRID::bs[b][s][0..1] pairs in order, boundary 1 first.  Where
+ * the reference prints a message and exits (a file it cannot open) these
+ * return FLOW_ERR_ARG with the message in flow_last_error(). */
+
+/* Pressure coefficient of write_surface_cp (grid_io.C:841-1375, its active
+ * branch grid_io.C:1292-1354) on boundary b: the boundary's segment nodes in
+ * first-appearance order (n0 before n1 of each segment) into nodes_out and
+ * Cp = (P/p_inf - 1) * 2/(gamma M^2), p_inf = 1/gamma, into cp_out, computed
+ * on the device.  *count receives the number of nodes; FLOW_ERR_ARG if it
+ * exceeds cap. */
+int flow_surface_cp(flow_ctx *ctx, const flow_params *p, int nb, const int *nbs, const int *seg,
+                    int b, int *nodes_out, double *cp_out, int cap, int *count);
+
+/* void write_surface_cp(GRID*, PARAMS)  (include/grid_io.h:34, grid_io.C:841-1375):
+ * one file dir/surface_<b>_pressure.dat per inviscid boundary (bbc[b] odd),
+ * lines "%f  %f" of (float) x and (float) Cp, ordered as the reference's
+ * `sort -g` orders them under the C locale (by the leading number, ties by
+ * the line's bytes).  dir NULL or "" writes into the working directory. */
+int flow_write_surface_cp(flow_ctx *ctx, const flow_params *p, const char *dir, int nb,
+                          const int *bbc, const int *nbs, const int *seg, const double *x);
+
+/* void write_tecplot_solutionC(char*, GRID*) (primitive = 0, include/grid_io.h:22,
+ * grid_io.C:102-199) and void write_tecplot_solutionP(char*, GRID*, double)
+ * (primitive != 0, include/grid_io.h:24, grid_io.C:216-331): the Tecplot point-data file of the nn real nodes
+ * (x, y and Q, or rho, u, v, P) with the element connectivity, the same
+ * bytes as the reference writes. */
+int flow_write_tecplot(flow_ctx *ctx, const flow_params *p, const char *path, int primitive,
+                       const double *x, int ntri, const int *tri, int nquad, const int *quad);
+
 /* Copy a named array back in the reference layout: "Q", "nQ", "pQ", "dQ",
  * "R", "RHS", "LHS", "grad", "phi", "hess" ((nn+1)*36), "point_value",
  * "dt", "xn_bedges".  n is the number of doubles the caller provides. */

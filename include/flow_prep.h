@@ -50,6 +50,19 @@ int flow_prep_initial_state(const flow_mesh *m, const flow_params *p, double *Q)
 /* nn_map of the renumbering (old 1-based id -> new id), nn+1 ints. */
 const int *flow_prep_node_map(const flow_mesh *m);
 
+/* Element connectivity after the renumbering (GRID::c2n[Tri] and
+ * GRID::c2n[Quad], reorder.C:58-303): 1-based rows with row 0 unused,
+ * (ntri+1)*3 and (nquad+1)*4 ints, valid while the mesh lives. */
+int flow_prep_elements(const flow_mesh *m, int *ntri, const int **tri, int *nquad,
+                       const int **quad);
+
+/* Boundaries after the renumbering: nb, bbc and nbs (nb+1 ints each, index
+ * 0 unused; GRID::nb, GRID::bbc, GRID::nbs) and the segments' (n0, n1) node
+ * pairs GRID::bs[b][s][0..1] of every boundary in order, boundary 1 first,
+ * 2 ints per segment. */
+int flow_prep_segments(const flow_mesh *m, int *nb, const int **bbc, const int **nbs,
+                       const int **seg);
+
 void flow_prep_free(flow_mesh *m);
 
 /* Message of the last failed flow_prep_* call of this thread. */

@@ -56,6 +56,9 @@ def lib():
         L.ref_cfl.restype = C.c_double
         L.ref_cfl.argtypes = [vp]
         L.ref_set_quiet.argtypes = [C.c_int]
+        L.ref_write_surface_cp.restype = C.c_int
+        L.ref_write_surface_cp.argtypes = [vp, C.c_char_p]
+        L.ref_write_tecplot.argtypes = [vp, C.c_char_p, C.c_int]
         _lib = L
     return _lib
 
@@ -188,3 +191,12 @@ class RefSolver:
 
     def cfl(self) -> float:
         return self.L.ref_cfl(self.h)
+
+    # ---- writers (grid_io.C) ----
+    def write_surface_cp(self, directory: str):
+        """write_surface_cp run in `directory` (its sort under LC_ALL=C)."""
+        if self.L.ref_write_surface_cp(self.h, directory.encode()) != 0:
+            raise RuntimeError(f"cannot enter {directory}")
+
+    def write_tecplot(self, path: str, primitive: bool = False):
+        self.L.ref_write_tecplot(self.h, path.encode(), 1 if primitive else 0)

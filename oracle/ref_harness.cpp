@@ -362,4 +362,39 @@ int ref_svd(void *h, int i, double **U, double **VT, double **S)
 
 double ref_cfl(void *h) { return ((RefCase *)h)->grid.cfl; }
 
+/* write_surface_cp (grid_io.C:841-1375) from the current GRID::Q: it writes
+ * surface_<b>_pressure.dat into the working directory and orders each file
+ * with the shell's `sort -g`, so the call runs in `dir` with LC_ALL=C for
+ * its duration (ties then order bytewise).  Returns 0, or -1 if dir cannot
+ * be entered. */
+int ref_write_surface_cp(void *h, const char *dir)
+{
+  RefCase *c = (RefCase *)h;
+  Cwd cwd(dir);
+  if (!cwd.ok) return -1;
+  const char *old = getenv("LC_ALL");
+  char saved[256] = {0};
+  if (old) strncpy(saved, old, sizeof(saved) - 1);
+  setenv("LC_ALL", "C", 1);
+  {
+    Mute mute;
+    write_surface_cp(&c->grid, c->p);
+  }
+  if (old) setenv("LC_ALL", saved, 1); else unsetenv("LC_ALL");
+  return 0;
+}
+
+/* write_tecplot_solutionC (primitive 0, grid_io.C:102-199) or
+ * write_tecplot_solutionP (grid_io.C:216-331) of the current GRID::Q. */
+void ref_write_tecplot(void *h, const char *path, int primitive)
+{
+  RefCase *c = (RefCase *)h;
+  char name[4096];
+  strncpy(name, path, sizeof(name) - 1);
+  name[sizeof(name) - 1] = 0;
+  Mute mute;
+  if (primitive) write_tecplot_solutionP(name, &c->grid, c->p.gamma);
+  else write_tecplot_solutionC(name, &c->grid);
+}
+
 }  // extern "C"
