@@ -706,8 +706,8 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
   for (int pp = 0; pp < nn; pp++) rinfo[pp] = make_int4(rows[pp], optr[pp], optr[pp + 1], 0);
   mt.rowinfo = upload_vec(c, rinfo);
   mt.lu32 = c->buf.alloc<float>((size_t)16 * nn);
-  mt.dq32 = c->buf.alloc<float>((size_t)4 * (nn + 1));
-  mt.dq32b = c->buf.alloc<float>((size_t)4 * (nn + 1));
+  if (!mt.dq32) mt.dq32 = c->buf.alloc<float>((size_t)4 * (nn + 1));
+  if (!mt.dq32b) mt.dq32b = c->buf.alloc<float>((size_t)4 * (nn + 1));
   mt.lhs32 = c->buf.alloc<float>((size_t)16 * std::max<size_t>(ocol.size(), 1));
   if (!mt.color_ptr || !mt.rows || !mt.pos || !mt.offd_ptr || !mt.offd_col || !mt.rowinfo || !mt.lu32 ||
       !mt.dq32 || !mt.dq32b || !mt.lhs32) {
@@ -719,6 +719,21 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
   cudaMemset(mt.dq32b, 0, sizeof(float) * 4 * (nn + 1));
   c->h_color_ptr = cptr;
   c->mt_ordered = ordered;
+  return 0;
+}
+
+// Mode 3 reads none of the mode 1 / 2 tables: only the FP32 iterate.
+int build_chunk_iterate(flow_ctx* c) {
+  MixedTables& mt = c->mt;
+  const size_t n = (size_t)4 * (c->nn + 1);
+  if (!mt.dq32) mt.dq32 = c->buf.alloc<float>(n);
+  if (!mt.dq32b) mt.dq32b = c->buf.alloc<float>(n);
+  if (!mt.dq32 || !mt.dq32b) {
+    set_error("precision form: device allocation failed");
+    return FLOW_ERR_CUDA;
+  }
+  cudaMemset(mt.dq32, 0, sizeof(float) * n);
+  cudaMemset(mt.dq32b, 0, sizeof(float) * n);
   return 0;
 }
 
@@ -738,6 +753,10 @@ int build_chunk_tables(flow_ctx* c) {
   const std::vector<int>& ja = c->h_ja;
   int bw = 1;
   for (int j = 1; j <= nn; j++) {
+    if (ia[j + 1] <= ia[j] || ja[ia[j + 1] - 1] != j) {
+      set_error("precision form: a row's diagonal block is not its last block");
+      return FLOW_ERR_ARG;
+    }
     if (ia[j + 1] - ia[j] - 1 > kRecBlocks) {
       set_error("precision mode 3: a row has more than 8 off-diagonal blocks");
       return FLOW_ERR_ARG;
@@ -867,16 +886,17 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
         set_error("precision mode 3: a chunk has more sub-levels than the sweep kernel holds");
         return FLOW_ERR_ARG;
       }
-    std::vector<SweepRec> rec(nn);
-    memset(rec.data(), 0, sizeof(SweepRec) * nn);
-    for (int i = 0; i < nn; i++) {
-      const int j = order[i];
-      const int nb = ia[j + 1] - ia[j] - 1;  // the diagonal block is the row's last
-      rec[i].hdr = make_int4(j, nb, 0, 0);
-      int* cols = reinterpret_cast<int*>(rec[i].cols);
-      for (int t = 0; t < nb; t++) cols[t] = ja[ia[j] + t];
+    // the records' static part is written on the device from the resident
+    // block pattern: only the order (4 bytes a row) crosses from the host
+    SweepRec* rec = c->buf.alloc<SweepRec>(nn);
+    const int* d_order = upload_vec(c, order);
+    if (rec && d_order) {
+      const long words = (long)nn * kRecInts;
+      k_fill_sweep_records<<<(unsigned)((words + 255) / 256), 256, 0, c->stream>>>(
+          rec, d_order, nn, c->m.ia, c->m.ja);
+      if (cudaGetLastError() != cudaSuccess) rec = nullptr;
     }
-    ct.rec[dir] = upload_vec(c, rec);
+    ct.rec[dir] = rec;
     ct.sub_start[dir] = upload_vec(c, ss);
     ct.chunk_sub[dir] = upload_vec(c, cs);
     ct.pos[dir] = upload_vec(c, pos);
@@ -1314,7 +1334,7 @@ int flow_set_precision(flow_ctx* c, int mode) {
   if (mode != 0) {
     cudaStreamSynchronize(c->stream);
     drop_graphs(c);
-    int rc = build_mixed_tables(c, mode >= 2);
+    int rc = mode == 3 ? build_chunk_iterate(c) : build_mixed_tables(c, mode >= 2);
     if (!rc && mode == 3) rc = build_chunk_tables(c);
     if (rc) return rc;
   }

@@ -978,6 +978,38 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Static part of mode 3's sweep records: record i holds row order[i]'s
+// header (row, off-diagonal block count; the diagonal block is the row's
+// last) and its off-diagonal column indices, every other word zero until
+// assembly writes the values.  One thread per 16-byte word: word 0 the
+// header, 1 the right-hand side, 2-5 the LU factors, 6-7 the columns, 8-39
+// the blocks.
+static_assert(offsetof(SweepRec, cols) == 6 * 16 && offsetof(SweepRec, a) == 8 * 16 &&
+                  sizeof(SweepRec) == 40 * 16,
+              "k_fill_sweep_records assumes the SweepRec word layout");
+__global__ void k_fill_sweep_records(SweepRec* __restrict__ rec, const int* __restrict__ order,
+                                     int nrec, const int* __restrict__ ia,
+                                     const int* __restrict__ ja) {
+  const long w = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (w >= (long)nrec * kRecInts) return;
+  const int i = (int)(w / kRecInts), k = (int)(w - (long)i * kRecInts);
+  int4 v = make_int4(0, 0, 0, 0);
+  if (k == 0 || k == 6 || k == 7) {
+    const int j = order[i];
+    const int k0 = ia[j], nb = ia[j + 1] - k0 - 1;
+    if (k == 0) {
+      v = make_int4(j, nb, 0, 0);
+    } else {
+      const int t0 = 4 * (k - 6);
+      v.x = t0 + 0 < nb ? ja[k0 + t0 + 0] : 0;
+      v.y = t0 + 1 < nb ? ja[k0 + t0 + 1] : 0;
+      v.z = t0 + 2 < nb ? ja[k0 + t0 + 2] : 0;
+      v.w = t0 + 3 < nb ? ja[k0 + t0 + 3] : 0;
+    }
+  }
+  reinterpret_cast<int4*>(rec)[w] = v;
+}
+
 template <int DIR>
 __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct, float* dq32,
                                                      int colour, int last) {

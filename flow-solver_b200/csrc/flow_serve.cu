@@ -19,6 +19,7 @@
 #include <chrono>
 #include <cmath>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <string>
 #include <thread>
@@ -30,6 +31,13 @@
 namespace {
 
 thread_local std::string g_serve_error;
+
+// Autotuned kernel variants by (device, order, precision, mesh-size bucket),
+// kept for the process and shared by every server: the variants give
+// bit-identical results and their speed depends only on the device and the
+// mesh, so a choice measured once holds for every later admission.
+std::mutex g_tuned_mutex;
+std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;
 
 struct Slot {
   flow_ctx* ctx = nullptr;
@@ -61,8 +69,6 @@ struct flow_server {
   int sched_sweeps = 0, sched_until = 0;  // sweep schedule of precision-form solves
   long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
   int priority_policy = 0;                // 1: larger meshes get greater stream priority
-  // autotuned kernel variants by (order, precision, mesh-size bucket)
-  std::map<std::tuple<int, int, int>, std::pair<int, int>> tuned;
 };
 
 namespace {
@@ -163,18 +169,27 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   }
   if (!rc) rc = flow_set_state(c, Q0);
   if (!rc && sv->autotune_steps > 0) {
-    // kernel variants: measured once per (order, precision, size bucket)
+    // kernel variants: measured once per (device, order, precision, size bucket)
     const long nn = flow_size(c, "dt") - 1;
     const int bucket = (int)std::floor(2.0 * std::log2((double)std::max(nn, 1L)));
-    const auto key = std::make_tuple(p->order, precision, bucket);
-    auto it = sv->tuned.find(key);
-    if (it != sv->tuned.end()) {
-      rc = flow_set_variants(c, it->second.first, it->second.second);
+    const auto key = std::make_tuple(flow::internal::device_of(c), p->order, precision, bucket);
+    std::pair<int, int> found(-1, -1);
+    {
+      std::lock_guard<std::mutex> lock(g_tuned_mutex);
+      auto it = g_tuned.find(key);
+      if (it != g_tuned.end()) found = it->second;
+    }
+    if (found.first >= 0) {
+      rc = flow_set_variants(c, found.first, found.second);
     } else {
       int v[2] = {0, 0};
       const int trc = flow_autotune(c, p, 1, sv->autotune_steps, v, nullptr);
-      if (trc & FLOW_ERR_CUDA) rc = trc;  // other bits: the tuning steps' physics, not fatal
-      else sv->tuned[key] = std::make_pair(v[0], v[1]);
+      if (trc & FLOW_ERR_CUDA) {
+        rc = trc;  // other bits: the tuning steps' physics, not fatal
+      } else {
+        std::lock_guard<std::mutex> lock(g_tuned_mutex);
+        g_tuned[key] = std::make_pair(v[0], v[1]);
+      }
     }
   }
   if (rc) {

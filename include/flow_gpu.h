@@ -399,9 +399,10 @@ int flow_server_result(flow_server *srv, int slot, double *Q, long nQ, double *f
 int flow_server_release(flow_server *srv, int slot);
 int flow_server_running(flow_server *srv);
 /* Autotune the kernel variants of each admitted solve over `steps` steps
- * (flow_autotune), once per (order, precision, mesh-size bucket of a factor
- * sqrt(2) in nodes); later admissions in the bucket reuse the choice.
- * 0 (default) turns it off. */
+ * (flow_autotune), once per (device, order, precision, mesh-size bucket of
+ * a factor sqrt(2) in nodes); later admissions in the bucket, by this server
+ * or any later one in the process, reuse the choice (the variants' results
+ * are bit-identical).  0 (default) turns it off. */
 int flow_server_set_autotune(flow_server *srv, int steps);
 /* Retire a running solve with FLOW_ERR_STALLED once its best ||R_rho||
  * (relative to its first step, tracked in factors of 10 at chunk
