@@ -175,6 +175,12 @@ struct flow_ctx {
   ChunkTables ct{};          // mode 3 tables and sweep records
   std::vector<int> h_col_ptr, h_chunk_start;
   int chunk_rows = 0, chunk_levels = 0;  // requested limits (0: defaults)
+  // sub-level tables of each ring shape of the chunk sweep (per direction);
+  // ct.sub_start / ct.chunk_sub point at those of the shape in use
+  const int* ring_sub_start[kRingShapes][2] = {};
+  const int* ring_chunk_sub[kRingShapes][2] = {};
+  bool ring_ok[kRingShapes] = {};
+  int ring = 0;  // requested shape: sub-levels of ring_rows(ring) rows
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
   // CUDA graphs of chunks of K steps with the step index advancing on the
@@ -394,7 +400,7 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
   if (c->precision == 3) {
     // coloured chunks of the reference order, in-place FP32 iterate
     const ChunkTables& ct = c->ct;
-    const size_t smem = 16 * kRecStride * kRecSlots * kRecRows + sizeof(float4) * ct.maxwin;
+    const size_t smem = 16 * kRecStride * kRingRecords + sizeof(float4) * ct.maxwin;
     for (int it = 0; it < p->subits; it++) {
       Timed t(c, 4);
       const int last = it == p->subits - 1, dir = it % 2;
@@ -402,10 +408,11 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
         const int col = dir == 0 ? ci : ct.ncol - 1 - ci;
         const int nb = c->h_col_ptr[col + 1] - c->h_col_ptr[col];
         if (nb <= 0) continue;
-        if (dir == 0)
-          k_sweep_chunk<0><<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
-        else
-          k_sweep_chunk<1><<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
+        auto kern = dir == 0 ? (ct.ring == 2 ? k_sweep_chunk<0, 16>
+                                : ct.ring == 1 ? k_sweep_chunk<0, 32> : k_sweep_chunk<0, 64>)
+                             : (ct.ring == 2 ? k_sweep_chunk<1, 16>
+                                : ct.ring == 1 ? k_sweep_chunk<1, 32> : k_sweep_chunk<1, 64>);
+        kern<<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
         rc |= launch_check(c);
       }
     }
@@ -775,7 +782,19 @@ int build_chunk_tables(flow_ctx* c) {
   }
 }
 
+// Point the chunk tables at the sub-levels of the requested ring shape (the
+// largest shape when the requested one does not fit a chunk).
+void apply_ring(flow_ctx* c) {
+  const int shape = c->ring_ok[c->ring] ? c->ring : 0;
+  for (int dir = 0; dir < 2; dir++) {
+    c->ct.sub_start[dir] = c->ring_sub_start[shape][dir];
+    c->ct.chunk_sub[dir] = c->ring_chunk_sub[shape][dir];
+  }
+  c->ct.ring = shape;
+}
+
 int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
+  for (int shape = 0; shape < kRingShapes; shape++) c->ring_ok[shape] = true;
   const int nn = c->nn;
   const std::vector<int>& ia = c->h_ia;
   const std::vector<int>& ja = c->h_ja;
@@ -833,7 +852,7 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
     win[q] = make_int2(a, b);
     maxwin = std::max(maxwin, b - a + 1);
   }
-  const size_t smem = 16 * kRecStride * kRecSlots * kRecRows + sizeof(float4) * maxwin;
+  const size_t smem = 16 * kRecStride * kRingRecords + sizeof(float4) * maxwin;
   if (smem + kChunkStaticSmem > 227 * 1024) {
     set_error("precision mode 3: a chunk's window does not fit in shared memory (bandwidth too large)");
     return FLOW_ERR_ARG;
@@ -848,7 +867,7 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
   // per direction: levels, sub-levels, records (static part)
   std::vector<int> levd(nn + 1);
   for (int dir = 0; dir < 2; dir++) {
-    std::vector<int> ss, cs(nch + 1, 0), pos(nn + 1, 0), order;
+    std::vector<int> pos(nn + 1, 0), order, lev_start, chunk_lev(nch + 1, 0);
     order.reserve(nn);
     for (int q = 0; q < nch; q++) {
       const int lo = start[q], hi = start[q + 1] - 1;
@@ -864,28 +883,47 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
         levd[j] = l;
         nlev = std::max(nlev, l + 1);
       }
-      cs[q] = (int)ss.size();
       for (int l = 0; l < nlev; l++) {
-        int in_sub = kRecRows;
+        lev_start.push_back((int)order.size());
         for (int j = lo; j <= hi; j++) {
           if (levd[j] != l) continue;
-          if (in_sub == kRecRows) {
-            ss.push_back((int)order.size());
-            in_sub = 0;
-          }
           pos[j] = (int)order.size();
           order.push_back(j);
-          in_sub++;
         }
       }
+      chunk_lev[q + 1] = (int)lev_start.size();
     }
-    cs[nch] = (int)ss.size();
-    ss.push_back((int)order.size());
-    for (int q = 0; q < nch; q++)
-      if (cs[q + 1] - cs[q] > kChunkSubMax) {
-        set_error("precision mode 3: a chunk has more sub-levels than the sweep kernel holds");
-        return FLOW_ERR_ARG;
+    lev_start.push_back((int)order.size());
+    // sub-levels of each ring shape: every level cut into runs of at most
+    // ring_rows(shape) rows (rows of one level are independent, so the cut
+    // changes the barriers, not the arithmetic)
+    for (int shape = 0; shape < kRingShapes; shape++) {
+      const int rows = ring_rows(shape);
+      std::vector<int> ss, cs(nch + 1, 0);
+      bool fits = true;
+      for (int q = 0; q < nch; q++) {
+        cs[q] = (int)ss.size();
+        for (int L = chunk_lev[q]; L < chunk_lev[q + 1]; L++)
+          for (int x = lev_start[L]; x < lev_start[L + 1]; x += rows) ss.push_back(x);
+        if ((int)ss.size() - cs[q] > kChunkSubMax) fits = false;
       }
+      cs[nch] = (int)ss.size();
+      ss.push_back((int)order.size());
+      if (!fits) {
+        if (shape == 0) {
+          set_error("precision mode 3: a chunk has more sub-levels than the sweep kernel holds");
+          return FLOW_ERR_ARG;
+        }
+        c->ring_ok[shape] = false;
+        continue;
+      }
+      c->ring_sub_start[shape][dir] = upload_vec(c, ss);
+      c->ring_chunk_sub[shape][dir] = upload_vec(c, cs);
+      if (!c->ring_sub_start[shape][dir] || !c->ring_chunk_sub[shape][dir]) {
+        set_error("precision mode 3: table upload failed");
+        return FLOW_ERR_CUDA;
+      }
+    }
     // the records' static part is written on the device from the resident
     // block pattern: only the order (4 bytes a row) crosses from the host
     SweepRec* rec = c->buf.alloc<SweepRec>(nn);
@@ -897,10 +935,8 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
       if (cudaGetLastError() != cudaSuccess) rec = nullptr;
     }
     ct.rec[dir] = rec;
-    ct.sub_start[dir] = upload_vec(c, ss);
-    ct.chunk_sub[dir] = upload_vec(c, cs);
     ct.pos[dir] = upload_vec(c, pos);
-    if (!ct.rec[dir] || !ct.sub_start[dir] || !ct.chunk_sub[dir] || !ct.pos[dir]) {
+    if (!ct.rec[dir] || !ct.pos[dir]) {
       set_error("precision mode 3: table upload failed");
       return FLOW_ERR_CUDA;
     }
@@ -912,13 +948,17 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
   // the limit is a property of the kernel, shared by every context: allow the
   // largest window any context may need, not this context's own
   const int smem_cap = 227 * 1024 - kChunkStaticSmem;
-  if (cudaFuncSetAttribute(k_sweep_chunk<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           smem_cap) != cudaSuccess ||
-      cudaFuncSetAttribute(k_sweep_chunk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           smem_cap) != cudaSuccess) {
+  bool attr_ok = true;
+  for (const void* f : {(const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
+                        (const void*)k_sweep_chunk<0, 32>, (const void*)k_sweep_chunk<1, 32>,
+                        (const void*)k_sweep_chunk<0, 16>, (const void*)k_sweep_chunk<1, 16>})
+    attr_ok = attr_ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              smem_cap) == cudaSuccess;
+  if (!attr_ok) {
     set_error("precision mode 3: cannot reserve shared memory for the sweep");
     return FLOW_ERR_CUDA;
   }
+  apply_ring(c);
   c->h_col_ptr = cptr;
   c->h_chunk_start = start;
   return 0;
@@ -1111,31 +1151,6 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   UP(nsub_ptr, nsub.ptr); UP(nsub, nsub.idx);
   UP(nbed_ptr, nbed.ptr); UP(nbed, nbed.idx);
   UP(nedg_ptr, nedg.ptr); UP(nedg, nedg.idx);
-  {
-    // node-major copies of the static face data each node reads
-    std::vector<double4> ngeo(nsub.idx.size());
-    std::vector<double2> nfdx(nsub.idx.size());
-    std::vector<double2> ngdx(p->order == 3 ? 3 * nsub.idx.size() : 1);
-    for (int n = 1; n <= nn; n++) {
-      for (int k = nsub.ptr[n]; k < nsub.ptr[n + 1]; k++) {
-        const int sb = nsub.idx[k] >> 1, side = nsub.idx[k] & 1;
-        ngeo[k] = sub_geo[sb];
-        nfdx[k] = side ? make_double2(sub_dx[sb].z, sub_dx[sb].w)
-                       : make_double2(sub_dx[sb].x, sub_dx[sb].y);
-        if (p->order == 3 && g->xg_subedges)
-          for (int gp = 0; gp < 3; gp++)
-            ngdx[3 * (size_t)k + gp] =
-                make_double2(g->xg_subedges[6 * (size_t)sb + 2 * gp] - g->x[2 * n],
-                             g->xg_subedges[6 * (size_t)sb + 2 * gp + 1] - g->x[2 * n + 1]);
-      }
-    }
-    std::vector<int> nother(nedg.idx.size());
-    for (size_t k = 0; k < nedg.idx.size(); k++) {
-      const int e = nedg.idx[k] >> 1, side = nedg.idx[k] & 1;
-      nother[k] = side ? edge_lr[e].x : edge_lr[e].y;
-    }
-    UP(nsub_geo, ngeo); UP(nsub_fdx, nfdx); UP(nsub_gdx, ngdx); UP(nedg_other, nother);
-  }
   UP(sub_lr, sub_lr); UP(sub_geo, sub_geo); UP(sub_dx, sub_dx);
   UP(edge_lr, edge_lr); UP(edge_w, edge_w);
   UP(csr_sub, csr_sub);
@@ -1339,6 +1354,30 @@ int flow_set_precision(flow_ctx* c, int mode) {
     if (rc) return rc;
   }
   c->precision = mode;
+  return 0;
+}
+
+int flow_set_sweep_ring(flow_ctx* c, int rows) {
+  int shape = -1;
+  for (int k = 0; k < kRingShapes; k++)
+    if (rows == ring_rows(k)) shape = k;
+  if (rows == 0) shape = 0;
+  if (!c || !c->ok || shape < 0) {
+    set_error("flow_set_sweep_ring: null context or rows not 0, 16, 32 or 64");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->ring = shape;
+  if (c->precision == 3) {
+    if (!c->ring_ok[shape]) {
+      c->ring = 0;
+      set_error("flow_set_sweep_ring: a chunk has more sub-levels of that size than the kernel holds");
+      return FLOW_ERR_ARG;
+    }
+    drop_graphs(c);
+    apply_ring(c);
+  }
   return 0;
 }
 

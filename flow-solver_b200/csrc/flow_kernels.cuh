@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
   #pragma unroll 4
   for (int k = s0; k < s1; k++) {
-    const double4 g = m.nsub_geo[k];  // the incident subedge's normal and length
+    const double4 g = m.sub_geo[m.nsub[k] >> 1];
     const double theta = uu * g.x + vv * g.y;
     const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
     const double w = tpc >= tmc ? tpc : tmc;
@@ -155,13 +155,14 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
   #pragma unroll 4
   for (int k = e0; k < e1; k++) {
-    const int other = m.nedg_other[k];  // the edge's other end
+    const int ed = m.nedg[k];
+    const int e = ed >> 1, side = ed & 1;
+    const int2 lr = m.edge_lr[e];
+    const int other = side ? lr.x : lr.y;
     const double qo = s.nQ[4 * (long)other + v];
     qmin = qmin <= qo ? qmin : qo;
     qmax = qmax >= qo ? qmax : qo;
     if (ORDER == 1 && a.do_grad) {
-      const int ed = m.nedg[k];
-      const int e = ed >> 1, side = ed & 1;
       const double4 w = m.edge_w[e];
       const double dq = side ? (q0v - qo) : (qo - q0v);  // nQ[R] - nQ[L]
       if (side == 0) {
@@ -214,19 +215,21 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   if (!a.do_lim) return;
   // ---- Venkatakrishnan bound of variable v over every face point ----
   double ph = 1.0;
+  const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
   #pragma unroll 4
   for (int k = s0; k < s1; k++) {
+    const int sd = m.nsub[k];
+    const int sub = sd >> 1, side = sd & 1;
     if (ORDER == 1) {
-      const double2 d = m.nsub_fdx[k];  // face point - x[n]
-      const double dx0 = d.x, dx1 = d.y;
+      const double4 d = m.sub_dx[sub];
+      const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
       const double qr = q0v + (g0 * dx0 + g1 * dx1);
       ph = venkat_fold(ph, qr, q0v, qmin, qmax);
     } else {
-      const double2* gd = m.nsub_gdx + 3 * (long)k;  // Gauss points - x[n]
+      const double* xg = m.sub_xg + 6 * (long)sub;
 #pragma unroll
       for (int gpt = 0; gpt < 3; gpt++) {
-        const double2 d = gd[gpt];
-        const double dx0 = d.x, dx1 = d.y;
+        const double dx0 = xg[2 * gpt] - xn0, dx1 = xg[2 * gpt + 1] - xn1;
         double qr = pv;
         qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
                h[4] * dx0 * dx1);
@@ -948,14 +951,19 @@ __global__ void k_prepare_sweep32(DevState s, const float* cur, float* next, int
 // chunk, 64 rows (one per quad of 4 lanes, lane r owning block row r) per
 // pass.  The CTA first copies its window of the FP32 iterate (every row its
 // chunk touches) into shared memory, then walks the chunk's sub-levels in
-// order: the records of sub-level u+2 are copied into a 3-slot ring with
+// order: the records of sub-level u+S-1 are copied into an S-slot ring with
 // cp.async while sub-level u is computed, so the dependency chain only ever
-// reads shared memory.  Rows of one sub-level are independent; a barrier
+// reads shared memory.  The ring holds kRingRecords records in one of three
+// shapes (ROWS rows a sub-level x S slots: 64 x 3, 32 x 6, 16 x 12): smaller
+// sub-levels prefetch further ahead for the same shared memory, at the
+// price of more barriers on levels wider than ROWS rows.  Rows of one sub-level are independent; a barrier
 // separates sub-levels.  Rows of other chunks in the window are not written
 // by any CTA of this launch (chunks of one colour share no block).  Per row
 // the arithmetic is that of k_sweep_color32.
-constexpr int kRecRows = 64;
-constexpr int kRecSlots = 3;
+constexpr int kRecRows = 64;        // rows of a sub-level in the largest ring shape
+constexpr int kRingRecords = 192;   // records the ring holds, whatever its shape
+constexpr int kRingShapes = 3;      // sub-levels of 64, 32 or 16 rows
+__host__ __device__ constexpr int ring_rows(int shape) { return 64 >> shape; }
 constexpr int kRecInts = (int)(sizeof(SweepRec) / 16);  // 16-byte words per record
 // records sit 704 bytes apart in shared memory (640 + 64 of padding), so the
 // two quads of a half-warp read disjoint bank ranges
@@ -1010,13 +1018,16 @@ __global__ void k_fill_sweep_records(SweepRec* __restrict__ rec, const int* __re
   reinterpret_cast<int4*>(rec)[w] = v;
 }
 
-template <int DIR>
+template <int DIR, int ROWS>
 __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct, float* dq32,
                                                      int colour, int last) {
+  constexpr int SLOTS = kRingRecords / ROWS;
+  static_assert(SLOTS * ROWS == kRingRecords && SLOTS >= 3 && 4 * ROWS <= 256,
+                "ring shape");
   if (*s.stop) return;  // the run has converged
   extern __shared__ __align__(16) unsigned char sweep_smem[];
   int4* slots = reinterpret_cast<int4*>(sweep_smem);
-  float4* win = reinterpret_cast<float4*>(sweep_smem + 16 * kRecStride * kRecSlots * kRecRows);
+  float4* win = reinterpret_cast<float4*>(sweep_smem + 16 * kRecStride * kRingRecords);
   const int tid = threadIdx.x;
   const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
   const int2 w = ct.window[q];
@@ -1036,7 +1047,7 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
     if (u < nsub) {
       const int r0 = ss[u], words = (ss[u + 1] - r0) * kRecInts;
       const int4* src = recs + (long)r0 * kRecInts;
-      int4* dst = slots + (u % kRecSlots) * kRecRows * kRecStride;
+      int4* dst = slots + (u % SLOTS) * ROWS * kRecStride;
       for (int i = tid; i < words; i += blockDim.x) {
         const int rr = i / kRecInts, ww = i - rr * kRecInts;
         cp_async16(dst + rr * kRecStride + ww, src + i);
@@ -1044,18 +1055,17 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
     }
     cp_async_commit();  // one group per sub-level, empty past the end
   };
-  issue(0);
-  issue(1);
+  for (int k = 0; k < SLOTS - 1; k++) issue(k);
   const int quad = tid >> 2, r = tid & 3;
   const int qbase = tid & 31 & ~3;
   const unsigned qmask = 0xFu << qbase;
-  cp_async_wait<1>();  // the window and sub-level 0 have landed
+  cp_async_wait<SLOTS - 2>();  // the window and sub-level 0 have landed
   __syncthreads();
   for (int u = 0; u < nsub; u++) {
-    issue(u + 2);
+    issue(u + SLOTS - 1);  // into the slot sub-level u-1 left
     if (quad < ss[u + 1] - ss[u]) {
       const SweepRec& R = *reinterpret_cast<const SweepRec*>(
-          slots + ((u % kRecSlots) * kRecRows + quad) * kRecStride);
+          slots + ((u % SLOTS) * ROWS + quad) * kRecStride);
       const int j = R.hdr.x, nb = R.hdr.y;
       const int* cols = reinterpret_cast<const int*>(R.cols);
       float acc = reinterpret_cast<const float*>(&R.rhs)[r];
@@ -1093,9 +1103,9 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
       }
     }
     // one barrier per sub-level: this level's results are visible to the
-    // next, and the next level's records (all but the newest copy group)
-    // have landed
-    cp_async_wait<1>();
+    // next, and the next level's records (all but the newest SLOTS-2 copy
+    // groups) have landed
+    cp_async_wait<SLOTS - 2>();
     __syncthreads();
   }
   cp_async_wait<0>();

@@ -25,16 +25,6 @@ struct DevMesh {
   // node -> incident subedges, (s << 1) | side, side 0 = node is the edge's L
   const int* nsub_ptr;
   const int* nsub;
-  // per incidence entry k of nsub (node-major copies of static face data,
-  // so a node reads its faces contiguously): the subedge's normal and
-  // length, the face point's offset from the node (k=1), and the three Gauss
-  // points' offsets from the node (k=2), each offset formed as the kernels
-  // formed them (point - x[node])
-  const double4* nsub_geo;
-  const double2* nsub_fdx;
-  const double2* nsub_gdx;  // 3 per entry
-  // per incidence entry of nedg: the edge's other end
-  const int* nedg_other;
   // node -> incident boundary edges (ascending)
   const int* nbed_ptr;
   const int* nbed;
@@ -114,6 +104,7 @@ struct ChunkTables {
   const int* sub_start[2];   // record index of each sub-level, plus the end
   const int* chunk_sub[2];   // first sub-level of each chunk, plus the end
   const int* pos[2];         // record index of each row (1..nn)
+  int ring;                  // ring shape of the sub-level tables: rows 64 >> ring
 };
 
 struct DevState {

@@ -266,6 +266,13 @@ int flow_set_sweep_schedule(flow_ctx *ctx, int sweeps, int until_step);
 /* Chunk limits of precision mode 3 (0: defaults, rows = twice the matrix
  * bandwidth up to 2048, levels = 32). */
 int flow_set_chunk(flow_ctx *ctx, int rows, int levels);
+/* Ring shape of the mode 3 sweep (no counterpart in the reference): the
+ * records of sub-levels of `rows` rows (64, 32 or 16; 0 = 64) are prefetched
+ * into a shared-memory ring of 3, 6 or 12 slots.  Rows of one dependency
+ * level are independent, so every shape gives the same results; smaller
+ * sub-levels prefetch further ahead.  FLOW_ERR_ARG (shape unchanged) if a
+ * chunk would hold more sub-levels than the sweep kernel does. */
+int flow_set_sweep_ring(flow_ctx *ctx, int rows);
 /* Mode 3 chunks in use: starts[0..nchunks] (first row of each chunk, then
  * nn+1; up to cap entries written), their number and the colour count. */
 int flow_chunk_starts(flow_ctx *ctx, int *starts, int cap, int *nchunks, int *ncolours);

@@ -57,17 +57,20 @@ def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
     gpu.close()
 
 
-@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,rows,levels", [
-    (32, 8, True, 3, 4, 6, 0, 0),
-    (128, 32, True, 3, 4, 4, 0, 0),
-    (64, 16, False, 1, 3, 4, 64, 0),
-    (128, 32, True, 3, 2, 3, 200, 6),
+@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,rows,levels,ring", [
+    (32, 8, True, 3, 4, 6, 0, 0, 0),
+    (128, 32, True, 3, 4, 4, 0, 0, 0),
+    (128, 32, True, 3, 4, 4, 0, 0, 32),
+    (128, 32, True, 3, 4, 4, 0, 0, 16),
+    (64, 16, False, 1, 3, 4, 64, 0, 16),
+    (128, 32, True, 3, 2, 3, 200, 6, 32),
 ])
-def test_chunked_steps_bitwise(nc, nr, curved, order, subits, steps, rows, levels):
+def test_chunked_steps_bitwise(nc, nr, curved, order, subits, steps, rows, levels, ring):
     """mode 3: coloured chunks of the reference order, against the oracle's
-    sweep in the same row permutation."""
+    sweep in the same row permutation, for each ring shape of the sweep."""
     mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits, 3)
     gpu.set_chunk(rows, levels)
+    gpu.set_sweep_ring(ring)
     starts, ncol = gpu.chunk_starts()
     nn = mesh.sizes["nn"]
     perm, ncol2 = chunk_order(og["ia"], og["ja"], starts)
