@@ -42,6 +42,7 @@ from __future__ import annotations
 
 import dataclasses
 import argparse
+import concurrent.futures as cf
 import json
 import os
 import subprocess
@@ -61,6 +62,7 @@ METRIC = "converged solves/s (1e-10 drop) served vs plain FP64 GPU; p50/p99 late
 UNIT = "solves/s"
 REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
 REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
+STAGE_THREADS = max(1, min(8, os.cpu_count() or 1))  # concurrent admissions per batch pass
 CPU_BASELINE_STEPS = 6      # pseudo-time steps timed for cpu_baseline
 
 
@@ -348,13 +350,15 @@ def run_batch(args, bw):
                           stall=bw.stall, priority_policy=bw.priority_policy)
         torch.cuda.synchronize()
         ev[0].record()
-        slots = []
-        for i, pr in enumerate(prep):  # context + mesh arrays + state to the device
-            sl = srv.submit(pr.mesh, pr.params, pr.Q0, precision=bw.precision, drop=bw.drop,
-                            max_steps=bw.max_steps, tag=i, hold=True)
-            if sl is None:
-                raise RuntimeError("the device arena cannot hold the whole batch")
-            slots.append(sl)
+        # context + mesh arrays + state to the device, several requests at a
+        # time (the server stages concurrently from host threads)
+        with cf.ThreadPoolExecutor(max_workers=STAGE_THREADS) as ex:
+            futs = [ex.submit(srv.submit, pr.mesh, pr.params, pr.Q0, precision=bw.precision,
+                              drop=bw.drop, max_steps=bw.max_steps, tag=i, hold=True)
+                    for i, pr in enumerate(prep)]
+            slots = [f.result() for f in futs]
+        if any(sl is None for sl in slots):
+            raise RuntimeError("the device arena cannot hold the whole batch")
         torch.cuda.synchronize()
         ev[1].record()
         for sl in slots:

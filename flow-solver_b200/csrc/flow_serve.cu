@@ -38,6 +38,9 @@ thread_local std::string g_serve_error;
 // mesh, so a choice measured once holds for every later admission.
 std::mutex g_tuned_mutex;
 std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;
+// one tuning run at a time, so that concurrent admissions do not time their
+// variants against each other's kernels
+std::mutex g_tuning_run_mutex;
 
 struct Slot {
   flow_ctx* ctx = nullptr;
@@ -45,7 +48,8 @@ struct Slot {
   double drop = 0.;
   int max_steps = 0;
   long long tag = 0;
-  int state = 0;       // 0 free, 1 running, 2 finished (result not yet released), 3 staged
+  int state = 0;       // 0 free, 1 running, 2 finished (result not yet released), 3 staged,
+                       // 4 reserved by a stage call still building its context
   int issued = 0;      // steps enqueued so far
   int inflight = 0;    // chunks whose flags have not been read (0..2)
   int next_flag = 0;   // flag slot of the next chunk
@@ -69,6 +73,10 @@ struct flow_server {
   int sched_sweeps = 0, sched_until = 0;  // sweep schedule of precision-form solves
   long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
   int priority_policy = 0;                // 1: larger meshes get greater stream priority
+  // guards the slot table and the counters: stage may run on several host
+  // threads at once (each builds its context outside the lock) beside
+  // progress / start / result / release
+  std::mutex mu;
 };
 
 namespace {
@@ -138,27 +146,42 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     return FLOW_ERR_ARG;
   }
   int idx = -1;
-  for (int i = 0; i < (int)sv->slots.size(); i++)
-    if (sv->slots[i].state == 0) { idx = i; break; }
-  if (idx < 0) {
-    g_serve_error = "flow_server_submit: every slot is busy";
-    return FLOW_ERR_BUDGET;
+  int autotune_steps = 0, sched_sweeps = 0, sched_until = 0, priority_policy = 0;
+  long sched_min_nodes = 0;
+  {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    for (int i = 0; i < (int)sv->slots.size(); i++)
+      if (sv->slots[i].state == 0) { idx = i; break; }
+    if (idx < 0) {
+      g_serve_error = "flow_server_submit: every slot is busy";
+      return FLOW_ERR_BUDGET;
+    }
+    sv->slots[idx].state = 4;  // reserved: the context is built outside the lock
+    autotune_steps = sv->autotune_steps;
+    sched_sweeps = sv->sched_sweeps;
+    sched_until = sv->sched_until;
+    sched_min_nodes = sv->sched_min_nodes;
+    priority_policy = sv->priority_policy;
   }
+  auto unreserve = [&]() {
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->slots[idx] = Slot();
+  };
   int st = 0;
   flow_ctx* c = flow_create_in(sv->arena, g, p, &st);
   if (!c) {
     // a failed carve from the arena is a budget refusal, not an error
     g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
+    unreserve();
     return st == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : (st ? st : FLOW_ERR_ARG);
   }
   int rc = flow_set_precision(c, precision);
   // mode 3 needs its chunk windows in shared memory; a mesh whose matrix
   // bandwidth is too large for that is served in mode 1 instead
   if (rc == FLOW_ERR_ARG && precision == 3) rc = flow_set_precision(c, 1);
-  if (!rc && precision != 0 && sv->sched_sweeps > 0 &&
-      flow_size(c, "dt") - 1 >= sv->sched_min_nodes)
-    rc = flow_set_sweep_schedule(c, sv->sched_sweeps, sv->sched_until);
-  if (!rc && sv->priority_policy == 1) {
+  if (!rc && precision != 0 && sched_sweeps > 0 && flow_size(c, "dt") - 1 >= sched_min_nodes)
+    rc = flow_set_sweep_schedule(c, sched_sweeps, sched_until);
+  if (!rc && priority_policy == 1) {
     // greatest priority from 256k nodes, one step down per halving of the mesh
     const long nn = flow_size(c, "dt") - 1;
     int steps_down = 0;
@@ -168,22 +191,27 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     rc = flow_set_stream_priority(c, std::min(lo, hi + steps_down));
   }
   if (!rc) rc = flow_set_state(c, Q0);
-  if (!rc && sv->autotune_steps > 0) {
+  if (!rc && autotune_steps > 0) {
     // kernel variants: measured once per (device, order, precision, size bucket)
     const long nn = flow_size(c, "dt") - 1;
     const int bucket = (int)std::floor(2.0 * std::log2((double)std::max(nn, 1L)));
     const auto key = std::make_tuple(flow::internal::device_of(c), p->order, precision, bucket);
-    std::pair<int, int> found(-1, -1);
-    {
+    auto lookup = [&]() {
       std::lock_guard<std::mutex> lock(g_tuned_mutex);
       auto it = g_tuned.find(key);
-      if (it != g_tuned.end()) found = it->second;
+      return it != g_tuned.end() ? it->second : std::make_pair(-1, -1);
+    };
+    std::pair<int, int> found = lookup();
+    std::unique_lock<std::mutex> run_lock(g_tuning_run_mutex, std::defer_lock);
+    if (found.first < 0) {
+      run_lock.lock();
+      found = lookup();  // another admission may have tuned this bucket meanwhile
     }
     if (found.first >= 0) {
       rc = flow_set_variants(c, found.first, found.second);
     } else {
       int v[2] = {0, 0};
-      const int trc = flow_autotune(c, p, 1, sv->autotune_steps, v, nullptr);
+      const int trc = flow_autotune(c, p, 1, autotune_steps, v, nullptr);
       if (trc & FLOW_ERR_CUDA) {
         rc = trc;  // other bits: the tuning steps' physics, not fatal
       } else {
@@ -195,8 +223,10 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   if (rc) {
     g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
     flow_destroy(c);
+    unreserve();
     return rc == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : rc;
   }
+  std::lock_guard<std::mutex> lock(sv->mu);
   Slot& sl = sv->slots[idx];
   sl = Slot();
   sl.ctx = c;
@@ -238,6 +268,7 @@ static int start_slot(flow_server* sv, int idx) {
 
 int flow_server_start(flow_server* sv, int slot) {
   if (!sv || slot < 0 || slot >= (int)sv->slots.size()) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   return start_slot(sv, slot);
 }
 
@@ -248,6 +279,7 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
   const auto t0 = std::chrono::steady_clock::now();
   for (;;) {
     bool any = false;
+    std::unique_lock<std::mutex> lock(sv->mu);
     for (int i = 0; i < (int)sv->slots.size() && n < max_out; i++) {
       Slot& sl = sv->slots[i];
       if (sl.state != 1) continue;
@@ -304,7 +336,9 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
         }
       }
     }
-    if (n > 0 || wait_us <= 0 || sv->running == 0) break;
+    const int running = sv->running;
+    lock.unlock();
+    if (n > 0 || wait_us <= 0 || running == 0) break;
     const auto dt = std::chrono::duration_cast<std::chrono::microseconds>(
                         std::chrono::steady_clock::now() - t0)
                         .count();
@@ -317,6 +351,7 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
 
 int flow_server_result(flow_server* sv, int slot, double* Q, long nQ, double* forces) {
   if (!sv || slot < 0 || slot >= (int)sv->slots.size()) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   Slot& sl = sv->slots[slot];
   if (sl.state != 2 || !sl.ctx) {
     g_serve_error = "flow_server_result: slot has no finished solve";
@@ -330,9 +365,10 @@ int flow_server_result(flow_server* sv, int slot, double* Q, long nQ, double* fo
 
 int flow_server_release(flow_server* sv, int slot) {
   if (!sv || slot < 0 || slot >= (int)sv->slots.size()) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   Slot& sl = sv->slots[slot];
-  if (sl.state == 1) {
-    g_serve_error = "flow_server_release: the solve is still running";
+  if (sl.state == 1 || sl.state == 4) {
+    g_serve_error = "flow_server_release: the solve is still running or being staged";
     return FLOW_ERR_ARG;
   }
   if (sl.ctx) flow_destroy(sl.ctx);
@@ -340,11 +376,16 @@ int flow_server_release(flow_server* sv, int slot) {
   return 0;
 }
 
-int flow_server_running(flow_server* sv) { return sv ? sv->running : -1; }
+int flow_server_running(flow_server* sv) {
+  if (!sv) return -1;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  return sv->running;
+}
 
 int flow_server_set_sweep_schedule(flow_server* sv, int sweeps, int until_step,
                                    long long min_nodes) {
   if (!sv || sweeps < 0 || until_step < 0 || min_nodes < 0) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   sv->sched_sweeps = sweeps;
   sv->sched_until = until_step;
   sv->sched_min_nodes = (long)min_nodes;
@@ -353,18 +394,21 @@ int flow_server_set_sweep_schedule(flow_server* sv, int sweeps, int until_step,
 
 int flow_server_set_priority_policy(flow_server* sv, int policy) {
   if (!sv || policy < 0 || policy > 1) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   sv->priority_policy = policy;
   return 0;
 }
 
 int flow_server_set_stall(flow_server* sv, int steps) {
   if (!sv || steps < 0) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   sv->stall_steps = steps;
   return 0;
 }
 
 int flow_server_set_autotune(flow_server* sv, int steps) {
   if (!sv || steps < 0) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
   sv->autotune_steps = steps;
   return 0;
 }

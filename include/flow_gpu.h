@@ -365,8 +365,12 @@ long long flow_ctx_device_bytes(flow_ctx *ctx);
  * and retires solves whose ||R_rho|| dropped by `drop` (status 0), that hit
  * max_steps (FLOW_ERR_NOT_CONVERGED) or failed.  Solves of any mesh, order,
  * flow condition and precision (flow_set_precision modes) share the GPU; each
- * one's iterates are those it has when run alone.  Single-threaded: call a
- * server from one host thread. */
+ * one's iterates are those it has when run alone.  Threads: flow_server_submit
+ * and flow_server_stage may be called from several host threads at once
+ * (each builds its context concurrently, then takes the server's lock to
+ * record it) beside one thread that drives progress / start / result /
+ * release; every call but flow_server_destroy is safe against the others,
+ * and flow_server_destroy comes after all of them have returned. */
 typedef struct flow_server flow_server;
 typedef struct {
   long long tag;     /* the submitter's tag */

@@ -142,3 +142,55 @@ def test_staged_meshes_of_different_sizes_all_start():
         srv.release(c["slot"])
     srv.close()
     arena.close()
+
+
+def test_concurrent_staging_from_threads_matches_solves_run_alone():
+    """Requests staged from several host threads at once (autotuning at
+    admission included), started while the other threads still stage, give
+    the results each solve gives alone; a bucket is tuned once."""
+    import concurrent.futures as cf
+    from flowgpu import capi
+    cases = [(_case(nc, nr, cv, o, m, a, sub), prec)
+             for (nc, nr, cv, o, m, a, prec, sub) in MIX] + \
+            [(_case(64, 16, True, 3, 0.7, 0.5, 4), 3), (_case(48, 12, False, 1, 0.6, 2.0, 3), 3)]
+    alone = []
+    for (wl, mesh), prec in cases:
+        fp = wl.params()
+        s = capi.Solver.from_mesh(mesh, fp, device=0)
+        s.set_precision(prec)
+        s.set_state(mesh.initial_state(fp))
+        steps, r0, r1 = s.converge(1, wl.max_steps, 1e-10, chunk=32, check=False)
+        alone.append((steps, s.get("Q"), s.body_forces()))
+        s.close()
+    arena = capi.Arena(2 << 30)
+    srv = capi.Server(arena, chunk=16, max_slots=len(cases), autotune=2)
+
+    def stage(i):
+        (wl, mesh), prec = cases[i]
+        fp = wl.params()
+        slot = srv.submit(mesh, fp, mesh.initial_state(fp), precision=prec, drop=1e-10,
+                          max_steps=wl.max_steps, tag=i)
+        assert slot is not None
+        return slot
+
+    got = {}
+    with cf.ThreadPoolExecutor(max_workers=4) as ex:
+        futs = [ex.submit(stage, i) for i in range(len(cases))]
+        while len(got) < len(cases):
+            done = srv.progress(wait_us=2000)
+            for c in done:
+                q, f = srv.result(c["slot"])
+                got[c["tag"]] = (c, q, f)
+                srv.release(c["slot"])
+            if not done and all(f.done() for f in futs) and srv.running() == 0 \
+                    and len(got) < len(cases):
+                break  # a stage call failed: its future raises below
+        for f in futs:
+            f.result()
+    for i, (steps, q, f) in enumerate(alone):
+        c, q2, f2 = got[i]
+        assert c["steps"] == steps, (i, c["steps"], steps)
+        assert np.array_equal(q[4:], q2[4:]), i
+        assert f == f2, i
+    srv.close()
+    arena.close()
