@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import math
+import threading
 import time
 from dataclasses import dataclass, replace
 
@@ -146,45 +147,56 @@ def run_poisson(reqs, rate_per_s: float, arena: capi.Arena, subits: int, max_ste
                 seed: int = 0, prep_threads: int = 8, autotune: int = 0,
                 stall: int = 0, ramp_sweeps: int = 0) -> dict:
     """Open-loop Poisson arrivals at `rate_per_s`: each request is prepared
-    on arrival (thread pool), admitted when prepared and when the arena has
-    room, and retired at its drop; latency = retirement - arrival."""
+    on arrival by a worker thread, which then admits it (stages its context
+    on the device and starts it) as soon as the arena has room; the main
+    thread only keeps the running solves' chunks in flight and retires them.
+    Latency = retirement - arrival."""
     rng = np.random.Generator(np.random.PCG64([seed, 7]))
     gaps = rng.exponential(1.0 / rate_per_s, size=len(reqs))
     arrivals = np.cumsum(gaps) - gaps[0]
     capi.load()
     srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall,
                       ramp_sweeps=ramp_sweeps)
-    ex = cf.ThreadPoolExecutor(max_workers=prep_threads)
+    recs = [dict() for _ in reqs]
+    lock = threading.Lock()
+    room = threading.Condition(lock)  # signalled whenever a solve is released
     t0 = time.perf_counter()
-    futures, ready, recs = {}, [], [dict() for _ in reqs]
+
+    def admit(i):
+        pr = prepare(reqs[i], subits, max_steps, drop)
+        while True:
+            slot = srv.submit(pr.mesh, pr.params, pr.Q0, precision=precision, drop=drop,
+                              max_steps=max_steps, tag=i)
+            if slot is not None:
+                break
+            with room:  # the arena or the slot table is full: wait for a release
+                room.wait(timeout=0.05)
+        with lock:
+            recs[i].update(admitted_s=time.perf_counter() - t0 - arrivals[i], prep_s=pr.prep_s,
+                           nodes=reqs[i].nodes, order=reqs[i].order)
+
+    ex = cf.ThreadPoolExecutor(max_workers=prep_threads)
+    futures = []
     nxt = done = 0
     while done < len(reqs):
         now = time.perf_counter() - t0
         while nxt < len(reqs) and arrivals[nxt] <= now:
-            futures[nxt] = ex.submit(prepare, reqs[nxt], subits, max_steps, drop)
+            futures.append(ex.submit(admit, nxt))
             nxt += 1
-        for i in [i for i, f in futures.items() if f.done()]:
-            ready.append((i, futures.pop(i).result()))
-        ready.sort(key=lambda t: t[0])
-        while ready:  # admission in arrival order, as the arena allows
-            i, pr = ready[0]
-            slot = srv.submit(pr.mesh, pr.params, pr.Q0, precision=precision, drop=drop,
-                              max_steps=max_steps, tag=i)
-            if slot is None:
-                break
-            ready.pop(0)
-            recs[i].update(admitted_s=time.perf_counter() - t0 - arrivals[i], prep_s=pr.prep_s,
-                           nodes=reqs[i].nodes, order=reqs[i].order, mesh_ref=pr)
         for c in srv.progress(wait_us=500 if srv.running() else 0):
             i = c["tag"]
             f = None
             if c["status"] in (0, capi.ERR_NOT_CONVERGED, capi.ERR_STALLED):
                 _, f = srv.result(c["slot"], want_q=False)
             srv.release(c["slot"])
-            recs[i].update(c, forces=f, latency_s=time.perf_counter() - t0 - arrivals[i])
-            recs[i].pop("mesh_ref", None)
+            with room:
+                recs[i].update(c, forces=f, latency_s=time.perf_counter() - t0 - arrivals[i])
+                room.notify_all()
             done += 1
-        if not srv.running() and not ready:
+        for fut in futures:
+            if fut.done() and fut.exception() is not None:
+                raise fut.exception()  # a request could not be prepared or admitted
+        if not srv.running():
             time.sleep(0.001)
     ex.shutdown()
     span = time.perf_counter() - t0

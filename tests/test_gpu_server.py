@@ -194,3 +194,21 @@ def test_concurrent_staging_from_threads_matches_solves_run_alone():
         assert f == f2, i
     srv.close()
     arena.close()
+
+
+def test_poisson_stream_admits_from_worker_threads_and_retires_every_request():
+    """The serving driver: requests prepared and admitted by worker threads
+    while the main thread keeps the running solves going; every request is
+    retired once, with its arrival-to-retirement latency."""
+    from flowgpu import capi, serve
+    reqs = [serve.sample_request(i, seed=5, n_min=2000, n_max=6000) for i in range(4)]
+    arena = capi.Arena(1 << 30)
+    r = serve.run_poisson(reqs, 50.0, arena, subits=4, max_steps=120, drop=1e-8, precision=3,
+                          chunk=16, max_slots=4, seed=5, prep_threads=3, autotune=2, stall=0)
+    arena.close()
+    assert len(r["records"]) == 4
+    for x in r["records"]:
+        # converged, at max_steps, or retired on a non-physical state
+        assert isinstance(x["status"], int) and 0 < x["steps"] <= 120
+        assert x["latency_s"] > 0. and x["admitted_s"] >= 0.
+        assert x["latency_s"] <= r["span_s"] + 1e-6
