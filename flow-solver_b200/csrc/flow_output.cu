@@ -84,6 +84,11 @@ int cuda_fail(const char* what, cudaError_t e) {
 int boundary_nodes(int nb, const int* nbs, const int* seg, int b, int nn,
                    std::vector<char>& seen, std::vector<int>& out) {
   long first = 0;
+  for (int k = 1; k <= nb; k++)
+    if (nbs[k] < 0) {
+      set_last_error("surface Cp: a boundary has a negative segment count");
+      return FLOW_ERR_ARG;
+    }
   for (int k = 1; k < b; k++) first += nbs[k];
   for (int s = 0; s < nbs[b]; s++)
     for (int h = 0; h < 2; h++) {
@@ -100,7 +105,8 @@ int boundary_nodes(int nb, const int* nbs, const int* seg, int b, int nn,
   return 0;
 }
 
-// Cp of the listed nodes, computed on the context's device and stream.
+// Cp of the listed nodes, computed on the context's device and stream (a
+// stream-ordered temporary of 12 bytes a node holds the list and the result).
 int device_cp(flow_ctx* c, const flow_params* p, const std::vector<int>& nodes,
               std::vector<double>& cp) {
   const double* Q = nullptr;

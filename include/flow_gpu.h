@@ -193,7 +193,9 @@ int flow_body_forces(flow_ctx *ctx, const flow_params *p, double *forces);
  * GRID::bbc and GRID::nbs (nb+1 ints, index 0 unused) and seg is every
  * boundary's GRID::bs[b][s][0..1] pairs in order, boundary 1 first.  Where
  * the reference prints a message and exits (a file it cannot open) these
- * return FLOW_ERR_ARG with the message in flow_last_error(). */
+ * return FLOW_ERR_ARG with the message in flow_last_error().  They work on
+ * the context's stream and take a small stream-ordered device temporary
+ * (cudaMallocAsync: 12 bytes a wall node, 32 bytes a node for Tecplot). */
 
 /* Pressure coefficient of write_surface_cp (grid_io.C:841-1375, its active
  * branch grid_io.C:1292-1354) on boundary b: the boundary's segment nodes in
