@@ -1036,6 +1036,19 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);
 
+  if (arena) {
+    // the state buffers alone (a lower bound of what the context carves):
+    // an arena without that much room refuses now, before the host work
+    const size_t nq = (size_t)(nn + ng + 1), n1 = (size_t)(nn + 1);
+    const size_t need = 8 * (12 * nq + n1 * (4 * 4 + 8 + 8 + 20 + 4 + 1 + 16)) +
+                        8 * (16 * (size_t)c->nnz + 36 * (size_t)(ns + 1));
+    size_t room;
+    {
+      std::lock_guard<std::mutex> lock(arena->mu);
+      room = arena->size - arena->used;
+    }
+    if (room < need) return fail(c, FLOW_ERR_CUDA, "the arena has no room for this mesh");
+  }
   // ---- host-side re-layout ----
   std::vector<std::pair<int, int>> items;
   Csr nsub, nbed, nedg;

@@ -212,3 +212,24 @@ def test_poisson_stream_admits_from_worker_threads_and_retires_every_request():
         assert isinstance(x["status"], int) and 0 < x["steps"] <= 120
         assert x["latency_s"] > 0. and x["admitted_s"] >= 0.
         assert x["latency_s"] <= r["span_s"] + 1e-6
+
+
+def test_arena_without_room_refuses_before_building_the_context():
+    """An arena with less room than the mesh's state buffers refuses the
+    context at once (a budget refusal, no host re-layout or upload first)."""
+    import ctypes as C
+    from flowgpu import capi
+    (wl, mesh) = _case(64, 16, True, 3, 0.8, 1.25, 4)
+    fp = wl.params()
+    arena = capi.Arena(1 << 20)
+    L = capi.load()
+    st = C.c_int(0)
+    p = capi.params_struct(fp)
+    ctx = L.flow_create_in(arena.h, C.byref(mesh.view), C.byref(p), C.byref(st))
+    assert not ctx and st.value == 2  # FLOW_ERR_CUDA: no device memory for it
+    assert b"no room" in L.flow_last_error()
+    srv = capi.Server(arena, chunk=16, max_slots=2)
+    assert srv.submit(mesh, fp, mesh.initial_state(fp), precision=3, max_steps=8) is None
+    assert srv.running() == 0
+    srv.close()
+    arena.close()
