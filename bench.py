@@ -391,6 +391,7 @@ def run_batch(args, bw):
     barrier(pg)
     dev_ms = e2e_ms = 0.
     lat, launches, n_conv, n_fail, n_stall = [], 0, 0, 0, 0
+    evals, node_evals = 0, 0  # residual(+Jacobian) evaluations: one per served step
     dforce = []
     with ClockSampler(local) as clk:
         for k in range(args.steps):
@@ -404,6 +405,8 @@ def run_batch(args, bw):
             e2e_ms += e_ms
             lat += [r["device_ms"] / 1e3 for r in recs]
             launches += sum(r["launches"] for r in recs)
+            evals += sum(r["steps"] for r in recs)
+            node_evals += sum(r["steps"] * prep[i].req.nodes for i, r in enumerate(recs))
             n_conv += sum(1 for r in recs if r["status"] == 0)
             n_fail += sum(1 for r in recs
                           if r["status"] not in (0, capi.ERR_NOT_CONVERGED, capi.ERR_STALLED))
@@ -412,6 +415,8 @@ def run_batch(args, bw):
     dev_ms_max = allreduce_max(pg, dev_ms)
     e2e_ms_max = allreduce_max(pg, e2e_ms)
     n_conv_all = allreduce_sum(pg, n_conv)
+    evals_all = allreduce_sum(pg, evals)
+    node_evals_all = allreduce_sum(pg, node_evals)
     value = n_conv_all / (dev_ms_max / 1e3)
     e2e = n_conv_all / (e2e_ms_max / 1e3)
 
@@ -511,6 +516,11 @@ def run_batch(args, bw):
             "e2e": {"value": round(e2e, 5), "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "roofline": roof, "roofline_sweep": roof_sweep, "gpu_launches": int(launches),
+            "residual_evaluations": {
+                "per_s": round(evals_all / (dev_ms_max / 1e3), 1),
+                "node_evals_per_s": round(node_evals_all / (dev_ms_max / 1e3)),
+                "what": "one residual + Jacobian evaluation per served pseudo-time step "
+                        "(all requests, device time of the timed passes)"},
             "clocks": clk.summary(), "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

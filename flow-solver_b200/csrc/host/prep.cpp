@@ -12,8 +12,11 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <array>
+#include <atomic>
 #include <string>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -682,6 +685,25 @@ void edge_weights(flow_mesh& m) {
   }
 }
 
+// body(lo, hi) over the nodes [1, n], in contiguous ranges on up to 16 host
+// threads; for work that is independent per node, so the split does not
+// change any result.
+template <class F>
+void for_node_ranges(int n, F&& body) {
+  const int hw = (int)std::thread::hardware_concurrency();
+  const int parts = n < 8192 ? 1 : std::max(1, std::min(hw, 16));
+  if (parts == 1) {
+    body(1, n + 1);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < parts; t++) {
+    const int lo = 1 + (int)((long)n * t / parts), hi = 1 + (int)((long)n * (t + 1) / parts);
+    pool.emplace_back([&body, lo, hi] { body(lo, hi); });
+  }
+  for (auto& th : pool) th.join();
+}
+
 // maps.C:1181-1551 generic layered stencils, grown as solve.C:57-114 does on
 // the first third-order step: one layer for every node, a second for every
 // node of order > 2, then up to three more for nodes with fewer than six
@@ -719,16 +741,21 @@ bool build_stencils(flow_mesh& m) {
     for (size_t l = 1; l < layers[i].size(); l++) n += (int)layers[i][l].size();
     return n;
   };
-  for (int i = 1; i <= nn; i++) layers[i].push_back({i});
-  for (int i = 1; i <= nn; i++) add_layer(i);
-  for (int i = 1; i <= nn; i++)
-    if (m.node_order[i] > 2) add_layer(i);
-  for (int i = 1; i <= nn; i++) {
-    if (m.node_order[i] < 3) continue;
-    int k = 0;
-    for (; nnb(i) < 6 && k < 3; k++) add_layer(i);
-    if (nnb(i) < 6) return false;
-  }
+  // a node's layers depend only on the mesh and its own earlier layers, so
+  // each node runs the three growth passes in turn, nodes in parallel
+  std::atomic<bool> ok(true);
+  for_node_ranges(nn, [&](int lo, int hi) {
+    for (int i = lo; i < hi; i++) {
+      layers[i].push_back({i});
+      add_layer(i);
+      if (m.node_order[i] > 2) add_layer(i);
+      if (m.node_order[i] < 3) continue;
+      int k = 0;
+      for (; nnb(i) < 6 && k < 3; k++) add_layer(i);
+      if (nnb(i) < 6) ok = false;
+    }
+  });
+  if (!ok) return false;
   m.gnsn.clear();
   m.gnnsn.assign(1, 0);
   m.gnnsn1.assign(nn + 2, 0);
@@ -753,10 +780,22 @@ bool factor_stencils(flow_mesh& m) {
   m.svd_U.clear();
   m.svd_VT.assign((size_t)(nn + 1) * 25, 0.);
   m.svd_S.assign((size_t)(nn + 1) * 5, 0.);
-  std::vector<double> A, U;
   const double* x = m.x.data();
   const double* mo = m.moments.data();
+  // U blocks in node order: offsets first, then each node factored on its own
+  long total = 0;
   for (int i = 1; i <= nn; i++) {
+    if (m.node_order[i] < 3) continue;
+    const int mr = m.gnnsn[m.gnnsn1[i + 1]] - m.gnnsn[m.gnnsn1[i] + 1];
+    m.svd_m[i] = mr;
+    m.svd_off[i] = total;
+    total += 5L * mr;
+  }
+  m.svd_U.assign((size_t)total, 0.);
+  std::atomic<bool> ok(true);
+  for_node_ranges(nn, [&](int lo, int hi) {
+  std::vector<double> A;
+  for (int i = lo; i < hi; i++) {
     if (m.node_order[i] < 3) continue;
     int a0 = m.gnnsn[m.gnnsn1[i] + 1], a1 = m.gnnsn[m.gnnsn1[i + 1]];
     int mr = a1 - a0;
@@ -782,15 +821,12 @@ bool factor_stencils(flow_mesh& m) {
                              (x[node * 2 + 1] - x[i * 2 + 1]) * (x[node * 2] - x[i * 2]) -
                              mo[i * 9 + 4]);
     }
-    U.assign((size_t)mr * 5, 0.);
-    if (flow_svd_jacobi(mr, 5, A.data(), &m.svd_S[(size_t)i * 5], U.data(),
+    if (flow_svd_jacobi(mr, 5, A.data(), &m.svd_S[(size_t)i * 5], &m.svd_U[m.svd_off[i]],
                         &m.svd_VT[(size_t)i * 25], 0) != 0)
-      return false;
-    m.svd_m[i] = mr;
-    m.svd_off[i] = (long)m.svd_U.size();
-    m.svd_U.insert(m.svd_U.end(), U.begin(), U.end());
+      ok = false;
   }
-  return true;
+  });
+  return ok;
 }
 
 flow_mesh* finish(flow_mesh* m, int reorder, int order, int* status) {

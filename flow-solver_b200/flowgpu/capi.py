@@ -179,6 +179,9 @@ def _load_locked():
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
     L.flow_prep_read.argtypes = [C.c_char_p, IP, C.c_int, C.c_int, C.c_int, IP]
+    L.flow_prep_build.restype = vp
+    L.flow_prep_build.argtypes = [C.c_int, DP, C.c_int, IP, C.c_int, IP, C.c_int, IP, IP, IP,
+                                  C.c_int, C.c_int, IP]
     L.flow_prep_view.argtypes = [vp, C.POINTER(FlowGridView)]
     L.flow_prep_initial_state.argtypes = [vp, C.POINTER(FlowParamsC), DP]
     L.flow_prep_node_map.restype = IP

@@ -132,17 +132,17 @@ def make_ogrid(nc: int, nr: int, seed: int = 0, curved: bool = False,
     def nid(i, k):
         return k * nc + (i % nc) + 1
 
-    # ---- triangles ----
+    # ---- triangles: two per quad, quads row by row; the seeded diagonal
+    # picks (a,b,c)+(a,c,d) or (a,b,d)+(b,c,d) ----
     diag = rng.integers(0, 2, size=(nr - 1, nc))
-    tris = []
-    for k in range(nr - 1):
-        for i in range(nc):
-            a, b, c, d = nid(i, k), nid(i + 1, k), nid(i + 1, k + 1), nid(i, k + 1)
-            if diag[k, i]:
-                tris.append((a, b, c)); tris.append((a, c, d))
-            else:
-                tris.append((a, b, d)); tris.append((b, c, d))
-    tris = np.array(tris, dtype=np.int64)
+    kk, ii = np.meshgrid(np.arange(nr - 1, dtype=np.int64), np.arange(nc, dtype=np.int64),
+                         indexing="ij")
+    a, b = nid(ii, kk), nid(ii + 1, kk)
+    c, d = nid(ii + 1, kk + 1), nid(ii, kk + 1)
+    on = (diag == 1)[..., None]
+    t1 = np.where(on, np.stack([a, b, c], -1), np.stack([a, b, d], -1))
+    t2 = np.where(on, np.stack([a, c, d], -1), np.stack([b, c, d], -1))
+    tris = np.stack([t1, t2], axis=2).reshape(-1, 3).astype(np.int64)
     p = x[tris - 1]
     area2 = (p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1]) \
         - (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 1, 1] - p[:, 0, 1])
@@ -152,8 +152,9 @@ def make_ogrid(nc: int, nr: int, seed: int = 0, curved: bool = False,
         raise ValueError("degenerate triangle")
 
     # ---- boundaries: far field CCW (domain inside), airfoil CW (domain outside)
-    far = np.array([(nid(i, nr - 1), nid(i + 1, nr - 1)) for i in range(nc)], dtype=np.int64)
-    wall = np.array([(nid(i + 1, 0), nid(i, 0)) for i in range(nc)], dtype=np.int64)
+    ic = np.arange(nc, dtype=np.int64)
+    far = np.stack([nid(ic, nr - 1), nid(ic + 1, nr - 1)], axis=1)
+    wall = np.stack([nid(ic + 1, 0), nid(ic, 0)], axis=1)
     bnds = [(0, far)]
     if curved:
         nh = nc // 2
@@ -168,13 +169,18 @@ def make_ogrid(nc: int, nr: int, seed: int = 0, curved: bool = False,
 
 def _check_segments(g: OGrid):
     """Every boundary segment n0->n1 must be a CCW edge of one triangle."""
-    edges = set()
-    for t in g.tris:
-        edges.add((t[0], t[1])); edges.add((t[1], t[2])); edges.add((t[2], t[0]))
+    t = np.asarray(g.tris, dtype=np.int64)
+    base = np.int64(g.nn + 1)
+    edges = np.sort(np.concatenate([t[:, 0] * base + t[:, 1], t[:, 1] * base + t[:, 2],
+                                    t[:, 2] * base + t[:, 0]]))
     for _, segs in g.boundaries:
-        for n0, n1 in segs:
-            if (n0, n1) not in edges:
-                raise ValueError(f"segment {n0}->{n1} has the domain on its right")
+        sg = np.asarray(segs, dtype=np.int64).reshape(-1, 2)
+        key = sg[:, 0] * base + sg[:, 1]
+        at = np.minimum(np.searchsorted(edges, key), len(edges) - 1)
+        bad = edges[at] != key
+        if bad.any():
+            n0, n1 = sg[np.argmax(bad)]
+            raise ValueError(f"segment {n0}->{n1} has the domain on its right")
 
 
 def write_mesh(path: str, g: OGrid):

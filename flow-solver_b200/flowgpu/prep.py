@@ -37,6 +37,35 @@ class Mesh:
         self.L.flow_prep_view(self.h, C.byref(self.view))
 
     @classmethod
+    def from_grid(cls, g, order: int, reorder: int = 1):
+        """From a generated grid in memory (flowgpu.meshgen.OGrid: x, 1-based
+        triangles, (bc, segments) per boundary) through flow_prep_build: the
+        same arrays flow_prep_read gives for the grid's mesh file, without the
+        file."""
+        self = cls.__new__(cls)
+        self.L = _lib()
+        x = np.ascontiguousarray(g.x, dtype=np.float64)
+        tri = np.ascontiguousarray(g.tris, dtype=np.int32)
+        nbs = np.array([len(segs) for _, segs in g.boundaries], dtype=np.int32)
+        seg = np.ascontiguousarray(np.concatenate([np.asarray(segs, dtype=np.int32).reshape(-1, 2)
+                                                   for _, segs in g.boundaries]))
+        bbc = np.array([bc for bc, _ in g.boundaries], dtype=np.int32)
+        quad = np.zeros(4, dtype=np.int32)
+        st = C.c_int(0)
+        self.h = self.L.flow_prep_build(int(x.shape[0]), x.ctypes.data_as(capi.DP), int(tri.shape[0]),
+                                        tri.ctypes.data_as(capi.IP), 0, quad.ctypes.data_as(capi.IP),
+                                        len(nbs), nbs.ctypes.data_as(capi.IP),
+                                        seg.ctypes.data_as(capi.IP), bbc.ctypes.data_as(capi.IP),
+                                        int(reorder), int(order), C.byref(st))
+        if not self.h:
+            raise capi.FlowError(st.value or 1, "flow_prep_build: " +
+                                 self.L.flow_prep_last_error().decode())
+        self.order = order
+        self.view = capi.FlowGridView()
+        self.L.flow_prep_view(self.h, C.byref(self.view))
+        return self
+
+    @classmethod
     def from_case(cls, casedir: str, order: int, mesh_name: str = "grid.mesh", reorder: int = 1):
         return cls(os.path.join(casedir, mesh_name), read_bc(os.path.join(casedir, "bc.dat")),
                    order, reorder)

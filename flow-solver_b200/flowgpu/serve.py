@@ -7,8 +7,9 @@ meshes), free-stream Mach uniform in [0.3, 0.85], angle of attack uniform in
 [-4, 6] degrees, reconstruction order k=1 (straight walls) or k=2 (curved
 walls), all drawn from one numpy PCG64 seed per request index.
 
-Host preprocessing (mesh generation, flow_prep_read: ordering, stencils, SVD)
-runs in a thread pool (the C library releases the GIL) and overlaps the GPU.
+Host preprocessing (mesh generation, then flow_prep_build on the generated
+arrays: ordering, stencils, SVD) runs in a thread pool (the C library
+releases the GIL) and overlaps the GPU.
 """
 from __future__ import annotations
 
@@ -68,9 +69,11 @@ class Prepared:
 
 
 def prepare(req: Request, subits: int, max_steps: int, drop: float) -> Prepared:
+    """Generate the request's grid and preprocess it in memory (no mesh file:
+    flow_prep_build gives the arrays flow_prep_read would give for it)."""
     t0 = time.perf_counter()
     wl = req.workload(subits, max_steps, drop)
-    mesh = Mesh.from_case(wl.write(), order=wl.order)
+    mesh = Mesh.from_grid(wl.grid(), order=wl.order)
     fp = wl.params()
     return Prepared(req, wl, mesh, fp, mesh.initial_state(fp), time.perf_counter() - t0)
 

@@ -20,6 +20,7 @@ FLOAT_KEYS = ("x", "cv_area", "el_cent", "xn_subedges", "xm_subedges", "xg_subed
 
 @pytest.mark.parametrize("nc,nr,curved,order", [
     (32, 8, False, 1), (64, 16, False, 1), (32, 8, True, 3), (64, 16, True, 3),
+    (128, 64, True, 3),  # 8192 nodes: stencils and SVD factored on host threads
 ])
 def test_prep_matches_reference_setup(ref_lib, nc, nr, curved, order):
     case = ParityCase(nc, nr, curved, order)
@@ -54,3 +55,40 @@ def test_prep_matches_reference_setup(ref_lib, nc, nr, curved, order):
             assert np.array_equal(a, b), i
     Q = mesh.initial_state(case.fp)
     assert np.array_equal(Q[4:], case.Q0[4:])
+
+
+@pytest.mark.parametrize("curved,order", [(False, 1), (True, 3)])
+def test_in_memory_grid_gives_the_arrays_of_its_mesh_file(curved, order, tmp_path):
+    """Mesh.from_grid (flow_prep_build on the generator's arrays) and
+    Mesh.from_case (the written mesh file through flow_prep_read) give the
+    same preprocessed arrays, bit for bit."""
+    from flowgpu import workloads
+    from flowgpu.prep import Mesh
+    wl = workloads.Workload("mem", 64, 16, curved, order, 0.7)
+    a = Mesh.from_case(wl.write(str(tmp_path)), order=order)
+    b = Mesh.from_grid(wl.grid(), order=order)
+    assert a.sizes == b.sizes
+    A, B = a.arrays(), b.arrays()
+    assert A.keys() == B.keys()
+    for k in A:
+        if A[k] is None:
+            assert B[k] is None, k
+        else:
+            assert np.array_equal(A[k], B[k]), k
+    for x, y in zip(a.elements(), b.elements()):
+        assert np.array_equal(x, y)
+    for x, y in zip(a.segments()[1:], b.segments()[1:]):
+        assert np.array_equal(x, y)
+    fp = wl.params()
+    assert np.array_equal(a.initial_state(fp), b.initial_state(fp))
+    a.close()
+    b.close()
+
+
+def test_generator_rejects_a_boundary_segment_with_the_domain_on_its_right():
+    from flowgpu import meshgen
+    g = meshgen.make_ogrid(64, 16, seed=1)
+    bc, segs = g.boundaries[0]
+    g.boundaries[0] = (bc, segs[:, ::-1].copy())
+    with pytest.raises(ValueError, match="domain on its right"):
+        meshgen._check_segments(g)
