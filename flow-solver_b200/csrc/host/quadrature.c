@@ -8,6 +8,7 @@
  * description, not from GSL.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include "quadrature.h"
 
@@ -41,6 +42,17 @@ static void gauss_legendre(int n, double *x, double *w)
     }
 }
 
+/* The two rules are the same on every call: computed once per process
+ * (pthread_once: preprocessing may run on several threads at a time). */
+static double g_xl[GL_LO], g_wl[GL_LO], g_xh[GL_HI], g_wh[GL_HI];
+static pthread_once_t g_rules_once = PTHREAD_ONCE_INIT;
+
+static void init_rules(void)
+{
+    gauss_legendre(GL_LO, g_xl, g_wl);
+    gauss_legendre(GL_HI, g_xh, g_wh);
+}
+
 typedef struct {
     flow_quad_fn f;
     void *params;
@@ -70,9 +82,8 @@ int flow_quad_adaptive(flow_quad_fn f, void *params, double a, double b,
                        double epsabs, double epsrel, int limit,
                        double *result, double *abserr)
 {
-    double xl[GL_LO], wl[GL_LO], xh[GL_HI], wh[GL_HI];
-    gauss_legendre(GL_LO, xl, wl);
-    gauss_legendre(GL_HI, xh, wh);
+    pthread_once(&g_rules_once, init_rules);
+    const double *xl = g_xl, *wl = g_wl, *xh = g_xh, *wh = g_wh;
 
     integrand_t g;
     g.f = f;
