@@ -351,22 +351,31 @@ bool build_boundary_edge_data(flow_mesh& m) {
   }
   // element owning each segment: the first element (triangles first) in
   // which n0 -> n1 are consecutive vertices (geometry.C:732-772)
-  std::unordered_map<long long, int> owner;
-  owner.reserve((size_t)nelem(m) * 4);
-  for (int type = kQuad; type >= kTri; type--) {
+  // Only the segments' keys are looked up: elements are scanned in order
+  // (triangles, then quads, each ascending) and a key keeps its first owner;
+  // edges that do not start at a boundary node cannot be a segment.
+  std::unordered_map<long long, int> owner;  // segment key -> element (0: none yet)
+  owner.reserve((size_t)m.nbe * 2);
+  for (int i = 1; i <= m.nbe; i++) {
+    int b = m.bedges[i * 5 + 3], s = m.bedges[i * 5 + 4];
+    owner.emplace((long long)m.bs[b][s][0] * (m.nn + 1) + m.bs[b][s][1], 0);
+  }
+  for (int type = kTri; type <= kQuad; type++) {
     int nv = nverts(type);
     const int* c = conn(m, type);
-    for (int j = count(m, type); j >= 1; j--)
+    for (int j = 1; j <= count(m, type); j++)
       for (int k = 0; k < nv; k++) {
-        long long key = (long long)c[j * nv + k] * (m.nn + 1) + c[j * nv + (k + 1) % nv];
-        owner[key] = global_id(m, j, type);
+        const int a = c[j * nv + k];
+        if (m.node_state[a] != kBoundary) continue;
+        auto it = owner.find((long long)a * (m.nn + 1) + c[j * nv + (k + 1) % nv]);
+        if (it != owner.end() && it->second == 0) it->second = global_id(m, j, type);
       }
   }
   for (int i = 1; i <= m.nbe; i++) {
     int b = m.bedges[i * 5 + 3], s = m.bedges[i * 5 + 4];
     int n0 = m.bs[b][s][0], n1 = m.bs[b][s][1];
     auto it = owner.find((long long)n0 * (m.nn + 1) + n1);
-    if (it == owner.end()) return false;
+    if (it == owner.end() || it->second == 0) return false;
     m.bedges[i * 5 + 2] = it->second;
     m.bedge_seg[i * 2] = n0;
     m.bedge_seg[i * 2 + 1] = n1;
