@@ -80,9 +80,10 @@ __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
       g[0] = z;
       g[1] = z;
       if (m.order == 3) {
-        double* h = s.hess5 + 20 * i;
+        // 20 doubles a node, 32-byte aligned: five vector stores
+        double4* h = reinterpret_cast<double4*>(s.hess5 + 20 * (long)i);
 #pragma unroll
-        for (int k = 0; k < 20; k++) h[k] = 0.;
+        for (int k = 0; k < 5; k++) h[k] = z;
       }
       if (reset_phi) {
         double4 o = make_double4(1., 1., 1., 1.);

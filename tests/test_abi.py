@@ -36,3 +36,13 @@ def test_null_arguments_are_rejected_without_a_device():
     assert L.flow_solve(None, None, 1, None, None) == 1
     assert L.flow_size(None, b"Q") == -1
     assert b"null" in L.flow_last_error()
+
+
+def test_setters_reject_bad_arguments_without_a_device():
+    from flowgpu import capi
+    L = capi.load()
+    assert L.flow_set_sweep_ring(None, 64) == 1
+    assert b"rows not 0, 16, 32 or 64" in L.flow_last_error()
+    assert L.flow_set_chunk(None, 0, 0) == 1
+    assert L.flow_surface_cp(None, None, 0, None, None, 1, None, None, 0, None) == 1
+    assert L.flow_write_tecplot(None, None, None, 0, None, 0, None, 0, None) == 1
