@@ -612,6 +612,8 @@ def run_profile(args):
     solver.set_precision(args.precision)
     if args.sweep_rows:
         solver.set_sweep_ring(args.sweep_rows)
+    if args.sweep_dataflow:
+        solver.set_sweep_dataflow(True)
     solver.set_state(mesh.initial_state(wl.params()))
     rh, dh = solver.run(1, args.profile_steps)
     out = {"workload": wl.name, "steps": args.profile_steps,
@@ -887,6 +889,8 @@ def main():
                     help="batch workloads: record the FP64 drop-in's step counts per request")
     ap.add_argument("--precision", type=int, default=0,
                     help="with --profile-steps: 0 FP64 drop-in, 1 FP32 multicolour sweeps")
+    ap.add_argument("--sweep-dataflow", action="store_true",
+                    help="with --profile-steps: one launch per mode 3 sweep (dataflow chunks)")
     ap.add_argument("--sweep-rows", type=int, default=0,
                     help="with --profile-steps: sub-level rows of the mode 3 sweep ring (64, 32, 16)")
     ap.add_argument("--subits", type=int, default=0,

@@ -181,6 +181,7 @@ struct flow_ctx {
   const int* ring_chunk_sub[kRingShapes][2] = {};
   bool ring_ok[kRingShapes] = {};
   int ring = 0;  // requested shape: sub-levels of ring_rows(ring) rows
+  int sweep_df = 0;  // 1: one-launch (dataflow) mode 3 sweeps (flow_set_sweep_dataflow)
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
   // CUDA graphs of chunks of K steps with the step index advancing on the
@@ -404,6 +405,18 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
     for (int it = 0; it < p->subits; it++) {
       Timed t(c, 4);
       const int last = it == p->subits - 1, dir = it % 2;
+      if (c->sweep_df && ct.ring == 0) {
+        // the whole sweep in one launch, one CTA per chunk
+        const long max_spin = 1L << 22;
+        if (dir == 0)
+          k_sweep_chunk_df<0><<<ct.nchunks, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, last,
+                                                                   max_spin);
+        else
+          k_sweep_chunk_df<1><<<ct.nchunks, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, last,
+                                                                   max_spin);
+        rc |= launch_check(c);
+        continue;
+      }
       for (int ci = 0; ci < ct.ncol; ci++) {
         const int col = dir == 0 ? ci : ct.ncol - 1 - ci;
         const int nb = c->h_col_ptr[col + 1] - c->h_col_ptr[col];
@@ -864,6 +877,30 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
   ct.col_ptr = upload_vec(c, cptr);
   ct.col_chunks = upload_vec(c, clist);
   ct.window = upload_vec(c, win);
+  {
+    // one-launch sweeps: dispensing order per direction (colours ascending
+    // forward, descending backward), each chunk's colour, the chunks its
+    // window overlaps, and zeroed flags and counters
+    std::vector<int> order_f, order_b, nbr_x(nch), nbr_y(nch);
+    for (int k = 0; k < ncol; k++)
+      for (int t = cptr[k]; t < cptr[k + 1]; t++) order_f.push_back(clist[t]);
+    for (int k = ncol - 1; k >= 0; k--)
+      for (int t = cptr[k]; t < cptr[k + 1]; t++) order_b.push_back(clist[t]);
+    std::vector<int2> nbr(nch);
+    for (int q = 0; q < nch; q++) nbr[q] = make_int2(chunk_of[win[q].x], chunk_of[win[q].y]);
+    ct.task_chunk[0] = upload_vec(c, order_f);
+    ct.task_chunk[1] = upload_vec(c, order_b);
+    ct.colour = upload_vec(c, colour);
+    ct.nbr = upload_vec(c, nbr);
+    ct.done = c->buf.alloc<int>(nch);
+    ct.sync = c->buf.alloc<unsigned>(4);
+    if (!ct.task_chunk[0] || !ct.task_chunk[1] || !ct.colour || !ct.nbr || !ct.done || !ct.sync ||
+        cudaMemset(ct.done, 0, sizeof(int) * nch) != cudaSuccess ||
+        cudaMemset(ct.sync, 0, sizeof(unsigned) * 4) != cudaSuccess) {
+      set_error("precision mode 3: table upload failed");
+      return FLOW_ERR_CUDA;
+    }
+  }
   // per direction: levels, sub-levels, records (static part)
   std::vector<int> levd(nn + 1);
   for (int dir = 0; dir < 2; dir++) {
@@ -949,7 +986,8 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
   // largest window any context may need, not this context's own
   const int smem_cap = 227 * 1024 - kChunkStaticSmem;
   bool attr_ok = true;
-  for (const void* f : {(const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
+  for (const void* f : {(const void*)k_sweep_chunk_df<0>, (const void*)k_sweep_chunk_df<1>,
+                        (const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
                         (const void*)k_sweep_chunk<0, 32>, (const void*)k_sweep_chunk<1, 32>,
                         (const void*)k_sweep_chunk<0, 16>, (const void*)k_sweep_chunk<1, 16>})
     attr_ok = attr_ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1391,6 +1429,18 @@ int flow_set_sweep_ring(flow_ctx* c, int rows) {
     drop_graphs(c);
     apply_ring(c);
   }
+  return 0;
+}
+
+int flow_set_sweep_dataflow(flow_ctx* c, int on) {
+  if (!c || !c->ok) {
+    set_error("flow_set_sweep_dataflow: null context");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  c->sweep_df = on ? 1 : 0;
   return 0;
 }
 

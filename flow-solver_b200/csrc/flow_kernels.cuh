@@ -1019,23 +1019,30 @@ __global__ void k_fill_sweep_records(SweepRec* __restrict__ rec, const int* __re
   reinterpret_cast<int4*>(rec)[w] = v;
 }
 
-template <int DIR, int ROWS>
-__global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct, float* dq32,
-                                                     int colour, int last) {
+// One chunk q of a mode 3 sweep, run by the whole CTA (256 threads).  The
+// colour-synchronous kernel (DF false) queues the chunk's window of the
+// iterate first and its first sub-levels' records after it; the dataflow
+// kernel (DF true) queues the records first, calls wait_deps() (which
+// returns once the chunk's earlier-colour neighbours have finished this
+// sweep, every thread past a barrier) and only then reads the window.
+template <int DIR, int ROWS, bool DF, class Wait>
+__device__ __forceinline__ void sweep_chunk_body(const DevState& s, const ChunkTables& ct,
+                                                 float* dq32, int q, int last, Wait&& wait_deps) {
   constexpr int SLOTS = kRingRecords / ROWS;
   static_assert(SLOTS * ROWS == kRingRecords && SLOTS >= 3 && 4 * ROWS <= 256,
                 "ring shape");
-  if (*s.stop) return;  // the run has converged
   extern __shared__ __align__(16) unsigned char sweep_smem[];
   int4* slots = reinterpret_cast<int4*>(sweep_smem);
   float4* win = reinterpret_cast<float4*>(sweep_smem + 16 * kRecStride * kRingRecords);
   const int tid = threadIdx.x;
-  const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
   const int2 w = ct.window[q];
   const int nwin = w.y - w.x + 1;
   float4* X = reinterpret_cast<float4*>(dq32);
-  for (int i = tid; i < nwin; i += blockDim.x) cp_async16(win + i, X + w.x + i);
-  cp_async_commit();
+  auto load_window = [&]() {
+    for (int i = tid; i < nwin; i += blockDim.x) cp_async16(win + i, X + w.x + i);
+    cp_async_commit();
+  };
+  if (!DF) load_window();
   const int S0 = ct.chunk_sub[DIR][q], nsub = ct.chunk_sub[DIR][q + 1] - S0;
   // the chunk's sub-level starts, read once into shared memory (they sit on
   // the loop's critical path); a chunk has at most kChunkSubMax sub-levels
@@ -1060,7 +1067,13 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
   const int quad = tid >> 2, r = tid & 3;
   const int qbase = tid & 31 & ~3;
   const unsigned qmask = 0xFu << qbase;
-  cp_async_wait<SLOTS - 2>();  // the window and sub-level 0 have landed
+  if (DF) {
+    wait_deps();
+    load_window();
+    cp_async_wait<0>();  // the window and the first sub-levels have landed
+  } else {
+    cp_async_wait<SLOTS - 2>();  // the window and sub-level 0 have landed
+  }
   __syncthreads();
   for (int u = 0; u < nsub; u++) {
     issue(u + SLOTS - 1);  // into the slot sub-level u-1 left
@@ -1110,6 +1123,82 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
     __syncthreads();
   }
   cp_async_wait<0>();
+}
+
+template <int DIR, int ROWS>
+__global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct, float* dq32,
+                                                     int colour, int last) {
+  if (*s.stop) return;  // the run has converged
+  const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
+  sweep_chunk_body<DIR, ROWS, false>(s, ct, dq32, q, last, [] {});
+}
+
+// A whole mode 3 sweep in one launch (one CTA per chunk): CTAs take chunks
+// from a dispenser in the sweep's colour order, and a chunk waits only for
+// the chunks of earlier colours its window overlaps (finished this sweep),
+// not for every chunk of the colour before it.  A chunk reads exactly what
+// it reads in the colour-synchronous sweep: its earlier-colour neighbours
+// after their update, its later-colour neighbours before theirs (they take
+// their chunks later and wait for this one), so the results are the same.
+// A chunk only waits for chunks dispensed before it, held by CTAs that are
+// running or done, so the waits end whatever the residency.  ct.sync: [0]
+// the dispenser, [1] chunks finished, [2] the sweep generation; the last
+// chunk to finish resets [0] and [1] and advances [2], and a finished chunk
+// stores generation + 1 in ct.done.  A wait gives up after max_spin polls,
+// sets FLOW_ERR_SWEEP_TIMEOUT and goes on (the chunk still finishes, so the
+// counters stay consistent).
+template <int DIR>
+__global__ void __launch_bounds__(256) k_sweep_chunk_df(DevState s, ChunkTables ct,
+                                                        float* dq32, int last, long max_spin) {
+  if (*s.stop) return;  // the run has converged (every CTA of the launch sees it)
+  __shared__ int task_q, task_gen;
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(&ct.sync[0], 1u);
+    task_gen = cuda::atomic_ref<unsigned, cuda::thread_scope_device>(ct.sync[2])
+                   .load(cuda::memory_order_relaxed);
+    task_q = t < (unsigned)ct.nchunks ? ct.task_chunk[DIR][t] : -1;
+  }
+  __syncthreads();
+  const int q = task_q;
+  const int gen = task_gen;
+  if (q < 0) {  // more CTAs than chunks: only a broken launch gets here
+    if (threadIdx.x == 0) atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+    return;
+  }
+  auto wait_deps = [&]() {
+    if (threadIdx.x == 0) {
+      const int mine = DIR == 0 ? ct.colour[q] : ct.ncol - 1 - ct.colour[q];
+      const int2 nr = ct.nbr[q];
+      for (int o = nr.x; o <= nr.y; o++) {
+        const int rank = DIR == 0 ? ct.colour[o] : ct.ncol - 1 - ct.colour[o];
+        if (o == q || rank >= mine) continue;
+        cuda::atomic_ref<int, cuda::thread_scope_device> flag(ct.done[o]);
+        long spin = 0;
+        while (flag.load(cuda::memory_order_acquire) != gen + 1) {
+          if (++spin > max_spin) {
+            atomicOr(s.status, ERR_SWEEP_TIMEOUT);
+            break;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  };
+  sweep_chunk_body<DIR, 64, true>(s, ct, dq32, q, last, wait_deps);
+  // publish: every thread's iterate writes before the chunk's flag
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<int, cuda::thread_scope_device>(ct.done[q])
+        .store(gen + 1, cuda::memory_order_release);
+    if (atomicAdd(&ct.sync[1], 1u) == (unsigned)ct.nchunks - 1) {
+      // every chunk of this sweep has finished (and read the generation)
+      atomicExch(&ct.sync[0], 0u);
+      atomicExch(&ct.sync[1], 0u);
+      __threadfence();
+      atomicAdd(&ct.sync[2], 1u);
+    }
+  }
 }
 
 // Before an ordered sweep: fill its result buffer with the not-ready

@@ -105,6 +105,12 @@ struct ChunkTables {
   const int* chunk_sub[2];   // first sub-level of each chunk, plus the end
   const int* pos[2];         // record index of each row (1..nn)
   int ring;                  // ring shape of the sub-level tables: rows 64 >> ring
+  // one-launch (dataflow) sweeps
+  const int* task_chunk[2];  // per direction: chunks in dispensing (colour) order
+  const int* colour;         // colour of each chunk
+  const int2* nbr;           // per chunk: first and last chunk its window overlaps
+  int* done;                 // per chunk: sweep generation + 1 once finished
+  unsigned* sync;            // dispenser, chunks finished, sweep generation
 };
 
 struct DevState {

@@ -33,7 +33,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_surface_cp",
            "flow_write_surface_cp", "flow_write_tecplot", "flow_get", "flow_size",
-           "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_set_sweep_ring", "flow_chunk_starts", "flow_set_graphs",
+           "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_set_sweep_ring", "flow_set_sweep_dataflow", "flow_chunk_starts", "flow_set_graphs",
            "flow_autotune", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
@@ -128,6 +128,7 @@ def _load_locked():
     L.flow_set_graphs.argtypes = [vp, C.c_int]
     L.flow_set_chunk.argtypes = [vp, C.c_int, C.c_int]
     L.flow_set_sweep_ring.argtypes = [vp, C.c_int]
+    L.flow_set_sweep_dataflow.argtypes = [vp, C.c_int]
     L.flow_autotune.argtypes = [vp, PP, C.c_int, C.c_int, IP, DP]
     L.flow_set_variants.argtypes = [vp, C.c_int, C.c_int]
     L.flow_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int]
@@ -535,6 +536,11 @@ class Solver:
     def set_sweep_ring(self, rows: int = 0):
         """Sub-level rows of the mode 3 sweep's prefetch ring (64, 32, 16)."""
         _check(self.L.flow_set_sweep_ring(self.ctx, int(rows)), "flow_set_sweep_ring")
+
+    def set_sweep_dataflow(self, on: bool = True):
+        """One launch per mode 3 sweep, chunks started by their dependencies."""
+        _check(self.L.flow_set_sweep_dataflow(self.ctx, 1 if on else 0),
+               "flow_set_sweep_dataflow")
 
     def chunk_starts(self):
         """(first row of each mode 3 chunk plus nn+1, number of colours)."""

@@ -275,6 +275,13 @@ int flow_set_chunk(flow_ctx *ctx, int rows, int levels);
  * sub-levels prefetch further ahead.  FLOW_ERR_ARG (shape unchanged) if a
  * chunk would hold more sub-levels than the sweep kernel does. */
 int flow_set_sweep_ring(flow_ctx *ctx, int rows);
+/* One-launch mode 3 sweeps (no counterpart in the reference): on != 0 runs
+ * each sweep as one launch in which a chunk starts as soon as the chunks of
+ * earlier colours that its window overlaps have finished, instead of one
+ * launch per colour; the same results (each chunk reads its neighbours at
+ * the same point of the sweep).  Waits are bounded: one that runs out sets
+ * FLOW_ERR_SWEEP_TIMEOUT.  Used with the 64-row ring shape. */
+int flow_set_sweep_dataflow(flow_ctx *ctx, int on);
 /* Mode 3 chunks in use: starts[0..nchunks] (first row of each chunk, then
  * nn+1; up to cap entries written), their number and the colour count. */
 int flow_chunk_starts(flow_ctx *ctx, int *starts, int cap, int *nchunks, int *ncolours);

@@ -57,20 +57,26 @@ def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
     gpu.close()
 
 
-@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,rows,levels,ring", [
-    (32, 8, True, 3, 4, 6, 0, 0, 0),
-    (128, 32, True, 3, 4, 4, 0, 0, 0),
-    (128, 32, True, 3, 4, 4, 0, 0, 32),
-    (128, 32, True, 3, 4, 4, 0, 0, 16),
-    (64, 16, False, 1, 3, 4, 64, 0, 16),
-    (128, 32, True, 3, 2, 3, 200, 6, 32),
+@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,rows,levels,ring,df", [
+    (32, 8, True, 3, 4, 6, 0, 0, 0, 0),
+    (128, 32, True, 3, 4, 4, 0, 0, 0, 0),
+    (128, 32, True, 3, 4, 4, 0, 0, 32, 0),
+    (128, 32, True, 3, 4, 4, 0, 0, 16, 0),
+    (64, 16, False, 1, 3, 4, 64, 0, 16, 0),
+    (128, 32, True, 3, 2, 3, 200, 6, 32, 0),
+    (32, 8, True, 3, 4, 6, 0, 0, 0, 1),
+    (128, 32, True, 3, 4, 4, 0, 0, 0, 1),
+    (64, 16, False, 1, 3, 4, 64, 0, 0, 1),
+    (128, 32, True, 3, 2, 3, 200, 6, 0, 1),
 ])
-def test_chunked_steps_bitwise(nc, nr, curved, order, subits, steps, rows, levels, ring):
+def test_chunked_steps_bitwise(nc, nr, curved, order, subits, steps, rows, levels, ring, df):
     """mode 3: coloured chunks of the reference order, against the oracle's
-    sweep in the same row permutation, for each ring shape of the sweep."""
+    sweep in the same row permutation, for each ring shape of the sweep and
+    with the one-launch (dataflow) sweep."""
     mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits, 3)
     gpu.set_chunk(rows, levels)
     gpu.set_sweep_ring(ring)
+    gpu.set_sweep_dataflow(bool(df))
     starts, ncol = gpu.chunk_starts()
     nn = mesh.sizes["nn"]
     perm, ncol2 = chunk_order(og["ia"], og["ja"], starts)
