@@ -405,19 +405,30 @@ bool fix_subedge_data(flow_mesh& m) {
   for (int b = 1; b <= m.nb; b++)
     if (m.bbc[b] > 10) any = true;
   if (!any) return true;
-  std::unordered_map<long long, int> first_sub;  // unordered node pair -> first subedge
-  for (int j = m.ns; j >= 1; j--) {
+  // unordered node pair of each curved segment -> its first subedge (lowest
+  // index); only edges joining two boundary nodes can be a segment's
+  std::unordered_map<long long, int> first_sub;
+  auto pair_key = [&](int a, int c) {
+    return (long long)std::min(a, c) * (m.nn + 1) + std::max(a, c);
+  };
+  for (int i = 1; i <= m.nbe; i++) {
+    int b = m.bedges[i * 5 + 3], s = m.bedges[i * 5 + 4];
+    if (m.bbc[b] > 10) first_sub.emplace(pair_key(m.bs[b][s][0], m.bs[b][s][1]), 0);
+  }
+  for (int j = 1; j <= m.ns; j++) {
     int e = m.subedges[2 * j];
     int a = m.edges[2 * e], c = m.edges[2 * e + 1];
-    first_sub[(long long)std::min(a, c) * (m.nn + 1) + std::max(a, c)] = j;
+    if (m.node_state[a] != kBoundary || m.node_state[c] != kBoundary) continue;
+    auto it = first_sub.find(pair_key(a, c));
+    if (it != first_sub.end() && it->second == 0) it->second = j;
   }
   for (int i = 1; i <= m.nbe; i++) {
     int ghost = m.bedges[i * 5 + 1], gelem = m.bedges[i * 5 + 2];
     int b = m.bedges[i * 5 + 3], s = m.bedges[i * 5 + 4];
     if (m.bbc[b] <= 10) continue;
     int nL = m.bs[b][s][0], nR = m.bs[b][s][1];
-    auto it = first_sub.find((long long)std::min(nL, nR) * (m.nn + 1) + std::max(nL, nR));
-    if (it == first_sub.end()) return false;
+    auto it = first_sub.find(pair_key(nL, nR));
+    if (it == first_sub.end() || it->second == 0) return false;
     int j = it->second;
     if (m.subedges[2 * j + 1] != gelem) return false;
     double XC0 = m.el_cent[2 * gelem], XC1 = m.el_cent[2 * gelem + 1];
