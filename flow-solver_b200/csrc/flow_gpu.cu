@@ -742,6 +742,33 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
   return 0;
 }
 
+// Kernel attributes belong to the process and device, not to a context: they
+// are set once per device, by the first context that needs them, so that a
+// context built while other solves run never changes a kernel that is in
+// flight.  The shared-memory caps are the largest any context may use.
+bool ensure_kernel_attrs(int device) {
+  static std::mutex mu;
+  static std::vector<char> done;
+  std::lock_guard<std::mutex> lock(mu);
+  if (device < 0) return false;
+  if ((int)done.size() <= device) done.resize(device + 1, 0);
+  if (done[device]) return true;
+  const int chunk_cap = 227 * 1024 - kChunkStaticSmem;
+  const int cta = (int)sizeof(SweepSmem);
+  bool ok = true;
+  for (const void* f : {(const void*)k_sweep_chunk_df<0>, (const void*)k_sweep_chunk_df<1>,
+                        (const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
+                        (const void*)k_sweep_chunk<0, 32>, (const void*)k_sweep_chunk<1, 32>,
+                        (const void*)k_sweep_chunk<0, 16>, (const void*)k_sweep_chunk<1, 16>})
+    ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    chunk_cap) == cudaSuccess;
+  for (const void* f : {(const void*)k_sweep_cta<true>, (const void*)k_sweep_cta<false>})
+    ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, cta) ==
+                   cudaSuccess;
+  if (ok) done[device] = 1;
+  return ok;
+}
+
 // Mode 3 reads none of the mode 1 / 2 tables: only the FP32 iterate.
 int build_chunk_iterate(flow_ctx* c) {
   MixedTables& mt = c->mt;
@@ -982,17 +1009,7 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
     set_error("precision mode 3: table upload failed");
     return FLOW_ERR_CUDA;
   }
-  // the limit is a property of the kernel, shared by every context: allow the
-  // largest window any context may need, not this context's own
-  const int smem_cap = 227 * 1024 - kChunkStaticSmem;
-  bool attr_ok = true;
-  for (const void* f : {(const void*)k_sweep_chunk_df<0>, (const void*)k_sweep_chunk_df<1>,
-                        (const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
-                        (const void*)k_sweep_chunk<0, 32>, (const void*)k_sweep_chunk<1, 32>,
-                        (const void*)k_sweep_chunk<0, 16>, (const void*)k_sweep_chunk<1, 16>})
-    attr_ok = attr_ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              smem_cap) == cudaSuccess;
-  if (!attr_ok) {
+  if (!ensure_kernel_attrs(c->device)) {
     set_error("precision mode 3: cannot reserve shared memory for the sweep");
     return FLOW_ERR_CUDA;
   }
@@ -1266,11 +1283,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
       c->sweep_tb.row_stage = d_row;
       c->sweep_tb.ja_pad = d_ja;
       c->sweep_tb.nstages = (int)rs.size() - 1;
-      const int smem = (int)sizeof(SweepSmem);
-      if (cudaFuncSetAttribute(k_sweep_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               smem) != cudaSuccess ||
-          cudaFuncSetAttribute(k_sweep_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               smem) != cudaSuccess)
+      if (!ensure_kernel_attrs(device))
         return fail(c, FLOW_ERR_CUDA, "cannot reserve shared memory for the sweep");
       c->sweep_cta_ok = true;
     }
