@@ -92,3 +92,29 @@ def test_generator_rejects_a_boundary_segment_with_the_domain_on_its_right():
     g.boundaries[0] = (bc, segs[:, ::-1].copy())
     with pytest.raises(ValueError, match="domain on its right"):
         meshgen._check_segments(g)
+
+
+def test_concurrent_in_memory_preprocessing_is_deterministic():
+    """flow_prep_build called from several Python threads at once (as the
+    serving workers do), each splitting its stencils and SVD over host
+    threads, gives the arrays a one-at-a-time build gives."""
+    import concurrent.futures as cf
+    from flowgpu import workloads
+    from flowgpu.prep import Mesh
+    wls = [workloads.Workload(f"conc{i}", 128, 64 + 8 * i, i % 2 == 0, 3 if i % 2 == 0 else 1,
+                              0.7, seed=20 + i) for i in range(4)]
+    grids = [wl.grid() for wl in wls]
+
+    def build(i):
+        m = Mesh.from_grid(grids[i], order=wls[i].order)
+        out = m.arrays()
+        m.close()
+        return out
+
+    alone = [build(i) for i in range(len(wls))]
+    with cf.ThreadPoolExecutor(max_workers=4) as ex:
+        together = list(ex.map(build, range(len(wls))))
+    for a, b in zip(alone, together):
+        assert a.keys() == b.keys()
+        for k in a:
+            assert (a[k] is None and b[k] is None) or np.array_equal(a[k], b[k]), k
