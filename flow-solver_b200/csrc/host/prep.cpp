@@ -945,7 +945,29 @@ flow_mesh* flow_prep_read(const char* path, const int* bbc, int nb_bc, int reord
   }
   char buf[256];
   auto line = [&]() -> bool { return fgets(buf, sizeof(buf), fp) != nullptr; };
-  auto read_int = [&](int* v) -> bool { return line() && line() && sscanf(buf, "%d", v) == 1; };
+  // n numbers from the line, in order (strtod / strtol: the conversions
+  // scanf's %lf / %d make, without its per-call format parsing)
+  auto doubles = [&](double* out, int n) -> bool {
+    char* p = buf;
+    for (int k = 0; k < n; k++) {
+      char* e = nullptr;
+      out[k] = strtod(p, &e);
+      if (e == p) return false;
+      p = e;
+    }
+    return true;
+  };
+  auto ints = [&](int* out, int n) -> bool {
+    char* p = buf;
+    for (int k = 0; k < n; k++) {
+      char* e = nullptr;
+      out[k] = (int)strtol(p, &e, 10);
+      if (e == p) return false;
+      p = e;
+    }
+    return true;
+  };
+  auto read_int = [&](int* v) -> bool { return line() && line() && ints(v, 1); };
   int nn = 0, nblk = 0, ntri = 0, nquad = 0, nb = 0;
   bool ok = read_int(&nn) && nn > 0;
   std::vector<double> x;
@@ -953,20 +975,19 @@ flow_mesh* flow_prep_read(const char* path, const int* bbc, int nb_bc, int reord
   if (ok) {
     x.resize((size_t)nn * 2);
     for (int i = 0; i < nn && ok; i++)
-      ok = line() && sscanf(buf, "%lf %lf", &x[2 * i], &x[2 * i + 1]) == 2;
+      ok = line() && doubles(&x[2 * i], 2);
   }
   ok = ok && read_int(&nblk) && nblk == 1 && read_int(&ntri) && ntri >= 0;
   if (ok) {
     tri.resize((size_t)ntri * 3);
     for (int t = 0; t < ntri && ok; t++)
-      ok = line() && sscanf(buf, "%d %d %d", &tri[3 * t], &tri[3 * t + 1], &tri[3 * t + 2]) == 3;
+      ok = line() && ints(&tri[3 * t], 3);
   }
   ok = ok && read_int(&nquad) && nquad >= 0;
   if (ok) {
     quad.resize((size_t)nquad * 4);
     for (int t = 0; t < nquad && ok; t++)
-      ok = line() && sscanf(buf, "%d %d %d %d", &quad[4 * t], &quad[4 * t + 1], &quad[4 * t + 2],
-                            &quad[4 * t + 3]) == 4;
+      ok = line() && ints(&quad[4 * t], 4);
   }
   ok = ok && read_int(&nb) && nb >= 1 && nb == nb_bc;
   for (int b = 0; b < nb && ok; b++) {
@@ -974,10 +995,10 @@ flow_mesh* flow_prep_read(const char* path, const int* bbc, int nb_bc, int reord
     ok = read_int(&n) && n >= 1;
     nbs.push_back(n);
     for (int s = 0; s < n && ok; s++) {
-      int a = 0, c = 0;
-      ok = line() && sscanf(buf, "%d %d", &a, &c) == 2;
-      seg.push_back(a);
-      seg.push_back(c);
+      int ac[2] = {0, 0};
+      ok = line() && ints(ac, 2);
+      seg.push_back(ac[0]);
+      seg.push_back(ac[1]);
     }
   }
   fclose(fp);
