@@ -74,3 +74,34 @@ def chunk_order(ia, ja, starts):
     order = [j for c in range(max(colour) + 1) for q in range(len(colour)) if colour[q] == c
              for j in range(starts[q], starts[q + 1])]
     return np.asarray(order, dtype=np.int32), max(colour) + 1
+
+
+def make_quad_case(nc, nr, seed, d, mach=0.6):
+    """An O-grid of quadrilaterals (the generator's nodes, quads not split),
+    written as a case directory the reference reads; returns its params."""
+    import os as _os
+    g = meshgen.make_ogrid(nc, nr, seed=seed)
+    x = g.x
+    nid = lambda i, k: k * nc + (i % nc) + 1
+    quads = []
+    for k in range(nr - 1):
+        for i in range(nc):
+            q = [nid(i, k), nid(i + 1, k), nid(i + 1, k + 1), nid(i, k + 1)]
+            p = x[np.array(q) - 1]
+            area = 0.5 * sum(p[j, 0] * p[(j + 1) % 4, 1] - p[(j + 1) % 4, 0] * p[j, 1]
+                             for j in range(4))
+            quads.append(q[::-1] if area < 0 else q)
+    lines = ["#Number of grid points", str(len(x))] + ["%.17g %.17g" % (a, b) for a, b in x]
+    lines += ["#Number of blocks", "1", "#Number of triangles", "0", "#Number of quads",
+              str(len(quads))] + ["%d %d %d %d" % tuple(q) for q in quads]
+    lines += ["#Number of boundaries", str(len(g.boundaries))]
+    for b, (_, segs) in enumerate(g.boundaries):
+        lines += ["#Number of edges on boundary %d" % (b + 1), str(len(segs))]
+        lines += ["%d %d" % (s0, s1) for s0, s1 in segs]
+    _os.makedirs(d, exist_ok=True)
+    with open(_os.path.join(d, "grid.mesh"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    meshgen.write_bc(_os.path.join(d, "bc.dat"), g)
+    fp = meshgen.FlowParams(order=1, mach=mach)
+    meshgen.write_params(_os.path.join(d, "euler.params"), fp)
+    return fp

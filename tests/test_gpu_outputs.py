@@ -93,3 +93,32 @@ def test_surface_cp_rejects_bad_arguments(ref_lib):
     s.close()
     mesh.close()
     ref.close()
+
+
+def test_tecplot_writer_quadrilateral_branch(ref_lib, tmp_path):
+    """flow_write_tecplot given quadrilaterals besides the triangles: the
+    quadrilateral zone, triangles written as degenerate quadrilaterals, and
+    the reference's other pressure form; against the oracle for the
+    context's state."""
+    import ctypes as C
+    from flowgpu import capi
+    from oracle import outputs
+    fp, ref, mesh, s = _pair(ref_lib, 32, 8, False, 1, 2)
+    Q = s.get("Q")
+    x = mesh.array("x")
+    nn = mesh.sizes["nn"]
+    tri, _ = mesh.elements()
+    quad = np.concatenate([np.zeros(4, dtype=np.int32),
+                           (np.arange(4 * 9, dtype=np.int32) * 7) % nn + 1])
+    L = capi.load()
+    for prim in (False, True):
+        path = tmp_path / f"quads_{int(prim)}.dat"
+        rc = L.flow_write_tecplot(s.ctx, C.byref(s.p), str(path).encode(), int(prim),
+                                  x.ctypes.data_as(capi.DP), len(tri) // 3 - 1,
+                                  tri.ctypes.data_as(capi.IP), len(quad) // 4 - 1,
+                                  quad.ctypes.data_as(capi.IP))
+        assert rc == 0
+        assert path.read_bytes() == outputs.tecplot_bytes(Q, x, nn, tri, quad, prim, fp.gamma)
+    s.close()
+    mesh.close()
+    ref.close()

@@ -102,3 +102,21 @@ def test_prep_connectivity_and_segments_match_the_reference(ref_lib, curved, ord
     assert np.array_equal(seg, np.asarray(flat, dtype=np.int32))
     m.close()
     r.close()
+
+
+def test_oracle_writers_on_a_quadrilateral_mesh(ref_lib, tmp_path):
+    """Quadrilaterals switch the Tecplot zone type, write no triangles and use
+    the reference's other pressure form in write_tecplot_solutionP."""
+    from cases import make_quad_case
+    d = str(tmp_path / "quads")
+    fp = make_quad_case(64, 16, 3, d)
+    r = ref_lib.RefSolver(d)
+    assert r.scalars()["nquad"] > 0 and r.scalars()["ntri"] == 0
+    rng = np.random.Generator(np.random.PCG64(2))
+    Q = r.array("Q").reshape(-1, 4)
+    Q[1:, 0] = rng.uniform(0.5, 1.5, len(Q) - 1)
+    Q[1:, 1:3] = rng.uniform(-0.5, 0.5, (len(Q) - 1, 2))
+    Q[1:, 3] = rng.uniform(2.0, 3.0, len(Q) - 1)
+    r.set_array("Q", Q.ravel())
+    _compare(r, fp, "quads")
+    r.close()
