@@ -27,8 +27,16 @@ class ParityCase:
     weights, k=2 stencils and SVD factors exist), with the state before that
     step kept to start the other implementations from."""
 
-    def __init__(self, nc, nr, curved, order, **kw):
-        self.dir, self.grid, self.fp = make_case(nc, nr, curved, order, **kw)
+    def __init__(self, nc, nr, curved, order, quads=False, **kw):
+        if quads:  # an O-grid of quadrilaterals with straight walls
+            self.dir = tempfile.mkdtemp(prefix=f"qcase_{nc}x{nr}_")
+            self.grid = None
+            # M 0.5: at M 0.8 the blunt trailing edge of the straight-wall
+            # grids drives the reference's k=2 ghost states non-physical
+            self.fp = make_quad_case(nc, nr, kw.get("seed", 3), self.dir,
+                                     mach=kw.get("mach") or 0.5, order=order)
+        else:
+            self.dir, self.grid, self.fp = make_case(nc, nr, curved, order, **kw)
         self.ref = RefSolver(self.dir)
         self.Q0 = self.ref.array("Q")
         self.xnb0 = self.ref.array("xn_bedges")
@@ -76,9 +84,10 @@ def chunk_order(ia, ja, starts):
     return np.asarray(order, dtype=np.int32), max(colour) + 1
 
 
-def make_quad_case(nc, nr, seed, d, mach=0.6):
-    """An O-grid of quadrilaterals (the generator's nodes, quads not split),
-    written as a case directory the reference reads; returns its params."""
+def make_quad_case(nc, nr, seed, d, mach=0.6, order=1, ramp=1111):
+    """An O-grid of quadrilaterals (the generator's nodes, quads not split,
+    straight walls), written as a case directory the reference reads;
+    returns its params."""
     import os as _os
     g = meshgen.make_ogrid(nc, nr, seed=seed)
     x = g.x
@@ -102,6 +111,6 @@ def make_quad_case(nc, nr, seed, d, mach=0.6):
     with open(_os.path.join(d, "grid.mesh"), "w") as f:
         f.write("\n".join(lines) + "\n")
     meshgen.write_bc(_os.path.join(d, "bc.dat"), g)
-    fp = meshgen.FlowParams(order=1, mach=mach)
+    fp = meshgen.FlowParams(order=order, mach=mach, ramp=ramp)
     meshgen.write_params(_os.path.join(d, "euler.params"), fp)
     return fp

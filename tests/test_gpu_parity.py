@@ -21,17 +21,20 @@ def _solver(case, sweep_mode=0):
     return s
 
 
-@pytest.mark.parametrize("nc,nr,curved,order,steps,mode", [
-    (32, 8, False, 1, 6, 0),
-    (128, 32, False, 1, 4, 0),
-    (32, 8, True, 3, 6, 0),
-    (128, 32, True, 3, 4, 0),
-    (128, 32, True, 3, 3, 1),
-    (64, 16, False, 1, 3, 1),
+@pytest.mark.parametrize("nc,nr,curved,order,steps,mode,quads,mach", [
+    (32, 8, False, 1, 6, 0, False, None),
+    (128, 32, False, 1, 4, 0, False, None),
+    (32, 8, True, 3, 6, 0, False, None),
+    (128, 32, True, 3, 4, 0, False, None),
+    (128, 32, True, 3, 3, 1, False, None),
+    (64, 16, False, 1, 3, 1, False, None),
+    (64, 16, False, 3, 4, 0, False, 0.5),  # k=2 with straight walls
+    (64, 16, False, 1, 4, 0, True, None),  # quadrilateral meshes
+    (64, 16, False, 3, 4, 0, True, None),
 ])
-def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode):
+def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode, quads, mach):
     """mode 0: grid-wide ordered sweep; mode 1: one-CTA ordered sweep."""
-    case = ParityCase(nc, nr, curved, order)
+    case = ParityCase(nc, nr, curved, order, quads=quads, mach=mach)
     gpu = _solver(case, mode)
     nn = case.sizes["nn"]
     for ts in range(1, steps + 1):

@@ -8,14 +8,17 @@ from cases import ParityCase, ndiff
 from oracle import port
 
 
-@pytest.mark.parametrize("nc,nr,curved,order,steps", [
-    (32, 8, False, 1, 8),
-    (32, 8, True, 3, 8),
-    (64, 16, True, 3, 4),
-    (64, 16, False, 1, 4),
+@pytest.mark.parametrize("nc,nr,curved,order,steps,quads,mach", [
+    (32, 8, False, 1, 8, False, None),
+    (32, 8, True, 3, 8, False, None),
+    (64, 16, True, 3, 4, False, None),
+    (64, 16, False, 1, 4, False, None),
+    (64, 16, False, 3, 6, False, 0.5),  # k=2 with straight walls
+    (64, 16, False, 1, 6, True, None),  # quadrilateral meshes
+    (64, 16, False, 3, 6, True, None),
 ])
-def test_oracle_matches_reference(ref_lib, nc, nr, curved, order, steps):
-    case = ParityCase(nc, nr, curved, order)
+def test_oracle_matches_reference(ref_lib, nc, nr, curved, order, steps, quads, mach):
+    case = ParityCase(nc, nr, curved, order, quads=quads, mach=mach)
     og = port.OracleGrid(case.sizes, case.arrays)
     p = port.params_from_flow(case.fp)
     nn = case.sizes["nn"]

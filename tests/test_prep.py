@@ -18,12 +18,14 @@ FLOAT_KEYS = ("x", "cv_area", "el_cent", "xn_subedges", "xm_subedges", "xg_subed
               "xg_bedges", "xgn_bedges")
 
 
-@pytest.mark.parametrize("nc,nr,curved,order", [
-    (32, 8, False, 1), (64, 16, False, 1), (32, 8, True, 3), (64, 16, True, 3),
-    (128, 64, True, 3),  # 8192 nodes: stencils and SVD factored on host threads
+@pytest.mark.parametrize("nc,nr,curved,order,quads", [
+    (32, 8, False, 1, False), (64, 16, False, 1, False), (32, 8, True, 3, False),
+    (64, 16, True, 3, False),
+    (128, 64, True, 3, False),  # 8192 nodes: stencils and SVD factored on host threads
+    (64, 16, False, 1, True), (64, 16, False, 3, True),  # quadrilateral meshes
 ])
-def test_prep_matches_reference_setup(ref_lib, nc, nr, curved, order):
-    case = ParityCase(nc, nr, curved, order)
+def test_prep_matches_reference_setup(ref_lib, nc, nr, curved, order, quads):
+    case = ParityCase(nc, nr, curved, order, quads=quads)
     mesh = _prep(case)
     mine = mesh.arrays()
     assert mesh.sizes["nn"] == case.sizes["nn"]
