@@ -34,7 +34,22 @@ def _solver(case, sweep_mode=0):
 ])
 def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode, quads, mach):
     """mode 0: grid-wide ordered sweep; mode 1: one-CTA ordered sweep."""
-    case = ParityCase(nc, nr, curved, order, quads=quads, mach=mach)
+    _steps_bitwise(ParityCase(nc, nr, curved, order, quads=quads, mach=mach), steps, mode)
+
+
+@pytest.mark.parametrize("curved,order,params", [
+    (True, 3, {"iter": 3, "jufreq": 2}),  # Newton iterations, Jacobian every 2nd
+    (False, 1, {"reorder": 0}),           # no Cuthill-McKee renumbering
+    (True, 3, {"subits": 3}),             # an odd number of sweeps
+    (True, 3, {"limit": 0}),              # no limiter
+    (False, 1, {"limit": 0}),
+])
+def test_parameter_variants_bitwise(ref_lib, curved, order, params):
+    _steps_bitwise(ParityCase(32, 8, curved, order, **params), 5, 0)
+
+
+def _steps_bitwise(case, steps, mode):
+    order = case.fp.order
     gpu = _solver(case, mode)
     nn = case.sizes["nn"]
     for ts in range(1, steps + 1):

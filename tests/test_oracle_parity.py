@@ -18,7 +18,21 @@ from oracle import port
     (64, 16, False, 3, 6, True, None),
 ])
 def test_oracle_matches_reference(ref_lib, nc, nr, curved, order, steps, quads, mach):
-    case = ParityCase(nc, nr, curved, order, quads=quads, mach=mach)
+    _oracle_steps(ParityCase(nc, nr, curved, order, quads=quads, mach=mach), steps)
+
+
+@pytest.mark.parametrize("curved,order,params", [
+    (True, 3, {"iter": 3, "jufreq": 2}),  # Newton iterations, Jacobian every 2nd
+    (False, 1, {"reorder": 0}),           # no Cuthill-McKee renumbering
+    (True, 3, {"subits": 3}),             # an odd number of sweeps
+    (True, 3, {"limit": 0}),              # no limiter
+    (False, 1, {"limit": 0}),
+])
+def test_oracle_matches_reference_parameter_variants(ref_lib, curved, order, params):
+    _oracle_steps(ParityCase(32, 8, curved, order, **params), 6)
+
+
+def _oracle_steps(case, steps):
     og = port.OracleGrid(case.sizes, case.arrays)
     p = port.params_from_flow(case.fp)
     nn = case.sizes["nn"]
