@@ -32,6 +32,13 @@ def test_oracle_matches_reference_parameter_variants(ref_lib, curved, order, par
     _oracle_steps(ParityCase(32, 8, curved, order, **params), 6)
 
 
+@pytest.mark.parametrize("curved,order", [(True, 3), (False, 1)])
+def test_oracle_matches_reference_after_first_order_steps(ref_lib, curved, order):
+    """foits = 3 first-order steps, then the scheme of the order."""
+    from cases import startup_parity_case
+    _oracle_steps(startup_parity_case(32, 8, curved, order, 3), 7)
+
+
 def _oracle_steps(case, steps):
     og = port.OracleGrid(case.sizes, case.arrays)
     p = port.params_from_flow(case.fp)
