@@ -182,6 +182,7 @@ struct flow_ctx {
   bool ring_ok[kRingShapes] = {};
   int ring = 0;  // requested shape: sub-levels of ring_rows(ring) rows
   int sweep_df = 0;  // 1: one-launch (dataflow) mode 3 sweeps (flow_set_sweep_dataflow)
+  bool has_edge_w = false;  // the grid view carried LSQ edge weights
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
   // CUDA graphs of chunks of K steps with the step index advancing on the
@@ -262,7 +263,10 @@ int check_params(flow_ctx* c, const flow_params* p) {
   if (p->unsteady != 0 || p->tacc != 0) { set_error("only steady runs are supported"); return FLOW_ERR_ARG; }
   if (p->limit != 0 && p->limit != 2) { set_error("only limit=0 or limit=2 is supported"); return FLOW_ERR_ARG; }
   if (p->iter < 1 || p->jufreq < 1 || p->subits < 0) { set_error("bad iter/jufreq/subits"); return FLOW_ERR_ARG; }
-  if (p->order == 3 && p->soits > 0) { set_error("order 3 with soits > 0 is not supported"); return FLOW_ERR_ARG; }
+  if (p->order == 3 && p->soits > 0 && !c->has_edge_w) {
+    set_error("order 3 with soits > 0 needs the LSQ edge weights in the grid view");
+    return FLOW_ERR_ARG;
+  }
   return 0;
 }
 
@@ -334,7 +338,9 @@ void launch_flux_variant(int v, F&& f) {
 int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   Timed tm(c, 0);
   int nb = grid_blocks(4 * c->nn, 128);
-  if (c->order == 1)
+  // the LSQ gradient (k=1, or the second-order start-up steps of k=2) is
+  // the k=1 kernel's work
+  if (c->order == 1 || a.do_grad)
     launch_variant(c->var[0], [&](auto V) {
       k_node_prepare4<1, V.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
     });
@@ -1132,6 +1138,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   items.clear();
   std::vector<int2> edge_lr(ne + 1);
   std::vector<double4> edge_w(ne + 1, make_double4(0, 0, 0, 0));
+  c->has_edge_w = g->edge_weight != nullptr;
   for (int e = 1; e <= ne; e++) {
     int L = g->edges[2 * e], R = g->edges[2 * e + 1];
     edge_lr[e] = make_int2(L, R);

@@ -880,7 +880,7 @@ flow_mesh* finish(flow_mesh* m, int reorder, int order, int* status) {
   for (int i = 1; i <= m->nn; i++) m->node_order[i] = order;
   for (int i = 1; i <= m->nbe; i++)
     m->node_order[m->bedges[i * 5 + 1] + m->nn] = m->node_order[m->bedges[i * 5]];
-  if (order == 1) edge_weights(*m);
+  edge_weights(*m);  // k=1, and the second-order start-up steps of k=2
   if (order == 3) {
     if (!build_stencils(*m)) return fail("a node's stencil stays below 6 neighbours");
     if (!factor_stencils(*m)) return fail("SVD of a stencil failed");

@@ -94,7 +94,8 @@ typedef struct flow_grid_view {
   const double *xn_bedges;    /* (nbedges+1)*3, initial values */
   const double *xg_bedges;    /* (nbedges+1)*6 */
   const double *xgn_bedges;   /* (nbedges+1)*9 */
-  const double *edge_weight;  /* (nedges+1)*4 (gradient.C:923-1121); NULL if order != 1 */
+  const double *edge_weight;  /* (nedges+1)*4 (gradient.C:923-1121); needed for order 1,
+                                 and for order 3 with soits > 0; may be NULL otherwise */
   const double *moments;      /* (nn+1)*9 (GRID::Moments); NULL if order != 3 */
   /* k=2 two-ring stencils after the growth of solve.C:57-114 (GRID::gnsn,
    * gnnsn, gnnsn1) and the SVD factors of compute_derivatives.C:845-940

@@ -116,20 +116,25 @@ def make_quad_case(nc, nr, seed, d, mach=0.6, order=1, ramp=1111):
     return fp
 
 
-def startup_parity_case(nc, nr, curved, order, foits, **kw):
-    """ParityCase for runs whose first `foits` steps are first order.  The
-    reference builds what its first higher-order step needs only then (k=1:
-    the LSQ edge weights, gradient.C:364-367; k=2: the grown stencils and
-    their SVD factors, solve.C:57-114); these depend on the mesh alone, so
-    they are taken from a second reference run advanced to that step."""
-    case = ParityCase(nc, nr, curved, order, foits=foits, **kw)
-    if foits > 0:
+def startup_parity_case(nc, nr, curved, order, foits, soits=0, **kw):
+    """ParityCase for runs that start with `foits` first-order steps (and,
+    for k=2, `soits` second-order ones).  The reference builds what a phase
+    needs at that phase's first step (the LSQ edge weights at the first
+    gradient, gradient.C:364-367; the grown k=2 stencils and their SVD
+    factors at the first k=2 step, solve.C:57-114); these depend on the mesh
+    alone, so they are taken from a second reference run advanced past
+    them."""
+    case = ParityCase(nc, nr, curved, order, foits=foits, soits=soits, **kw)
+    if foits + soits > 0:
         geo = RefSolver(case.dir)
-        for ts in range(1, foits + 2):
+        for ts in range(1, foits + soits + 2):
             geo.solve(ts)
         _, a = port.reference_arrays(geo, with_svd=(order == 3))
-        keys = (("gnsn", "gnnsn", "gnnsn1", "svd_m", "svd_off", "svd_U", "svd_VT", "svd_S")
-                if order == 3 else ("edge_weight",))
+        keys = []
+        if order == 1 or soits > 0:
+            keys.append("edge_weight")
+        if order == 3:
+            keys += ["gnsn", "gnnsn", "gnnsn1", "svd_m", "svd_off", "svd_U", "svd_VT", "svd_S"]
         for k in keys:
             case.arrays[k] = a[k]
         geo.close()

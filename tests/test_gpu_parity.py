@@ -48,11 +48,15 @@ def test_parameter_variants_bitwise(ref_lib, curved, order, params):
     _steps_bitwise(ParityCase(32, 8, curved, order, **params), 5, 0)
 
 
-@pytest.mark.parametrize("curved,order", [(True, 3), (False, 1)])
-def test_steps_after_first_order_steps_bitwise(ref_lib, curved, order):
-    """foits = 3 first-order steps, then the scheme of the order."""
+@pytest.mark.parametrize("curved,order,foits,soits", [
+    (True, 3, 3, 0), (False, 1, 3, 0),
+    (True, 3, 0, 3), (True, 3, 2, 2),  # k=2 after second-order start-up steps
+])
+def test_steps_after_start_up_steps_bitwise(ref_lib, curved, order, foits, soits):
+    """foits first-order steps (and soits second-order ones for k=2), then
+    the scheme of the order."""
     from cases import startup_parity_case
-    _steps_bitwise(startup_parity_case(32, 8, curved, order, 3), 7, 0)
+    _steps_bitwise(startup_parity_case(32, 8, curved, order, foits, soits), 7, 0)
 
 
 def _steps_bitwise(case, steps, mode):
