@@ -27,8 +27,12 @@ class ParityCase:
     weights, k=2 stencils and SVD factors exist), with the state before that
     step kept to start the other implementations from."""
 
-    def __init__(self, nc, nr, curved, order, quads=False, **kw):
-        if quads:  # an O-grid of quadrilaterals with straight walls
+    def __init__(self, nc, nr, curved, order, quads=False, cylinder=False, **kw):
+        if cylinder:  # triangles around the unit circle (curved wall bc 11)
+            self.dir = tempfile.mkdtemp(prefix=f"cyl_{nc}x{nr}_")
+            self.grid = None
+            self.fp = make_cylinder_case(nc, nr, kw.get("seed", 4), self.dir, order=order)
+        elif quads:  # an O-grid of quadrilaterals with straight walls
             self.dir = tempfile.mkdtemp(prefix=f"qcase_{nc}x{nr}_")
             self.grid = None
             # M 0.5: at M 0.8 the blunt trailing edge of the straight-wall
@@ -139,3 +143,45 @@ def startup_parity_case(nc, nr, curved, order, foits, soits=0, **kw):
             case.arrays[k] = a[k]
         geo.close()
     return case
+
+
+def make_cylinder_case(nc, nr, seed, d, mach=0.3, order=3, wall_bc=11, ramp=1111):
+    """An O-grid of triangles around the unit circle (the reference's curved
+    circular wall, bc 11) out to radius 20 (far field, bc 0), written as a
+    case directory the reference reads; returns its params."""
+    import os as _os
+    rng = np.random.Generator(np.random.PCG64(seed))
+    th = 2.0 * np.pi * np.arange(nc) / nc
+    ratio = 20.0 ** (1.0 / (nr - 1))
+    r = ratio ** np.arange(nr)
+    r[-1] = 20.0
+    x = np.stack([np.outer(r, np.cos(th)).ravel(), np.outer(r, np.sin(th)).ravel()], axis=1)
+    nid = lambda i, k: k * nc + (i % nc) + 1
+    diag = rng.integers(0, 2, size=(nr - 1, nc))
+    tris = []
+    for k in range(nr - 1):
+        for i in range(nc):
+            a, b, c, e = nid(i, k), nid(i + 1, k), nid(i + 1, k + 1), nid(i, k + 1)
+            for t in ([a, b, c], [a, c, e]) if diag[k, i] else ([a, b, e], [b, c, e]):
+                p = x[np.array(t) - 1]
+                area = ((p[1, 0] - p[0, 0]) * (p[2, 1] - p[0, 1])
+                        - (p[2, 0] - p[0, 0]) * (p[1, 1] - p[0, 1]))
+                tris.append(t if area > 0 else [t[0], t[2], t[1]])
+    far = [(nid(i, nr - 1), nid(i + 1, nr - 1)) for i in range(nc)]
+    wall = [(nid(i + 1, 0), nid(i, 0)) for i in range(nc)]
+    bnds = [(0, far), (wall_bc, wall)]
+    lines = ["#Number of grid points", str(len(x))] + ["%.17g %.17g" % (a, b) for a, b in x]
+    lines += ["#Number of blocks", "1", "#Number of triangles", str(len(tris))]
+    lines += ["%d %d %d" % tuple(t) for t in tris]
+    lines += ["#Number of quads", "0", "#Number of boundaries", str(len(bnds))]
+    for b, (_, segs) in enumerate(bnds):
+        lines += ["#Number of edges on boundary %d" % (b + 1), str(len(segs))]
+        lines += ["%d %d" % (s0, s1) for s0, s1 in segs]
+    _os.makedirs(d, exist_ok=True)
+    with open(_os.path.join(d, "grid.mesh"), "w") as f:
+        f.write("\n".join(lines) + "\n")
+    with open(_os.path.join(d, "bc.dat"), "w") as f:
+        f.write("".join("%d\n" % bc for bc, _ in bnds))
+    fp = meshgen.FlowParams(order=order, mach=mach, ramp=ramp, alpha=0.0)
+    meshgen.write_params(_os.path.join(d, "euler.params"), fp)
+    return fp

@@ -37,6 +37,12 @@ def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode, quads, mach)
     _steps_bitwise(ParityCase(nc, nr, curved, order, quads=quads, mach=mach), steps, mode)
 
 
+@pytest.mark.parametrize("order", [1, 3])
+def test_steps_on_a_circular_wall_bitwise(ref_lib, order):
+    """Triangles around the unit circle: the reference's curved wall bc 11."""
+    _steps_bitwise(ParityCase(48, 12, True, order, cylinder=True), 5, 0)
+
+
 @pytest.mark.parametrize("curved,order,params", [
     (True, 3, {"iter": 3, "jufreq": 2}),  # Newton iterations, Jacobian every 2nd
     (False, 1, {"reorder": 0}),           # no Cuthill-McKee renumbering

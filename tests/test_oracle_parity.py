@@ -21,6 +21,12 @@ def test_oracle_matches_reference(ref_lib, nc, nr, curved, order, steps, quads, 
     _oracle_steps(ParityCase(nc, nr, curved, order, quads=quads, mach=mach), steps)
 
 
+@pytest.mark.parametrize("order", [1, 3])
+def test_oracle_matches_reference_on_a_circular_wall(ref_lib, order):
+    """Triangles around the unit circle: the reference's curved wall bc 11."""
+    _oracle_steps(ParityCase(48, 12, True, order, cylinder=True), 6)
+
+
 @pytest.mark.parametrize("curved,order,params", [
     (True, 3, {"iter": 3, "jufreq": 2}),  # Newton iterations, Jacobian every 2nd
     (False, 1, {"reorder": 0}),           # no Cuthill-McKee renumbering
