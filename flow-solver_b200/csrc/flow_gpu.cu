@@ -2338,6 +2338,15 @@ int state_of(flow_ctx* c, const double** Q, int* nn, int* ng) {
   return 0;
 }
 void set_last_error(const char* msg) { set_error(msg); }
+int step_position(flow_ctx* c, int* citer, double* cfl) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
+      cudaMemcpy(citer, c->s.citer, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(cfl, c->s.scalars + 3, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return FLOW_ERR_CUDA;
+  return 0;
+}
 
 }  // namespace internal
 }  // namespace flow

@@ -31,6 +31,9 @@ int device_of(flow_ctx* c);
 int state_of(flow_ctx* c, const double** Q, int* nn, int* ng);
 // Message returned by flow_last_error() on this thread.
 void set_last_error(const char* msg);
+// The pseudo-time step the context last ran (GRID::citer) and its CFL
+// (GRID::cfl), read from the device after the context's work has finished.
+int step_position(flow_ctx* c, int* citer, double* cfl);
 
 }  // namespace internal
 }  // namespace flow

@@ -336,4 +336,59 @@ int flow_write_tecplot(flow_ctx* c, const flow_params* p, const char* path, int 
   return 0;
 }
 
+int flow_write_restart(flow_ctx* c, const flow_params* p, const char* path, const double* x,
+                       int ntri, const int* tri, int nquad, const int* quad, int nb,
+                       const int* nbs, const int* seg) {
+  if (!c || !p || !path || !x || ntri < 0 || nquad < 0 || (ntri > 0 && !tri) ||
+      (nquad > 0 && !quad) || nb < 1 || !nbs || !seg) {
+    set_last_error("flow_write_restart: bad argument");
+    return FLOW_ERR_ARG;
+  }
+  const double* Q = nullptr;
+  int nn = 0, ng = 0;
+  if (flow::internal::state_of(c, &Q, &nn, &ng)) {
+    set_last_error("flow_write_restart: null or failed context");
+    return FLOW_ERR_ARG;
+  }
+  int citer = 0;
+  double cfl = 0.;
+  int rc = flow::internal::step_position(c, &citer, &cfl);
+  if (rc) return rc;
+  std::vector<double> q((size_t)(nn + 1) * 4);
+  cudaError_t e = cudaMemcpy(q.data(), Q, q.size() * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail("flow_write_restart", e);
+  FILE* fp = fopen(path, "w");
+  if (!fp) {
+    set_last_error((std::string("flow_write_restart: cannot open ") + path).c_str());
+    return FLOW_ERR_ARG;
+  }
+  // the mesh as write_mesh prints it (mesh_io.C:318-379)
+  fprintf(fp, "#Number of grid points\n%d\n", nn);
+  for (int n = 1; n <= nn; n++) fprintf(fp, "%.15e %.15e\n", x[2 * n], x[2 * n + 1]);
+  fprintf(fp, "#Number of blocks\n%d\n", 1);
+  fprintf(fp, "#Number of triangles\n%d\n", ntri);
+  for (int i = 1; i <= ntri; i++)
+    fprintf(fp, "%d %d %d\n", tri[i * 3], tri[i * 3 + 1], tri[i * 3 + 2]);
+  fprintf(fp, "#Number of quads\n%d\n", nquad);
+  for (int i = 1; i <= nquad; i++)
+    fprintf(fp, "%d %d %d %d\n", quad[i * 4], quad[i * 4 + 1], quad[i * 4 + 2], quad[i * 4 + 3]);
+  fprintf(fp, "#Number of boundaries\n%d\n", nb);
+  long k = 0;
+  for (int b = 1; b <= nb; b++) {
+    fprintf(fp, "#Number of edges for boundary %d\n%d\n", b, nbs[b]);
+    for (int t = 0; t < nbs[b]; t++, k++) fprintf(fp, "%d %d\n", seg[2 * k], seg[2 * k + 1]);
+  }
+  // the restart block (mesh_io.C:380-390): step, CFL, the real nodes' Q
+  fprintf(fp, "#Number of Constants\n%d\n%d\n%.15E\n", 2, citer, cfl);
+  fprintf(fp, "#Number of Variables\n%d\n", 4);
+  for (int n = 1; n <= nn; n++)
+    fprintf(fp, "%.15e %.15e %.15e %.15e\n", q[4 * (size_t)n], q[4 * (size_t)n + 1],
+            q[4 * (size_t)n + 2], q[4 * (size_t)n + 3]);
+  if (fclose(fp) != 0) {
+    set_last_error((std::string("flow_write_restart: cannot write ") + path).c_str());
+    return FLOW_ERR_ARG;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -40,6 +40,10 @@ struct flow_mesh {
   std::vector<int> nbs;               // nb+1
   std::vector<std::vector<std::array<int, 2>>> bs;  // bs[b][s], b,s 1-based
   std::vector<int> seg_flat;          // bs of every boundary in order, 2 per segment
+  bool restart = false;               // the file carried a restart block
+  int restart_citer = 0;
+  double restart_cfl = 0.;
+  std::vector<double> restart_q;      // 4 per node, in the file's node order
   std::vector<int> bbc;
   std::vector<int> nn_map;
   std::vector<int> csn, ncsn, nsn, nnsn, esn, edges;
@@ -1001,14 +1005,71 @@ flow_mesh* flow_prep_read(const char* path, const int* bbc, int nb_bc, int reord
       seg.push_back(ac[1]);
     }
   }
+  // an optional restart block, as write_mesh appends it (mesh_io.C:380-390,
+  // read back by mesh_io.C:217-262): constants (the last step, its CFL) and
+  // the conserved variables of every node, in the file's node order
+  bool restart = false;
+  int r_citer = 0;
+  double r_cfl = 0.;
+  std::vector<double> r_q;
+  auto blank = [&]() {
+    for (const char* q = buf; *q; q++)
+      if (*q != ' ' && *q != '\t' && *q != '\r' && *q != '\n') return false;
+    return true;
+  };
+  bool more = false;  // a comment line after the boundaries opens the block
+  while (ok && line()) {
+    if (blank()) continue;
+    more = buf[0] == '#';
+    break;
+  }
+  if (more) {
+    int nconst = 0, nvar = 0;
+    bool rok = line() && ints(&nconst, 1) && nconst == 2 && line() && ints(&r_citer, 1) &&
+               line() && doubles(&r_cfl, 1) && read_int(&nvar) && nvar == 4;
+    if (rok) {
+      r_q.resize((size_t)nn * 4);
+      for (int i = 0; i < nn && rok; i++) rok = line() && doubles(&r_q[4 * (size_t)i], 4);
+    }
+    if (!rok) ok = false;
+    restart = rok;
+  }
   fclose(fp);
   if (!ok) {
-    g_prep_error = "malformed mesh file or boundary count differs from bc list";
+    g_prep_error = "malformed mesh file, restart block or boundary count differs from bc list";
     if (status) *status = FLOW_ERR_ARG;
     return nullptr;
   }
-  return flow_prep_build(nn, x.data(), ntri, tri.data(), nquad, quad.data(), nb, nbs.data(),
-                         seg.data(), bbc, reorder, order, status);
+  flow_mesh* m = flow_prep_build(nn, x.data(), ntri, tri.data(), nquad, quad.data(), nb,
+                                 nbs.data(), seg.data(), bbc, reorder, order, status);
+  if (m && restart) {
+    m->restart = true;
+    m->restart_citer = r_citer;
+    m->restart_cfl = r_cfl;
+    m->restart_q = std::move(r_q);
+  }
+  return m;
+}
+
+int flow_prep_restart_state(const flow_mesh* m, double* Q, long nQ, int* citer, double* cfl) {
+  if (!m || !Q || nQ < (long)(m->nn + m->ng + 1) * 4) return FLOW_ERR_ARG;
+  if (!m->restart) {
+    g_prep_error = "the mesh file had no restart block";
+    return FLOW_ERR_NOT_FOUND;
+  }
+  std::fill(Q, Q + (size_t)(m->nn + m->ng + 1) * 4, 0.);
+  // the file's node i is node nn_map[i] after the renumbering (none when the
+  // file is read without reordering, as the reference reads a restart)
+  for (int i = 1; i <= m->nn; i++)
+    for (int v = 0; v < 4; v++) Q[4 * (size_t)m->nn_map[i] + v] = m->restart_q[4 * (size_t)(i - 1) + v];
+  // ghosts copied from their real node (main.C:602-622, ic.C:84-96)
+  for (int i = 1; i <= m->nbe; i++) {
+    const int n = m->bedges[i * 5], g = m->bedges[i * 5 + 1] + m->nn;
+    for (int v = 0; v < 4; v++) Q[4 * (size_t)g + v] = Q[4 * (size_t)n + v];
+  }
+  if (citer) *citer = m->restart_citer;
+  if (cfl) *cfl = m->restart_cfl;
+  return 0;
 }
 
 int flow_prep_view(const flow_mesh* m, flow_grid_view* v) {

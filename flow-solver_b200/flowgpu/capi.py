@@ -32,7 +32,8 @@ ERR_SWEEP_TIMEOUT = 64
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
            "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_surface_cp",
-           "flow_write_surface_cp", "flow_write_tecplot", "flow_get", "flow_size",
+           "flow_write_surface_cp", "flow_write_tecplot", "flow_write_restart", "flow_get",
+           "flow_size",
            "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_set_sweep_ring", "flow_set_sweep_dataflow", "flow_chunk_starts", "flow_set_graphs",
            "flow_autotune", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
@@ -120,6 +121,8 @@ def _load_locked():
     L.flow_surface_cp.argtypes = [vp, PP, C.c_int, IP, IP, C.c_int, IP, DP, C.c_int, IP]
     L.flow_write_surface_cp.argtypes = [vp, PP, C.c_char_p, C.c_int, IP, IP, IP, DP]
     L.flow_write_tecplot.argtypes = [vp, PP, C.c_char_p, C.c_int, DP, C.c_int, IP, C.c_int, IP]
+    L.flow_write_restart.argtypes = [vp, PP, C.c_char_p, DP, C.c_int, IP, C.c_int, IP, C.c_int,
+                                     IP, IP]
     L.flow_get.argtypes = [vp, C.c_char_p, DP, C.c_long]
     L.flow_size.restype = C.c_long
     L.flow_size.argtypes = [vp, C.c_char_p]
@@ -188,6 +191,7 @@ def _load_locked():
     L.flow_prep_node_map.restype = IP
     L.flow_prep_node_map.argtypes = [vp]
     L.flow_prep_elements.argtypes = [vp, IP, C.POINTER(IP), IP, C.POINTER(IP)]
+    L.flow_prep_restart_state.argtypes = [vp, DP, C.c_long, IP, DP]
     L.flow_prep_segments.argtypes = [vp, IP, C.POINTER(IP), C.POINTER(IP), C.POINTER(IP)]
     L.flow_prep_free.argtypes = [vp]
     L.flow_prep_last_error.restype = C.c_char_p
@@ -514,6 +518,17 @@ class Solver:
                                          len(tri) // 3 - 1, tri.ctypes.data_as(IP),
                                          len(quad) // 4 - 1, quad.ctypes.data_as(IP)),
                "flow_write_tecplot")
+
+    def write_restart(self, mesh, path: str):
+        """The mesh with the restart block of the current state (write_mesh)."""
+        tri, quad = mesh.elements()
+        nb, bbc, nbs, seg = mesh.segments()
+        x = mesh.array("x")
+        _check(self.L.flow_write_restart(self.ctx, C.byref(self.p), path.encode(),
+                                         x.ctypes.data_as(DP), len(tri) // 3 - 1,
+                                         tri.ctypes.data_as(IP), len(quad) // 4 - 1,
+                                         quad.ctypes.data_as(IP), nb, nbs.ctypes.data_as(IP),
+                                         seg.ctypes.data_as(IP)), "flow_write_restart")
 
     def get(self, name: str) -> np.ndarray:
         n = self.L.flow_size(self.ctx, name.encode())

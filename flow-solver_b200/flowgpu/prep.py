@@ -155,5 +155,18 @@ class Mesh:
                else np.zeros(1, dtype=np.int32))
         return nb.value, bbc, nbs, seg
 
+    def restart_state(self):
+        """(Q, last step, its CFL) from the file's restart block, or None."""
+        v = self.view
+        Q = np.zeros((v.nn + v.nn_ghost + 1) * 4)
+        citer, cfl = C.c_int(0), C.c_double(0.)
+        rc = self.L.flow_prep_restart_state(self.h, Q.ctypes.data_as(capi.DP), Q.size,
+                                            C.byref(citer), C.byref(cfl))
+        if rc == 128:  # FLOW_ERR_NOT_FOUND: no restart block
+            return None
+        if rc:
+            raise capi.FlowError(rc, "flow_prep_restart_state")
+        return Q, citer.value, cfl.value
+
     def node_map(self) -> np.ndarray:
         return np.ctypeslib.as_array(self.L.flow_prep_node_map(self.h), shape=(self.view.nn + 1,)).copy()

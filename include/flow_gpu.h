@@ -223,6 +223,15 @@ int flow_write_surface_cp(flow_ctx *ctx, const flow_params *p, const char *dir, 
 int flow_write_tecplot(flow_ctx *ctx, const flow_params *p, const char *path, int primitive,
                        const double *x, int ntri, const int *tri, int nquad, const int *quad);
 
+/* void write_mesh(char*, GRID*)  (include/mesh_io.h:21, mesh_io.C:300-393):
+ * the mesh followed by the restart block (the last step run, its CFL and the
+ * conserved variables of the nn real nodes), the same bytes as the
+ * reference writes; flow_prep_read and flow_prep_restart_state read it back
+ * to resume the solve. */
+int flow_write_restart(flow_ctx *ctx, const flow_params *p, const char *path, const double *x,
+                       int ntri, const int *tri, int nquad, const int *quad, int nb,
+                       const int *nbs, const int *seg);
+
 /* Copy a named array back in the reference layout: "Q", "nQ", "pQ", "dQ",
  * "R", "RHS", "LHS", "grad", "phi", "hess" ((nn+1)*36), "point_value",
  * "dt", "xn_bedges".  n is the number of doubles the caller provides. */

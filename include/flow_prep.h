@@ -47,6 +47,16 @@ int flow_prep_view(const flow_mesh *m, flow_grid_view *view);
  * real node (ic.C:84-96): Q has (nn+nn_ghost+1)*4 entries. */
 int flow_prep_initial_state(const flow_mesh *m, const flow_params *p, double *Q);
 
+/* The restart block of the mesh file, if it had one (as the reference's
+ * write_mesh appends it, mesh_io.C:380-390, and read_mesh reads it back with
+ * isrestart = 1, mesh_io.C:217-262): Q receives the conserved variables of
+ * every node ((nn+nn_ghost+1)*4 doubles; each ghost a copy of its real node,
+ * main.C:602-622), *citer the last step run and *cfl its CFL (either may be
+ * NULL); the solve resumes at step *citer + 1.  Read a restart file without
+ * reordering, as the reference does.  FLOW_ERR_NOT_FOUND if the file had no
+ * restart block. */
+int flow_prep_restart_state(const flow_mesh *m, double *Q, long nQ, int *citer, double *cfl);
+
 /* nn_map of the renumbering (old 1-based id -> new id), nn+1 ints. */
 const int *flow_prep_node_map(const flow_mesh *m);
 

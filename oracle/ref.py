@@ -59,6 +59,7 @@ def lib():
         L.ref_write_surface_cp.restype = C.c_int
         L.ref_write_surface_cp.argtypes = [vp, C.c_char_p]
         L.ref_write_tecplot.argtypes = [vp, C.c_char_p, C.c_int]
+        L.ref_write_mesh.argtypes = [vp, C.c_char_p]
         _lib = L
     return _lib
 
@@ -197,6 +198,10 @@ class RefSolver:
         """write_surface_cp run in `directory` (its sort under LC_ALL=C)."""
         if self.L.ref_write_surface_cp(self.h, directory.encode()) != 0:
             raise RuntimeError(f"cannot enter {directory}")
+
+    def write_mesh(self, path: str):
+        """write_mesh: the mesh and the restart block of the current state."""
+        self.L.ref_write_mesh(self.h, path.encode())
 
     def write_tecplot(self, path: str, primitive: bool = False):
         self.L.ref_write_tecplot(self.h, path.encode(), 1 if primitive else 0)

@@ -384,6 +384,18 @@ int ref_write_surface_cp(void *h, const char *dir)
   return 0;
 }
 
+/* write_mesh (mesh_io.C:300-393): the mesh and the restart block of the
+ * current GRID::Q, GRID::citer and GRID::cfl. */
+void ref_write_mesh(void *h, const char *path)
+{
+  RefCase *c = (RefCase *)h;
+  char name[4096];
+  strncpy(name, path, sizeof(name) - 1);
+  name[sizeof(name) - 1] = 0;
+  Mute mute;
+  write_mesh(name, &c->grid);
+}
+
 /* write_tecplot_solutionC (primitive 0, grid_io.C:102-199) or
  * write_tecplot_solutionP (grid_io.C:216-331) of the current GRID::Q. */
 void ref_write_tecplot(void *h, const char *path, int primitive)
