@@ -32,13 +32,14 @@ class ParityCase:
             self.dir = tempfile.mkdtemp(prefix=f"cyl_{nc}x{nr}_")
             self.grid = None
             self.fp = make_cylinder_case(nc, nr, kw.get("seed", 4), self.dir, order=order)
-        elif quads:  # an O-grid of quadrilaterals with straight walls
+        elif quads:  # quadrilaterals (quads="mixed": inner half quads, outer triangles)
             self.dir = tempfile.mkdtemp(prefix=f"qcase_{nc}x{nr}_")
             self.grid = None
             # M 0.5: at M 0.8 the blunt trailing edge of the straight-wall
             # grids drives the reference's k=2 ghost states non-physical
             self.fp = make_quad_case(nc, nr, kw.get("seed", 3), self.dir,
-                                     mach=kw.get("mach") or 0.5, order=order)
+                                     mach=kw.get("mach") or 0.5, order=order,
+                                     quad_rings=(nr - 1) // 2 if quads == "mixed" else None)
         else:
             self.dir, self.grid, self.fp = make_case(nc, nr, curved, order, **kw)
         self.ref = RefSolver(self.dir)
@@ -88,16 +89,19 @@ def chunk_order(ia, ja, starts):
     return np.asarray(order, dtype=np.int32), max(colour) + 1
 
 
-def make_quad_case(nc, nr, seed, d, mach=0.6, order=1, ramp=1111):
+def make_quad_case(nc, nr, seed, d, mach=0.6, order=1, ramp=1111, quad_rings=None):
     """An O-grid of quadrilaterals (the generator's nodes, quads not split,
     straight walls), written as a case directory the reference reads;
-    returns its params."""
+    returns its params.  quad_rings: only the first that many rings of cells
+    are quadrilaterals, the rest the generator's triangles (a mixed mesh)."""
     import os as _os
     g = meshgen.make_ogrid(nc, nr, seed=seed)
     x = g.x
     nid = lambda i, k: k * nc + (i % nc) + 1
+    nq = nr - 1 if quad_rings is None else quad_rings
+    tris = [t for t in g.tris.tolist() if min(t) > nq * nc] if nq < nr - 1 else []
     quads = []
-    for k in range(nr - 1):
+    for k in range(nq):
         for i in range(nc):
             q = [nid(i, k), nid(i + 1, k), nid(i + 1, k + 1), nid(i, k + 1)]
             p = x[np.array(q) - 1]
@@ -105,8 +109,9 @@ def make_quad_case(nc, nr, seed, d, mach=0.6, order=1, ramp=1111):
                              for j in range(4))
             quads.append(q[::-1] if area < 0 else q)
     lines = ["#Number of grid points", str(len(x))] + ["%.17g %.17g" % (a, b) for a, b in x]
-    lines += ["#Number of blocks", "1", "#Number of triangles", "0", "#Number of quads",
-              str(len(quads))] + ["%d %d %d %d" % tuple(q) for q in quads]
+    lines += ["#Number of blocks", "1", "#Number of triangles", str(len(tris))]
+    lines += ["%d %d %d" % tuple(t) for t in tris]
+    lines += ["#Number of quads", str(len(quads))] + ["%d %d %d %d" % tuple(q) for q in quads]
     lines += ["#Number of boundaries", str(len(g.boundaries))]
     for b, (_, segs) in enumerate(g.boundaries):
         lines += ["#Number of edges on boundary %d" % (b + 1), str(len(segs))]

@@ -31,6 +31,8 @@ def _solver(case, sweep_mode=0):
     (64, 16, False, 3, 4, 0, False, 0.5),  # k=2 with straight walls
     (64, 16, False, 1, 4, 0, True, None),  # quadrilateral meshes
     (64, 16, False, 3, 4, 0, True, None),
+    (64, 16, False, 1, 4, 0, "mixed", None),  # quadrilaterals inside, triangles outside
+    (64, 16, False, 3, 4, 0, "mixed", None),
 ])
 def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode, quads, mach):
     """mode 0: grid-wide ordered sweep; mode 1: one-CTA ordered sweep."""

@@ -16,6 +16,8 @@ from oracle import port
     (64, 16, False, 3, 6, False, 0.5),  # k=2 with straight walls
     (64, 16, False, 1, 6, True, None),  # quadrilateral meshes
     (64, 16, False, 3, 6, True, None),
+    (64, 16, False, 1, 5, "mixed", None),  # quadrilaterals inside, triangles outside
+    (64, 16, False, 3, 5, "mixed", None),
 ])
 def test_oracle_matches_reference(ref_lib, nc, nr, curved, order, steps, quads, mach):
     _oracle_steps(ParityCase(nc, nr, curved, order, quads=quads, mach=mach), steps)

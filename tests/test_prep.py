@@ -23,6 +23,7 @@ FLOAT_KEYS = ("x", "cv_area", "el_cent", "xn_subedges", "xm_subedges", "xg_subed
     (64, 16, True, 3, False),
     (128, 64, True, 3, False),  # 8192 nodes: stencils and SVD factored on host threads
     (64, 16, False, 1, True), (64, 16, False, 3, True),  # quadrilateral meshes
+    (64, 16, False, 3, "mixed"),  # quadrilaterals inside, triangles outside
     (48, 12, True, 1, "cylinder"), (48, 12, True, 3, "cylinder"),  # circular wall, bc 11
 ])
 def test_prep_matches_reference_setup(ref_lib, nc, nr, curved, order, quads):
