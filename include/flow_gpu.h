@@ -6,8 +6,8 @@
  * functions over its GRID / SYS_MEM / PARAMS objects.  Every entry point
  * below replaces one of them and takes the same data as plain pointers in the
  * reference's own array layout (1-based, array-of-structs), so a C++ shim
- * with the reference's signatures can forward GRID fields directly (see
- * INTEGRATION.md).  No torch or CUDA types appear in the signatures.
+ * with the reference's signatures can forward GRID fields directly.  No
+ * torch or CUDA types appear in the signatures.
  *
  * Error behaviour: where the reference prints and calls exit() (cvbc.C:330,
  * init_memory.C:257-268, limiter.C:965-977, cv_calc.C:868-875), these entry
