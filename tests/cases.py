@@ -190,3 +190,122 @@ def make_cylinder_case(nc, nr, seed, d, mach=0.3, order=3, wall_bc=11, ramp=1111
     fp = meshgen.FlowParams(order=order, mach=mach, ramp=ramp, alpha=0.0)
     meshgen.write_params(_os.path.join(d, "euler.params"), fp)
     return fp
+
+
+# ---- known-answer fields (the reference's DEBUG_GRAD / DEBUG_DERIVS checks) ----
+# Linear fields q_v = c0 + cx x + cy y, one row per conserved variable, chosen
+# so that density and pressure stay positive on meshes out to radius 20.5.
+LINEAR_COEF = np.array([[10.0, 0.125, 0.25],
+                        [0.0, 0.375, 0.5],
+                        [0.0, 0.625, 0.75],
+                        [500.0, 0.875, 1.0]])
+# Quadratics q_v = c0 + cx x + cy y + cxx x^2/2 + cyy y^2/2 + cxy x y.
+QUAD_COEF = np.array([[30.0, 0.1, 0.1, 0.002, 0.002, 0.001],
+                      [0.0, 0.3, -0.2, 0.001, -0.001, 0.002],
+                      [0.0, -0.1, 0.4, -0.002, 0.001, 0.001],
+                      [600.0, 0.5, 0.5, 0.003, 0.003, -0.002]])
+
+
+def linear_state(Q0, x, nn):
+    """Q0 with the real nodes' rows set to LINEAR_COEF at their coordinates
+    (the ghost rows keep Q0's values)."""
+    Q = Q0.reshape(-1, 4).copy()
+    X = x.reshape(-1, 2)[1:nn + 1]
+    Q[1:nn + 1] = LINEAR_COEF[:, :1].T + X @ LINEAR_COEF[:, 1:].T
+    return Q.ravel()
+
+
+def quad_derivs(X):
+    """(fx, fy, fxx, fyy, fxy) of every QUAD_COEF row at points X: (n, 4, 5)."""
+    c = QUAD_COEF
+    x, y = X[:, :1], X[:, 1:2]
+    return np.stack([c[:, 1] + c[:, 3] * x + c[:, 5] * y, c[:, 2] + c[:, 4] * y + c[:, 5] * x,
+                     np.broadcast_to(c[:, 3], (len(X), 4)), np.broadcast_to(c[:, 4], (len(X), 4)),
+                     np.broadcast_to(c[:, 5], (len(X), 4))], axis=2)
+
+
+def quad_values(X):
+    """QUAD_COEF's four quadratics at points X: (n, 4)."""
+    c = QUAD_COEF
+    x, y = X[:, :1], X[:, 1:2]
+    return c[:, 0] + c[:, 1] * x + c[:, 2] * y + c[:, 3] * x * x / 2 + c[:, 4] * y * y / 2 \
+        + c[:, 5] * x * y
+
+
+def quadratic_state(Q0, x, moments, nn):
+    """Q0 with the real nodes' rows set to the control-volume averages of the
+    QUAD_COEF quadratics.  A quadratic's Taylor series about the node is
+    exact, so its average over the node's volume is the node value plus the
+    derivatives times the volume's moments about the node (moments[0..4]:
+    the averages of dx, dy, dx^2, dy^2 and dx dy)."""
+    Q = Q0.reshape(-1, 4).copy()
+    X = x.reshape(-1, 2)[1:nn + 1]
+    mo = moments.reshape(-1, 9)[1:nn + 1, :5]
+    D = quad_derivs(X)
+    w = np.array([1.0, 1.0, 0.5, 0.5, 1.0])
+    Q[1:nn + 1] = quad_values(X) + np.einsum("nvk,nk->nv", D, mo * w)
+    return Q.ravel()
+
+
+def interior_nodes(bedges, nbedges, nn):
+    """Nodes with no boundary face (1-based)."""
+    b = np.unique(np.asarray(bedges).reshape(-1, 5)[1:nbedges + 1, 0])
+    return np.setdiff1d(np.arange(1, nn + 1), b)
+
+
+def closure_leak(mesh):
+    """Per node |sum of the outward face normals| / (sum of the face lengths)
+    of its median-dual control volume (cv_calc.C:379-640, cv_calc_check_closure):
+    interior faces from the subedges (+ for the edge's left node, - for its
+    right), boundary pieces from each boundary node to the segment's midpoint
+    (the subedge's face point, the curved midpoint on a curved wall), each
+    the integral of the outward normal along it, which is the piece's chord
+    turned clockwise."""
+    A, S = mesh.arrays(), mesh.sizes
+    nn, ns = S["nn"], S["nsubedges"]
+    se = A["subedges"].reshape(-1, 2)[1:ns + 1]
+    ed = A["edges"].reshape(-1, 2)
+    xn = A["xn_subedges"].reshape(-1, 3)[1:ns + 1]
+    xm = A["xm_subedges"].reshape(-1, 2)[1:ns + 1]
+    x = A["x"].reshape(-1, 2)
+    L, R = ed[se[:, 0], 0], ed[se[:, 0], 1]
+    f = xn[:, :2] * xn[:, 2:3]
+    v = np.zeros((nn + 1, 2))
+    per = np.zeros(nn + 1)
+    np.add.at(v, L, f)
+    np.add.at(v, R, -f)
+    np.add.at(per, L, xn[:, 2])
+    np.add.at(per, R, xn[:, 2])
+    lo, hi = np.minimum(L, R).astype(np.int64), np.maximum(L, R).astype(np.int64)
+    keys = lo * (nn + 1) + hi
+    order = np.argsort(keys, kind="stable")
+    _, _, _, seg = mesh.segments()
+    seg = seg.reshape(-1, 2).astype(np.int64)
+    sk = np.minimum(seg[:, 0], seg[:, 1]) * (nn + 1) + np.maximum(seg[:, 0], seg[:, 1])
+    pos = np.searchsorted(keys[order], sk)
+    assert np.array_equal(keys[order][pos], sk), "a boundary segment without its subedge"
+    M = xm[order[pos]]
+    for a, b, node in ((x[seg[:, 0]], M, seg[:, 0]), (M, x[seg[:, 1]], seg[:, 1])):
+        d = b - a
+        np.add.at(v, node, np.stack([d[:, 1], -d[:, 0]], axis=1))
+        np.add.at(per, node, np.hypot(d[:, 0], d[:, 1]))
+    return np.hypot(v[1:, 0], v[1:, 1]) / per[1:]
+
+
+KAT_KINDS = ["triangles", "curved", "quads", "mixed", "cylinder"]
+
+
+def kat_mesh(kind, order):
+    """A 64x16 O-grid (48x12 around the unit circle for 'cylinder') of one of
+    KAT_KINDS, preprocessed by the library; returns (mesh, params)."""
+    from flowgpu.prep import Mesh
+    d = tempfile.mkdtemp(prefix=f"kat_{kind}_")
+    if kind in ("triangles", "curved"):
+        _, _, fp = make_case(64, 16, kind == "curved", order, tmp=d)
+    elif kind == "quads":
+        fp = make_quad_case(64, 16, 3, d, order=order)
+    elif kind == "mixed":
+        fp = make_quad_case(64, 16, 3, d, order=order, quad_rings=7)
+    else:
+        fp = make_cylinder_case(48, 12, 4, d, order=order)
+    return Mesh.from_case(d, order=order), fp
