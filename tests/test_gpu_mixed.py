@@ -40,6 +40,8 @@ def _setup(nc, nr, curved, order, subits, mode=1):
     (32, 8, True, 3, 2, 6, 2),
     (128, 32, True, 3, 2, 4, 2),
     (64, 16, False, 1, 3, 4, 2),
+    (8, 3, False, 1, 2, 5, 1),  # 24 nodes
+    (12, 4, True, 3, 2, 5, 2),  # 48 nodes
 ])
 def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
     """mode 1: multicolour sweeps; mode 2: sweeps in the reference's row order."""
@@ -68,6 +70,8 @@ def test_mixed_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
     (128, 32, True, 3, 4, 4, 0, 0, 0, 1),
     (64, 16, False, 1, 3, 4, 64, 0, 0, 1),
     (128, 32, True, 3, 2, 3, 200, 6, 0, 1),
+    (8, 3, False, 1, 3, 5, 0, 0, 0, 0),  # 24 nodes: one chunk
+    (12, 4, True, 3, 4, 5, 0, 0, 0, 1),
 ])
 def test_chunked_steps_bitwise(nc, nr, curved, order, subits, steps, rows, levels, ring, df):
     """mode 3: coloured chunks of the reference order, against the oracle's

@@ -33,6 +33,9 @@ def _solver(case, sweep_mode=0):
     (64, 16, False, 3, 4, 0, True, None),
     (64, 16, False, 1, 4, 0, "mixed", None),  # quadrilaterals inside, triangles outside
     (64, 16, False, 3, 4, 0, "mixed", None),
+    (8, 3, False, 1, 6, 0, False, None),  # 24 nodes: smaller than one CTA of the node kernels
+    (8, 3, False, 1, 4, 1, False, None),
+    (12, 4, True, 3, 6, 0, False, None),  # 48 nodes, k=2 (8x3 is too small for the k=2 stencils)
 ])
 def test_steps_bitwise(ref_lib, nc, nr, curved, order, steps, mode, quads, mach):
     """mode 0: grid-wide ordered sweep; mode 1: one-CTA ordered sweep."""

@@ -18,6 +18,8 @@ from oracle import port
     (64, 16, False, 3, 6, True, None),
     (64, 16, False, 1, 5, "mixed", None),  # quadrilaterals inside, triangles outside
     (64, 16, False, 3, 5, "mixed", None),
+    (8, 3, False, 1, 6, False, None),   # 24 nodes: smaller than one CTA of the node kernels
+    (12, 4, True, 3, 6, False, None),   # 48 nodes, k=2 (8x3 is too small for the k=2 stencils)
 ])
 def test_oracle_matches_reference(ref_lib, nc, nr, curved, order, steps, quads, mach):
     _oracle_steps(ParityCase(nc, nr, curved, order, quads=quads, mach=mach), steps)
