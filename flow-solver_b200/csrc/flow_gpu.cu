@@ -204,6 +204,14 @@ bool upload(flow_ctx* c, void* dst, const void* src, size_t bytes) {
   return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
 }
 
+// Synchronous device-to-host read of a few results; false (with the CUDA
+// message in flow_last_error) when the copy fails.
+bool download(void* dst, const void* src, size_t bytes) {
+  const cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) set_error(cudaGetErrorString(e));
+  return e == cudaSuccess;
+}
+
 template <class T>
 T* upload_vec(flow_ctx* c, const std::vector<T>& v) {
   T* d = c->buf.alloc<T>(v.size());
@@ -1546,8 +1554,9 @@ int flow_solve(flow_ctx* c, const flow_params* p, int ts, double* dq_norm, doubl
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
   double h[2] = {0., 0.};
-  cudaMemcpy(&h[0], c->d_hist, sizeof(double), cudaMemcpyDeviceToHost);
-  cudaMemcpy(&h[1], c->d_hist + c->hist_cap, sizeof(double), cudaMemcpyDeviceToHost);
+  if (!download(&h[0], c->d_hist, sizeof(double)) ||
+      !download(&h[1], c->d_hist + c->hist_cap, sizeof(double)))
+    return st | FLOW_ERR_CUDA;
   if (dq_norm) *dq_norm = h[0];
   if (r_rho) *r_rho = h[1];
   return st;
@@ -1569,9 +1578,9 @@ int flow_run(flow_ctx* c, const flow_params* p, int ts0, int nsteps, double* r_h
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
-  if (dq_hist) cudaMemcpy(dq_hist, c->d_hist, sizeof(double) * nsteps, cudaMemcpyDeviceToHost);
-  if (r_hist)
-    cudaMemcpy(r_hist, c->d_hist + c->hist_cap, sizeof(double) * nsteps, cudaMemcpyDeviceToHost);
+  if (dq_hist && !download(dq_hist, c->d_hist, sizeof(double) * nsteps)) st |= FLOW_ERR_CUDA;
+  if (r_hist && !download(r_hist, c->d_hist + c->hist_cap, sizeof(double) * nsteps))
+    st |= FLOW_ERR_CUDA;
   return st;
 }
 
@@ -1602,7 +1611,7 @@ int flow_converge(flow_ctx* c, const flow_params* p, int ts0, int max_steps, dou
     harvest(c);
     if (stop) break;
     int st = 0;
-    cudaMemcpy(&st, c->s.status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (!download(&st, c->s.status, sizeof(int))) return FLOW_ERR_CUDA;
     if (st) break;
   }
   cudaEventRecord(c->ev1, c->stream);
@@ -1611,10 +1620,10 @@ int flow_converge(flow_ctx* c, const flow_params* p, int ts0, int max_steps, dou
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
-  double sc[8];
-  cudaMemcpy(sc, c->s.scalars, sizeof(sc), cudaMemcpyDeviceToHost);
-  cudaMemcpy(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost);
-  cudaMemcpy(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost);
+  double sc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  if (!download(sc, c->s.scalars, sizeof(sc)) || !download(&done, c->s.steps_done, sizeof(int)) ||
+      !download(&stop, c->s.stop, sizeof(int)))
+    st |= FLOW_ERR_CUDA;
   // leave the device in the no-target state for later calls
   reset_run(c, 0.);
   cudaStreamSynchronize(c->stream);
@@ -1689,8 +1698,8 @@ int flow_converge_batch(flow_ctx** ctxs, int n, const flow_params* p, int ts0, i
     cudaEventRecord(c->ev1, c->stream);
     int st = read_status(c);
     int done = 0, stop = 0;
-    cudaMemcpy(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost);
-    cudaMemcpy(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost);
+    if (!download(&done, c->s.steps_done, sizeof(int)) || !download(&stop, c->s.stop, sizeof(int)))
+      st |= FLOW_ERR_CUDA;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
     c->last_ms = ms;
@@ -1763,7 +1772,7 @@ int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
   if (rms) {
     double v = 10.;
     if (c->precision != 0) v = -1.;  // the precision form forms no b-Ax RMS
-    else if (p->subits > 0) cudaMemcpy(&v, c->s.scalars, sizeof(double), cudaMemcpyDeviceToHost);
+    else if (p->subits > 0 && !download(&v, c->s.scalars, sizeof(double))) st |= FLOW_ERR_CUDA;
     *rms = v;
   }
   return st;
