@@ -10,8 +10,10 @@
  *   solve                    -> flow_create (first call), flow_solve, flow_get
  *   Compute_Body_Forces      -> flow_body_forces
  *   write_surface_cp         -> flow_write_surface_cp
- *   write_tecplot_solutionC  -> flow_write_tecplot (conserved)
- *   write_tecplot_solutionP  -> flow_write_tecplot (primitive)
+ * The Tecplot and mesh writers stay the reference's own: main.C calls
+ * write_tecplot_solutionC before the first solve() (main.C:704), when no
+ * device context exists yet, and solve() copies the state back into the
+ * GRID after every step, so the host writers see the current solution.
  * Where the library returns an error bit, the shim prints the message and
  * exits as the reference does at the same points (cvbc.C:330-382,
  * init_memory.C:257-268, limiter.C:965-977).
@@ -21,11 +23,11 @@
 #include "grid.h"
 #include "sys_mem.h"
 #include "params.h"
+#include "gradient.h"
 #include "flow_gpu.h"
 
 static flow_ctx *g_ctx = NULL;
 static const GRID *g_grid = NULL;
-static flow_params g_fp;  /* the PARAMS of the last solve(), for the writers */
 
 static flow_params to_flow(const PARAMS &p) {
   flow_params f = {p.nsteps, p.iter, p.jufreq, p.CFL, p.ramp, p.gamma, p.alpha, p.mach,
@@ -37,11 +39,19 @@ static flow_params to_flow(const PARAMS &p) {
 
 double solve(GRID *grid, SYS_MEM *smem, PARAMS p, int ts) {
   flow_params fp = to_flow(p);
-  g_fp = fp;
+  long nq = (long)(grid->nn + grid->nn_ghost + 1) * 4;
   if (g_ctx == NULL || g_grid != grid) {
     // k=2: grow the stencils and factor them first, exactly as solve.C:57-114
     // and compute_derivatives.C:845-940 do on the first high-order step
-    // (or take them from flow_prep); k=1: Compute_Edge_Weights(grid).
+    // (or take them from flow_prep); k=1: the edge weights the reference
+    // builds on its first gradient (gradient.C:363-366).
+    if (p.order == 1 && grid->edge_weight == NULL) Compute_Edge_Weights(grid);
+    // the state arrays the reference's solve() allocates on first use
+    // (solve.C:239-286); the GRID destructor frees them
+    if (grid->nQ == NULL) grid->nQ = (double *)calloc(nq, sizeof(double));
+    if (grid->pQ == NULL) grid->pQ = (double *)calloc(nq, sizeof(double));
+    if (grid->R == NULL) grid->R = (double *)calloc((grid->nn + 1) * 4, sizeof(double));
+    if (grid->dQ == NULL) grid->dQ = (double *)calloc((grid->nn + 1) * 4, sizeof(double));
     static int *seg = NULL;  // bs[b][s][0..1] per bedge
     seg = (int *)realloc(seg, sizeof(int) * 2 * (grid->nbedges + 1));
     for (int i = 1; i <= grid->nbedges; i++) {
@@ -71,7 +81,15 @@ double solve(GRID *grid, SYS_MEM *smem, PARAMS p, int ts) {
   double dq = 0.;
   int rc = flow_solve(g_ctx, &fp, ts, &dq, NULL);
   if (rc) { printf("FATAL ERROR: flow_solve status %d (%s)\n", rc, flow_last_error()); exit(1); }
-  long nq = (long)(grid->nn + grid->nn_ghost + 1) * 4;
+  // GRID::cfl, which the reference's build_matrix sets for the step
+  // (init_memory.C:200-224) and write_mesh prints into the restart block
+  if (p.method == 1)
+    grid->cfl = grid->citer < p.ramp ? 1. + (1. * (grid->citer - 1)) / (1. * p.ramp) * (p.CFL - 1.)
+                                     : p.CFL;
+  else if (p.method == 0)
+    grid->cfl = 1.0;
+  else
+    grid->cfl = p.CFL;
   flow_get(g_ctx, "Q", grid->Q, nq);
   flow_get(g_ctx, "nQ", grid->nQ, nq);
   flow_get(g_ctx, "pQ", grid->pQ, nq);
@@ -101,22 +119,6 @@ void write_surface_cp(GRID *grid, PARAMS p) {
     printf("%s\n", flow_last_error()); exit(0);
   }
   free(seg);
-}
-
-void write_tecplot_solutionP(char *name, GRID *grid, double gamma) {
-  flow_params fp = g_fp;  /* the PARAMS of the last solve() */
-  fp.gamma = gamma;
-  if (flow_write_tecplot(g_ctx, &fp, name, 1, grid->x, grid->num_elem[Tri], grid->c2n[Tri],
-                         grid->num_elem[Quad], grid->c2n[Quad])) {
-    printf("%s\n", flow_last_error()); exit(0);
-  }
-}
-
-void write_tecplot_solutionC(char *name, GRID *grid) {
-  if (flow_write_tecplot(g_ctx, &g_fp, name, 0, grid->x, grid->num_elem[Tri], grid->c2n[Tri],
-                         grid->num_elem[Quad], grid->c2n[Quad])) {
-    printf("%s\n", flow_last_error()); exit(0);
-  }
 }
 
 void Compute_Body_Forces(GRID *grid, PARAMS p, double *Forces) {

@@ -1,6 +1,5 @@
 """The reference-side shim (flow-solver_b200/shim/solve_gpu.C: solve(),
-Compute_Body_Forces(), write_surface_cp() and the Tecplot writers forwarded
-to the C ABI) compiles against the reference's own headers and
+Compute_Body_Forces() and write_surface_cp() forwarded to the C ABI) compiles against the reference's own headers and
 include/flow_gpu.h with the reference's compiler flags (Makefile:19,
 -ansi -pedantic; long long in the C ABI is allowed).  Skipped where the
 reference's headers are not present.  CPU only."""
@@ -33,11 +32,7 @@ def test_shim_forwards_every_replaced_reference_function():
     for sig, target in [("double solve(GRID *grid, SYS_MEM *smem, PARAMS p, int ts)", "flow_solve"),
                         ("void Compute_Body_Forces(GRID *grid, PARAMS p, double *Forces)",
                          "flow_body_forces"),
-                        ("void write_surface_cp(GRID *grid, PARAMS p)", "flow_write_surface_cp"),
-                        ("void write_tecplot_solutionC(char *name, GRID *grid)",
-                         "flow_write_tecplot"),
-                        ("void write_tecplot_solutionP(char *name, GRID *grid, double gamma)",
-                         "flow_write_tecplot")]:
+                        ("void write_surface_cp(GRID *grid, PARAMS p)", "flow_write_surface_cp")]:
         assert sig in src
         body = src[src.index(sig):]
         body = body[:body.index("\n}\n")]
