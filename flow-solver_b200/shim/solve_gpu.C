@@ -14,6 +14,9 @@
  * write_tecplot_solutionC before the first solve() (main.C:704), when no
  * device context exists yet, and solve() copies the state back into the
  * GRID after every step, so the host writers see the current solution.
+ * As written it wires the k=1 scheme completely.  For k=2 the view also
+ * takes the grown stencils and SVD factors (gnsn, SVD_U/V/S) once the
+ * reference has built them, or those of flow_prep (include/flow_prep.h).
  * Where the library returns an error bit, the shim prints the message and
  * exits as the reference does at the same points (cvbc.C:330-382,
  * init_memory.C:257-268, limiter.C:965-977).
