@@ -19,6 +19,7 @@
 #include <type_traits>
 #include <map>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <vector>
 
@@ -36,7 +37,14 @@ thread_local std::string g_last_error;
 
 void set_error(const char* msg) { g_last_error = msg; }
 
+std::shared_mutex g_device_gate;
+
+// Exclusive hold of the device gate for a call that may synchronise the device.
+using DeviceWide = std::unique_lock<std::shared_mutex>;
+
 }  // namespace
+
+std::shared_mutex& flow::internal::device_gate() { return g_device_gate; }
 
 // One device allocation carved into the buffers of many contexts
 // (offset-indexed, 256-byte aligned first fit with coalescing free list).
@@ -96,24 +104,36 @@ struct flow_arena {
 namespace {
 
 // Device buffers of one context: cudaMalloc'ed, or carved from an arena.
+// carve_failed records that an allocation found no room (in an arena that is
+// a budget refusal, FLOW_ERR_BUDGET, not a CUDA error).
 struct Buffers {
   flow_arena* arena = nullptr;
   std::vector<void*> ptrs;
   size_t bytes = 0;
+  bool carve_failed = false;
   template <class T>
   T* alloc(size_t n) {
     if (n == 0) n = 1;
     void* p = nullptr;
     if (arena) {
       p = arena->alloc(n * sizeof(T));
-      if (!p) return nullptr;
-    } else if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
-      return nullptr;
+      if (!p) {
+        carve_failed = true;
+        return nullptr;
+      }
+    } else {
+      DeviceWide gate(g_device_gate);
+      if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) {
+        cudaGetLastError();
+        carve_failed = true;
+        return nullptr;
+      }
     }
     ptrs.push_back(p);
     bytes += (n * sizeof(T) + 255) & ~size_t(255);
     return static_cast<T*>(p);
   }
+  // Caller holds the device gate when the buffers are cudaMalloc'ed.
   void release() {
     for (void* p : ptrs) {
       if (arena) arena->release(p);
@@ -183,6 +203,7 @@ struct flow_ctx {
   int ring = 0;  // requested shape: sub-levels of ring_rows(ring) rows
   int sweep_df = 0;  // 1: one-launch (dataflow) mode 3 sweeps (flow_set_sweep_dataflow)
   bool has_edge_w = false;  // the grid view carried LSQ edge weights
+  bool has_stencils = false;  // order 3: the view carried the k=2 stencils and SVD factors
   std::vector<int> h_color_ptr;
   std::vector<int> h_ia, h_ja;  // host copy of the block pattern
   // CUDA graphs of chunks of K steps with the step index advancing on the
@@ -195,21 +216,36 @@ struct flow_ctx {
     long launches = 0;
   };
   std::vector<ChunkGraph> graphs;
+  // a chunk whose capture fails is launched eagerly instead (same kernels,
+  // same results); capture_fault discards the next captures on purpose
+  // (flow_set_capture_fault), capture_fallbacks counts the eager chunks
+  int capture_fault = 0;
+  long capture_fallbacks = 0;
 };
 
 namespace {
 
+// Host-to-device copy on the context's stream.  The source may be pageable:
+// cudaMemcpyAsync returns once it has been staged, so it may be freed after.
+// Nothing here touches the legacy default stream or synchronises the device.
 bool upload(flow_ctx* c, void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return true;
-  return cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice) == cudaSuccess;
+  return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream) == cudaSuccess;
 }
 
-// Synchronous device-to-host read of a few results; false (with the CUDA
-// message in flow_last_error) when the copy fails.
-bool download(void* dst, const void* src, size_t bytes) {
-  const cudaError_t e = cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost);
+// Device-to-host read of a few results on the context's stream, waited for;
+// false (with the CUDA message in flow_last_error) when the copy fails.
+bool download(flow_ctx* c, void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) set_error(cudaGetErrorString(e));
   return e == cudaSuccess;
+}
+
+// Error code of an allocation that failed: a full arena refuses (budget),
+// anything else is a CUDA error.
+int carve_error(const flow_ctx* c) {
+  return c->buf.arena && c->buf.carve_failed ? FLOW_ERR_BUDGET : FLOW_ERR_CUDA;
 }
 
 template <class T>
@@ -344,6 +380,10 @@ void launch_flux_variant(int v, F&& f) {
 }
 
 int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
+  if (a.do_derivs && !c->has_stencils) {
+    set_error("k=2 derivatives on the device need the stencils and SVD factors in the grid view");
+    return FLOW_ERR_ARG;
+  }
   Timed tm(c, 0);
   int nb = grid_blocks(4 * c->nn, 128);
   // the LSQ gradient (k=1, or the second-order start-up steps of k=2) is
@@ -636,22 +676,44 @@ int enqueue_chunk(flow_ctx* c, const flow_params* p, int ts0, int K) {
     ng.p = *p;
     const long l0 = c->launches;
     cudaGraph_t graph = nullptr;
-    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      set_error("stream capture could not begin");
-      return FLOW_ERR_CUDA;
+    cudaError_t e = cudaSuccess;
+    {
+      // no device-wide call of this library runs while the capture is open
+      std::shared_lock<std::shared_mutex> gate(g_device_gate);
+      e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+      if (e == cudaSuccess) {
+        for (int i = 0; i < K; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
+        e = cudaStreamEndCapture(c->stream, &graph);
+      }
     }
-    for (int i = 0; i < K; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
-    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
-    if (rc || e != cudaSuccess || !graph) {
-      if (graph) cudaGraphDestroy(graph);
-      set_error("step capture failed");
-      return rc ? rc : FLOW_ERR_CUDA;
+    if (e == cudaSuccess && !rc && graph) {
+      e = cudaGraphInstantiate(&ng.exec, graph, 0);
+      if (e != cudaSuccess) ng.exec = nullptr;
     }
-    e = cudaGraphInstantiate(&ng.exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      set_error("graph instantiation failed");
-      return FLOW_ERR_CUDA;
+    if (graph) cudaGraphDestroy(graph);
+    const bool faulted = c->capture_fault > 0;
+    if (faulted && ng.exec) {
+      cudaGraphExecDestroy(ng.exec);  // a discarded capture (flow_set_capture_fault)
+      ng.exec = nullptr;
+    }
+    if (faulted) c->capture_fault--;
+    if (rc || e != cudaSuccess || !ng.exec) {
+      // The capture was invalidated (a device-wide call outside this library,
+      // from another thread) or could not be instantiated.  Nothing of it ran:
+      // launch the chunk eagerly, which does the same work.  A stream that is
+      // somehow still capturing, or an eager launch that fails, is an error.
+      cudaGetLastError();
+      c->launches = l0;
+      c->capture_fallbacks++;
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(c->stream, &cs) != cudaSuccess ||
+          cs != cudaStreamCaptureStatusNone) {
+        set_error("step capture failed and the stream is still capturing");
+        return FLOW_ERR_CUDA;
+      }
+      rc = 0;
+      for (int i = 0; i < K && !rc; i++) rc |= enqueue_step(c, p, ts0 + i, -1, -1, true);
+      return rc;
     }
     ng.launches = c->launches - l0;
     c->launches = l0;
@@ -745,12 +807,16 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
   mt.lhs32 = c->buf.alloc<float>((size_t)16 * std::max<size_t>(ocol.size(), 1));
   if (!mt.color_ptr || !mt.rows || !mt.pos || !mt.offd_ptr || !mt.offd_col || !mt.rowinfo || !mt.lu32 ||
       !mt.dq32 || !mt.dq32b || !mt.lhs32) {
-    set_error("precision form: device allocation failed");
+    set_error("precision form: device allocation or upload failed");
+    mt.lhs32 = nullptr;
+    return carve_error(c);
+  }
+  if (cudaMemsetAsync(mt.dq32, 0, sizeof(float) * 4 * (nn + 1), c->stream) != cudaSuccess ||
+      cudaMemsetAsync(mt.dq32b, 0, sizeof(float) * 4 * (nn + 1), c->stream) != cudaSuccess) {
+    set_error("precision form: clearing the FP32 iterates failed");
     mt.lhs32 = nullptr;
     return FLOW_ERR_CUDA;
   }
-  cudaMemset(mt.dq32, 0, sizeof(float) * 4 * (nn + 1));
-  cudaMemset(mt.dq32b, 0, sizeof(float) * 4 * (nn + 1));
   c->h_color_ptr = cptr;
   c->mt_ordered = ordered;
   return 0;
@@ -760,6 +826,43 @@ int build_mixed_tables(flow_ctx* c, bool ordered) {
 // are set once per device, by the first context that needs them, so that a
 // context built while other solves run never changes a kernel that is in
 // flight.  The shared-memory caps are the largest any context may use.
+//
+// The same first call loads every kernel of the step into the device's
+// context (cudaFuncGetAttributes forces CUDA's lazy module loading).  Loading
+// a module may synchronise the device, so it must not happen at a kernel's
+// first launch while another thread captures a chunk of steps into a graph.
+bool preload_kernels() {
+  cudaFuncAttributes fa;
+  bool ok = true;
+  for (const void* f :
+       {(const void*)k_step_args, (const void*)k_begin_step,
+        (const void*)k_node_prepare4<1, 0>, (const void*)k_node_prepare4<1, 10>,
+        (const void*)k_node_prepare4<1, 12>, (const void*)k_node_prepare4<3, 0>,
+        (const void*)k_node_prepare4<3, 10>, (const void*)k_node_prepare4<3, 12>,
+        (const void*)k_assemble4<true, 0>, (const void*)k_assemble4<false, 0>,
+        (const void*)k_assemble4<true, 1>, (const void*)k_assemble4<false, 1>,
+        (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
+        (const void*)k_boundary_add4<true>, (const void*)k_boundary_add4<false>,
+        (const void*)k_diag_lu,
+        (const void*)k_subedge_flux<0, true, 3>, (const void*)k_subedge_flux<0, true, 4>,
+        (const void*)k_subedge_flux<0, true, 5>, (const void*)k_subedge_flux<0, false, 3>,
+        (const void*)k_subedge_flux<0, false, 4>, (const void*)k_subedge_flux<0, false, 5>,
+        (const void*)k_subedge_flux<1, true, 3>, (const void*)k_subedge_flux<1, true, 4>,
+        (const void*)k_subedge_flux<1, true, 5>, (const void*)k_subedge_flux<1, false, 3>,
+        (const void*)k_subedge_flux<1, false, 4>, (const void*)k_subedge_flux<1, false, 5>,
+        (const void*)k_boundary<true>, (const void*)k_boundary<false>,
+        (const void*)k_diag_only, (const void*)k_sweep_ordered<true>,
+        (const void*)k_sweep_ordered<false>, (const void*)k_sweep_color32<true>,
+        (const void*)k_sweep_color32<false>, (const void*)k_sweep_ordered32<true>,
+        (const void*)k_sweep_ordered32<false>, (const void*)k_prepare_sweep32,
+        (const void*)k_fill_sweep_records, (const void*)k_prepare_sweep,
+        (const void*)k_lin_residual, (const void*)k_finalize_rms, (const void*)k_finish_step,
+        (const void*)k_finalize_step, (const void*)k_body_forces,
+        (const void*)k_body_forces_sum})
+    ok = ok && cudaFuncGetAttributes(&fa, f) == cudaSuccess;
+  return ok;
+}
+
 bool ensure_kernel_attrs(int device) {
   static std::mutex mu;
   static std::vector<char> done;
@@ -767,9 +870,10 @@ bool ensure_kernel_attrs(int device) {
   if (device < 0) return false;
   if ((int)done.size() <= device) done.resize(device + 1, 0);
   if (done[device]) return true;
+  DeviceWide gate(g_device_gate);
   const int chunk_cap = 227 * 1024 - kChunkStaticSmem;
   const int cta = (int)sizeof(SweepSmem);
-  bool ok = true;
+  bool ok = preload_kernels();
   for (const void* f : {(const void*)k_sweep_chunk_df<0>, (const void*)k_sweep_chunk_df<1>,
                         (const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
                         (const void*)k_sweep_chunk<0, 32>, (const void*)k_sweep_chunk<1, 32>,
@@ -791,10 +895,13 @@ int build_chunk_iterate(flow_ctx* c) {
   if (!mt.dq32b) mt.dq32b = c->buf.alloc<float>(n);
   if (!mt.dq32 || !mt.dq32b) {
     set_error("precision form: device allocation failed");
+    return carve_error(c);
+  }
+  if (cudaMemsetAsync(mt.dq32, 0, sizeof(float) * n, c->stream) != cudaSuccess ||
+      cudaMemsetAsync(mt.dq32b, 0, sizeof(float) * n, c->stream) != cudaSuccess) {
+    set_error("precision form: clearing the FP32 iterates failed");
     return FLOW_ERR_CUDA;
   }
-  cudaMemset(mt.dq32, 0, sizeof(float) * n);
-  cudaMemset(mt.dq32b, 0, sizeof(float) * n);
   return 0;
 }
 
@@ -935,10 +1042,13 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
     ct.nbr = upload_vec(c, nbr);
     ct.done = c->buf.alloc<int>(nch);
     ct.sync = c->buf.alloc<unsigned>(4);
-    if (!ct.task_chunk[0] || !ct.task_chunk[1] || !ct.colour || !ct.nbr || !ct.done || !ct.sync ||
-        cudaMemset(ct.done, 0, sizeof(int) * nch) != cudaSuccess ||
-        cudaMemset(ct.sync, 0, sizeof(unsigned) * 4) != cudaSuccess) {
-      set_error("precision mode 3: table upload failed");
+    if (!ct.task_chunk[0] || !ct.task_chunk[1] || !ct.colour || !ct.nbr || !ct.done || !ct.sync) {
+      set_error("precision mode 3: table allocation or upload failed");
+      return carve_error(c);
+    }
+    if (cudaMemsetAsync(ct.done, 0, sizeof(int) * nch, c->stream) != cudaSuccess ||
+        cudaMemsetAsync(ct.sync, 0, sizeof(unsigned) * 4, c->stream) != cudaSuccess) {
+      set_error("precision mode 3: clearing the sweep counters failed");
       return FLOW_ERR_CUDA;
     }
   }
@@ -998,8 +1108,8 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
       c->ring_sub_start[shape][dir] = upload_vec(c, ss);
       c->ring_chunk_sub[shape][dir] = upload_vec(c, cs);
       if (!c->ring_sub_start[shape][dir] || !c->ring_chunk_sub[shape][dir]) {
-        set_error("precision mode 3: table upload failed");
-        return FLOW_ERR_CUDA;
+        set_error("precision mode 3: table allocation or upload failed");
+        return carve_error(c);
       }
     }
     // the records' static part is written on the device from the resident
@@ -1015,13 +1125,13 @@ int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
     ct.rec[dir] = rec;
     ct.pos[dir] = upload_vec(c, pos);
     if (!ct.rec[dir] || !ct.pos[dir]) {
-      set_error("precision mode 3: table upload failed");
-      return FLOW_ERR_CUDA;
+      set_error("precision mode 3: table allocation or upload failed");
+      return carve_error(c);
     }
   }
   if (!ct.col_ptr || !ct.col_chunks || !ct.window) {
-    set_error("precision mode 3: table upload failed");
-    return FLOW_ERR_CUDA;
+    set_error("precision mode 3: table allocation or upload failed");
+    return carve_error(c);
   }
   if (!ensure_kernel_attrs(c->device)) {
     set_error("precision mode 3: cannot reserve shared memory for the sweep");
@@ -1039,7 +1149,7 @@ int ensure_hist(flow_ctx* c, int n) {
   double* h = c->buf.alloc<double>((size_t)2 * n);  // the old block stays with the context
   if (!h) {
     set_error("history allocation failed");
-    return FLOW_ERR_CUDA;
+    return carve_error(c);
   }
   c->d_hist = h;
   c->hist_cap = n;
@@ -1085,9 +1195,16 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
       !g->x || !g->cv_area || !g->xn_subedges || !g->bedges || !g->bbc || !g->node_order)
     return fail(nullptr, FLOW_ERR_ARG, "incomplete grid view");
   if (p->order == 1 && !g->edge_weight) return fail(nullptr, FLOW_ERR_ARG, "order 1 needs edge_weight");
-  if (p->order == 3 && (!g->gnsn || !g->gnnsn || !g->gnnsn1 || !g->svd_m || !g->svd_off ||
-                        !g->svd_U || !g->svd_VT || !g->svd_S || !g->moments || !g->xg_subedges))
-    return fail(nullptr, FLOW_ERR_ARG, "order 3 needs stencils, SVD factors, moments, Gauss points");
+  // order 3: the stencils and SVD factors may be left out (all NULL) by a
+  // caller that forms the k=2 derivatives itself (the stage entry points);
+  // device steps of the k=2 scheme then refuse
+  const bool any_st = g->gnsn || g->gnnsn || g->gnnsn1 || g->svd_m || g->svd_off || g->svd_U ||
+                      g->svd_VT || g->svd_S;
+  const bool all_st = g->gnsn && g->gnnsn && g->gnnsn1 && g->svd_m && g->svd_off && g->svd_U &&
+                      g->svd_VT && g->svd_S;
+  if (p->order == 3 && (!g->moments || !g->xg_subedges || (any_st && !all_st)))
+    return fail(nullptr, FLOW_ERR_ARG,
+                "order 3 needs moments and Gauss points, and all or none of the stencils and SVD factors");
   for (int i = 1; i <= nn; i++)
     if (g->node_order[i] != p->order)
       return fail(nullptr, FLOW_ERR_ARG, "mixed node_order is not supported");
@@ -1104,6 +1221,9 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
     return fail(c, FLOW_ERR_CUDA, "stream creation failed");
   cudaEventCreate(&c->ev0);
   cudaEventCreate(&c->ev1);
+  // kernel attributes and module loading, once per device, before any work
+  if (!ensure_kernel_attrs(device))
+    return fail(c, FLOW_ERR_CUDA, "cannot load the kernels or reserve their shared memory");
 
   if (arena) {
     // the state buffers alone (a lower bound of what the context carves):
@@ -1116,7 +1236,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
       std::lock_guard<std::mutex> lock(arena->mu);
       room = arena->size - arena->used;
     }
-    if (room < need) return fail(c, FLOW_ERR_CUDA, "the arena has no room for this mesh");
+    if (room < need) return fail(c, FLOW_ERR_BUDGET, "the arena has no room for this mesh");
   }
   // ---- host-side re-layout ----
   std::vector<std::pair<int, int>> items;
@@ -1199,7 +1319,8 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   std::vector<int> st_ptr(nn + 2, 0), st_idx;
   std::vector<double> st_w, U1, VT((size_t)(nn + 1) * 25, 0.), S((size_t)(nn + 1) * 5, 1.);
   int stencil_max = 0;
-  if (p->order == 3) {
+  c->has_stencils = p->order == 3 && all_st;
+  if (c->has_stencils) {
     for (int i = 1; i <= nn; i++) {
       int a0 = g->gnnsn[g->gnnsn1[i] + 1], a1 = g->gnnsn[g->gnnsn1[i + 1]];
       int mrows = a1 - a0;
@@ -1258,12 +1379,12 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
     if (g->moments) std::copy(g->moments, g->moments + mo.size(), mo.begin());
     UP(moments, mo);
   }
-  if (p->order == 3) {
+  if (c->has_stencils) {
     UP(st_ptr, st_ptr); UP(st_idx, st_idx); UP(st_w, st_w);
     UP(svd_U1, U1); UP(svd_VT, VT); UP(svd_S, S);
   }
 #undef UP
-  if (!okk) return fail(c, FLOW_ERR_CUDA, "device allocation or upload failed");
+  if (!okk) return fail(c, carve_error(c), "device allocation or upload failed");
 
   // ---- stage tables of the one-CTA ordered sweep ----
   {
@@ -1293,13 +1414,11 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
       int* d_rs = upload_vec(c, rs);
       int* d_row = upload_vec(c, row_stage);
       int* d_ja = upload_vec(c, japad);
-      if (!d_rs || !d_row || !d_ja) return fail(c, FLOW_ERR_CUDA, "sweep table upload failed");
+      if (!d_rs || !d_row || !d_ja) return fail(c, carve_error(c), "sweep table upload failed");
       c->sweep_tb.stage_row0 = d_rs;
       c->sweep_tb.row_stage = d_row;
       c->sweep_tb.ja_pad = d_ja;
       c->sweep_tb.nstages = (int)rs.size() - 1;
-      if (!ensure_kernel_attrs(device))
-        return fail(c, FLOW_ERR_CUDA, "cannot reserve shared memory for the sweep");
       c->sweep_cta_ok = true;
     }
   }
@@ -1341,34 +1460,43 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
       !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
       !s.Jb || !s.bforce || !s.done || !s.counter || !s.status || !s.skip || !s.partial ||
       !s.scalars || !s.stop || !s.steps_done || !s.citer)
-    return fail(c, FLOW_ERR_CUDA, "device state allocation failed");
-  cudaMemset(s.Q, 0, nq * 8);
-  cudaMemset(s.nQ, 0, nq * 8);
-  cudaMemset(s.pQ, 0, nq * 8);
-  cudaMemset(s.dQ, 0, (size_t)(nn + 1) * 32);
-  cudaMemset(s.dQ2, 0, (size_t)(nn + 1) * 32);
-  cudaMemset(s.R, 0, (size_t)(nn + 1) * 32);
-  cudaMemset(s.RHS, 0, (size_t)(nn + 1) * 32);
-  cudaMemset(s.grad, 0, (size_t)(nn + 1) * 64);
-  cudaMemset(s.phi, 0, (size_t)(nn + 1) * 64);
-  cudaMemset(s.hess5, 0, (size_t)(nn + 1) * 160);
-  cudaMemset(s.pv, 0, (size_t)(nn + 1) * 32);
-  cudaMemset(s.dt, 0, (size_t)(nn + 1) * 8);
-  cudaMemset(s.LHS, 0, (size_t)nnz * 128);
-  cudaMemset(s.done, 0, (size_t)(nn + 1) * 4);
-  cudaMemset(s.status, 0, 4);
-  cudaMemset(s.skip, 0, 4);
-  cudaMemset(s.stop, 0, 4);
-  cudaMemset(s.steps_done, 0, 4);
-  cudaMemset(s.citer, 0, 4);
-  cudaMemset(s.scalars, 0, 64);
+    return fail(c, carve_error(c), "device state allocation failed");
+  bool zero_ok = true;
+  auto zero = [&](void* ptr, size_t bytes) {
+    zero_ok = zero_ok && cudaMemsetAsync(ptr, 0, bytes, c->stream) == cudaSuccess;
+  };
+  zero(s.Q, nq * 8);
+  zero(s.nQ, nq * 8);
+  zero(s.pQ, nq * 8);
+  zero(s.dQ, (size_t)(nn + 1) * 32);
+  zero(s.dQ2, (size_t)(nn + 1) * 32);
+  zero(s.R, (size_t)(nn + 1) * 32);
+  zero(s.RHS, (size_t)(nn + 1) * 32);
+  zero(s.grad, (size_t)(nn + 1) * 64);
+  zero(s.phi, (size_t)(nn + 1) * 64);
+  zero(s.hess5, (size_t)(nn + 1) * 160);
+  zero(s.pv, (size_t)(nn + 1) * 32);
+  zero(s.dt, (size_t)(nn + 1) * 8);
+  zero(s.LHS, (size_t)nnz * 128);
+  zero(s.done, (size_t)(nn + 1) * 4);
+  zero(s.status, 4);
+  zero(s.skip, 4);
+  zero(s.stop, 4);
+  zero(s.steps_done, 4);
+  zero(s.citer, 4);
+  zero(s.scalars, 64);
+  if (!zero_ok) return fail(c, FLOW_ERR_CUDA, "clearing the device state failed");
   std::vector<double> xnb((size_t)(nbe + 1) * 3, 0.);
   std::copy(g->xn_bedges, g->xn_bedges + xnb.size(), xnb.begin());
   c->xnb0 = c->buf.alloc<double>(xnb.size());
-  if (!c->xnb0 || !upload(c, s.xn_bedges, xnb.data(), xnb.size() * 8) ||
+  if (!c->xnb0) return fail(c, carve_error(c), "device allocation failed");
+  if (!upload(c, s.xn_bedges, xnb.data(), xnb.size() * 8) ||
       !upload(c, c->xnb0, xnb.data(), xnb.size() * 8))
     return fail(c, FLOW_ERR_CUDA, "upload failed");
-  if (cudaDeviceSynchronize() != cudaSuccess) return fail(c, FLOW_ERR_CUDA, "device error at set-up");
+  // the context's own stream only: a device-wide synchronisation here would
+  // invalidate a graph capture another thread has open
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+    return fail(c, FLOW_ERR_CUDA, "device error at set-up");
   c->ok = true;
   if (status) *status = 0;
   return c;
@@ -1379,6 +1507,8 @@ void flow_destroy(flow_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   harvest(c);
+  // pinned frees and cudaFree synchronise the device: not while a capture is open
+  DeviceWide gate(g_device_gate);
   drop_graphs(c);
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   if (c->ev_flag) cudaEventDestroy(c->ev_flag);
@@ -1524,6 +1654,7 @@ int flow_set_stream_priority(flow_ctx* c, int priority) {
     return FLOW_ERR_CUDA;
   }
   harvest(c);
+  DeviceWide gate(g_device_gate);
   cudaStreamDestroy(c->stream);
   c->stream = st;
   return 0;
@@ -1537,6 +1668,20 @@ int flow_set_graphs(flow_ctx* c, int on) {
   c->use_graphs = on ? 1 : 0;
   return 0;
 }
+
+int flow_set_capture_fault(flow_ctx* c, int count) {
+  if (!c || !c->ok || count < 0) {
+    set_error("flow_set_capture_fault: null context or negative count");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);  // the next chunk captures again
+  c->capture_fault = count;
+  return 0;
+}
+
+long flow_capture_fallbacks(flow_ctx* c) { return c ? c->capture_fallbacks : -1; }
 
 int flow_solve(flow_ctx* c, const flow_params* p, int ts, double* dq_norm, double* r_rho) {
   if (!c || !c->ok) return FLOW_ERR_ARG;
@@ -1554,8 +1699,8 @@ int flow_solve(flow_ctx* c, const flow_params* p, int ts, double* dq_norm, doubl
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
   double h[2] = {0., 0.};
-  if (!download(&h[0], c->d_hist, sizeof(double)) ||
-      !download(&h[1], c->d_hist + c->hist_cap, sizeof(double)))
+  if (!download(c, &h[0], c->d_hist, sizeof(double)) ||
+      !download(c, &h[1], c->d_hist + c->hist_cap, sizeof(double)))
     return st | FLOW_ERR_CUDA;
   if (dq_norm) *dq_norm = h[0];
   if (r_rho) *r_rho = h[1];
@@ -1578,8 +1723,8 @@ int flow_run(flow_ctx* c, const flow_params* p, int ts0, int nsteps, double* r_h
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
-  if (dq_hist && !download(dq_hist, c->d_hist, sizeof(double) * nsteps)) st |= FLOW_ERR_CUDA;
-  if (r_hist && !download(r_hist, c->d_hist + c->hist_cap, sizeof(double) * nsteps))
+  if (dq_hist && !download(c, dq_hist, c->d_hist, sizeof(double) * nsteps)) st |= FLOW_ERR_CUDA;
+  if (r_hist && !download(c, r_hist, c->d_hist + c->hist_cap, sizeof(double) * nsteps))
     st |= FLOW_ERR_CUDA;
   return st;
 }
@@ -1605,24 +1750,31 @@ int flow_converge(flow_ctx* c, const flow_params* p, int ts0, int max_steps, dou
       issued += n;
     }
     if (rc) break;
-    cudaMemcpyAsync(&stop, c->s.stop, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
-    cudaMemcpyAsync(&done, c->s.steps_done, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
-    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return FLOW_ERR_CUDA;
-    harvest(c);
-    if (stop) break;
     int st = 0;
-    if (!download(&st, c->s.status, sizeof(int))) return FLOW_ERR_CUDA;
-    if (st) break;
+    if (!download(c, &stop, c->s.stop, sizeof(int)) ||
+        !download(c, &done, c->s.steps_done, sizeof(int)) ||
+        !download(c, &st, c->s.status, sizeof(int))) {
+      rc |= FLOW_ERR_CUDA;  // the clean-up below still runs
+      break;
+    }
+    harvest(c);
+    if (stop || st) break;
   }
   cudaEventRecord(c->ev1, c->stream);
-  if (rc) return rc;
+  if (rc) {
+    // leave the device in the no-target state for later calls
+    reset_run(c, 0.);
+    cudaStreamSynchronize(c->stream);
+    harvest(c);
+    return rc;
+  }
   int st = read_status(c);
   float ms = 0.f;
   cudaEventElapsedTime(&ms, c->ev0, c->ev1);
   c->last_ms = ms;
   double sc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
-  if (!download(sc, c->s.scalars, sizeof(sc)) || !download(&done, c->s.steps_done, sizeof(int)) ||
-      !download(&stop, c->s.stop, sizeof(int)))
+  if (!download(c, sc, c->s.scalars, sizeof(sc)) || !download(c, &done, c->s.steps_done, sizeof(int)) ||
+      !download(c, &stop, c->s.stop, sizeof(int)))
     st |= FLOW_ERR_CUDA;
   // leave the device in the no-target state for later calls
   reset_run(c, 0.);
@@ -1647,6 +1799,7 @@ int flow_converge_batch(flow_ctx** ctxs, int n, const flow_params* p, int ts0, i
     cudaSetDevice(c->device);
     if ((rc = ensure_hist(c, 1))) return rc;
     if (!c->h_flags) {
+      DeviceWide gate(g_device_gate);
       if (cudaHostAlloc(&c->h_flags, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess)
         return FLOW_ERR_CUDA;
     }
@@ -1698,7 +1851,7 @@ int flow_converge_batch(flow_ctx** ctxs, int n, const flow_params* p, int ts0, i
     cudaEventRecord(c->ev1, c->stream);
     int st = read_status(c);
     int done = 0, stop = 0;
-    if (!download(&done, c->s.steps_done, sizeof(int)) || !download(&stop, c->s.stop, sizeof(int)))
+    if (!download(c, &done, c->s.steps_done, sizeof(int)) || !download(c, &stop, c->s.stop, sizeof(int)))
       st |= FLOW_ERR_CUDA;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, c->ev0, c->ev1);
@@ -1772,7 +1925,7 @@ int flow_linear_solve(flow_ctx* c, const flow_params* p, double* rms) {
   if (rms) {
     double v = 10.;
     if (c->precision != 0) v = -1.;  // the precision form forms no b-Ax RMS
-    else if (p->subits > 0 && !download(&v, c->s.scalars, sizeof(double))) st |= FLOW_ERR_CUDA;
+    else if (p->subits > 0 && !download(c, &v, c->s.scalars, sizeof(double))) st |= FLOW_ERR_CUDA;
     *rms = v;
   }
   return st;
@@ -1840,6 +1993,7 @@ long flow_size(flow_ctx* c, const char* name) {
   if (n == "dt") return nn + 1;
   if (n == "LHS") return (long)c->nnz * 16;
   if (n == "xn_bedges") return (long)(c->nbe + 1) * 3;
+  if (n == "cfl") return 1;
   return -1;
 }
 
@@ -1871,10 +2025,10 @@ int flow_get(flow_ctx* c, const char* name, double* out, long n) {
       return FLOW_ERR_CUDA;
     return 0;
   }
+  if (nm == "cfl") return download(c, out, c->s.scalars + 3, sizeof(double)) ? 0 : FLOW_ERR_CUDA;
   if (nm == "hess") {
     std::vector<double> h((size_t)(c->nn + 1) * 20);
-    if (cudaMemcpy(h.data(), c->s.hess5, h.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
-      return FLOW_ERR_CUDA;
+    if (!download(c, h.data(), c->s.hess5, h.size() * 8)) return FLOW_ERR_CUDA;
     std::fill(out, out + need, 0.);
     for (long i = 0; i <= c->nn; i++)
       for (int v = 0; v < 4; v++)
@@ -1882,6 +2036,112 @@ int flow_get(flow_ctx* c, const char* name, double* out, long n) {
     return 0;
   }
   return FLOW_ERR_NOT_FOUND;
+}
+
+int flow_set(flow_ctx* c, const char* name, const double* in, long n) {
+  if (!c || !c->ok || !name || !in) return FLOW_ERR_ARG;
+  const std::string nm(name);
+  const long need = flow_size(c, name);
+  if (need < 0 || nm == "cfl") return FLOW_ERR_NOT_FOUND;
+  if (n < need) {
+    set_error("flow_set: fewer values than the array holds");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  double* dst = nullptr;
+  if (nm == "Q") dst = c->s.Q;
+  else if (nm == "nQ") dst = c->s.nQ;
+  else if (nm == "pQ") dst = c->s.pQ;
+  else if (nm == "dQ") dst = c->s.dQ;
+  else if (nm == "R") dst = c->s.R;
+  else if (nm == "RHS") dst = c->s.RHS;
+  else if (nm == "grad") dst = c->s.grad;
+  else if (nm == "phi") dst = c->s.phi;
+  else if (nm == "dt") dst = c->s.dt;
+  else if (nm == "LHS") dst = c->s.LHS;
+  else if (nm == "xn_bedges") dst = c->s.xn_bedges;
+  else if (nm == "point_value") dst = c->s.pv;
+  int rc = 0;
+  if (dst) {
+    if (!upload(c, dst, in, sizeof(double) * need)) rc = FLOW_ERR_CUDA;
+  } else if (nm == "hess") {
+    // the five derivatives of each variable the k=2 scheme keeps
+    std::vector<double> h((size_t)(c->nn + 1) * 20);
+    for (long i = 0; i <= c->nn; i++)
+      for (int v = 0; v < 4; v++)
+        for (int k = 0; k < 5; k++) h[i * 20 + v * 5 + k] = in[i * 36 + v * 9 + k];
+    if (!upload(c, c->s.hess5, h.data(), h.size() * 8)) rc = FLOW_ERR_CUDA;
+    else if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FLOW_ERR_CUDA;
+  } else {
+    return FLOW_ERR_NOT_FOUND;
+  }
+  if (!rc && nm == "LHS") {
+    // the sweeps read the LU factors of the diagonal blocks: form them anew
+    k_diag_lu<<<grid_blocks(c->nn, 128), 128, 0, c->stream>>>(c->m, c->s);
+    rc |= launch_check(c);
+  }
+  if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FLOW_ERR_CUDA;
+  if (rc & FLOW_ERR_CUDA) set_error("flow_set: copy to the device failed");
+  return rc;
+}
+
+int flow_residual_stage(flow_ctx* c, const flow_params* p, int jupdate, int ts, int stage) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  if (stage != FLOW_STAGE_INTERIOR && stage != FLOW_STAGE_BOUNDARY) {
+    set_error("flow_residual_stage: stage must be FLOW_STAGE_INTERIOR or FLOW_STAGE_BOUNDARY");
+    return FLOW_ERR_ARG;
+  }
+  if (c->precision != 0) {
+    set_error("flow_residual_stage: the FP64 drop-in only (precision mode 0)");
+    return FLOW_ERR_ARG;
+  }
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  reset_run(c, 0.);
+  StepArgs a = make_args(p, ts);
+  c->citer = ts;
+  if (stage == FLOW_STAGE_INTERIOR) {
+    // faces, then the per-node sums of the interior faces only
+    a.skip_bnd = 1;
+    {
+      Timed t(c, 1);
+      const int nbs = grid_blocks(c->ns, 128);
+      launch_flux_variant(c->var[1], [&](auto V) {
+        if (a.recon == 1) {
+          if (jupdate) k_subedge_flux<1, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+          else k_subedge_flux<1, false, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        } else {
+          if (jupdate) k_subedge_flux<0, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+          else k_subedge_flux<0, false, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        }
+      });
+      rc |= launch_check(c);
+    }
+    Timed t(c, 3);
+    const MixedTables& mt = c->mt;
+    const ChunkTables& ct = c->ct;
+    const int nbn = grid_blocks(4 * c->nn, 128);
+    if (jupdate) k_assemble4<true, 0><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+    else k_assemble4<false, 0><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+    rc |= launch_check(c);
+  } else if (c->nbe > 0) {
+    // ghost states, boundary fluxes and Jacobians, added onto the interior sums
+    {
+      Timed t(c, 2);
+      const int nbb = grid_blocks(c->nbe, 128);
+      if (jupdate) k_boundary<true><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
+      else k_boundary<false><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
+      rc |= launch_check(c);
+    }
+    Timed t(c, 3);
+    const int nbn = grid_blocks(4 * c->nn, 128);
+    if (jupdate) k_boundary_add4<true><<<nbn, 128, 0, c->stream>>>(c->m, c->s);
+    else k_boundary_add4<false><<<nbn, 128, 0, c->stream>>>(c->m, c->s);
+    rc |= launch_check(c);
+  }
+  if (rc) return rc;
+  return read_status(c);
 }
 
 int flow_save_state(flow_ctx* c) {
@@ -2034,6 +2294,7 @@ flow_arena* flow_arena_create(int device, long long bytes, int* status) {
   flow_arena* a = new flow_arena();
   a->device = device;
   a->size = ((size_t)bytes + 255) & ~size_t(255);
+  DeviceWide gate(g_device_gate);
   if (cudaMalloc((void**)&a->base, a->size) != cudaSuccess) {
     cudaGetLastError();
     delete a;
@@ -2049,6 +2310,7 @@ flow_arena* flow_arena_create(int device, long long bytes, int* status) {
 void flow_arena_destroy(flow_arena* a) {
   if (!a) return;
   cudaSetDevice(a->device);
+  DeviceWide gate(g_device_gate);
   cudaFree(a->base);
   delete a;
 }
@@ -2160,29 +2422,36 @@ __global__ void __launch_bounds__(kRedThreads) k_rms(int nn, double* scratch) {
 }
 
 std::mutex g_mu;
-double* g_ptr[kMaxDevices] = {};
+bool g_loaded[kMaxDevices] = {};
 
-// Device address of the scratch array on device `dev` (the current device),
-// looked up on the first call for that device.
+// Device address of the scratch array on device `dev` (the current device).
+// It is looked up on every call, so a module reloaded after cudaDeviceReset
+// is followed; the first call on a device loads the module, under the device
+// gate (loading may synchronise the device), later lookups allocate nothing.
 double* scratch_for(int dev, int* rc) {
-  std::lock_guard<std::mutex> lock(g_mu);
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("flow_linear_residual_noalloc: device ordinal outside 0..63");
     *rc = FLOW_ERR_ARG;
     return nullptr;
   }
-  if (!g_ptr[dev]) {
-    double* ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || !ptr) {
-      set_error((std::string("flow_linear_residual_noalloc: cudaGetSymbolAddress failed: ") +
-                 cudaGetErrorString(e)).c_str());
-      *rc = FLOW_ERR_CUDA;
-      return nullptr;
+  double* ptr = nullptr;
+  cudaError_t e = cudaSuccess;
+  {
+    std::lock_guard<std::mutex> lock(g_mu);
+    if (!g_loaded[dev]) {
+      DeviceWide gate(g_device_gate);
+      e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+      g_loaded[dev] = e == cudaSuccess;
     }
-    g_ptr[dev] = ptr;
   }
-  return g_ptr[dev];
+  if (e == cudaSuccess && !ptr) e = cudaGetSymbolAddress((void**)&ptr, g_noalloc_scratch);
+  if (e != cudaSuccess || !ptr) {
+    set_error((std::string("flow_linear_residual_noalloc: cudaGetSymbolAddress failed: ") +
+               cudaGetErrorString(e)).c_str());
+    *rc = FLOW_ERR_CUDA;
+    return nullptr;
+  }
+  return ptr;
 }
 
 }  // namespace noalloc
@@ -2267,6 +2536,7 @@ int begin_run(flow_ctx* c, const flow_params* p, double drop) {
   cudaSetDevice(c->device);
   if ((rc = ensure_hist(c, 1))) return rc;
   if (!c->h_run) {
+    DeviceWide gate(g_device_gate);
     if (cudaHostAlloc(&c->h_run, 6 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
         cudaHostAlloc(&c->h_runr, 4 * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
       set_error("pinned flag allocation failed");
@@ -2350,9 +2620,7 @@ void set_last_error(const char* msg) { set_error(msg); }
 int step_position(flow_ctx* c, int* citer, double* cfl) {
   if (!c || !c->ok) return FLOW_ERR_ARG;
   cudaSetDevice(c->device);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess ||
-      cudaMemcpy(citer, c->s.citer, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(cfl, c->s.scalars + 3, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (!download(c, citer, c->s.citer, sizeof(int)) || !download(c, cfl, c->s.scalars + 3, sizeof(double)))
     return FLOW_ERR_CUDA;
   return 0;
 }

@@ -2,10 +2,21 @@
 // the serving engine (flow_serve.cu).  Not part of the C ABI.
 #pragma once
 #include <cuda_runtime.h>
+
+#include <shared_mutex>
+
 #include "flow_gpu.h"
 
 namespace flow {
 namespace internal {
+
+// Process-wide gate between CUDA stream captures and calls that may
+// synchronise a whole device.  A device-wide synchronisation (cudaFree,
+// cudaFreeHost, cudaDeviceSynchronize, loading a kernel module) issued by one
+// thread while another thread captures a chunk of steps into a CUDA graph
+// invalidates that capture.  Captures hold the gate shared (several contexts
+// may capture at once); the library's device-wide calls hold it exclusive.
+std::shared_mutex& device_gate();
 
 // Start a run on the context's stream: clear the stop flag and step count,
 // set the target drop of ||R_rho|| and record the run's start event.

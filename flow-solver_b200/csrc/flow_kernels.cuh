@@ -45,6 +45,7 @@ struct StepArgs {
   int gauss;                // k=2 Gauss pass active (curved-boundary side effects)
   int jac;                  // Jacobian update
   int steady_diag;          // V/dt diagonal (steady runs)
+  int skip_bnd;             // assembly of the interior faces only (build_interior_residuals)
 };
 
 // ---------------------------------------------------------------------------
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
       }
     }
   }
-  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  const int b0 = a.skip_bnd ? 0 : m.nbed_ptr[n], b1 = a.skip_bnd ? 0 : m.nbed_ptr[n + 1];
   for (int k = b0; k < b1; k++) {
     const int b = m.nbed[k];
     r += s.Fb[4 * (long)b + q];
@@ -386,6 +387,68 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
   } else {
     reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] = make_double4(o0, o1, o2, o3);
   }
+}
+
+// ---------------------------------------------------------------------------
+// build_boundary_residuals after an interior-only assembly (a.skip_bnd): the
+// boundary fluxes and approximate Jacobians of each node's boundary edges,
+// in ascending order, added to the node's R and diagonal block as the full
+// assembly adds them after the interior faces (residual.C:1147-1167), so
+// interior + boundary gives the bits of the one-pass assembly.  The LU
+// factors of the changed diagonal blocks are formed again.  FP64 only.
+template <bool JAC>
+__global__ void __launch_bounds__(128) k_boundary_add4(DevMesh m, DevState s) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = (tid >> 2) + 1, q = tid & 3;
+  const int qbase = threadIdx.x & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (n > m.nn) return;
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  if (b0 == b1) return;  // whole quads leave together
+  double r = s.R[4 * (long)n + q];
+  double4* drow = reinterpret_cast<double4*>(s.LHS + 16 * (long)m.iau[n]) + q;
+  double4 d = *drow;
+  for (int k = b0; k < b1; k++) {
+    const int b = m.nbed[k];
+    r += s.Fb[4 * (long)b + q];
+    if (JAC) {
+      const double4 J = reinterpret_cast<const double4*>(s.Jb + 16 * (long)b)[q];
+      d.x += J.x; d.y += J.y; d.z += J.z; d.w += J.w;
+    }
+  }
+  s.R[4 * (long)n + q] = r;
+  s.RHS[4 * (long)n + q] = -(r);
+  *drow = d;
+  double M[16];
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    M[4 * row + 0] = __shfl_sync(qmask, d.x, qbase + row);
+    M[4 * row + 1] = __shfl_sync(qmask, d.y, qbase + row);
+    M[4 * row + 2] = __shfl_sync(qmask, d.z, qbase + row);
+    M[4 * row + 3] = __shfl_sync(qmask, d.w, qbase + row);
+  }
+  lu4(M);
+  reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] =
+      make_double4(M[4 * q], M[4 * q + 1], M[4 * q + 2], M[4 * q + 3]);
+}
+
+// LU factors of every diagonal block (linear_algebra.C:226-246), from an LHS
+// the caller supplied (flow_set "LHS"): what the assembly would have formed.
+__global__ void __launch_bounds__(128) k_diag_lu(DevMesh m, DevState s) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (n > m.nn) return;
+  const double4* src = reinterpret_cast<const double4*>(s.LHS + 16 * (long)m.iau[n]);
+  double M[16];
+#pragma unroll
+  for (int row = 0; row < 4; row++) {
+    const double4 v = src[row];
+    M[4 * row] = v.x; M[4 * row + 1] = v.y; M[4 * row + 2] = v.z; M[4 * row + 3] = v.w;
+  }
+  lu4(M);
+  double4* dst = reinterpret_cast<double4*>(s.LUd + 16 * (long)n);
+#pragma unroll
+  for (int row = 0; row < 4; row++)
+    dst[row] = make_double4(M[4 * row], M[4 * row + 1], M[4 * row + 2], M[4 * row + 3]);
 }
 
 // ---------------------------------------------------------------------------

@@ -170,10 +170,11 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   int st = 0;
   flow_ctx* c = flow_create_in(sv->arena, g, p, &st);
   if (!c) {
-    // a failed carve from the arena is a budget refusal, not an error
+    // FLOW_ERR_BUDGET (the arena has no room now: retry after a release) is
+    // kept apart from a CUDA error, which retrying does not cure
     g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
     unreserve();
-    return st == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : (st ? st : FLOW_ERR_ARG);
+    return st ? st : FLOW_ERR_ARG;
   }
   int rc = flow_set_precision(c, precision);
   // mode 3 needs its chunk windows in shared memory; a mesh whose matrix
@@ -221,10 +222,12 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     }
   }
   if (rc) {
+    // the precision tables carved from the arena may not fit (FLOW_ERR_BUDGET);
+    // every other failure is returned as it is
     g_serve_error = std::string("flow_server_submit: ") + flow_last_error();
     flow_destroy(c);
     unreserve();
-    return rc == FLOW_ERR_CUDA ? FLOW_ERR_BUDGET : rc;
+    return rc;
   }
   std::lock_guard<std::mutex> lock(sv->mu);
   Slot& sl = sv->slots[idx];

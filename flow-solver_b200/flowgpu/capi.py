@@ -31,10 +31,11 @@ ERR_SWEEP_TIMEOUT = 64
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
            "flow_converge", "flow_converge_batch", "flow_build_matrix", "flow_reconstruct",
-           "flow_residuals", "flow_linear_solve", "flow_body_forces", "flow_surface_cp",
+           "flow_residuals", "flow_residual_stage", "flow_linear_solve", "flow_body_forces", "flow_surface_cp",
            "flow_write_surface_cp", "flow_write_tecplot", "flow_write_restart", "flow_get",
-           "flow_size",
+           "flow_size", "flow_set",
            "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_set_sweep_ring", "flow_set_sweep_dataflow", "flow_chunk_starts", "flow_set_graphs",
+           "flow_set_capture_fault", "flow_capture_fallbacks",
            "flow_autotune", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
@@ -116,6 +117,7 @@ def _load_locked():
     L.flow_build_matrix.argtypes = [vp, PP, C.c_int]
     L.flow_reconstruct.argtypes = [vp, PP, C.c_int]
     L.flow_residuals.argtypes = [vp, PP, C.c_int, C.c_int]
+    L.flow_residual_stage.argtypes = [vp, PP, C.c_int, C.c_int, C.c_int]
     L.flow_linear_solve.argtypes = [vp, PP, DP]
     L.flow_body_forces.argtypes = [vp, PP, DP]
     L.flow_surface_cp.argtypes = [vp, PP, C.c_int, IP, IP, C.c_int, IP, DP, C.c_int, IP]
@@ -126,9 +128,13 @@ def _load_locked():
     L.flow_get.argtypes = [vp, C.c_char_p, DP, C.c_long]
     L.flow_size.restype = C.c_long
     L.flow_size.argtypes = [vp, C.c_char_p]
+    L.flow_set.argtypes = [vp, C.c_char_p, DP, C.c_long]
     L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
     L.flow_set_precision.argtypes = [vp, C.c_int]
     L.flow_set_graphs.argtypes = [vp, C.c_int]
+    L.flow_set_capture_fault.argtypes = [vp, C.c_int]
+    L.flow_capture_fallbacks.restype = C.c_long
+    L.flow_capture_fallbacks.argtypes = [vp]
     L.flow_set_chunk.argtypes = [vp, C.c_int, C.c_int]
     L.flow_set_sweep_ring.argtypes = [vp, C.c_int]
     L.flow_set_sweep_dataflow.argtypes = [vp, C.c_int]
@@ -475,6 +481,13 @@ class Solver:
     def residuals(self, jupdate: int, ts: int):
         _check(self.L.flow_residuals(self.ctx, C.byref(self.p), jupdate, ts), "flow_residuals")
 
+    STAGE_INTERIOR, STAGE_BOUNDARY = 1, 2
+
+    def residual_stage(self, jupdate: int, ts: int, stage: int):
+        """build_interior_residuals (stage 1) or build_boundary_residuals (2)."""
+        _check(self.L.flow_residual_stage(self.ctx, C.byref(self.p), jupdate, ts, stage),
+               "flow_residual_stage")
+
     def linear_solve(self) -> float:
         r = C.c_double()
         _check(self.L.flow_linear_solve(self.ctx, C.byref(self.p), C.byref(r)), "flow_linear_solve")
@@ -538,6 +551,12 @@ class Solver:
         _check(self.L.flow_get(self.ctx, name.encode(), out.ctypes.data_as(DP), n), f"get {name}")
         return out
 
+    def set(self, name: str, values: np.ndarray):
+        """Copy a named array into the context (flow_set, reference layout)."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        _check(self.L.flow_set(self.ctx, name.encode(), v.ctypes.data_as(DP), v.size),
+               f"set {name}")
+
     def set_precision(self, mode: int):
         """0: FP64 reference-order drop-in; 1: FP32 blocks, multicolour sweeps;
         2: FP32 blocks, sweeps in the reference's row order; 3: FP32 blocks,
@@ -596,6 +615,14 @@ class Solver:
     def set_graphs(self, on: bool):
         """Replay full chunks of flow_converge steps from CUDA graphs (default on)."""
         _check(self.L.flow_set_graphs(self.ctx, int(bool(on))), "flow_set_graphs")
+
+    def set_capture_fault(self, count: int):
+        """Test hook: discard the next `count` chunk captures (eager fallback)."""
+        _check(self.L.flow_set_capture_fault(self.ctx, int(count)), "flow_set_capture_fault")
+
+    def capture_fallbacks(self) -> int:
+        """Chunks launched eagerly after a failed (or discarded) capture."""
+        return self.L.flow_capture_fallbacks(self.ctx)
 
     def set_sweep_mode(self, mode: int):
         _check(self.L.flow_set_sweep_mode(self.ctx, int(mode)), "flow_set_sweep_mode")

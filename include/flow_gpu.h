@@ -67,7 +67,11 @@ typedef struct flow_params {
 
 /* Read-only view of a pre-processed grid in the reference's layout
  * (include/grid.h:223-307 and include/sys_mem.h:43-49).  Array lengths are
- * those the reference allocates (index 0 unused unless noted). */
+ * those the reference allocates (index 0 unused unless noted).  For order 3
+ * the stencil and SVD fields may all be NULL when the caller forms the k=2
+ * derivatives itself (flow_set "hess" / "point_value"); steps of the k=2
+ * scheme on the device (flow_solve, flow_run, flow_reconstruct ...) then
+ * return FLOW_ERR_ARG. */
 typedef struct flow_grid_view {
   int nn;          /* GRID::nn */
   int nn_ghost;    /* GRID::nn_ghost */
@@ -178,6 +182,21 @@ int flow_reconstruct(flow_ctx *ctx, const flow_params *p, int ts);
  * of the diagonal written by flow_build_matrix. */
 int flow_residuals(flow_ctx *ctx, const flow_params *p, int jupdate, int ts);
 
+/* The same two functions one at a time, as the reference's solve() calls
+ * them (solve.C:689, 729) with host code between them:
+ * stage FLOW_STAGE_INTERIOR is build_interior_residuals (residual.C:40-342):
+ * the interior faces' fluxes and, with jupdate, their Jacobians summed into
+ * R and onto the LHS blocks that flow_build_matrix left; FLOW_STAGE_BOUNDARY
+ * is build_boundary_residuals (residual.C:359-1230): the ghost states, the
+ * boundary fluxes and approximate Jacobians added to R and the diagonal
+ * blocks.  Interior then boundary gives the bits flow_residuals gives.  The
+ * reconstruction inputs (grad, phi, hess, point_value) are those on the
+ * device: flow_reconstruct's, or the caller's own through flow_set.  FP64
+ * drop-in only (precision mode 0). */
+#define FLOW_STAGE_INTERIOR 1
+#define FLOW_STAGE_BOUNDARY 2
+int flow_residual_stage(flow_ctx *ctx, const flow_params *p, int jupdate, int ts, int stage);
+
 /* double linear_solve(GRID*, SYS_MEM*, PARAMS)  (include/linear_algebra.h:23,
  * linear_algebra.C:122-401): p->subits alternating ordered block Gauss-Seidel
  * sweeps from dQ = 0; *rms receives the returned b-Ax RMS. */
@@ -236,8 +255,18 @@ int flow_write_restart(flow_ctx *ctx, const flow_params *p, const char *path, co
  * "R", "RHS", "LHS", "grad", "phi", "hess" ((nn+1)*36), "point_value",
  * "dt", "xn_bedges".  n is the number of doubles the caller provides. */
 int flow_get(flow_ctx *ctx, const char *name, double *out, long n);
-/* Number of doubles flow_get(name) writes, or -1. */
+/* Number of doubles flow_get(name) writes, or -1.  "cfl" (1 double, get
+ * only) is GRID::cfl of the last step run: the CFL the ramp of build_matrix
+ * set (init_memory.C:200-224). */
 long flow_size(flow_ctx *ctx, const char *name);
+/* Copy a named array from the host into the context, in the reference
+ * layout, the inverse of flow_get: every name flow_get takes but "cfl".  A
+ * caller that runs some stages of solve() itself (its own gradient, limiter
+ * or k=2 derivatives) hands their results over this way.  "hess" keeps the
+ * five derivatives of each variable the k=2 scheme uses; "LHS" also forms the
+ * LU factors of the diagonal blocks that the sweeps read.  n is the number
+ * of doubles provided (at least flow_size(name)). */
+int flow_set(flow_ctx *ctx, const char *name, const double *in, long n);
 
 /* Sweep kernel; both reproduce the reference's sequential block
  * Gauss-Seidel sweeps exactly: 0 = rows dispensed in order to warps across
@@ -300,8 +329,20 @@ int flow_chunk_starts(flow_ctx *ctx, int *starts, int cap, int *nchunks, int *nc
  * (the default) every full chunk after the first is replayed from a CUDA
  * graph captured once per chunk length, with the step index and the CFL
  * ramp advancing on the device.  Results are identical either way; off
- * launches every kernel from the host. */
+ * launches every kernel from the host.  A capture that fails (another
+ * thread of the host application synchronised the whole device while it was
+ * open) is dropped and its chunk launched kernel by kernel instead, with the
+ * same results; only a failure of those launches fails the call.  The
+ * library's own device-wide calls (allocation, pinned memory, kernel
+ * loading, context teardown) wait for open captures, so several threads may
+ * create, run and destroy contexts at once. */
 int flow_set_graphs(flow_ctx *ctx, int on);
+/* Test hook (no counterpart in the reference): the next `count` chunk
+ * captures of this context are discarded as if they had failed, so their
+ * chunks take the eager path.  flow_capture_fallbacks returns how many
+ * chunks of this context were launched eagerly after a failed capture. */
+int flow_set_capture_fault(flow_ctx *ctx, int count);
+long flow_capture_fallbacks(flow_ctx *ctx);
 
 /* Recreate the context's stream with a CUDA stream priority (clamped to the
  * device's range; numerically lower is served first).  Kernels of
@@ -370,7 +411,8 @@ void flow_arena_destroy(flow_arena *arena);
 long long flow_arena_free_bytes(flow_arena *arena);
 long long flow_arena_largest_free(flow_arena *arena);
 /* flow_create with every device buffer carved from `arena` (on its device);
- * NULL with *status = FLOW_ERR_CUDA when the arena has no room. */
+ * NULL with *status = FLOW_ERR_BUDGET when the arena has no room for it, and
+ * with FLOW_ERR_CUDA for a CUDA error (a failed copy, a device fault). */
 flow_ctx *flow_create_in(flow_arena *arena, const flow_grid_view *g, const flow_params *p,
                          int *status);
 /* Device bytes a context holds. */
@@ -379,7 +421,8 @@ long long flow_ctx_device_bytes(flow_ctx *ctx);
 /* ---- Serving engine (no counterpart in the reference) ---------------------
  * Continuous batching of steady solves on one GPU: each submitted solve gets
  * a context in the arena (admission fails with FLOW_ERR_BUDGET while the
- * arena or the slot table is full) and its own stream; flow_server_progress
+ * arena or the slot table is full, and only then: a CUDA error during
+ * admission is returned as FLOW_ERR_CUDA) and its own stream; flow_server_progress
  * keeps two chunks of `chunk` pseudo-time steps in flight per running solve
  * and retires solves whose ||R_rho|| dropped by `drop` (status 0), that hit
  * max_steps (FLOW_ERR_NOT_CONVERGED) or failed.  Solves of any mesh, order,
@@ -466,7 +509,9 @@ const char *flow_server_last_error(void);
  * Layout (the reference's SYS_MEM): row j = 1..nn owns blocks
  * ia[j] .. ia[j+1]-1, ja[k] is the 1-based column of block k, lhs holds 16
  * doubles per block (row-major 4x4), rhs and x hold (nn+1)*4 doubles with
- * row 0 unused.  All five are device pointers on the current device.  The
+ * row 0 unused.  ia holds nn+2 entries (ia[nn+1] is read); nnz = ia[nn+1],
+ * and ja and lhs hold nnz blocks (ja nnz ints, lhs 16*nnz doubles).  All
+ * five are device pointers on the current device.  The
  * work runs on `stream` (NULL: the legacy default stream); the call waits
  * for it and stores the RMS in the host double *rms.  A row pointer or
  * column outside the system is reported as FLOW_ERR_ARG.
@@ -474,9 +519,11 @@ const char *flow_server_last_error(void);
  * Scratch: one file-scope __device__ array per device (about 2 MB), sized
  * for FLOW_NOALLOC_MAX_ROWS rows; a larger nn is rejected with FLOW_ERR_ARG
  * and a message in flow_last_error().  The first call on each device does a
- * one-time set-up (it looks up the array's device address, which also loads
+ * one-time set-up (its look-up of the array's device address also loads
  * this library's device code on that device): make that first call before
- * any stream capture starts.  Every call on a device shares the array, which
+ * any stream capture starts.  Later calls look the address up again, which
+ * allocates nothing and follows a module reloaded after cudaDeviceReset.
+ * Every call on a device shares the array, which
  * keeps the last call's contents; each call clears the one word that must
  * start at zero.  Calls whose GPU work overlaps (several host threads on
  * different streams) race on the array and return wrong results: serialise

@@ -226,7 +226,7 @@ def test_arena_without_room_refuses_before_building_the_context():
     st = C.c_int(0)
     p = capi.params_struct(fp)
     ctx = L.flow_create_in(arena.h, C.byref(mesh.view), C.byref(p), C.byref(st))
-    assert not ctx and st.value == 2  # FLOW_ERR_CUDA: no device memory for it
+    assert not ctx and st.value == 512  # FLOW_ERR_BUDGET: no room in the arena now
     assert b"no room" in L.flow_last_error()
     srv = capi.Server(arena, chunk=16, max_slots=2)
     assert srv.submit(mesh, fp, mesh.initial_state(fp), precision=3, max_steps=8) is None

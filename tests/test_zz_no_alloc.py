@@ -39,14 +39,20 @@ def _system(nc, nr, order):
     return out
 
 
-def _noalloc(sysd):
+def _on_device(sysd):
+    """The system's arrays in the caller's own device memory (torch's)."""
     import torch
-    from flowgpu import capi
     dev = torch.device("cuda", 0)
     t = {k: torch.from_numpy(sysd[k]).to(dev) for k in ("ia", "ja", "LHS", "RHS", "dQ")}
     torch.cuda.synchronize()
+    return t
+
+
+def _noalloc(sysd, t):
+    import torch
+    from flowgpu import capi
     nnz = int(sysd["ia"][sysd["nn"] + 1])
-    stream = torch.cuda.current_stream(dev).cuda_stream
+    stream = torch.cuda.current_stream(torch.device("cuda", 0)).cuda_stream
     return capi.linear_residual_noalloc(t["ia"].data_ptr(), t["ja"].data_ptr(),
                                         t["LHS"].data_ptr(), t["RHS"].data_ptr(),
                                         t["dQ"].data_ptr(), sysd["nn"], nnz, stream)
@@ -58,10 +64,21 @@ def test_noalloc_residual_matches_linear_solve_on_calls_in_a_row():
     big = _system(64, 16, 3)
     small = _system(32, 8, 1)
     assert big["nn"] > small["nn"]
-    for sysd in (big, small, big):
-        got = _noalloc(sysd)
+    tb, ts = _on_device(big), _on_device(small)
+    # the first call loads the module (a one-time set-up); from then on the
+    # calls take no device memory: neither the device's free bytes nor
+    # torch's allocated bytes move
+    first = _noalloc(big, tb)
+    assert first == pytest.approx(big["rms"], rel=RTOL, abs=0.)
+    torch.cuda.synchronize()
+    free0, alloc0 = torch.cuda.mem_get_info(0)[0], torch.cuda.memory_allocated(0)
+    for sysd, t in ((big, tb), (small, ts), (big, tb)):
+        got = _noalloc(sysd, t)
         assert np.isfinite(got) and got > 0.
         assert got == pytest.approx(sysd["rms"], rel=RTOL, abs=0.)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free0
+    assert torch.cuda.memory_allocated(0) == alloc0
 
 
 def test_noalloc_rejects_rows_beyond_the_scratch():
