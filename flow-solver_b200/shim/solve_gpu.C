@@ -14,11 +14,12 @@
  * write_tecplot_solutionC before the first solve() (main.C:704), when no
  * device context exists yet, and solve() copies the state back into the
  * GRID after every step, so the host writers see the current solution.
- * As written it wires the k=1 scheme completely.  For k=2 the view also
- * takes the grown stencils and SVD factors (gnsn, SVD_U/V/S) once the
- * reference has built them, or those of flow_prep (include/flow_prep.h).
- * Where the library returns an error bit, the shim prints the message and
- * exits as the reference does at the same points (cvbc.C:330-382,
+ * k=1 and k=2 are wired: the device context takes the LSQ edge weights
+ * (k=1, or k=2 with second-order start-up steps) and, for k=2, the grown
+ * two-ring stencils and their SVD factors, made on the host by the
+ * reference's own functions before the context is created.  Where the
+ * library returns an error bit, the shim prints the message and exits as
+ * the reference does at the same points (cvbc.C:330-382,
  * init_memory.C:257-268, limiter.C:965-977).
  */
 #include <stdio.h>
@@ -27,10 +28,14 @@
 #include "sys_mem.h"
 #include "params.h"
 #include "gradient.h"
+#include "maps.h"
+#include "compute_derivatives.h"
 #include "flow_gpu.h"
+#include "grid_view.h"
 
 static flow_ctx *g_ctx = NULL;
 static const GRID *g_grid = NULL;
+static ShimView g_view;
 
 static flow_params to_flow(const PARAMS &p) {
   flow_params f = {p.nsteps, p.iter, p.jufreq, p.CFL, p.ramp, p.gamma, p.alpha, p.mach,
@@ -40,66 +45,103 @@ static flow_params to_flow(const PARAMS &p) {
   return f;
 }
 
+static int stencil_rows(const GRID *grid, int i) {
+  return grid->gnnsn[grid->gnnsn1[i + 1]] - grid->gnnsn[grid->gnnsn1[i] + 1];
+}
+
+static void add_layer(GRID *grid, int i) {
+  Add_Layer_to_GNSN(grid->nn, grid->num_elem, grid->c2n, grid->esn, grid->nnsn, grid->edges,
+                    &(grid->gnsn), &(grid->gnnsn), grid->gnnsn1, grid->node_fill_level, i);
+}
+
+/* The k=2 stencils the reference's solve() builds on its first high-order
+ * step (solve.C:57-114): one layer of neighbours for every node, a second
+ * for the nodes of order 3, then up to three more for any k=2 node whose
+ * stencil still has fewer than 6 rows (a node that needs more ends the run,
+ * as there).  All through the reference's own Add_Layer_to_GNSN.  The
+ * stencils depend on the mesh alone, so building them at the run's first
+ * step gives the arrays the reference builds later. */
+static void grow_stencils(GRID *grid) {
+  for (int i = 1; i <= grid->nn; i++) add_layer(grid, i);
+  for (int i = 1; i <= grid->nn; i++)
+    if (grid->node_order[i] > 2) add_layer(grid, i);
+  for (int i = 1; i <= grid->nn; i++) {
+    if (grid->node_order[i] < 3) continue;
+    int extra = 0;
+    while (stencil_rows(grid, i) < 6) {
+      if (extra == 3) {
+        printf("FATAL ERROR: Node %d has attempted to add too many layers of neighbors. "
+               "Halting...\n", i);
+        fflush(stdout);
+        exit(0);
+      }
+      add_layer(grid, i);
+      extra++;
+    }
+  }
+}
+
+/* A device context for `grid`: the view, plus for k=2 the stencils and the
+ * pseudo-inverse factors.  The factors come from the reference's own
+ * Compute_Derivatives (compute_derivatives.C:274-1072 factors every node on
+ * its first call), run once here on the host from the current state. */
+static void make_context(GRID *grid, SYS_MEM *smem, const PARAMS &p) {
+  const flow_params fp = to_flow(p);
+  const long nq = (long)(grid->nn + grid->nn_ghost + 1) * 4;
+  // the LSQ edge weights the reference builds on its first gradient
+  // (gradient.C:363-366): k=1, and the second-order start-up steps of k=2
+  if ((p.order == 1 || (p.order == 3 && p.soits > 0)) && grid->edge_weight == NULL)
+    Compute_Edge_Weights(grid);
+  if (p.order == 3) {
+    if (grid->SVD_U == NULL) {
+      for (long k = 0; k < nq; k++) grid->nQ[k] = grid->Q[k];
+      grow_stencils(grid);
+      Compute_Derivatives(grid, p, 3);
+    }
+  }
+  shim_view_fill(grid, smem, p.order == 3, &g_view);
+  int st = 0;
+  if (g_ctx) flow_destroy(g_ctx);  // a new GRID: the old device mirror goes
+  g_ctx = flow_create(&g_view.v, &fp, 0, &st);
+  if (!g_ctx) { printf("flow_create failed: %s\n", flow_last_error()); exit(1); }
+  g_grid = grid;
+  if (flow_set_state(g_ctx, grid->Q)) {
+    printf("FATAL ERROR: flow_set_state failed (%s)\n", flow_last_error());
+    exit(1);
+  }
+}
+
 double solve(GRID *grid, SYS_MEM *smem, PARAMS p, int ts) {
   flow_params fp = to_flow(p);
   long nq = (long)(grid->nn + grid->nn_ghost + 1) * 4;
   if (g_ctx == NULL || g_grid != grid) {
-    // k=2: grow the stencils and factor them first, exactly as solve.C:57-114
-    // and compute_derivatives.C:845-940 do on the first high-order step
-    // (or take them from flow_prep); k=1: the edge weights the reference
-    // builds on its first gradient (gradient.C:363-366).
-    if (p.order == 1 && grid->edge_weight == NULL) Compute_Edge_Weights(grid);
-    // the state arrays the reference's solve() allocates on first use
+    // the arrays the reference's solve() allocates on first use
     // (solve.C:239-286); the GRID destructor frees them
     if (grid->nQ == NULL) grid->nQ = (double *)calloc(nq, sizeof(double));
     if (grid->pQ == NULL) grid->pQ = (double *)calloc(nq, sizeof(double));
     if (grid->R == NULL) grid->R = (double *)calloc((grid->nn + 1) * 4, sizeof(double));
     if (grid->dQ == NULL) grid->dQ = (double *)calloc((grid->nn + 1) * 4, sizeof(double));
-    static int *seg = NULL;  // bs[b][s][0..1] per bedge
-    seg = (int *)realloc(seg, sizeof(int) * 2 * (grid->nbedges + 1));
-    for (int i = 1; i <= grid->nbedges; i++) {
-      int b = grid->bedges[i * 5 + 3], s = grid->bedges[i * 5 + 4];
-      seg[2 * i] = grid->bs[b][s][0];
-      seg[2 * i + 1] = grid->bs[b][s][1];
-    }
-    flow_grid_view v = {0};
-    v.nn = grid->nn; v.nn_ghost = grid->nn_ghost; v.nedges = grid->nedges;
-    v.nsubedges = grid->nsubedges; v.nbedges = grid->nbedges; v.nb = grid->nb;
-    v.nelem = grid->num_elem[Tri] + grid->num_elem[Quad];
-    v.edges = grid->edges; v.subedges = grid->subedges; v.bedges = grid->bedges;
-    v.bedge_seg = seg; v.bbc = grid->bbc; v.node_order = grid->node_order;
-    v.ia = smem->ia; v.iau = smem->iau; v.ja = smem->ja;
-    v.x = grid->x; v.cv_area = grid->cv_area; v.el_cent = grid->el_cent;
-    v.xn_subedges = grid->xn_subedges; v.xm_subedges = grid->xm_subedges;
-    v.xg_subedges = grid->xg_subedges; v.xn_bedges = grid->xn_bedges;
-    v.xg_bedges = grid->xg_bedges; v.xgn_bedges = grid->xgn_bedges;
-    v.edge_weight = grid->edge_weight; v.moments = grid->Moments;
-    /* k=2: v.gnsn/gnnsn/gnnsn1 = grid->gnsn/..., v.svd_* from grid->SVD_U/V/S */
-    int st = 0;
-    g_ctx = flow_create(&v, &fp, 0, &st);
-    if (!g_ctx) { printf("flow_create failed: %s\n", flow_last_error()); exit(1); }
-    g_grid = grid;
-    flow_set_state(g_ctx, grid->Q);
+    if (grid->hess == NULL) grid->hess = (double *)calloc((grid->nn + 1) * 36, sizeof(double));
+    make_context(grid, smem, p);
   }
   double dq = 0.;
   int rc = flow_solve(g_ctx, &fp, ts, &dq, NULL);
   if (rc) { printf("FATAL ERROR: flow_solve status %d (%s)\n", rc, flow_last_error()); exit(1); }
-  // GRID::cfl, which the reference's build_matrix sets for the step
-  // (init_memory.C:200-224) and write_mesh prints into the restart block
-  if (p.method == 1)
-    grid->cfl = grid->citer < p.ramp ? 1. + (1. * (grid->citer - 1)) / (1. * p.ramp) * (p.CFL - 1.)
-                                     : p.CFL;
-  else if (p.method == 0)
-    grid->cfl = 1.0;
-  else
-    grid->cfl = p.CFL;
-  flow_get(g_ctx, "Q", grid->Q, nq);
-  flow_get(g_ctx, "nQ", grid->nQ, nq);
-  flow_get(g_ctx, "pQ", grid->pQ, nq);
-  flow_get(g_ctx, "R", grid->R, (long)(grid->nn + 1) * 4);
-  flow_get(g_ctx, "dQ", grid->dQ, (long)(grid->nn + 1) * 4);
-  flow_get(g_ctx, "xn_bedges", grid->xn_bedges, (long)(grid->nbedges + 1) * 3);
-  if (grid->phi) flow_get(g_ctx, "phi", grid->phi, (long)(grid->nn + 1) * 8);
+  // the state back into the GRID for the reference's writers, with GRID::cfl
+  // (the ramp's CFL of this step, which write_mesh prints); a failed read
+  // would hand them the previous step's arrays, so it ends the run
+  rc = flow_get(g_ctx, "Q", grid->Q, nq);
+  rc |= flow_get(g_ctx, "nQ", grid->nQ, nq);
+  rc |= flow_get(g_ctx, "pQ", grid->pQ, nq);
+  rc |= flow_get(g_ctx, "R", grid->R, (long)(grid->nn + 1) * 4);
+  rc |= flow_get(g_ctx, "dQ", grid->dQ, (long)(grid->nn + 1) * 4);
+  rc |= flow_get(g_ctx, "xn_bedges", grid->xn_bedges, (long)(grid->nbedges + 1) * 3);
+  rc |= flow_get(g_ctx, "cfl", &grid->cfl, 1);
+  if (grid->phi) rc |= flow_get(g_ctx, "phi", grid->phi, (long)(grid->nn + 1) * 8);
+  if (rc) {
+    printf("FATAL ERROR: reading the state back failed (status %d: %s)\n", rc, flow_last_error());
+    exit(1);
+  }
   return dq;
 }
 

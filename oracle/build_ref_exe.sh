@@ -11,13 +11,23 @@
 #                                 made weak so that
 #                                 the shim's definitions link (the integration
 #                                 a maintainer makes, without editing a
-#                                 reference file), linked to libflowgpu.so.
+#                                 reference file), linked to libflowgpu.so;
+#   oracle/_ref/field_solver_stages  the reference's own solve() with
+#                                 build_matrix, build_interior_residuals,
+#                                 build_boundary_residuals and linear_solve
+#                                 from flow-solver_b200/shim/stages_gpu.C
+#                                 (the reference's made weak), linked to
+#                                 libflowgpu.so.
 # Test infrastructure: tests/test_gpu_dropin_exe.py runs both on one case and
 # compares their output files.  Needs flow-solver_b200/lib/libflowgpu.so.
-# Usage: sh oracle/build_ref_exe.sh [reference_dir]
+# Usage: sh oracle/build_ref_exe.sh reference_dir   (or FLOW_REFERENCE_DIR=... sh oracle/build_ref_exe.sh)
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-/root/reference}
+REF=${1:-$FLOW_REFERENCE_DIR}
+if [ -z "$REF" ]; then
+  echo "build_ref_exe.sh: give the reference directory as the argument or in FLOW_REFERENCE_DIR" >&2
+  exit 1
+fi
 OUT="$HERE/_ref"
 OBJ="$OUT/exe_obj"
 HOST="$HERE/../flow-solver_b200/csrc/host"
@@ -62,4 +72,32 @@ g++ -x c++ $CFLAGS -Wno-long-long $INC -I"$HERE/../include" -c \
     "$HERE/../flow-solver_b200/shim/solve_gpu.C" -o "$OBJ/solve_gpu.o"
 g++ -o "$OUT/field_solver_gpu" $REFOBJ "$OBJ/solve_gpu.o" "$OBJ/grid_io_weak.o" $SHIMS \
     -L"$LIBDIR" -lflowgpu -Wl,-rpath,'$ORIGIN/../../flow-solver_b200/lib' -lm
-echo "built $OUT/field_solver and $OUT/field_solver_gpu"
+# the reference's own solve() over the stage shim: build_matrix,
+# build_interior_residuals, build_boundary_residuals and linear_solve made
+# weak in copies of their objects, the shim's definitions linked instead
+weaken() {  # object, functions...
+  obj=$1; shift
+  flags=""
+  for fn in "$@"; do
+    sym=$(nm "$OBJ/$obj.o" | awk -v f="$fn" '$2 == "T" && $3 ~ ("^_Z[0-9]+" f "P") {print $3}')
+    [ -n "$sym" ] || { echo "build_ref_exe.sh: $fn not found in $obj.o" >&2; exit 1; }
+    flags="$flags --weaken-symbol=$sym"
+  done
+  objcopy $flags "$OBJ/$obj.o" "$OBJ/${obj}_weak.o"
+}
+weaken init_memory build_matrix
+weaken residual build_interior_residuals build_boundary_residuals
+weaken linear_algebra linear_solve
+STAGEOBJ=""
+for f in "$REF"/*.C; do
+  b=$(basename "$f" .C)
+  case "$b" in
+    init_memory|residual|linear_algebra) STAGEOBJ="$STAGEOBJ $OBJ/${b}_weak.o" ;;
+    *) STAGEOBJ="$STAGEOBJ $OBJ/$b.o" ;;
+  esac
+done
+g++ -x c++ $CFLAGS -Wno-long-long $INC -I"$HERE/../include" -c \
+    "$HERE/../flow-solver_b200/shim/stages_gpu.C" -o "$OBJ/stages_gpu.o"
+g++ -o "$OUT/field_solver_stages" $STAGEOBJ "$OBJ/stages_gpu.o" $SHIMS \
+    -L"$LIBDIR" -lflowgpu -Wl,-rpath,'$ORIGIN/../../flow-solver_b200/lib' -lm
+echo "built $OUT/field_solver, $OUT/field_solver_gpu and $OUT/field_solver_stages"

@@ -1,8 +1,13 @@
-"""The reference's own driver (main.C, unmodified) over the shim and
+"""The reference's own driver (main.C, unmodified) over the shims and
 libflowgpu.so, against the reference as shipped.  oracle/build_ref_exe.sh
-builds both executables from the reference's sources; each runs the same
-k=1 case for 8 pseudo-time steps in its own directory, and every file the
-run writes is compared:
+builds the executables from the reference's sources:
+* field_solver_gpu: solve() replaced whole (flow-solver_b200/shim/solve_gpu.C);
+* field_solver_stages: the reference's own solve() with build_matrix,
+  build_interior_residuals, build_boundary_residuals and linear_solve
+  replaced (flow-solver_b200/shim/stages_gpu.C).
+Each runs the same case (k=1 straight walls, k=2 curved walls) for 8
+pseudo-time steps in its own directory, and every file the run writes is
+compared:
 * residuals.dat holds the step norm ||dQ|| that solve() returns, which the
   GPU reduces in a different order: compared to 1e-12 relative;
 * time.dat holds wall-clock times: only its presence is compared;
@@ -25,7 +30,8 @@ pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_EXE = os.path.join(ROOT, "oracle", "_ref", "field_solver")
-GPU_EXE = os.path.join(ROOT, "oracle", "_ref", "field_solver_gpu")
+GPU_EXES = {"whole": os.path.join(ROOT, "oracle", "_ref", "field_solver_gpu"),
+            "stages": os.path.join(ROOT, "oracle", "_ref", "field_solver_stages")}
 NORM_RTOL = 1e-12
 
 
@@ -49,10 +55,13 @@ def _numbers_close(a, b):
         assert fy == pytest.approx(fx, rel=NORM_RTOL, abs=0.0)
 
 
-def test_reference_driver_over_the_shim_writes_the_reference_files():
+@pytest.mark.parametrize("shim", ["whole", "stages"])
+@pytest.mark.parametrize("curved,order", [(False, 1), (True, 3)])
+def test_reference_driver_over_the_shim_writes_the_reference_files(shim, curved, order):
+    GPU_EXE = GPU_EXES[shim]
     if not (os.path.exists(REF_EXE) and os.path.exists(GPU_EXE)):
         pytest.skip("oracle/build_ref_exe.sh has not been run")
-    d, _, _ = make_case(64, 16, False, 1, nsteps=8)
+    d, _, _ = make_case(64, 16, curved, order, nsteps=8)
     r_ref, w_ref = _run(REF_EXE, d)
     r_gpu, w_gpu = _run(GPU_EXE, d)
     assert "Finished Iteration 8" in r_ref.stdout

@@ -74,3 +74,67 @@ def test_stage_entry_points_match_the_reference(ref_lib, nc, nr, curved, order):
     s.close()
     mesh.close()
     ref.close()
+
+
+@pytest.mark.parametrize("nc,nr,curved,order", [(64, 16, False, 1), (64, 16, True, 3)])
+def test_split_residual_stages_and_host_reconstruction(ref_lib, nc, nr, curved, order):
+    """build_interior_residuals and build_boundary_residuals one at a time
+    (flow_residual_stage), in a context given the reference's own gradient,
+    limiter and k=2 derivatives through flow_set: the arrays after each stage
+    equal the reference's after the same stage, bit for bit.  For k=2 the
+    context is made without device stencils (the derivatives are the
+    host's), as a caller that keeps the reference's Compute_Derivatives
+    makes it; its device k=2 steps refuse."""
+    from flowgpu import capi
+    from flowgpu.prep import Mesh
+    d, _, fp = make_case(nc, nr, curved, order)
+    ref = ref_lib.RefSolver(d)
+    mesh = Mesh.from_case(d, order=order)
+    sizes, arrays = mesh.sizes, mesh.arrays()
+    if order == 3:
+        for k in ("gnsn", "gnnsn", "gnnsn1", "svd_m", "svd_off", "svd_U", "svd_VT", "svd_S"):
+            arrays[k] = None
+    s = capi.Solver(sizes, arrays, fp, device=0)
+    s.set_state(mesh.initial_state(fp))
+    ref.solve(1)
+    for name in ("Q", "nQ", "pQ", "xn_bedges"):  # the reference's state after step 1
+        s.set(name, ref.array(name))
+    if order == 3:
+        with pytest.raises(capi.FlowError):
+            s.reconstruct(2)  # k=2 derivatives on the device need the stencils
+    ref.set_citer(2)
+    ref.build_matrix()
+    s.build_matrix(2)
+    assert ndiff(ref.array("LHS"), s.get("LHS")) == 0
+    if order == 1:
+        ref.gradient()
+    else:
+        ref.derivatives(3)
+    ref.limiter()
+    names = ("grad", "phi") if order == 1 else ("hess", "point_value", "phi")
+    for name in names:
+        s.set(name, ref.array(name))
+    ref.interior(1, 2)
+    s.residual_stage(1, 2, capi.Solver.STAGE_INTERIOR)
+    assert ndiff(ref.array("R")[4:], s.get("R")[4:]) == 0
+    assert ndiff(ref.array("LHS"), s.get("LHS")) == 0
+    ref.boundary(1)
+    s.residual_stage(1, 2, capi.Solver.STAGE_BOUNDARY)
+    assert ndiff(ref.array("R")[4:], s.get("R")[4:]) == 0
+    assert ndiff(ref.array("LHS"), s.get("LHS")) == 0
+    assert ndiff(ref.array("xn_bedges")[3:], s.get("xn_bedges")[3:]) == 0
+    assert ndiff(ref.array("nQ")[4:], s.get("nQ")[4:]) == 0
+    # the linear solve from the caller's LHS and RHS (LU factors formed anew)
+    ref.set_array("RHS", -ref.array("R"))
+    ref.set_array("dQ", np.zeros_like(ref.array("dQ")))
+    s.set("LHS", ref.array("LHS"))
+    s.set("RHS", ref.array("RHS"))
+    r_ref = ref.linear_solve()
+    r_gpu = s.linear_solve()
+    assert ndiff(ref.array("dQ")[4:], s.get("dQ")[4:]) == 0
+    assert r_gpu == pytest.approx(r_ref, rel=RMS_RTOL)
+    assert s.get("cfl")[0] == ref.cfl()
+    assert s.status() == 0
+    s.close()
+    mesh.close()
+    ref.close()
