@@ -99,3 +99,37 @@ def _steps_bitwise(case, steps, mode):
             assert rr == pytest.approx(np.sqrt((R * R).sum()), rel=1e-12)
         assert gpu.body_forces() == ref.body_forces()
     assert gpu.status() == 0
+
+
+def test_transonic_k2_at_full_size_bitwise(ref_lib):
+    """The plain drop-in check at its own size: 512 x 128 O-grid (65,536
+    nodes), k=2, M 0.8, curved NACA walls (the curved boundary path of
+    residual.C:1103-1143 and the k=2 derivatives of
+    compute_derivatives.C:1438-1534), three steps bit for bit."""
+    _steps_bitwise(ParityCase(512, 128, True, 3, mach=0.8), 3, 0)
+
+
+@pytest.mark.parametrize("nc,nr,curved,order,mach,steps", [
+    (128, 32, False, 1, 0.5, 300),   # the k=1 case: 128 x 32, M 0.5
+    (128, 32, True, 3, 0.8, 200),    # k=2, curved walls, M 0.8
+])
+def test_long_residual_history(ref_lib, nc, nr, curved, order, mach, steps):
+    """The drop-in reproduces the reference's residual-drop history: every
+    step's ||R_rho|| over a long run (the GPU forms the norm as a tree
+    reduction: 1e-12 relative), and the state after the last step bit for
+    bit (so every step's sweeps took the reference's path, including the
+    b - Ax RMS test of linear_algebra.C:348-387)."""
+    case = ParityCase(nc, nr, curved, order, mach=mach)
+    gpu = _solver(case)
+    r_gpu, _dq = gpu.run(1, steps)
+    r_ref = []
+    for ts in range(1, steps + 1):
+        case.ref_step()
+        R = case.ref.array("R").reshape(-1, 4)[1:, 0]
+        r_ref.append(np.sqrt((R * R).sum()))
+    r_ref = np.asarray(r_ref)
+    np.testing.assert_allclose(np.asarray(r_gpu), r_ref, rtol=1e-12, atol=0.)
+    assert r_ref[-1] < r_ref[0]  # the history falls
+    assert ndiff(case.ref.array("Q")[4:], gpu.get("Q")[4:]) == 0
+    assert gpu.body_forces() == case.ref.body_forces()
+    assert gpu.status() == 0
