@@ -4,23 +4,27 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl flow|reference]
                     [--workload NAME]
 
-Default workload: the batching form ``batch16`` -- 16 independent steady
+Default workload: the batching form ``batch64`` -- 64 independent steady
 solves per GPU from the seeded request stream (meshes of 2k..200k nodes,
-Mach 0.3..0.85, angle of attack -4..6 degrees, k=1 or k=2), admitted
-together to the serving engine (one device arena, one stream per solve,
-CUDA-graph chunks of pseudo-time steps) in the precision form (FP32 blocks,
-multicolour Gauss-Seidel), each retired at a 1e-10 drop of ||R_rho|| or at
-its step limit.  A "step" of this benchmark is one pass over the batch.
+log-uniform, 4:1 O-grids; Mach 0.3..0.85, angle of attack -4..6 degrees,
+k=1 or k=2), admitted together to the serving engine (one device arena, one
+stream per solve, CUDA-graph chunks of pseudo-time steps) in the precision
+form (FP64 residual, FP32 blocks, Gauss-Seidel in coloured chunks of the
+reference order), each retired at a 1e-10 drop of ||R_rho||, at its step
+limit or when it stalls.  A "step" of this benchmark is one pass over the
+batch.
 
 * value: converged solves / device time of the passes (CUDA events), with
   every mesh and initial state already on the device (staged).
-* e2e: the same through the C ABI from host buffers: staging (mesh arrays
-  and state copied to the device) and the read-back of every converged
-  state and of the lift/drag forces inside the timed region.
+* e2e: the same through the C ABI from host buffers, served continuously:
+  requests admitted from host threads (mesh arrays and state copied to the
+  device), started as they land, every state and the lift/drag forces read
+  back as each solve retires, all inside the timed region.
 * latency: p50/p95/p99 of the per-solve device time from start to retirement.
 * plain_fp64: the same requests solved one at a time by the FP64 drop-in
-  (bit-identical to the reference): the recorded FP64 step count of each
-  request x its measured FP64 ms/step.
+  (bit-identical to the reference), modelled: the recorded FP64 step count
+  of each request x its measured FP64 ms/step; two requests are also solved
+  to convergence in the run and the model's error on them is printed.
 * roofline: k_node_prepare4 (the largest kernel of a step) on the batch's
   largest mesh, compulsory bytes over its measured duration against the
   measured HBM copy bandwidth.
@@ -62,6 +66,7 @@ for p in (ROOT, PKG):
 METRIC = "converged solves/s (1e-10 drop) served vs plain FP64 GPU; p50/p99 latency"
 UNIT = "solves/s"
 REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
+BENCH_BUDGET_S = 1500.      # wall-clock target of a whole batch run (warm-up and checks included)
 REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
 STAGE_THREADS = max(1, min(8, os.cpu_count() or 1))  # concurrent admissions per batch pass
 CPU_BASELINE_STEPS = 6      # pseudo-time steps timed for cpu_baseline
@@ -332,6 +337,7 @@ def run_batch(args, bw):
     import torch
     from flowgpu import capi, roofline, serve
 
+    t_run0 = time.time()
     world, rank, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     reqs = [serve.sample_request(rank * bw.n + i, seed=bw.seed) for i in range(bw.n)]
@@ -436,13 +442,20 @@ def run_batch(args, bw):
         return [recs[i] for i in range(len(prep))], ev[0].elapsed_time(ev[1])
 
     first = None
+    pass_s = []
     for _ in range(args.warmup):
+        tw = time.time()
         recs, _f, _a, _b = one_pass()
+        pass_s.append(time.time() - tw)
         sig = [(r["status"], r["steps"]) for r in recs]
         if first is None:
             first = sig
         elif sig != first:
             raise RuntimeError("non-deterministic batch: step counts differ between passes")
+    # the first pass also tunes the kernel variants of every size bucket
+    t_pass = (sum(pass_s[1:]) / len(pass_s[1:])) if len(pass_s) > 1 else (pass_s[0] if pass_s
+                                                                           else 0.)
+    log(f"[rank {rank}] {bw.name}: warm-up passes {[round(x, 1) for x in pass_s]} s")
     barrier(pg)
     dev_ms = e2e_ms = 0.
     lat, launches, n_conv, n_fail, n_stall = [], 0, 0, 0, 0
@@ -468,7 +481,15 @@ def run_batch(args, bw):
             n_stall += sum(1 for r in recs if r["status"] == capi.ERR_STALLED)
         stream_ms = 0.
         refusals = []
-        for k in range(args.steps):
+        # the streamed (end-to-end) passes repeat the value passes' work from
+        # host buffers; as many as the run's time target leaves room for, at
+        # least 3 and at most K (every rank runs the same number)
+        left = BENCH_BUDGET_S - (time.time() - t_run0) - 120.
+        n_e2e = int(max(3, min(args.steps, left // max(1.1 * t_pass, 1e-3))))
+        n_e2e = int(allreduce_max(pg, n_e2e)) if pg is not None else n_e2e
+        log(f"[rank {rank}] {bw.name}: value passes done at {time.time() - t_run0:.0f} s; "
+            f"{n_e2e} streamed passes")
+        for k in range(n_e2e):
             recs, ms = stream_pass()
             if first is not None and [(r["status"], r["steps"]) for r in recs] != first:
                 raise RuntimeError("non-deterministic batch: streamed pass differs")
@@ -481,7 +502,8 @@ def run_batch(args, bw):
     evals_all = allreduce_sum(pg, evals)
     node_evals_all = allreduce_sum(pg, node_evals)
     value = n_conv_all / (dev_ms_max / 1e3)
-    e2e = n_conv_all / (stream_ms_max / 1e3)
+    # a streamed pass converges the same solves as a value pass (checked above)
+    e2e = n_conv_all / max(args.steps, 1) * n_e2e / (stream_ms_max / 1e3)
     e2e_staged = n_conv_all / (e2e_ms_max / 1e3)
 
     # ---- roofline: k_node_prepare4 on the largest mesh of the batch, served form ----
@@ -526,23 +548,42 @@ def run_batch(args, bw):
     if bw.fp64_steps is not None and rank == 0 and world == 1:
         tot = 0.
         per = []
+        n = 96
         for i, pr in enumerate(prep):
             s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params, subits=2),
                                       device=local)
             s.set_state(pr.Q0)
-            n = 96
             s.converge(1, n, 1e-300, chunk=32, check=False)
             ms_step = s.last_device_ms() / n
             s.close()
             per.append(round(ms_step, 4))
             tot += bw.fp64_steps[i] * ms_step / 1e3
         conv64 = sum(1 for st in bw.fp64_status if st == 0)
+        # the model checked on two requests solved to convergence here: the
+        # converged ones whose modelled time is largest below 6 s
+        est = {i: bw.fp64_steps[i] * per[i] / 1e3 for i in range(len(prep))
+               if bw.fp64_status[i] == 0}
+        pick = sorted((i for i in est if est[i] < 6.0), key=lambda i: -est[i])[:2]
+        checks = []
+        for i in pick:
+            pr = prep[i]
+            s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params, subits=2),
+                                      device=local)
+            s.set_state(pr.Q0)
+            steps_i, _r0, _r1 = s.converge(1, bw.max_steps, bw.drop, chunk=32, check=False)
+            real = s.last_device_ms() / 1e3
+            s.close()
+            checks.append({"request": i, "nodes": pr.req.nodes, "steps": steps_i,
+                           "recorded_steps": bw.fp64_steps[i], "modelled_s": round(est[i], 3),
+                           "measured_s": round(real, 3),
+                           "model_error": round(est[i] / real - 1.0, 4)})
         plain = {"value": round(conv64 / tot, 5), "unit": UNIT, "converged": conv64,
-                 "seconds": round(tot, 2), "ms_per_step": per,
+                 "seconds": round(tot, 2), "ms_per_step": per, "modelled": True,
                  "how": "recorded FP64 step count of each request (capped at max_steps; the "
                         "drop-in runs every solve to its drop or max_steps, as the reference's "
                         "driver does) x its FP64 drop-in ms/step measured over 96 steps (graph "
-                        "chunks), solved one after the other"}
+                        "chunks), solved one after the other",
+                 "model_checked_on": checks}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and bw.fp64_steps is not None:
@@ -553,8 +594,9 @@ def run_batch(args, bw):
             "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(dev_ms_max / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 residual / f32 Jacobian+sweeps",
+            "data": "synthetic (seeded O-grids and flow conditions of the batching form)",
             "config": {"workload": bw.name, "form": "batching (served, all admitted together)",
                        "requests_per_gpu": bw.n, "stream_seed": bw.seed,
                        "nodes": [r.nodes for r in reqs], "orders": [r.order for r in reqs],
@@ -582,6 +624,7 @@ def run_batch(args, bw):
                     "how": "requests admitted from host threads and started as their inputs "
                            "land (continuous batching), states and forces read back as they "
                            "retire; separate timed passes",
+                    "passes": n_e2e,
                     "admission_retries": len(refusals),
                     "first_refusal": refusals[0] if refusals else None},
             "e2e_staged": {"value": round(e2e_staged, 5), "unit": UNIT,
@@ -628,6 +671,7 @@ def batch_cpu_baseline(prep, bw) -> dict:
                 for i, pr in enumerate(prep))
     conv64 = sum(1 for st in bw.fp64_status if st == 0)
     return {"value": round(conv64 / total, 8), "unit": UNIT, "cores": 1, "kind": "reference",
+            "modelled": True,
             "sample": f"{CPU_BASELINE_STEPS} timed steps on each of the {len(small)} smallest "
                       f"meshes ({', '.join(str(p.req.nodes) for p in small)} nodes); "
                       f"s per node-step by order {dict((o, f'{c:.3e}') for o, c in cost.items())}"
@@ -635,19 +679,26 @@ def batch_cpu_baseline(prep, bw) -> dict:
 
 
 def measure_fp64(args, bw):
-    """Record the FP64 drop-in's step count and status on every request of
-    the batch (the reference's own, since the drop-in is bit-identical)."""
+    """Record the FP64 drop-in's step count, status and forces on every
+    request of the batch (the reference's own, since the drop-in is
+    bit-identical).  The solves run side by side in one server in precision
+    mode 0; a served solve's iterates are those it has alone."""
     import torch
     from flowgpu import capi, serve
     torch.cuda.set_device(0)
     reqs = [serve.sample_request(i, seed=bw.seed) for i in range(bw.n)]
     prep = serve.prepare_all(reqs, 2, bw.max_steps, bw.drop)
-    r = serve.run_sequential(prep, precision=0)
-    steps = tuple(x["steps"] for x in r["records"])
-    status = tuple(x["status"] for x in r["records"])
+    free, _ = torch.cuda.mem_get_info(0)
+    arena = capi.Arena(int(min(free * 0.85, 150e9)))
+    r = serve.run_batch(prep, arena, precision=0, chunk=64, max_slots=bw.n)
+    arena.close()
+    recs = r["records"]
+    steps = tuple(x["steps"] for x in recs)
+    status = tuple(x["status"] for x in recs)
+    forces = tuple(tuple(x["forces"]) if x["status"] == 0 else None for x in recs)
     print(json.dumps({"workload": bw.name, "fp64_steps": steps, "fp64_status": status,
-                      "seconds": round(r["total_s"], 2),
-                      "forces": [x["forces"] for x in r["records"]]}), flush=True)
+                      "seconds": round(r["makespan_s"], 2), "fp64_forces": forces}),
+          flush=True)
 
 
 def cpu_baseline(casedir: str, steps_conv: int) -> dict:
@@ -810,7 +861,7 @@ def run_reference_batch(args, bw):
             "config": {"workload": bw.name, "nodes": [r.nodes for r in reqs],
                        "s_per_step": [round(per_step[i], 4) for i in range(bw.n)]},
             "cpu_baseline": {"value": round(rate, 8), "unit": UNIT, "cores": cores,
-                             "kind": "reference", "sample": sample},
+                             "kind": "reference", "modelled": True, "sample": sample},
             "e2e": {"value": round(rate, 8), "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -945,6 +996,25 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+def torchrun_argv(argv, gpus: int, port: int) -> list:
+    """The command that runs this script as `gpus` ranks, one per GPU, the
+    way a multi-GPU launch does: torchrun on this node over 127.0.0.1."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+            os.path.abspath(__file__), *argv]
+
+
+def relaunch_as_ranks(argv, gpus: int) -> int:
+    """`--gpus N` (N > 1) outside torchrun: start the N ranks here instead of
+    silently running one.  Returns torchrun's exit code."""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    log(f"--gpus {gpus} without torchrun: launching {gpus} ranks")
+    return subprocess.call(torchrun_argv(argv, gpus, port))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -975,6 +1045,11 @@ def main():
                     help="one mesh (--workload): the precision form (--precision, default 3) "
                          "against the FP64 drop-in, each to a 1e-10 drop")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_as_ranks(sys.argv[1:], args.gpus))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world != args.gpus:
+        log(f"--gpus {args.gpus} but WORLD_SIZE={world}: running {world} rank(s)")
     if args.serve_rate > 0:
         run_serve(args)
         return

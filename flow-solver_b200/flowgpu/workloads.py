@@ -72,7 +72,7 @@ WORKLOADS = {
 }
 
 DEFAULT = "ogrid512x128_k2_m080"   # the single-mesh drop-in workload
-DEFAULT_BENCH = "batch16"           # bench.py's default: the batching form
+DEFAULT_BENCH = "batch64"           # bench.py's default: the batching form, 64 solves per GPU
 
 
 def get(name: str) -> Workload:
@@ -120,6 +120,11 @@ class BatchWorkload:
 
 
 BATCHES = {
+    # the batching form as specified: 64 independent solves in one arena
+    # (requests 0..63 of stream 0 on rank 0, the next 64 on rank 1, ...)
+    "batch64": BatchWorkload("batch64", 0, 64, 8000, 1e-10, 3, 4, stall=2000, autotune=4,
+                             priority_policy=1),
+    # its first 16 requests: a quarter of the work, for quick runs
     "batch16": BatchWorkload(
         "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=2000, autotune=4, priority_policy=1,
         fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065,

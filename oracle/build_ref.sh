@@ -6,10 +6,14 @@
 #     LAPACK dgesvd_ (neither library is part of the reference tree),
 #   - ref_harness.cpp: C entry points replacing main.C's driver loop.
 # Output: oracle/_ref/libflowref.so (git-ignored; travels with the tree).
-# Usage: sh oracle/build_ref.sh [reference_dir]
+# Usage: sh oracle/build_ref.sh reference_dir   (or FLOW_REFERENCE_DIR=... sh oracle/build_ref.sh)
 set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-/root/reference}
+REF=${1:-$FLOW_REFERENCE_DIR}
+if [ -z "$REF" ]; then
+  echo "build_ref.sh: give the reference directory as the argument or in FLOW_REFERENCE_DIR" >&2
+  exit 1
+fi
 OUT="$HERE/_ref"
 HOST="$HERE/../flow-solver_b200/csrc/host"
 if [ ! -f "$REF/solve.C" ]; then

@@ -65,3 +65,27 @@ def test_reference_arm_other_ranks_exit_without_work(monkeypatch, capsys):
         gpus, steps, warmup = 2, 1, 1
     bench.run_reference_batch(A(), workloads.BATCHES["batch16"])
     assert capsys.readouterr().out == ""
+
+
+def test_gpus_without_torchrun_relaunches_as_ranks(monkeypatch):
+    """bench.py --gpus N outside torchrun starts N ranks (torchrun on this
+    node over 127.0.0.1) instead of silently running one."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "flow-solver_b200")]
+    import bench
+    argv = bench.torchrun_argv(["--gpus", "4", "--steps", "2"], 4, 29512)
+    assert argv[1:4] == ["-m", "torch.distributed.run", "--nnodes=1"]
+    assert "--nproc-per-node=4" in argv and "--master-addr=127.0.0.1" in argv
+    assert "--master-port=29512" in argv
+    assert argv[-4:] == ["--gpus", "4", "--steps", "2"]
+    assert argv[-5].endswith("bench.py")
+    calls = []
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    monkeypatch.setattr(bench.subprocess, "call", lambda cmd: calls.append(cmd) or 0)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "2"])
+    import pytest as _pt
+    with _pt.raises(SystemExit) as ex:
+        bench.main()
+    assert ex.value.code == 0 and len(calls) == 1
+    assert "--nproc-per-node=2" in calls[0]
