@@ -149,10 +149,12 @@ __device__ __forceinline__ double roe_weight(double rhoL, double rhoR) {
 }
 
 // ogm1 = 1 / (gamma - 1), a per-run constant of the eigenvector matrix.
+// Rm (may be null): the dissipation matrix |A~| = T |Lambda| T^-1 the flux
+// formed on the way, row-major, the bits roe_matrix gives for ql, qr.
 __device__ __forceinline__ void roe_core(double nx, double ny, double len, double gamma,
                                          double ogm1, const double* ql, const double* qr,
                                          const RoeSide& L, const RoeSide& R, double bg,
-                                         double* flux) {
+                                         double* flux, double* Rm = nullptr) {
   const double ubar = L.u + bg * (R.u - L.u);
   const double vbar = L.v + bg * (R.v - L.v);
   const double hbar = L.h + bg * (R.h - L.h);
@@ -209,11 +211,38 @@ __device__ __forceinline__ void roe_core(double nx, double ny, double len, doubl
       double rm = 0.;
 #pragma unroll
       for (int k = 0; k < 4; k++) rm += T[i * 4 + k] * (lam[k] * Ti[k * 4 + j]);
+      if (Rm) Rm[i * 4 + j] = rm;
       sd += rm * dq[j];
     }
     const double diss = sd * len;
     flux[i] = 0.5 * (L.F[i] + R.F[i] - diss);
   }
+}
+
+// jacobian.C:764-866: the physical flux's Jacobian A(q) = dF/dq of one
+// state for a unit normal (no length), row-major (row = flux component).
+__device__ __forceinline__ void euler_jacobian(const double* q, double nx, double ny,
+                                               double gamma, double* d) {
+  const double rhoL = q[0], uL = q[1] / q[0], vL = q[2] / q[0], EL = q[3];
+  const double th = uL * nx + vL * ny;
+  const double ph = 0.5 * (gamma - 1.) * (uL * uL + vL * vL);
+  d[0] = 0.;
+  d[1] = nx;
+  d[2] = ny;
+  d[3] = 0.;
+  d[4] = ph * nx - uL * th;
+  d[5] = (2. - gamma) * uL * nx + th;
+  d[6] = uL * ny - (gamma - 1.) * vL * nx;
+  d[7] = (gamma - 1.) * nx;
+  d[8] = ph * ny - vL * th;
+  d[9] = vL * nx - (gamma - 1.) * uL * ny;
+  d[10] = th + (2. - gamma) * vL * ny;
+  d[11] = (gamma - 1.) * ny;
+  const double ger = gamma * EL / rhoL;
+  d[12] = (2. * ph - ger) * th;
+  d[13] = (1. - gamma) * uL * th + nx * (ger - ph);
+  d[14] = (1. - gamma) * vL * th + ny * (ger - ph);
+  d[15] = gamma * th;
 }
 
 // cv_calc.C:840-866: max(|theta+c|, |theta-c|) for one node state.
@@ -230,15 +259,30 @@ __device__ __forceinline__ double max_wave(const double* q, double nx, double ny
 
 // limiter.C:672-700: one reconstructed value's Venkatakrishnan bound
 // (phi(y) = (y^2+2y)/(y^2+y+2), no epsilon), folded into phi with MIN().
+//
+// phi starts at 1 and only falls, so a point whose computed bound is at
+// least 1 leaves it unchanged.  For y in [2.001, 1e14] the computed bound is
+// at least 1: numerator - denominator is y - 2 in exact arithmetic, and the
+// three roundings on either side (each at most 2^-53 of t^2+2t+2) stay far
+// below it; a quotient of a numerator above its denominator rounds to 1 or
+// more.  Such points are recognised from two products instead of the two
+// divisions: a >= 2.002 d and a <= 0.9e14 d (signs folded for d < 0) put
+// fl(a/d) inside that range even after the products' and the quotient's own
+// roundings, for any normal d.  Every other point, a NaN phi or a NaN
+// operand takes the reference's expressions, so phi is the same bits.
 __device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0, double qmin,
                                               double qmax) {
   double d = qrec - q0;
   if (d > 0.) {
-    double t = (qmax - q0) / (qrec - q0);
+    const double a = qmax - q0;
+    if (ph == ph && d >= 1e-290 && a >= 2.002 * d && a <= 0.9e14 * d) return ph;
+    double t = a / (qrec - q0);
     t = (t * t + 2. * t) / (t * t + t + 2.);
     return ph <= t ? ph : t;
   } else if (d < 0.) {
-    double t = (qmin - q0) / (qrec - q0);
+    const double a = qmin - q0;
+    if (ph == ph && d <= -1e-290 && a <= 2.002 * d && a >= 0.9e14 * d) return ph;
+    double t = a / (qrec - q0);
     t = (t * t + 2. * t) / (t * t + t + 2.);
     return ph <= t ? ph : t;
   }

@@ -221,6 +221,7 @@ struct flow_ctx {
   // (flow_set_capture_fault), capture_fallbacks counts the eager chunks
   int capture_fault = 0;
   long capture_fallbacks = 0;
+  int jac_mode = 0;  // face Jacobians of the precision form (flow_set_jacobian)
 };
 
 namespace {
@@ -404,14 +405,18 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   {
     Timed t(c, 1);
     int nbs = grid_blocks(c->ns, 128);
+    // the approximate Roe Jacobian only in the precision form
+    const bool approx = jac && c->jac_mode == 1 && c->precision != 0;
     if (a.recon == 1) {
       launch_flux_variant(c->var[1], [&](auto V) {
-        if (jac) k_subedge_flux<1, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        if (approx) k_subedge_flux<1, true, V.value, 1><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        else if (jac) k_subedge_flux<1, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
         else k_subedge_flux<1, false, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
       });
     } else {
       launch_flux_variant(c->var[1], [&](auto V) {
-        if (jac) k_subedge_flux<0, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        if (approx) k_subedge_flux<0, true, V.value, 1><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
+        else if (jac) k_subedge_flux<0, true, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
         else k_subedge_flux<0, false, V.value><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
       });
     }
@@ -850,6 +855,9 @@ bool preload_kernels() {
         (const void*)k_subedge_flux<1, true, 3>, (const void*)k_subedge_flux<1, true, 4>,
         (const void*)k_subedge_flux<1, true, 5>, (const void*)k_subedge_flux<1, false, 3>,
         (const void*)k_subedge_flux<1, false, 4>, (const void*)k_subedge_flux<1, false, 5>,
+        (const void*)k_subedge_flux<0, true, 3, 1>, (const void*)k_subedge_flux<0, true, 4, 1>,
+        (const void*)k_subedge_flux<0, true, 5, 1>, (const void*)k_subedge_flux<1, true, 3, 1>,
+        (const void*)k_subedge_flux<1, true, 4, 1>, (const void*)k_subedge_flux<1, true, 5, 1>,
         (const void*)k_boundary<true>, (const void*)k_boundary<false>,
         (const void*)k_diag_only, (const void*)k_sweep_ordered<true>,
         (const void*)k_sweep_ordered<false>, (const void*)k_sweep_color32<true>,
@@ -1666,6 +1674,18 @@ int flow_set_graphs(flow_ctx* c, int on) {
   cudaStreamSynchronize(c->stream);
   if (!on) drop_graphs(c);
   c->use_graphs = on ? 1 : 0;
+  return 0;
+}
+
+int flow_set_jacobian(flow_ctx* c, int mode) {
+  if (!c || !c->ok || mode < 0 || mode > 1) {
+    set_error("flow_set_jacobian: null context or mode not 0..1");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  c->jac_mode = mode;
   return 0;
 }
 

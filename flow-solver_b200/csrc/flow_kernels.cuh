@@ -454,7 +454,11 @@ __global__ void __launch_bounds__(128) k_diag_lu(DevMesh m, DevState s) {
 // ---------------------------------------------------------------------------
 // Per subedge: face states, Roe flux, forward-difference Jacobian
 // (residual.C:112-333, reconstruct.C:181-203, jacobian.C:45-110).
-template <int RECON, bool JAC, int MINB>
+// JMODE 0: the reference's forward differences.  JMODE 1 (precision form
+// only): the approximate Roe Jacobian dF/dqL = (A(qL) + |A~|) len / 2,
+// dF/dqR = (A(qR) - |A~|) len / 2 (|A~| frozen: the form jacobian.C:681-962
+// gives the boundary faces), from the |A~| the flux formed anyway.
+template <int RECON, bool JAC, int MINB, int JMODE = 0>
 __global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
   int sub = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -485,6 +489,27 @@ __global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState 
   roe_side(qR, g.x, g.y, g.z, a.gamma, SR);
   const double bg = roe_weight(SL.rho, SR.rho);
   double flux[4];
+  if (JAC && JMODE == 1) {
+    double Rm[16], dL[16], dR[16];
+    roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qR, SL, SR, bg, flux, Rm);
+    reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
+    euler_jacobian(qL, g.x, g.y, a.gamma, dL);
+    euler_jacobian(qR, g.x, g.y, a.gamma, dR);
+    double4* JLo = reinterpret_cast<double4*>(s.JL + 16 * (long)sub);
+    double4* JRo = reinterpret_cast<double4*>(s.JR + 16 * (long)sub);
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      double o[4], p[4];
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        o[c] = 0.5 * (dL[4 * r + c] + Rm[4 * r + c]) * g.z;
+        p[c] = 0.5 * (dR[4 * r + c] - Rm[4 * r + c]) * g.z;
+      }
+      JLo[r] = make_double4(o[0], o[1], o[2], o[3]);
+      JRo[r] = make_double4(p[0], p[1], p[2], p[3]);
+    }
+    return;
+  }
   roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qR, SL, SR, bg, flux);
   reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
   if (!JAC) return;
@@ -614,27 +639,8 @@ __global__ void __launch_bounds__(128) k_boundary(DevMesh m, DevState s, StepArg
   if (!JAC) return;
   double Rm[16];
   roe_matrix(nx, ny, gamma, qL, qg, Rm);
-  double rhoL = qL[0], uL = qL[1] / qL[0], vL = qL[2] / qL[0], EL = qL[3];
-  double th = uL * nx + vL * ny;
-  double ph = 0.5 * (gamma - 1.) * (uL * uL + vL * vL);
   double d[16];
-  d[0] = 0.;
-  d[1] = nx;
-  d[2] = ny;
-  d[3] = 0.;
-  d[4] = ph * nx - uL * th;
-  d[5] = (2. - gamma) * uL * nx + th;
-  d[6] = uL * ny - (gamma - 1.) * vL * nx;
-  d[7] = (gamma - 1.) * nx;
-  d[8] = ph * ny - vL * th;
-  d[9] = vL * nx - (gamma - 1.) * uL * ny;
-  d[10] = th + (2. - gamma) * vL * ny;
-  d[11] = (gamma - 1.) * ny;
-  double ger = gamma * EL / rhoL;
-  d[12] = (2. * ph - ger) * th;
-  d[13] = (1. - gamma) * uL * th + nx * (ger - ph);
-  d[14] = (1. - gamma) * vL * th + ny * (ger - ph);
-  d[15] = gamma * th;
+  euler_jacobian(qL, nx, ny, gamma, d);
   double* Jo = s.Jb + 16 * (long)b;
 #pragma unroll
   for (int k = 0; k < 16; k++) Jo[k] = 0.5 * (d[k] + Rm[k]) * len;

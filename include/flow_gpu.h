@@ -298,6 +298,16 @@ int flow_set_sweep_mode(flow_ctx *ctx, int mode);
  * most 8 off-diagonal blocks per row and a matrix bandwidth whose chunk
  * windows fit in shared memory; otherwise switching to it fails. */
 int flow_set_precision(flow_ctx *ctx, int mode);
+/* Face Jacobians of the precision form (no reference counterpart): mode 0
+ * (default) the reference's forward differences (jacobian.C:45-185, eight
+ * extra Roe fluxes per face); mode 1 the approximate Roe Jacobian
+ * dF/dqL = (A(qL) + |A~|) len / 2, dF/dqR = (A(qR) - |A~|) len / 2 with the
+ * dissipation matrix |A~| frozen (the form the reference gives its boundary
+ * faces, jacobian.C:681-962), which costs no extra flux.  The residual is
+ * unchanged, so the converged state is too; only the preconditioner
+ * differs.  Used in precision modes 1-3 only: the FP64 drop-in (mode 0)
+ * always differences, as the reference does. */
+int flow_set_jacobian(flow_ctx *ctx, int mode);
 /* Sweep schedule (no reference counterpart): steps up to `until_step` (0:
  * the end of the CFL ramp, p->ramp) run `sweeps` Gauss-Seidel sweeps instead
  * of p->subits; sweeps = 0 turns the schedule off (default).  Fewer sweeps

@@ -477,6 +477,56 @@ static void numerical_jacobian(orc_grid *g, const orc_params *p, int L, int R,
     if (g->ja[i] == L) add_block(&g->LHS[(long)i * 16], dL, -1.0);
 }
 
+/* The flux Jacobian A(q) of one state for a unit normal (jacobian.C:764-866,
+ * the terms boundary_jacobian uses), row-major. */
+static void euler_jacobian(const double *Q, double nx, double ny, double gamma, double (*d)[4])
+{
+  double rhoL = Q[0], uL = Q[1] / Q[0], vL = Q[2] / Q[0], EL = Q[3];
+  double theta = uL * nx + vL * ny;
+  double phi = 0.5 * (gamma - 1.) * (uL * uL + vL * vL);
+  d[0][0] = 0.;
+  d[0][1] = nx;
+  d[0][2] = ny;
+  d[0][3] = 0.;
+  d[1][0] = phi * nx - uL * theta;
+  d[1][1] = (2. - gamma) * uL * nx + theta;
+  d[1][2] = uL * ny - (gamma - 1.) * vL * nx;
+  d[1][3] = (gamma - 1.) * nx;
+  d[2][0] = phi * ny - vL * theta;
+  d[2][1] = vL * nx - (gamma - 1.) * uL * ny;
+  d[2][2] = theta + (2. - gamma) * vL * ny;
+  d[2][3] = (gamma - 1.) * ny;
+  d[3][0] = (2. * phi - gamma * EL / rhoL) * theta;
+  d[3][1] = (1. - gamma) * uL * theta + nx * (gamma * EL / rhoL - phi);
+  d[3][2] = (1. - gamma) * vL * theta + ny * (gamma * EL / rhoL - phi);
+  d[3][3] = gamma * theta;
+}
+
+/* Precision form, jac_approx: dF/dqL = (A(qL) + |A~|) len/2 and
+ * dF/dqR = (A(qR) - |A~|) len/2, |A~| the Roe dissipation matrix of the face
+ * (no reference counterpart; the reference's boundary faces use this form,
+ * jacobian.C:681-962), accumulated like numerical_jacobian's blocks. */
+static void approximate_jacobian(orc_grid *g, const orc_params *p, int L, int R,
+                                 const double *QL, const double *QR, double nx, double ny,
+                                 double len)
+{
+  double Rm[16], dL[4][4], dR[4][4];
+  roe_matrix(nx, ny, p->gamma, QL, QR, Rm);
+  euler_jacobian(QL, nx, ny, p->gamma, dL);
+  euler_jacobian(QR, nx, ny, p->gamma, dR);
+  for (int i = 0; i < 4; i++)
+    for (int k = 0; k < 4; k++) {
+      dL[i][k] = 0.5 * (dL[i][k] + Rm[i * 4 + k]) * len;
+      dR[i][k] = 0.5 * (dR[i][k] - Rm[i * 4 + k]) * len;
+    }
+  add_block(&g->LHS[(long)g->iau[L] * 16], dL, 1.0);
+  add_block(&g->LHS[(long)g->iau[R] * 16], dR, -1.0);
+  for (int i = g->ia[L]; i < g->ia[L + 1]; i++)
+    if (g->ja[i] == R) add_block(&g->LHS[(long)i * 16], dR, 1.0);
+  for (int i = g->ia[R]; i < g->ia[R + 1]; i++)
+    if (g->ja[i] == L) add_block(&g->LHS[(long)i * 16], dL, -1.0);
+}
+
 void orc_interior_residuals(orc_grid *g, const orc_params *p, int jupdate, int ts)
 {
   int nn = g->nn;
@@ -498,7 +548,8 @@ void orc_interior_residuals(orc_grid *g, const orc_params *p, int jupdate, int t
       reconstruct_face(g, p, s, L, R, ts, qL, qR, 1);
       orc_roe_flux(nx, ny, len, p->gamma, qL, qR, flux);
     }
-    if (jupdate) numerical_jacobian(g, p, L, R, qL, qR, flux, nx, ny, len);
+    if (jupdate && p->jac_approx) approximate_jacobian(g, p, L, R, qL, qR, nx, ny, len);
+    else if (jupdate) numerical_jacobian(g, p, L, R, qL, qR, flux, nx, ny, len);
     for (int k = 0; k < NV; k++) {
       g->R[L * NV + k] += flux[k];
       g->R[R * NV + k] -= flux[k];

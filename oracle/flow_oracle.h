@@ -26,6 +26,9 @@ typedef struct {
   int iter, jufreq, ramp, subits, unsteady, tacc, method, order;
   int foits, soits, toits, limit;
   double CFL, gamma, alpha, mach, mintime;
+  /* precision form only (no reference counterpart): 1 = interior face
+   * Jacobians by the approximate Roe form instead of forward differences */
+  int jac_approx;
 } orc_params;
 
 typedef struct {

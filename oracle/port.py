@@ -24,7 +24,8 @@ LP = C.POINTER(C.c_long)
 class OrcParams(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("iter", "jufreq", "ramp", "subits", "unsteady", "tacc",
                                        "method", "order", "foits", "soits", "toits", "limit")] + \
-               [(n, C.c_double) for n in ("CFL", "gamma", "alpha", "mach", "mintime")]
+               [(n, C.c_double) for n in ("CFL", "gamma", "alpha", "mach", "mintime")] + \
+               [("jac_approx", C.c_int)]
 
 
 _GRID_INTS = ("nn", "nn_ghost", "nedges", "nsubedges", "nbedges", "nb")

@@ -138,3 +138,61 @@ def test_sweep_schedule_bitwise():
         assert ndiff(og["Q"][4:], gpu.get("Q")[4:]) == 0, ts
         assert ndiff(og["dQ"][4:4 * (nn + 1)], gpu.get("dQ")[4:]) == 0, ts
     gpu.close()
+
+
+@pytest.mark.parametrize("nc,nr,curved,order,subits,steps,mode", [
+    (32, 8, True, 3, 4, 6, 1),
+    (64, 16, False, 1, 3, 5, 1),
+    (32, 8, True, 3, 4, 6, 3),
+    (128, 32, True, 3, 4, 4, 3),
+    (64, 16, False, 1, 3, 5, 3),
+])
+def test_approximate_jacobian_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
+    """flow_set_jacobian(ctx, 1): the interior face Jacobians by the
+    approximate Roe form, against the oracle's restatement step by step (the
+    residual is the FP64 one; only the FP32 blocks differ from mode 0's)."""
+    mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits, mode)
+    gpu.set_jacobian(1)
+    p.jac_approx = 1
+    nn = mesh.sizes["nn"]
+    perm = None
+    if mode == 3:
+        starts, _ = gpu.chunk_starts()
+        perm, _ = chunk_order(og["ia"], og["ja"], starts)
+    for ts in range(1, steps + 1):
+        if mode == 3:
+            og.solve_mixed_order(p, ts, perm)
+        else:
+            og.solve_mixed(p, ts)
+        gpu.solve(ts)
+        for name in ("Q", "nQ"):
+            assert ndiff(og[name][4:], gpu.get(name)[4:]) == 0, (name, ts)
+        for name in ("R", "dQ"):
+            assert ndiff(og[name][4:4 * (nn + 1)], gpu.get(name)[4:]) == 0, (name, ts)
+    assert gpu.status() == 0
+    gpu.close()
+
+
+@pytest.mark.parametrize("order", [1, 3])
+def test_approximate_jacobian_converges_to_the_fp64_answer(order):
+    """The approximate Jacobian changes the preconditioner, not the residual:
+    the converged forces are the FP64 drop-in's within 1e-8."""
+    from flowgpu import capi, workloads
+    from flowgpu.prep import Mesh
+    wl = workloads.Workload(f"approxconv{order}", 64, 16, order == 3, order,
+                            0.8 if order == 3 else 0.5, subits=4, limit=2 if order == 3 else 0)
+    mesh = Mesh.from_case(wl.write(), order=order)
+    fp = wl.params()
+    out = {}
+    for mode, jac in ((0, 0), (3, 1)):
+        s = capi.Solver.from_mesh(mesh, fp, device=0)
+        s.set_precision(mode)
+        s.set_jacobian(jac)
+        s.set_state(mesh.initial_state(fp))
+        steps, r0, r1 = s.converge(1, 20000, 1e-10)
+        assert r1 < 1e-10 * r0
+        out[mode] = (steps, s.body_forces())
+        s.close()
+    (n0, f0), (n1, f1) = out[0], out[3]
+    assert abs(f1[0] - f0[0]) <= 1e-8 * max(1.0, abs(f0[0]))
+    assert abs(f1[1] - f0[1]) <= 1e-8 * max(1.0, abs(f0[1]))
