@@ -222,6 +222,10 @@ struct flow_ctx {
   int capture_fault = 0;
   long capture_fallbacks = 0;
   int jac_mode = 0;  // face Jacobians of the precision form (flow_set_jacobian)
+  // staged node kernel (node_prepare variant 3): largest per-tile slices and
+  // whether its shared memory fits, per order of the kernel
+  StageCaps stage_caps{};
+  bool stage_ok[2] = {false, false};  // [0] the k=1 kernel, [1] the k=2 kernel
 };
 
 namespace {
@@ -367,6 +371,10 @@ void harvest(flow_ctx* c) {
 // k_node_prepare4: variant 0, 1, 2 -> 0 (compiler's choice), 10, 12 blocks.
 // k_subedge_flux:  variant 0, 1, 2 -> 4, 5, 3 blocks.
 constexpr int kVariants = 3;
+// k_node_prepare4 has a fourth: variant 3 = k_node_stage (gathers staged in
+// shared memory), where its shared memory fits the mesh.
+constexpr int kNodeVariants = 4;
+constexpr size_t kStageSmemMax = 110 * 1024;  // two CTAs per SM at most
 template <class F>
 void launch_variant(int v, F&& f) {
   if (v == 1) f(std::integral_constant<int, 10>());
@@ -389,7 +397,18 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   int nb = grid_blocks(4 * c->nn, 128);
   // the LSQ gradient (k=1, or the second-order start-up steps of k=2) is
   // the k=1 kernel's work
-  if (c->order == 1 || a.do_grad)
+  const bool k1 = c->order == 1 || a.do_grad;
+  if (c->var[0] == 3 && c->stage_ok[k1 ? 0 : 1]) {
+    const int tiles = grid_blocks(c->nn, kStageNodes);
+    if (k1)
+      k_node_stage<1><<<tiles, 128, stage_smem_bytes(1, c->stage_caps), c->stream>>>(
+          c->m, c->s, a, c->stage_caps);
+    else
+      k_node_stage<3><<<tiles, 128, stage_smem_bytes(3, c->stage_caps), c->stream>>>(
+          c->m, c->s, a, c->stage_caps);
+    return launch_check(c);
+  }
+  if (k1)
     launch_variant(c->var[0], [&](auto V) {
       k_node_prepare4<1, V.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
     });
@@ -848,6 +867,7 @@ bool preload_kernels() {
         (const void*)k_assemble4<true, 1>, (const void*)k_assemble4<false, 1>,
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
         (const void*)k_boundary_add4<true>, (const void*)k_boundary_add4<false>,
+        (const void*)k_node_stage<1>, (const void*)k_node_stage<3>,
         (const void*)k_diag_lu,
         (const void*)k_subedge_flux<0, true, 3>, (const void*)k_subedge_flux<0, true, 4>,
         (const void*)k_subedge_flux<0, true, 5>, (const void*)k_subedge_flux<0, false, 3>,
@@ -888,6 +908,9 @@ bool ensure_kernel_attrs(int device) {
                         (const void*)k_sweep_chunk<0, 16>, (const void*)k_sweep_chunk<1, 16>})
     ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     chunk_cap) == cudaSuccess;
+  for (const void* f : {(const void*)k_node_stage<1>, (const void*)k_node_stage<3>})
+    ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kStageSmemMax) == cudaSuccess;
   for (const void* f : {(const void*)k_sweep_cta<true>, (const void*)k_sweep_cta<false>})
     ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, cta) ==
                    cudaSuccess;
@@ -1285,6 +1308,11 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
     items.push_back({R, (e << 1) | 1});
   }
   nedg.build(nn, items);
+  std::vector<int> nedg_nbr(nedg.idx.size());
+  for (size_t k = 0; k < nedg.idx.size(); k++) {
+    const int e = nedg.idx[k] >> 1, side = nedg.idx[k] & 1;
+    nedg_nbr[k] = side ? edge_lr[e].x : edge_lr[e].y;
+  }
   // subedges of each edge, ascending
   std::vector<int2> edge_sub(ne + 1, make_int2(-1, -1));
   for (int s = 1; s <= ns; s++) {
@@ -1354,6 +1382,20 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
     st_ptr[nn + 1] = (int)st_idx.size();
   }
 
+  // ---- staged node kernel: the largest slice of each list any tile holds ----
+  {
+    StageCaps cap{0, 0, 0};
+    for (int n0 = 1; n0 <= nn; n0 += kStageNodes) {
+      const int n1 = std::min(n0 + kStageNodes, nn + 1);
+      cap.sub = std::max(cap.sub, nsub.ptr[n1] - nsub.ptr[n0]);
+      cap.edg = std::max(cap.edg, nedg.ptr[n1] - nedg.ptr[n0]);
+      if (c->has_stencils) cap.sten = std::max(cap.sten, st_ptr[n1] - st_ptr[n0]);
+    }
+    c->stage_caps = cap;
+    c->stage_ok[0] = stage_smem_bytes(1, cap) <= kStageSmemMax;
+    c->stage_ok[1] = c->has_stencils && stage_smem_bytes(3, cap) <= kStageSmemMax;
+  }
+
   // ---- device mesh ----
   DevMesh& m = c->m;
   m.nn = nn; m.ng = ng; m.ne = ne; m.ns = ns; m.nbe = nbe; m.nnz = nnz; m.order = p->order;
@@ -1362,7 +1404,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
 #define UP(field, vec) do { auto* d = upload_vec(c, vec); okk = okk && d; m.field = d; } while (0)
   UP(nsub_ptr, nsub.ptr); UP(nsub, nsub.idx);
   UP(nbed_ptr, nbed.ptr); UP(nbed, nbed.idx);
-  UP(nedg_ptr, nedg.ptr); UP(nedg, nedg.idx);
+  UP(nedg_ptr, nedg.ptr); UP(nedg, nedg.idx); UP(nedg_nbr, nedg_nbr);
   UP(sub_lr, sub_lr); UP(sub_geo, sub_geo); UP(sub_dx, sub_dx);
   UP(edge_lr, edge_lr); UP(edge_w, edge_w);
   UP(csr_sub, csr_sub);
@@ -2194,9 +2236,13 @@ int flow_restore_state(flow_ctx* c) {
 }
 
 int flow_set_variants(flow_ctx* c, int node_prepare, int flux) {
-  if (!c || !c->ok || node_prepare < 0 || node_prepare >= kVariants || flux < 0 ||
+  if (!c || !c->ok || node_prepare < 0 || node_prepare >= kNodeVariants || flux < 0 ||
       flux >= kVariants) {
-    set_error("flow_set_variants: null context or variant outside 0..2");
+    set_error("flow_set_variants: null context, node variant outside 0..3 or flux outside 0..2");
+    return FLOW_ERR_ARG;
+  }
+  if (node_prepare == 3 && !c->stage_ok[0] && !c->stage_ok[1]) {
+    set_error("flow_set_variants: the staged node kernel's shared memory does not fit this mesh");
     return FLOW_ERR_ARG;
   }
   if (c->var[0] != node_prepare || c->var[1] != flux) {
@@ -2226,7 +2272,12 @@ int flow_autotune(flow_ctx* c, const flow_params* p, int ts, int steps, int* var
   for (int k = 0; k < 2 && !rc; k++) {  // class 0: k_node_prepare4, class 1: k_subedge_flux
     int best = c->var[k];
     double best_ms = 1e30;
-    for (int v = 0; v < kVariants && !rc; v++) {
+    const int nv = k == 0 ? kNodeVariants : kVariants;
+    for (int v = 0; v < nv && !rc; v++) {
+      if (k == 0 && v == 3 && !c->stage_ok[0] && !c->stage_ok[1]) {
+        if (ms) ms[v] = 1e30;  // the staged kernel does not fit this mesh
+        continue;
+      }
       c->var[k] = v;
       rc |= flow_restore_state(c);
       reset_run(c, 0.);
@@ -2241,7 +2292,7 @@ int flow_autotune(flow_ctx* c, const flow_params* p, int ts, int steps, int* var
       if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc |= FLOW_ERR_CUDA;
       harvest(c);
       const double t = c->kcount[k] ? c->kms[k] / c->kcount[k] : 1e30;
-      if (ms) ms[k * kVariants + v] = t;
+      if (ms) ms[(k == 0 ? 0 : kNodeVariants) + v] = t;
       if (t < best_ms) {
         best_ms = t;
         best = v;

@@ -96,6 +96,22 @@ __global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
   }
 }
 
+// 16-byte asynchronous global -> shared copies (no register staging, many in
+// flight per thread) and their completion.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Per node: cv_calc_eigenvalue_contribution (cv_calc.C:819-953) and the dt /
 // V/dt of build_matrix (init_memory.C:200-290); then the LSQ gradient
@@ -240,6 +256,235 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
     }
   }
   // min over the variables in order 0..3 (limiter.C:895-906)
+  const double p1 = __shfl_sync(qmask, ph, qbase + 1);
+  const double p2 = __shfl_sync(qmask, ph, qbase + 2);
+  const double p3 = __shfl_sync(qmask, ph, qbase + 3);
+  double pmin = ph;
+  pmin = pmin <= p1 ? pmin : p1;
+  pmin = pmin <= p2 ? pmin : p2;
+  pmin = pmin <= p3 ? pmin : p3;
+  const double out = v == 0 ? pmin : ph;
+  reinterpret_cast<double2*>(s.phi + 8 * (long)n)[v] = make_double2(out, out);
+  if (out < 0.0 || out > 1.0) atomicOr(s.status, ERR_LIMITER);
+}
+
+// ---------------------------------------------------------------------------
+// k_node_prepare4 with its gathers staged in shared memory: the same per-lane
+// arithmetic in the same order (so the same bits), but a CTA of kStageNodes
+// consecutive nodes first copies its slices of the incidence lists and the
+// stencil (contiguous, coalesced), then issues every face-record and
+// neighbour-state gather at once as 16-byte cp.async copies, so the chains
+// incidence -> face record -> neighbour state cost one round trip each for
+// the whole tile instead of one per loop iteration.  StageCaps holds the
+// largest slice any tile has (host-computed), which sizes the shared memory.
+constexpr int kStageNodes = 32;
+
+struct StageCaps {
+  int sub;   // subedge incidences of a tile
+  int edg;   // edge incidences of a tile
+  int sten;  // k=2 stencil rows of a tile
+};
+
+__host__ __device__ inline size_t stage_smem_bytes(int order, StageCaps c) {
+  const size_t face = order == 3 ? 32 + 48 : 32 + 32;  // geometry + Gauss points or offsets
+  const size_t edge = order == 1 ? 64 : 32;            // neighbour state (+ LSQ weights)
+  return face * c.sub + edge * c.edg + 32 * (size_t)c.sten +
+         4 * ((size_t)c.sub + 2 * (size_t)c.edg + (size_t)c.sten);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_node_stage(DevMesh m, DevState s, StepArgs a,
+                                                    StageCaps cap) {
+  if (*s.stop) return;  // the run has converged
+  extern __shared__ __align__(16) unsigned char sm[];
+  double4* s_geo = reinterpret_cast<double4*>(sm);
+  char* p = reinterpret_cast<char*>(s_geo + cap.sub);
+  double2* s_xg = reinterpret_cast<double2*>(p);  // k=2: 3 Gauss points per incidence
+  double4* s_dx = reinterpret_cast<double4*>(p);  // k=1: face-point offsets
+  p += (size_t)cap.sub * (ORDER == 3 ? 48 : 32);
+  double4* s_nqe = reinterpret_cast<double4*>(p);  // edge neighbours' states
+  double4* s_ew = s_nqe + cap.edg;                 // k=1: LSQ weights
+  p += (size_t)cap.edg * (ORDER == 1 ? 64 : 32);
+  double4* s_nqs = reinterpret_cast<double4*>(p);  // k=2: stencil neighbours' states
+  int* s_sub = reinterpret_cast<int*>(s_nqs + cap.sten);
+  int* s_edg = s_sub + cap.sub;
+  int* s_nbr = s_edg + cap.edg;
+  int* s_st = s_nbr + cap.edg;
+
+  const int n0 = blockIdx.x * kStageNodes + 1;
+  const int nlast = min(n0 + kStageNodes - 1, m.nn);
+  const int K0 = m.nsub_ptr[n0], K1 = m.nsub_ptr[nlast + 1];
+  const bool rest = a.do_grad || a.do_derivs || a.do_lim;
+  const int E0 = m.nedg_ptr[n0], E1 = rest ? m.nedg_ptr[nlast + 1] : E0;
+  const bool derivs = ORDER == 3 && a.do_derivs;
+  const int R0 = derivs ? m.st_ptr[n0] : 0, R1 = derivs ? m.st_ptr[nlast + 1] : 0;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  // the tile's slices of the lists (contiguous)
+  for (int k = tid; k < K1 - K0; k += nt) s_sub[k] = m.nsub[K0 + k];
+  for (int k = tid; k < E1 - E0; k += nt) {
+    s_edg[k] = m.nedg[E0 + k];
+    s_nbr[k] = m.nedg_nbr[E0 + k];
+  }
+  for (int k = tid; k < R1 - R0; k += nt) s_st[k] = m.st_idx[R0 + k];
+  __syncthreads();
+  // every gather of the tile in flight at once
+  const double4* nq4 = reinterpret_cast<const double4*>(s.nQ);
+  for (int k = tid; k < K1 - K0; k += nt) {
+    const int sub = s_sub[k] >> 1;
+    const char* g = reinterpret_cast<const char*>(m.sub_geo + sub);
+    cp_async16(&s_geo[k], g);
+    cp_async16(reinterpret_cast<char*>(&s_geo[k]) + 16, g + 16);
+    if (a.do_lim) {
+      if (ORDER == 1) {
+        const char* d = reinterpret_cast<const char*>(m.sub_dx + sub);
+        cp_async16(&s_dx[k], d);
+        cp_async16(reinterpret_cast<char*>(&s_dx[k]) + 16, d + 16);
+      } else {
+        const double2* x = reinterpret_cast<const double2*>(m.sub_xg + 6 * (long)sub);
+        cp_async16(&s_xg[3 * k], x);
+        cp_async16(&s_xg[3 * k + 1], x + 1);
+        cp_async16(&s_xg[3 * k + 2], x + 2);
+      }
+    }
+  }
+  for (int k = tid; k < E1 - E0; k += nt) {
+    const char* q = reinterpret_cast<const char*>(nq4 + s_nbr[k]);
+    cp_async16(&s_nqe[k], q);
+    cp_async16(reinterpret_cast<char*>(&s_nqe[k]) + 16, q + 16);
+    if (ORDER == 1 && a.do_grad) {
+      const char* w = reinterpret_cast<const char*>(m.edge_w + (s_edg[k] >> 1));
+      cp_async16(&s_ew[k], w);
+      cp_async16(reinterpret_cast<char*>(&s_ew[k]) + 16, w + 16);
+    }
+  }
+  for (int k = tid; k < R1 - R0; k += nt) {
+    const char* q = reinterpret_cast<const char*>(nq4 + s_st[k]);
+    cp_async16(&s_nqs[k], q);
+    cp_async16(reinterpret_cast<char*>(&s_nqs[k]) + 16, q + 16);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // ---- per node and variable, as k_node_prepare4 ----
+  const int n = n0 + (tid >> 2), v = tid & 3;
+  const int qbase = tid & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (n > nlast) return;  // whole quads leave together; no barrier follows
+  const double4 q4 = nq4[n];
+  const double q0v = v == 0 ? q4.x : v == 1 ? q4.y : v == 2 ? q4.z : q4.w;
+  const double rho = q4.x, uu = q4.y / rho, vv = q4.z / rho;
+  const double P = (a.gamma - 1.0) * (q4.w - 0.5 * rho * (uu * uu + vv * vv));
+  const double cs = sqrt((a.gamma * P) / rho);
+  double ev = 0.;
+  int bad = 0;
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  #pragma unroll 4
+  for (int k = s0; k < s1; k++) {
+    const double4 g = s_geo[k - K0];
+    const double theta = uu * g.x + vv * g.y;
+    const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+    const double w = tpc >= tmc ? tpc : tmc;
+    if (!isfinite(w)) bad = 1;
+    ev += (w * g.z);
+  }
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  for (int k = b0; k < b1; k++) {
+    const double* xn = s.xn_bedges + 3 * m.nbed[k];
+    const double theta = uu * xn[0] + vv * xn[1];
+    const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+    const double w = tpc >= tmc ? tpc : tmc;
+    if (!isfinite(w)) bad = 1;
+    ev += (w * xn[2]);
+  }
+  if (v == 0) {
+    const double dt = s.scalars[3] * (m.cv_area[n] / ev);
+    s.dt[n] = dt;
+    if (bad) atomicOr(s.status, ERR_EIGEN);
+    if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
+  }
+  if (!rest) return;
+
+  double qmin = q0v, qmax = q0v, g0 = 0., g1 = 0.;
+  const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
+  #pragma unroll 4
+  for (int k = e0; k < e1; k++) {
+    const int side = s_edg[k - E0] & 1;
+    const double qo = reinterpret_cast<const double*>(&s_nqe[k - E0])[v];
+    qmin = qmin <= qo ? qmin : qo;
+    qmax = qmax >= qo ? qmax : qo;
+    if (ORDER == 1 && a.do_grad) {
+      const double4 w = s_ew[k - E0];
+      const double dq = side ? (q0v - qo) : (qo - q0v);
+      if (side == 0) {
+        g0 += w.x * dq;
+        g1 += w.y * dq;
+      } else {
+        g0 -= w.z * dq;
+        g1 -= w.w * dq;
+      }
+    }
+  }
+  if (ORDER == 1 && a.do_grad)
+    reinterpret_cast<double2*>(s.grad + 8 * (long)n)[v] = make_double2(g0, g1);
+
+  double h[5], pv = 0.;
+  if (derivs) {
+    const int t0 = m.st_ptr[n], t1 = m.st_ptr[n + 1];
+    const int mrows = t1 - t0;
+    const double* U = m.svd_U1 + 5 * (long)t0;
+    double acc[5] = {0., 0., 0., 0., 0.};
+#pragma unroll 4
+    for (int k = 0; k < mrows; k++) {
+      const double qn = reinterpret_cast<const double*>(&s_nqs[t0 - R0 + k])[v];
+      const double bv = m.st_w[t0 + k] * (qn - q0v);
+#pragma unroll
+      for (int c = 0; c < 5; c++) acc[c] += bv * U[5 * k + c];
+    }
+    const double* VT = m.svd_VT + 25 * (long)n;
+    const double* S = m.svd_S + 5 * (long)n;
+    double t1v[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) t1v[c] = acc[c] / S[c];
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      double sum = 0.;
+#pragma unroll
+      for (int c = 0; c < 5; c++) sum += VT[j * 5 + c] * t1v[c];
+      h[j] = sum;
+    }
+    const double* mo = m.moments + 9 * (long)n;
+    pv = q0v - mo[0] * h[0] - mo[1] * h[1] - mo[2] * h[2] * 0.5 - mo[3] * h[3] * 0.5 -
+         mo[4] * h[4];
+    double* hd = s.hess5 + 20 * (long)n + 5 * v;
+#pragma unroll
+    for (int c = 0; c < 5; c++) hd[c] = h[c];
+    s.pv[4 * (long)n + v] = pv;
+  }
+
+  if (!a.do_lim) return;
+  double ph = 1.0;
+  const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
+  #pragma unroll 4
+  for (int k = s0; k < s1; k++) {
+    const int side = s_sub[k - K0] & 1;
+    if (ORDER == 1) {
+      const double4 d = s_dx[k - K0];
+      const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
+      const double qr = q0v + (g0 * dx0 + g1 * dx1);
+      ph = venkat_fold(ph, qr, q0v, qmin, qmax);
+    } else {
+#pragma unroll
+      for (int gpt = 0; gpt < 3; gpt++) {
+        const double2 xg = s_xg[3 * (k - K0) + gpt];
+        const double dx0 = xg.x - xn0, dx1 = xg.y - xn1;
+        double qr = pv;
+        qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
+               h[4] * dx0 * dx1);
+        ph = venkat_fold(ph, qr, q0v, qmin, qmax);
+      }
+    }
+  }
   const double p1 = __shfl_sync(qmask, ph, qbase + 1);
   const double p2 = __shfl_sync(qmask, ph, qbase + 2);
   const double p3 = __shfl_sync(qmask, ph, qbase + 3);
@@ -1042,19 +1287,6 @@ constexpr int kChunkSubMax = 256;   // sub-levels per chunk (host-checked)
 // shared memory the chunk sweep declares statically (room left for the rest)
 constexpr int kChunkStaticSmem = 2048;
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
-                   static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
 
 // Static part of mode 3's sweep records: record i holds row order[i]'s
 // header (row, off-diagonal block count; the diagonal block is the row's

@@ -28,9 +28,10 @@ struct DevMesh {
   // node -> incident boundary edges (ascending)
   const int* nbed_ptr;
   const int* nbed;
-  // node -> incident edges, (e << 1) | side
+  // node -> incident edges, (e << 1) | side, and the node at the edge's other end
   const int* nedg_ptr;
   const int* nedg;
+  const int* nedg_nbr;
   // block CSR (reference Build_CRS layout: diagonal block last in each row)
   const int* ia;
   const int* iau;

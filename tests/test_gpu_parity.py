@@ -133,3 +133,25 @@ def test_long_residual_history(ref_lib, nc, nr, curved, order, mach, steps):
     assert ndiff(case.ref.array("Q")[4:], gpu.get("Q")[4:]) == 0
     assert gpu.body_forces() == case.ref.body_forces()
     assert gpu.status() == 0
+
+
+@pytest.mark.parametrize("nc,nr,curved,order,steps", [
+    (128, 32, False, 1, 4), (128, 32, True, 3, 4), (12, 4, True, 3, 4), (8, 3, False, 1, 4),
+])
+def test_staged_node_kernel_bitwise(ref_lib, nc, nr, curved, order, steps):
+    """Node variant 3 (gathers staged in shared memory), step by step against
+    the reference, including meshes smaller than one tile of 32 nodes."""
+    case = ParityCase(nc, nr, curved, order)
+    gpu = _solver(case)
+    gpu.set_variants(3, 0)
+    nn = case.sizes["nn"]
+    for ts in range(1, steps + 1):
+        case.ref_step()
+        gpu.solve(ts)
+        assert ndiff(case.ref.array("Q")[4:], gpu.get("Q")[4:]) == 0, ts
+        for name in ("phi", "grad"):
+            a, b = case.ref.array(name), gpu.get(name)
+            w = a.size // (nn + 1)
+            assert ndiff(a[w:], b[w:]) == 0, (name, ts)
+        assert ndiff(case.ref.array("LHS"), gpu.get("LHS")) == 0, ts
+    assert gpu.status() == 0
