@@ -222,6 +222,7 @@ struct flow_ctx {
   int capture_fault = 0;
   long capture_fallbacks = 0;
   int jac_mode = 0;  // face Jacobians of the precision form (flow_set_jacobian)
+  bool fused_ok = false;  // every row has at most kRecBlocks off-diagonal blocks
   // staged node kernel (node_prepare variant 3): largest per-tile slices and
   // whether its shared memory fits, per order of the kernel
   StageCaps stage_caps{};
@@ -421,11 +422,38 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
 
 int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
   int rc = 0;
+  if (jac && c->jac_mode == 1 && c->precision != 0 && c->fused_ok) {
+    // approximate Jacobian: boundary faces first, then the interior faces
+    // formed and summed by the nodes (k_faces_assemble)
+    const int nbb = grid_blocks(c->nbe, 128);
+    if (nbb > 0) {
+      Timed t(c, 2);
+      k_boundary<true><<<nbb, 128, 0, c->stream>>>(c->m, c->s, a);
+      rc |= launch_check(c);
+    }
+    Timed t(c, 1);
+    const int nb = grid_blocks(c->nn, kFusedNodes);
+    const MixedTables& mt = c->mt;
+    const ChunkTables& ct = c->ct;
+    if (c->precision == 3) {
+      if (a.recon == 1)
+        k_faces_assemble<1, 2><<<nb, 128, kFusedSmem, c->stream>>>(c->m, c->s, a, mt, ct);
+      else
+        k_faces_assemble<0, 2><<<nb, 128, kFusedSmem, c->stream>>>(c->m, c->s, a, mt, ct);
+    } else {
+      if (a.recon == 1)
+        k_faces_assemble<1, 1><<<nb, 128, kFusedSmem, c->stream>>>(c->m, c->s, a, mt, ct);
+      else
+        k_faces_assemble<0, 1><<<nb, 128, kFusedSmem, c->stream>>>(c->m, c->s, a, mt, ct);
+    }
+    rc |= launch_check(c);
+    return rc;
+  }
   {
     Timed t(c, 1);
     int nbs = grid_blocks(c->ns, 128);
     // the approximate Roe Jacobian only in the precision form
-    const bool approx = jac && c->jac_mode == 1 && c->precision != 0;
+    const bool approx = jac && c->jac_mode != 0 && c->precision != 0;
     if (a.recon == 1) {
       launch_flux_variant(c->var[1], [&](auto V) {
         if (approx) k_subedge_flux<1, true, V.value, 1><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
@@ -868,6 +896,8 @@ bool preload_kernels() {
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
         (const void*)k_boundary_add4<true>, (const void*)k_boundary_add4<false>,
         (const void*)k_node_stage<1>, (const void*)k_node_stage<3>,
+        (const void*)k_faces_assemble<0, 1>, (const void*)k_faces_assemble<1, 1>,
+        (const void*)k_faces_assemble<0, 2>, (const void*)k_faces_assemble<1, 2>,
         (const void*)k_diag_lu,
         (const void*)k_subedge_flux<0, true, 3>, (const void*)k_subedge_flux<0, true, 4>,
         (const void*)k_subedge_flux<0, true, 5>, (const void*)k_subedge_flux<0, false, 3>,
@@ -911,6 +941,10 @@ bool ensure_kernel_attrs(int device) {
   for (const void* f : {(const void*)k_node_stage<1>, (const void*)k_node_stage<3>})
     ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)kStageSmemMax) == cudaSuccess;
+  for (const void* f : {(const void*)k_faces_assemble<0, 1>, (const void*)k_faces_assemble<1, 1>,
+                        (const void*)k_faces_assemble<0, 2>, (const void*)k_faces_assemble<1, 2>})
+    ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kFusedSmem) == cudaSuccess;
   for (const void* f : {(const void*)k_sweep_cta<true>, (const void*)k_sweep_cta<false>})
     ok = ok && cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, cta) ==
                    cudaSuccess;
@@ -1338,6 +1372,21 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
       csr_sub[k] = make_int4(edge_sub[found].x, edge_sub[found].y, role, 0);
     }
   }
+  // per subedge incidence: the row position of the block (node, other end)
+  std::vector<int> nsub_slot(nsub.idx.size(), 0);
+  c->fused_ok = true;
+  for (int n = 1; n <= nn; n++) {
+    if (g->ia[n + 1] - g->ia[n] - 1 > kRecBlocks) c->fused_ok = false;
+    for (int k = nsub.ptr[n]; k < nsub.ptr[n + 1]; k++) {
+      const int sub = nsub.idx[k] >> 1, side = nsub.idx[k] & 1;
+      const int other = side ? sub_lr[sub].x : sub_lr[sub].y;
+      int pos = -1;
+      for (int b = g->ia[n]; b < g->ia[n + 1]; b++)
+        if (g->ja[b] == other) pos = b - g->ia[n];
+      if (pos < 0 || pos >= kRecBlocks) c->fused_ok = false;
+      nsub_slot[k] = pos < 0 ? 0 : std::min(pos, kRecBlocks - 1);
+    }
+  }
   std::vector<int4> bed_info(nbe + 1, make_int4(0, 0, 0, 0));
   std::vector<double2> bed_cnrm(nbe + 1, make_double2(0., 0.));
   for (int b = 1; b <= nbe; b++) {
@@ -1402,7 +1451,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   m.stencil_max = stencil_max;
   bool okk = true;
 #define UP(field, vec) do { auto* d = upload_vec(c, vec); okk = okk && d; m.field = d; } while (0)
-  UP(nsub_ptr, nsub.ptr); UP(nsub, nsub.idx);
+  UP(nsub_ptr, nsub.ptr); UP(nsub, nsub.idx); UP(nsub_slot, nsub_slot);
   UP(nbed_ptr, nbed.ptr); UP(nbed, nbed.idx);
   UP(nedg_ptr, nedg.ptr); UP(nedg, nedg.idx); UP(nedg_nbr, nedg_nbr);
   UP(sub_lr, sub_lr); UP(sub_geo, sub_geo); UP(sub_dx, sub_dx);
@@ -1720,8 +1769,8 @@ int flow_set_graphs(flow_ctx* c, int on) {
 }
 
 int flow_set_jacobian(flow_ctx* c, int mode) {
-  if (!c || !c->ok || mode < 0 || mode > 1) {
-    set_error("flow_set_jacobian: null context or mode not 0..1");
+  if (!c || !c->ok || mode < 0 || mode > 2) {
+    set_error("flow_set_jacobian: null context or mode not 0..2");
     return FLOW_ERR_ARG;
   }
   cudaSetDevice(c->device);

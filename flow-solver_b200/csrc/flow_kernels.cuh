@@ -498,6 +498,50 @@ __global__ void __launch_bounds__(128) k_node_stage(DevMesh m, DevState s, StepA
 }
 
 // ---------------------------------------------------------------------------
+// The two face states of subedge sub: the node states, reconstructed to the
+// face point (reconstruct.C:181-203) when RECON is 1.
+template <int RECON>
+__device__ __forceinline__ void face_states(const DevMesh& m, const DevState& s, int sub,
+                                            int2 lr, double* qL, double* qR) {
+  const double4 qa = reinterpret_cast<const double4*>(s.nQ)[lr.x];
+  const double4 qb = reinterpret_cast<const double4*>(s.nQ)[lr.y];
+  qL[0] = qa.x; qL[1] = qa.y; qL[2] = qa.z; qL[3] = qa.w;
+  qR[0] = qb.x; qR[1] = qb.y; qR[2] = qb.z; qR[3] = qb.w;
+  if (RECON == 1) {
+    const double4 d = m.sub_dx[sub];
+    const double* gL = s.grad + 8 * (long)lr.x;
+    const double* gR = s.grad + 8 * (long)lr.y;
+    const double phL = s.phi[8 * (long)lr.x], phR = s.phi[8 * (long)lr.y];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      qL[j] += (phL * gL[2 * j] * d.x + phL * gL[2 * j + 1] * d.y);
+      qR[j] += (phR * gR[2 * j] * d.z + phR * gR[2 * j + 1] * d.w);
+    }
+  }
+}
+
+// The Roe flux of a face and its approximate Jacobians (JL, JR row-major):
+// dF/dqL = (A(qL) + |A~|) len / 2, dF/dqR = (A(qR) - |A~|) len / 2.
+__device__ __forceinline__ void face_flux_approx(double4 g, double gamma, const double* qL,
+                                                 const double* qR, double* flux, double* JL,
+                                                 double* JR) {
+  const double ogm1 = 1.0 / (gamma - 1.0);
+  RoeSide SL, SR;
+  roe_side(qL, g.x, g.y, g.z, gamma, SL);
+  roe_side(qR, g.x, g.y, g.z, gamma, SR);
+  const double bg = roe_weight(SL.rho, SR.rho);
+  double Rm[16], dL[16], dR[16];
+  roe_core(g.x, g.y, g.z, gamma, ogm1, qL, qR, SL, SR, bg, flux, Rm);
+  euler_jacobian(qL, g.x, g.y, gamma, dL);
+  euler_jacobian(qR, g.x, g.y, gamma, dR);
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    JL[k] = 0.5 * (dL[k] + Rm[k]) * g.z;
+    JR[k] = 0.5 * (dR[k] - Rm[k]) * g.z;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Per node: R and RHS = -R, the diagonal block (V/dt plus the face Jacobians
 // in face order), the off-diagonal blocks of the node's LHS row, and the LU
 // factors of the diagonal block for the sweeps (linear_algebra.C:226-246).
@@ -506,17 +550,12 @@ __global__ void __launch_bounds__(128) k_node_stage(DevMesh m, DevState s, StepA
 // precision form) writes FP32 off-diagonal blocks and FP32 LU factors with
 // reciprocal pivots instead of the FP64 row: into the mode 1/2 tables
 // (MIXED 1) or into the row's forward and backward sweep records (MIXED 2).
-template <bool JAC, int MIXED>
-__global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a,
-                                                   MixedTables mt, ChunkTables ct) {
-  if (*s.stop) return;  // the run has converged
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  const int n = (tid >> 2) + 1, q = tid & 3;
-  const int qbase = threadIdx.x & ~3 & 31;
-  const unsigned qmask = 0xFu << qbase;
-  if (n > m.nn) return;
-  double r = 0.;
-  double D0 = 0., D1 = 0., D2 = 0., D3 = 0.;
+
+// The V/dt diagonal row q of node n's block (build_matrix).
+__device__ __forceinline__ void diag_row(const DevMesh& m, const DevState& s, const StepArgs& a,
+                                         int n, int q, double& D0, double& D1, double& D2,
+                                         double& D3) {
+  D0 = D1 = D2 = D3 = 0.;
   const double diag = m.cv_area[n] / (s.dt[n]);
   if (a.steady_diag) {
     if (q == 0) D0 = diag;
@@ -524,28 +563,22 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
     if (q == 2) D2 = diag;
     if (q == 3) D3 = diag;
   }
-  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
-  for (int k = s0; k < s1; k++) {
-    const int sd = m.nsub[k];
-    const int sub = sd >> 1, side = sd & 1;
-    const double f = s.F[4 * (long)sub + q];
-    if (side == 0) r += f;
-    else r -= f;
-    if (JAC) {
-      const double4 J =
-          reinterpret_cast<const double4*>((side ? s.JR : s.JL) + 16 * (long)sub)[q];
-      if (side == 0) {
-        D0 += J.x; D1 += J.y; D2 += J.z; D3 += J.w;
-      } else {
-        D0 -= J.x; D1 -= J.y; D2 -= J.z; D3 -= J.w;
-      }
-    }
-  }
+}
+
+// Row q of node n after the interior faces were summed into r and D: the
+// boundary edges' terms, R and RHS, the row's blocks (offb(k, B) gives
+// off-diagonal block k's row q) and the LU factors of the diagonal block.
+template <int MIXED, class OffBlock>
+__device__ __forceinline__ void assemble_row(const DevMesh& m, const DevState& s,
+                                             const StepArgs& a, const MixedTables& mt,
+                                             const ChunkTables& ct, int n, int q, int qbase,
+                                             unsigned qmask, bool jac, double r, double D0,
+                                             double D1, double D2, double D3, OffBlock&& offb) {
   const int b0 = a.skip_bnd ? 0 : m.nbed_ptr[n], b1 = a.skip_bnd ? 0 : m.nbed_ptr[n + 1];
   for (int k = b0; k < b1; k++) {
     const int b = m.nbed[k];
     r += s.Fb[4 * (long)b + q];
-    if (JAC) {
+    if (jac) {
       const double4 J = reinterpret_cast<const double4*>(s.Jb + 16 * (long)b)[q];
       D0 += J.x; D1 += J.y; D2 += J.z; D3 += J.w;
     }
@@ -571,20 +604,7 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
       continue;
     }
     double B0 = 0., B1 = 0., B2 = 0., B3 = 0.;
-    if (JAC) {
-      const int4 cs = m.csr_sub[k];
-      const double* src = cs.z == 0 ? s.JR : s.JL;
-      for (int t = 0; t < 2; t++) {
-        const int sub = t == 0 ? cs.x : cs.y;
-        if (sub < 0) break;
-        const double4 J = reinterpret_cast<const double4*>(src + 16 * (long)sub)[q];
-        if (cs.z == 0) {
-          B0 += J.x; B1 += J.y; B2 += J.z; B3 += J.w;
-        } else {
-          B0 -= J.x; B1 -= J.y; B2 -= J.z; B3 -= J.w;
-        }
-      }
-    }
+    offb(k, B0, B1, B2, B3);
     const float4 b32 = make_float4(__double2float_rn(B0), __double2float_rn(B1),
                                    __double2float_rn(B2), __double2float_rn(B3));
     if (MIXED == 1) {
@@ -632,6 +652,129 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
   } else {
     reinterpret_cast<double4*>(s.LUd + 16 * (long)n)[q] = make_double4(o0, o1, o2, o3);
   }
+}
+
+template <bool JAC, int MIXED>
+__global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a,
+                                                   MixedTables mt, ChunkTables ct) {
+  if (*s.stop) return;  // the run has converged
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = (tid >> 2) + 1, q = tid & 3;
+  const int qbase = threadIdx.x & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (n > m.nn) return;
+  double r = 0.;
+  double D0, D1, D2, D3;
+  diag_row(m, s, a, n, q, D0, D1, D2, D3);
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int k = s0; k < s1; k++) {
+    const int sd = m.nsub[k];
+    const int sub = sd >> 1, side = sd & 1;
+    const double f = s.F[4 * (long)sub + q];
+    if (side == 0) r += f;
+    else r -= f;
+    if (JAC) {
+      const double4 J =
+          reinterpret_cast<const double4*>((side ? s.JR : s.JL) + 16 * (long)sub)[q];
+      if (side == 0) {
+        D0 += J.x; D1 += J.y; D2 += J.z; D3 += J.w;
+      } else {
+        D0 -= J.x; D1 -= J.y; D2 -= J.z; D3 -= J.w;
+      }
+    }
+  }
+  assemble_row<MIXED>(m, s, a, mt, ct, n, q, qbase, qmask, JAC, r, D0, D1, D2, D3,
+                      [&](int k, double& B0, double& B1, double& B2, double& B3) {
+    if (!JAC) return;
+    const int4 cs = m.csr_sub[k];
+    const double* src = cs.z == 0 ? s.JR : s.JL;
+    for (int t = 0; t < 2; t++) {
+      const int sub = t == 0 ? cs.x : cs.y;
+      if (sub < 0) break;
+      const double4 J = reinterpret_cast<const double4*>(src + 16 * (long)sub)[q];
+      if (cs.z == 0) {
+        B0 += J.x; B1 += J.y; B2 += J.z; B3 += J.w;
+      } else {
+        B0 -= J.x; B1 -= J.y; B2 -= J.z; B3 -= J.w;
+      }
+    }
+  });
+}
+
+// ---------------------------------------------------------------------------
+// Precision form with the approximate Jacobian (flow_set_jacobian 1): the
+// interior faces' fluxes and Jacobians formed by the nodes that gather them,
+// instead of written per face and read back (k_subedge_flux + k_assemble4:
+// 288 bytes a face through HBM).  The four lanes of a node take its faces
+// four at a time (face_states / face_flux_approx, the arithmetic of
+// k_subedge_flux<., true, ., 1>), leave F, JL, JR in shared memory, and then
+// each lane sums its row in face order as k_assemble4 does; an off-diagonal
+// block gathers the faces of its edge in a shared-memory accumulator, in the
+// same order (its first subedge, then its second).  So R, every block and the
+// factors are the bits of the two-kernel path; each face is formed twice (once
+// per end), which costs less than the round trip.  k_boundary runs first.
+// Rows with more than kRecBlocks off-diagonal blocks take the two-kernel path
+// (host-checked).
+constexpr int kFusedNodes = 32;
+// per node 4 face buffers of 36 doubles (+1: consecutive nodes start on
+// different banks); per lane kRecBlocks block rows of 4 doubles (+1, same)
+constexpr int kFusedFace = 4 * 36 + 1, kFusedOff = kRecBlocks * 4 + 1;
+constexpr size_t kFusedSmem = (size_t)kFusedNodes * kFusedFace * 8 +
+                              (size_t)kFusedNodes * 4 * kFusedOff * 8;
+
+template <int RECON, int MIXED>
+__global__ void __launch_bounds__(128) k_faces_assemble(DevMesh m, DevState s, StepArgs a,
+                                                        MixedTables mt, ChunkTables ct) {
+  if (*s.stop) return;  // the run has converged
+  extern __shared__ __align__(16) double fsm[];
+  const int tid = threadIdx.x, nl = tid >> 2, q = tid & 3;
+  const int n = blockIdx.x * kFusedNodes + nl + 1;
+  const int qbase = tid & ~3 & 31;
+  const unsigned qmask = 0xFu << qbase;
+  if (n > m.nn) return;  // whole quads leave together; only quad-wide syncs follow
+  double* face = fsm + (size_t)nl * kFusedFace;  // F (4), JL (16), JR (16) of 4 faces
+  double* off = fsm + (size_t)kFusedNodes * kFusedFace + ((size_t)nl * 4 + q) * kFusedOff;
+#pragma unroll
+  for (int t = 0; t < kRecBlocks * 4; t++) off[t] = 0.;
+  double r = 0.;
+  double D0, D1, D2, D3;
+  diag_row(m, s, a, n, q, D0, D1, D2, D3);
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int base = s0; base < s1; base += 4) {
+    if (base + q < s1) {
+      const int sub = m.nsub[base + q] >> 1;
+      double qL[4], qR[4];
+      face_states<RECON>(m, s, sub, m.sub_lr[sub], qL, qR);
+      double* fb = face + q * 36;
+      face_flux_approx(m.sub_geo[sub], a.gamma, qL, qR, fb, fb + 4, fb + 20);
+    }
+    __syncwarp(qmask);
+    const int cnt = min(4, s1 - base);
+    for (int f = 0; f < cnt; f++) {
+      const int side = m.nsub[base + f] & 1;
+      const double* fb = face + f * 36;
+      const double fl = fb[q];
+      if (side == 0) r += fl;
+      else r -= fl;
+      const double* JL = fb + 4 + 4 * q;
+      const double* JR = fb + 20 + 4 * q;
+      double* o = off + 4 * m.nsub_slot[base + f];
+      if (side == 0) {
+        D0 += JL[0]; D1 += JL[1]; D2 += JL[2]; D3 += JL[3];
+        o[0] += JR[0]; o[1] += JR[1]; o[2] += JR[2]; o[3] += JR[3];
+      } else {
+        D0 -= JR[0]; D1 -= JR[1]; D2 -= JR[2]; D3 -= JR[3];
+        o[0] -= JL[0]; o[1] -= JL[1]; o[2] -= JL[2]; o[3] -= JL[3];
+      }
+    }
+    __syncwarp(qmask);
+  }
+  const int k0 = m.ia[n];
+  assemble_row<MIXED>(m, s, a, mt, ct, n, q, qbase, qmask, true, r, D0, D1, D2, D3,
+                      [&](int k, double& B0, double& B1, double& B2, double& B3) {
+    const double* o = off + 4 * (k - k0);
+    B0 = o[0]; B1 = o[1]; B2 = o[2]; B3 = o[3];
+  });
 }
 
 // ---------------------------------------------------------------------------
@@ -708,22 +851,23 @@ __global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState 
   if (*s.stop) return;  // the run has converged
   int sub = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (sub > m.ns) return;
-  int2 lr = m.sub_lr[sub];
-  double4 g = m.sub_geo[sub];
-  double4 qa = reinterpret_cast<const double4*>(s.nQ)[lr.x];
-  double4 qb = reinterpret_cast<const double4*>(s.nQ)[lr.y];
-  double qL[4] = {qa.x, qa.y, qa.z, qa.w};
-  double qR[4] = {qb.x, qb.y, qb.z, qb.w};
-  if (RECON == 1) {
-    double4 d = m.sub_dx[sub];
-    const double* gL = s.grad + 8 * (long)lr.x;
-    const double* gR = s.grad + 8 * (long)lr.y;
-    double phL = s.phi[8 * (long)lr.x], phR = s.phi[8 * (long)lr.y];
+  const int2 lr = m.sub_lr[sub];
+  const double4 g = m.sub_geo[sub];
+  double qL[4], qR[4];
+  face_states<RECON>(m, s, sub, lr, qL, qR);
+  double flux[4];
+  if (JAC && JMODE == 1) {
+    double JL[16], JR[16];
+    face_flux_approx(g, a.gamma, qL, qR, flux, JL, JR);
+    reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
+    double4* JLo = reinterpret_cast<double4*>(s.JL + 16 * (long)sub);
+    double4* JRo = reinterpret_cast<double4*>(s.JR + 16 * (long)sub);
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      qL[j] += (phL * gL[2 * j] * d.x + phL * gL[2 * j + 1] * d.y);
-      qR[j] += (phR * gR[2 * j] * d.z + phR * gR[2 * j + 1] * d.w);
+    for (int r = 0; r < 4; r++) {
+      JLo[r] = make_double4(JL[4 * r], JL[4 * r + 1], JL[4 * r + 2], JL[4 * r + 3]);
+      JRo[r] = make_double4(JR[4 * r], JR[4 * r + 1], JR[4 * r + 2], JR[4 * r + 3]);
     }
+    return;
   }
   // Roe_flux_centered and its 8 forward differences (jacobian.C:45-185): the
   // unperturbed side's quantities and, unless the density is perturbed, the
@@ -733,28 +877,6 @@ __global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState 
   roe_side(qL, g.x, g.y, g.z, a.gamma, SL);
   roe_side(qR, g.x, g.y, g.z, a.gamma, SR);
   const double bg = roe_weight(SL.rho, SR.rho);
-  double flux[4];
-  if (JAC && JMODE == 1) {
-    double Rm[16], dL[16], dR[16];
-    roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qR, SL, SR, bg, flux, Rm);
-    reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
-    euler_jacobian(qL, g.x, g.y, a.gamma, dL);
-    euler_jacobian(qR, g.x, g.y, a.gamma, dR);
-    double4* JLo = reinterpret_cast<double4*>(s.JL + 16 * (long)sub);
-    double4* JRo = reinterpret_cast<double4*>(s.JR + 16 * (long)sub);
-#pragma unroll
-    for (int r = 0; r < 4; r++) {
-      double o[4], p[4];
-#pragma unroll
-      for (int c = 0; c < 4; c++) {
-        o[c] = 0.5 * (dL[4 * r + c] + Rm[4 * r + c]) * g.z;
-        p[c] = 0.5 * (dR[4 * r + c] - Rm[4 * r + c]) * g.z;
-      }
-      JLo[r] = make_double4(o[0], o[1], o[2], o[3]);
-      JRo[r] = make_double4(p[0], p[1], p[2], p[3]);
-    }
-    return;
-  }
   roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qR, SL, SR, bg, flux);
   reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
   if (!JAC) return;

@@ -25,6 +25,8 @@ struct DevMesh {
   // node -> incident subedges, (s << 1) | side, side 0 = node is the edge's L
   const int* nsub_ptr;
   const int* nsub;
+  const int* nsub_slot;  // per incidence: the row position (k - ia[node]) of the block
+                         // (node, the face's other node); used by k_faces_assemble
   // node -> incident boundary edges (ascending)
   const int* nbed_ptr;
   const int* nbed;

@@ -305,7 +305,11 @@ int flow_set_precision(flow_ctx *ctx, int mode);
  * dissipation matrix |A~| frozen (the form the reference gives its boundary
  * faces, jacobian.C:681-962), which costs no extra flux.  The residual is
  * unchanged, so the converged state is too; only the preconditioner
- * differs.  Used in precision modes 1-3 only: the FP64 drop-in (mode 0)
+ * differs.  With mode 1 the interior faces are formed by the nodes that sum
+ * them, in one kernel with the assembly (no per-face arrays through device
+ * memory; rows of at most 8 off-diagonal blocks, else as mode 2); mode 2 is
+ * the same arithmetic in two kernels (faces written, then gathered): the
+ * same bits.  Used in precision modes 1-3 only: the FP64 drop-in (mode 0)
  * always differences, as the reference does. */
 int flow_set_jacobian(flow_ctx *ctx, int mode);
 /* Sweep schedule (no reference counterpart): steps up to `until_step` (0:

@@ -140,19 +140,22 @@ def test_sweep_schedule_bitwise():
     gpu.close()
 
 
+@pytest.mark.parametrize("jmode", [1, 2])
 @pytest.mark.parametrize("nc,nr,curved,order,subits,steps,mode", [
     (32, 8, True, 3, 4, 6, 1),
     (64, 16, False, 1, 3, 5, 1),
     (32, 8, True, 3, 4, 6, 3),
     (128, 32, True, 3, 4, 4, 3),
     (64, 16, False, 1, 3, 5, 3),
+    (8, 3, False, 1, 3, 4, 3),  # 24 nodes: less than one CTA of the fused kernel
 ])
-def test_approximate_jacobian_steps_bitwise(nc, nr, curved, order, subits, steps, mode):
-    """flow_set_jacobian(ctx, 1): the interior face Jacobians by the
-    approximate Roe form, against the oracle's restatement step by step (the
-    residual is the FP64 one; only the FP32 blocks differ from mode 0's)."""
+def test_approximate_jacobian_steps_bitwise(nc, nr, curved, order, subits, steps, mode, jmode):
+    """flow_set_jacobian: the interior face Jacobians by the approximate Roe
+    form, fused with the assembly (1) or in two kernels (2), against the
+    oracle's restatement step by step (the residual is the FP64 one; only the
+    FP32 blocks differ from mode 0's)."""
     mesh, fp, og, p, gpu = _setup(nc, nr, curved, order, subits, mode)
-    gpu.set_jacobian(1)
+    gpu.set_jacobian(jmode)
     p.jac_approx = 1
     nn = mesh.sizes["nn"]
     perm = None
