@@ -223,6 +223,7 @@ struct flow_ctx {
   long capture_fallbacks = 0;
   int jac_mode = 0;  // face Jacobians of the precision form (flow_set_jacobian)
   bool fused_ok = false;  // every row has at most kRecBlocks off-diagonal blocks
+  int exact_rms = 0;      // every b-Ax RMS in the reference's order (flow_set_exact_rms)
   // staged node kernel (node_prepare variant 3): largest per-tile slices and
   // whether its shared memory fits, per order of the kernel
   StageCaps stage_caps{};
@@ -614,7 +615,10 @@ int launch_linear_solve(flow_ctx* c, const flow_params* p, bool final_rms) {
       Timed t(c, 5);
       k_lin_residual<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->m, c->s);
       rc |= launch_check(c);
-      k_finalize_rms<<<1, kRedThreads, 0, c->stream>>>(c->s, kRedBlocks, c->nn);
+      k_finalize_rms<<<1, kRedThreads, 0, c->stream>>>(c->s, kRedBlocks, c->nn,
+                                                       c->exact_rms);
+      rc |= launch_check(c);
+      k_exact_rms<<<1, 256, 0, c->stream>>>(c->m, c->s);
       rc |= launch_check(c);
     }
   }
@@ -914,7 +918,8 @@ bool preload_kernels() {
         (const void*)k_sweep_color32<false>, (const void*)k_sweep_ordered32<true>,
         (const void*)k_sweep_ordered32<false>, (const void*)k_prepare_sweep32,
         (const void*)k_fill_sweep_records, (const void*)k_prepare_sweep,
-        (const void*)k_lin_residual, (const void*)k_finalize_rms, (const void*)k_finish_step,
+        (const void*)k_lin_residual, (const void*)k_finalize_rms, (const void*)k_exact_rms,
+        (const void*)k_finish_step,
         (const void*)k_finalize_step, (const void*)k_body_forces,
         (const void*)k_body_forces_sum})
     ok = ok && cudaFuncGetAttributes(&fa, f) == cudaSuccess;
@@ -1550,6 +1555,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   s.counter = c->buf.alloc<unsigned>(4);
   s.status = c->buf.alloc<int>(1);
   s.skip = c->buf.alloc<int>(1);
+  s.exact = c->buf.alloc<int>(1);
   s.stop = c->buf.alloc<int>(1);
   s.steps_done = c->buf.alloc<int>(1);
   s.citer = c->buf.alloc<int>(1);
@@ -1558,7 +1564,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.dQ2 || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
       !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
       !s.Jb || !s.bforce || !s.done || !s.counter || !s.status || !s.skip || !s.partial ||
-      !s.scalars || !s.stop || !s.steps_done || !s.citer)
+      !s.scalars || !s.stop || !s.steps_done || !s.citer || !s.exact)
     return fail(c, carve_error(c), "device state allocation failed");
   bool zero_ok = true;
   auto zero = [&](void* ptr, size_t bytes) {
@@ -1580,6 +1586,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   zero(s.done, (size_t)(nn + 1) * 4);
   zero(s.status, 4);
   zero(s.skip, 4);
+  zero(s.exact, 4);
   zero(s.stop, 4);
   zero(s.steps_done, 4);
   zero(s.citer, 4);
@@ -1777,6 +1784,18 @@ int flow_set_jacobian(flow_ctx* c, int mode) {
   cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   c->jac_mode = mode;
+  return 0;
+}
+
+int flow_set_exact_rms(flow_ctx* c, int on) {
+  if (!c || !c->ok) {
+    set_error("flow_set_exact_rms: null context");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  c->exact_rms = on ? 1 : 0;
   return 0;
 }
 

@@ -142,6 +142,7 @@ struct DevState {
   unsigned int* counter;  // row dispenser for the ordered sweeps
   int* status;      // sticky error bits (FLOW_ERR_*)
   int* skip;        // set when the linear residual dropped below 1e-15
+  int* exact;       // set when that test needs the reference's summation order
   int* stop;        // set once the run's density residual dropped below its target
   int* steps_done;  // pseudo-time steps completed since the last reset
   int* citer;       // pseudo-time step index of the step in flight (drives the CFL ramp)

@@ -202,6 +202,14 @@ int flow_residual_stage(flow_ctx *ctx, const flow_params *p, int jupdate, int ts
  * sweeps from dQ = 0; *rms receives the returned b-Ax RMS. */
 int flow_linear_solve(flow_ctx *ctx, const flow_params *p, double *rms);
 
+/* The b - Ax RMS that stops linear_solve's sweep loop below 1e-15
+ * (linear_algebra.C:348-387) is reduced as a tree on the device; when it
+ * lies within the tree sum's rounding bound of 1e-15, it is summed again in
+ * the reference's row order, so the loop stops where the reference's does.
+ * on != 0 sums every RMS in that order (slow; for checking the returned RMS
+ * bit for bit). */
+int flow_set_exact_rms(flow_ctx *ctx, int on);
+
 /* void Compute_Body_Forces(GRID*, PARAMS, double*)  (include/grid_io.h:36,
  * grid_io.C:1390-1697): raw pressure lift and drag on the wall boundaries. */
 int flow_body_forces(flow_ctx *ctx, const flow_params *p, double *forces);
