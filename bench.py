@@ -67,6 +67,9 @@ METRIC = "converged solves/s (1e-10 drop) served vs plain FP64 GPU; p50/p99 late
 UNIT = "solves/s"
 REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
 BENCH_BUDGET_S = 1500.      # wall-clock target of a whole batch run (warm-up and checks included)
+SERVE_RATES = (0.5, 2.0)    # requests/s of the serving measurement in the batch run
+SERVE_REQUESTS = 16
+SERVE_MIN_LEFT_S = 240.     # run the serving measurement only with this much time left
 REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
 STAGE_THREADS = max(1, min(8, os.cpu_count() or 1))  # concurrent admissions per batch pass
 CPU_BASELINE_STEPS = 6      # pseudo-time steps timed for cpu_baseline
@@ -345,7 +348,8 @@ def run_batch(args, bw):
     prep = serve.prepare_all(reqs, bw.subits, bw.max_steps, bw.drop)
     prep_s = time.time() - t0
     free, _total = torch.cuda.mem_get_info(local)
-    arena = capi.Arena(int(min(free * 0.85, 150e9)), device=local)
+    arena_bytes = int(min(free * 0.85, 150e9))
+    arena = capi.Arena(arena_bytes, device=local)
     h2d = sum(_view_bytes(p.mesh) + p.Q0.nbytes for p in prep)
     d2h = sum(p.Q0.nbytes + 16 for p in prep)
     log(f"[rank {rank}] {bw.name}: {bw.n} requests, {sum(r.nodes for r in reqs)} nodes, "
@@ -354,7 +358,8 @@ def run_batch(args, bw):
     def one_pass():
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n, autotune=bw.autotune,
-                          stall=bw.stall, priority_policy=bw.priority_policy)
+                          stall=bw.stall, priority_policy=bw.priority_policy,
+                          jacobian=bw.jacobian)
         torch.cuda.synchronize()
         ev[0].record()
         # context + mesh arrays + state to the device, several requests at a
@@ -393,7 +398,8 @@ def run_batch(args, bw):
         # each state and force read back as its solve retires
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n, autotune=bw.autotune,
-                          stall=bw.stall, priority_policy=bw.priority_policy)
+                          stall=bw.stall, priority_policy=bw.priority_policy,
+                          jacobian=bw.jacobian)
         torch.cuda.synchronize()
         ev[0].record()
         recs = {}
@@ -589,6 +595,17 @@ def run_batch(args, bw):
     if rank == 0 and world == 1 and not args.no_cpu_baseline and bw.fp64_steps is not None:
         cpu = batch_cpu_baseline(prep, bw)
 
+    # ---- the serving form (Poisson arrivals of 4k..500k-node requests at two
+    # rates, the same requests at each), when the run's time target leaves room
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        left = BENCH_BUDGET_S - (time.time() - t_run0)
+        if left >= SERVE_MIN_LEFT_S:
+            serving = [serving_run(rate, SERVE_REQUESTS, arena, arena_bytes, bw.jacobian)
+                       for rate in SERVE_RATES]
+        else:
+            serving = {"skipped": f"the run's time target left {left:.0f} s"}
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": world,
@@ -631,6 +648,7 @@ def run_batch(args, bw):
                            "how": "every request staged from host buffers first, then all "
                                   "started, states and forces read back at the end (the "
                                   "value passes)"},
+            "serving": serving,
             "roofline": roof, "roofline_sweep": roof_sweep, "gpu_launches": int(launches),
             "residual_evaluations": {
                 "per_s": round(evals_all / (dev_ms_max / 1e3), 1),
@@ -953,15 +971,44 @@ def run_compare_precision(args):
     print(json.dumps(line), flush=True)
 
 
-def run_serve(args):
-    """The serving form: an open-loop Poisson stream of requests (node counts
-    log-uniform in [4k, 500k], the batching stream's flow conditions and
-    orders, seed 1), each prepared on arrival, admitted as the arena allows,
-    retired at a 1e-8 drop (or stalled / at max_steps).  One line: converged
-    solves per second of the run's span and p50/p95/p99 latency from arrival
-    to retirement."""
-    import torch
+def serving_run(rate: float, n: int, arena, budget: int, jacobian: int = 0,
+                index0: int = 0) -> dict:
+    """The serving form: an open-loop Poisson stream of n requests (node
+    counts log-uniform in [4k, 500k], the batching stream's flow conditions
+    and orders, stream seed 1, request indices index0..), each prepared on
+    arrival by a worker thread, admitted as the arena allows, retired at a
+    1e-8 drop (or stalled / at max_steps).  Converged solves per second of
+    the run's span and p50/p95/p99 latency from arrival to retirement."""
     from flowgpu import capi, serve
+    reqs = [serve.sample_request(index0 + i, seed=1, n_min=4000, n_max=500000)
+            for i in range(n)]
+    r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
+                          precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
+                          stall=2000, ramp_sweeps=2, jacobian=jacobian)
+    recs = r["records"]
+    conv = [x for x in recs if x.get("status") == 0]
+    return {"value": round(len(conv) / r["span_s"], 5), "unit": UNIT,
+            "form": "serving (open-loop Poisson arrivals)", "requests": n,
+            "rate_per_s": rate, "span_s": round(r["span_s"], 2), "converged": len(conv),
+            "stalled": sum(1 for x in recs if x.get("status") == capi.ERR_STALLED),
+            "not_converged": sum(1 for x in recs if x.get("status") == capi.ERR_NOT_CONVERGED),
+            "failed": sum(1 for x in recs if x.get("status") not in
+                          (0, capi.ERR_STALLED, capi.ERR_NOT_CONVERGED)),
+            "latency_s_converged": serve.percentiles([x["latency_s"] for x in conv]),
+            "latency_s_all": serve.percentiles([x["latency_s"] for x in recs]),
+            "admission_wait_s": serve.percentiles([x.get("admitted_s", 0.) for x in recs]),
+            "nodes": [x.get("nodes") for x in recs], "steps": [x.get("steps") for x in recs],
+            "status": [x.get("status") for x in recs],
+            "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
+                       "jacobian": jacobian, "ramp_sweeps_on_meshes_from_250k_nodes": 2,
+                       "stall_retire_steps": 2000, "arena_bytes": budget, "stream_seed": 1,
+                       "first_request": index0, "nodes_range": [4000, 500000]}}
+
+
+def run_serve(args):
+    """The serving form alone (bench.py --serve-rate R): one line."""
+    import torch
+    from flowgpu import capi, serve, workloads
     torch.cuda.set_device(0)
     n, rate = args.serve_requests, args.serve_rate
     reqs = [serve.sample_request(i, seed=1, n_min=4000, n_max=500000) for i in range(n)]
@@ -971,7 +1018,8 @@ def run_serve(args):
     with ClockSampler(0) as clk:
         r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
                               precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
-                              stall=2000, ramp_sweeps=2)
+                              stall=2000, ramp_sweeps=2,
+                              jacobian=workloads.BATCHES[workloads.DEFAULT_BENCH].jacobian)
     arena.close()
     recs = r["records"]
     conv = [x for x in recs if x.get("status") == 0]
@@ -1023,6 +1071,8 @@ def main():
     ap.add_argument("--impl", default="flow", choices=("flow", "reference"))
     ap.add_argument("--workload", default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="batch workloads: leave out the serving-form measurement")
     ap.add_argument("--kernel-times", action="store_true",
                     help="with --profile-steps: also print per-kernel device times")
     ap.add_argument("--profile-steps", type=int, default=0,

@@ -73,6 +73,7 @@ struct flow_server {
   int sched_sweeps = 0, sched_until = 0;  // sweep schedule of precision-form solves
   long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
   int priority_policy = 0;                // 1: larger meshes get greater stream priority
+  int jacobian = 0;                       // face Jacobians of precision-form solves
   // guards the slot table and the counters: stage may run on several host
   // threads at once (each builds its context outside the lock) beside
   // progress / start / result / release
@@ -146,7 +147,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     return FLOW_ERR_ARG;
   }
   int idx = -1;
-  int autotune_steps = 0, sched_sweeps = 0, sched_until = 0, priority_policy = 0;
+  int autotune_steps = 0, sched_sweeps = 0, sched_until = 0, priority_policy = 0, jacobian = 0;
   long sched_min_nodes = 0;
   {
     std::lock_guard<std::mutex> lock(sv->mu);
@@ -162,6 +163,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     sched_until = sv->sched_until;
     sched_min_nodes = sv->sched_min_nodes;
     priority_policy = sv->priority_policy;
+    jacobian = sv->jacobian;
   }
   auto unreserve = [&]() {
     std::lock_guard<std::mutex> lock(sv->mu);
@@ -180,6 +182,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   // mode 3 needs its chunk windows in shared memory; a mesh whose matrix
   // bandwidth is too large for that is served in mode 1 instead
   if (rc == FLOW_ERR_ARG && precision == 3) rc = flow_set_precision(c, 1);
+  if (!rc && precision != 0 && jacobian != 0) rc = flow_set_jacobian(c, jacobian);
   if (!rc && precision != 0 && sched_sweeps > 0 && flow_size(c, "dt") - 1 >= sched_min_nodes)
     rc = flow_set_sweep_schedule(c, sched_sweeps, sched_until);
   if (!rc && priority_policy == 1) {
@@ -406,6 +409,13 @@ int flow_server_set_stall(flow_server* sv, int steps) {
   if (!sv || steps < 0) return FLOW_ERR_ARG;
   std::lock_guard<std::mutex> lock(sv->mu);
   sv->stall_steps = steps;
+  return 0;
+}
+
+int flow_server_set_jacobian(flow_server* sv, int mode) {
+  if (!sv || mode < 0 || mode > 2) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  sv->jacobian = mode;
   return 0;
 }
 

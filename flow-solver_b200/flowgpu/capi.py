@@ -47,7 +47,8 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_server_release", "flow_server_running", "flow_server_last_error",
            "flow_server_set_autotune", "flow_server_set_stall",
            "flow_server_set_sweep_schedule", "flow_set_stream_priority",
-           "flow_server_set_priority_policy", "flow_selftest_sweep_timeout")
+           "flow_server_set_priority_policy", "flow_server_set_jacobian",
+           "flow_selftest_sweep_timeout")
 
 
 class FlowParamsC(C.Structure):
@@ -188,6 +189,7 @@ def _load_locked():
     L.flow_server_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int, C.c_longlong]
     L.flow_set_stream_priority.argtypes = [vp, C.c_int]
     L.flow_server_set_priority_policy.argtypes = [vp, C.c_int]
+    L.flow_server_set_jacobian.argtypes = [vp, C.c_int]
     L.flow_selftest_sweep_timeout.argtypes = [vp, C.c_long, IP]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
@@ -259,7 +261,7 @@ class Server:
 
     def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64, autotune: int = 0,
                  stall: int = 0, ramp_sweeps: int = 0, ramp_min_nodes: int = 250000,
-                 priority_policy: int = 0):
+                 priority_policy: int = 0, jacobian: int = 0):
         self.L = load()
         st = C.c_int(0)
         self.arena = arena
@@ -276,6 +278,8 @@ class Server:
         if priority_policy:
             _check(self.L.flow_server_set_priority_policy(self.h, int(priority_policy)),
                    "priority policy")
+        if jacobian:
+            _check(self.L.flow_server_set_jacobian(self.h, int(jacobian)), "jacobian")
         self._keep = {}
         self._out = (FlowCompletion * 64)()
 

@@ -117,6 +117,7 @@ class BatchWorkload:
     autotune: int = 0
     fp64_forces: tuple | None = None  # raw lift/drag of the FP64 drop-in per request
     priority_policy: int = 0          # 1: larger meshes on higher-priority streams
+    jacobian: int = 0                 # precision-form face Jacobians (flow_set_jacobian)
 
 
 BATCHES = {

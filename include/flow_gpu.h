@@ -514,6 +514,9 @@ int flow_server_set_stall(flow_server *srv, int steps);
  * 1 the larger the mesh, the greater its stream priority (the longest solves
  * of a batch keep the GPU first, the small ones fill the gaps). */
 int flow_server_set_priority_policy(flow_server *srv, int policy);
+/* flow_set_jacobian(mode) for every precision-form solve admitted later
+ * (0, the default: forward differences). */
+int flow_server_set_jacobian(flow_server *srv, int mode);
 /* flow_set_sweep_schedule for every precision-form solve admitted later on
  * a mesh of at least min_nodes nodes (measured: the 1.05M-node O-grid needs
  * 2 sweeps during the CFL ramp, meshes up to 124k nodes converge faster
