@@ -513,27 +513,49 @@ def run_batch(args, bw):
     e2e_staged = n_conv_all / (e2e_ms_max / 1e3)
 
     # ---- roofline: k_node_prepare4 on the largest mesh of the batch, served form ----
+    # the served configuration of that mesh: its precision form and Jacobian,
+    # the kernel variants the autotuner picks for it
     big = max(prep, key=lambda p: p.req.nodes)
     s = capi.Solver.from_mesh(big.mesh, big.params, device=local)
     s.set_precision(bw.precision)
+    s.set_jacobian(bw.jacobian)
     s.set_state(big.Q0)
+    variants, _ = s.autotune(ts=2, steps=4)
     s.run(1, 8)
     s.set_timing(True)
     s.run(9, 24)
     kt = s.kernel_times()
     s.close()
     peaks, peak_kind = measured_peaks()
-    cnt, ms = kt["node_prepare"]
-    np_ms = ms / max(cnt, 1)
-    np_bytes = roofline.node_prepare_bytes(big.mesh)
-    achieved = np_bytes / (np_ms * 1e-3) / 1e9
-    share = ms / max(sum(v[1] for v in kt.values()), 1e-30)
-    roof = {"bound": "hbm", "kernel": "k_node_prepare4", "mesh": f"{big.req.nc}x{big.req.nr}",
+    fused = bw.jacobian == 1 and bw.precision != 0
+    # algorithmic bytes per launch of each kernel class (flowgpu/roofline.py)
+    names = {"node_prepare": "k_node_stage" if variants[0] == 3 else "k_node_prepare4",
+             "subedge_flux": "k_faces_assemble" if fused else "k_subedge_flux",
+             "assemble": "k_assemble4"}
+    per_launch = {"node_prepare": roofline.node_prepare_bytes(big.mesh),
+                  "subedge_flux": (roofline.faces_assemble_bytes(big.mesh) if fused else
+                                   roofline.subedge_flux_bytes(big.mesh)),
+                  "assemble": roofline.assemble_bytes(big.mesh, bw.precision)}
+    if bw.precision == 3:  # one sweep: its colour launches
+        names["sweep"] = "k_sweep_chunk (one sweep)"
+        per_launch["sweep"] = roofline.chunk_sweep_bytes(big.mesh)
+    total_ms = max(sum(v[1] for v in kt.values()), 1e-30)
+    top = max(per_launch, key=lambda k: kt[k][1])  # the class with the largest device time
+    cnt, ms = kt[top]
+    k_ms = ms / max(cnt, 1)
+    achieved = per_launch[top] / (k_ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": names[top], "mesh": f"{big.req.nc}x{big.req.nr}",
             "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "peak_kind": peak_kind,
             "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
-            "traffic": ncu_traffic(f"{bw.name}:{big.req.nc}x{big.req.nr}", "node_prepare_dram_bytes"),
-            "algorithmic_bytes_per_launch": np_bytes, "avg_launch_ms": round(np_ms, 4),
-            "share_of_step": round(share, 3),
+            "traffic": ncu_traffic(f"{bw.name}:{big.req.nc}x{big.req.nr}",
+                                   f"{names[top]}_dram_bytes"),
+            "algorithmic_bytes_per_launch": per_launch[top], "avg_launch_ms": round(k_ms, 4),
+            "share_of_step": round(ms / total_ms, 3), "variants": list(variants),
+            "others": {names[k]: {"avg_launch_ms": round(kt[k][1] / max(kt[k][0], 1), 4),
+                                  "achieved_gbs": round(per_launch[k] / max(
+                                      kt[k][1] / max(kt[k][0], 1), 1e-9) * 1e-6, 1),
+                                  "share_of_step": round(kt[k][1] / total_ms, 3)}
+                       for k in per_launch if k != top and kt[k][0]},
             "kernels_ms": {k: round(t / max(c, 1), 4) for k, (c, t) in kt.items() if c}}
     scnt, sms = kt["sweep"]
     if bw.precision == 3 and scnt:
@@ -752,6 +774,10 @@ def run_profile(args):
     solver = capi.Solver.from_mesh(mesh, wl.params(), device=0)
     solver.set_sweep_mode(args.sweep_mode)
     solver.set_precision(args.precision)
+    if args.jacobian:
+        solver.set_jacobian(args.jacobian)
+    if args.node_variant >= 0:
+        solver.set_variants(args.node_variant, 0)
     if args.sweep_rows:
         solver.set_sweep_ring(args.sweep_rows)
     if args.sweep_dataflow:
@@ -1086,6 +1112,10 @@ def main():
                     help="with --profile-steps: one launch per mode 3 sweep (dataflow chunks)")
     ap.add_argument("--sweep-rows", type=int, default=0,
                     help="with --profile-steps: sub-level rows of the mode 3 sweep ring (64, 32, 16)")
+    ap.add_argument("--jacobian", type=int, default=0,
+                    help="with --profile-steps: precision-form face Jacobians (flow_set_jacobian)")
+    ap.add_argument("--node-variant", type=int, default=-1,
+                    help="with --profile-steps: node kernel variant (3: staged in shared memory)")
     ap.add_argument("--subits", type=int, default=0,
                     help="with --profile-steps: Gauss-Seidel sweeps per step (0: the workload's)")
     ap.add_argument("--serve-rate", type=float, default=0.,

@@ -72,3 +72,38 @@ def chunk_sweep_bytes(mesh) -> int:
     chunk's window and written back (16 + 16)."""
     z = _sizes(mesh)
     return int(z["nn"] * (640 + 16 + 16))
+
+
+def subedge_flux_bytes(mesh, jacobian: bool = True) -> int:
+    """k_subedge_flux: per subedge its end nodes 8, normal/length 32 and the
+    two node states 64 read (k=1 reconstruction: the two nodes' gradients
+    128, limiters 16 and the face-point offsets 32), the flux 32 written and,
+    with the Jacobian, dF/dqL and dF/dqR 256."""
+    z = _sizes(mesh)
+    per = 8 + 32 + 64 + (0 if mesh.order == 3 else 128 + 16 + 32) + 32 + (256 if jacobian else 0)
+    return int(z["ns"] * per)
+
+
+def assemble_bytes(mesh, precision: int = 3) -> int:
+    """k_assemble4: per subedge incidence (two a subedge) its entry 4, the
+    face's flux 32 and Jacobian 128 read; per off-diagonal block its
+    subedge pair 16 and the one or two face Jacobians (two a block on these
+    meshes) 256 read; per node dt, cv_area 16 read, R and RHS 64 written and
+    its row written: two 640-byte sweep records (mode 3), or FP64 blocks
+    128 a block and LU factors 128 (mode 0)."""
+    z = _sizes(mesh)
+    offd = z["nnz"] - z["nn"]
+    row = 2 * 640 if precision == 3 else 128 * z["nnz"] / max(z["nn"], 1) + 128
+    return int(2 * z["ns"] * (4 + 32 + 128) + offd * (16 + 256) + z["nn"] * (16 + 64 + row))
+
+
+def faces_assemble_bytes(mesh) -> int:
+    """k_faces_assemble (precision form, approximate Jacobian): per subedge
+    incidence its entry and block slot 8, the face's end nodes 8,
+    normal/length 32 and the other node's state 32 read (k=1: the two nodes'
+    gradients and limiters 144 and the offsets 32); per node its own state
+    32, dt and cv_area 16, R and RHS 64 and its two 640-byte sweep records;
+    per boundary edge its flux and Jacobian 160 read."""
+    z = _sizes(mesh)
+    per_inc = 8 + 8 + 32 + 32 + (0 if mesh.order == 3 else 144 + 32)
+    return int(2 * z["ns"] * per_inc + z["nn"] * (32 + 16 + 64 + 2 * 640) + z["nbe"] * 160)
