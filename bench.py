@@ -730,7 +730,8 @@ def measure_fp64(args, bw):
     prep = serve.prepare_all(reqs, 2, bw.max_steps, bw.drop)
     free, _ = torch.cuda.mem_get_info(0)
     arena = capi.Arena(int(min(free * 0.85, 150e9)))
-    r = serve.run_batch(prep, arena, precision=0, chunk=64, max_slots=bw.n)
+    # 16 at a time: the FP64 drop-in's ordered sweeps poll across the GPU
+    r = serve.run_batch(prep, arena, precision=0, chunk=64, max_slots=16)
     arena.close()
     recs = r["records"]
     steps = tuple(x["steps"] for x in recs)
