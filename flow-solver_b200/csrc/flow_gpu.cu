@@ -1813,6 +1813,8 @@ int flow_set_capture_fault(flow_ctx* c, int count) {
 
 long flow_capture_fallbacks(flow_ctx* c) { return c ? c->capture_fallbacks : -1; }
 
+int flow_precision_of(flow_ctx* c) { return c ? c->precision : -1; }
+
 int flow_solve(flow_ctx* c, const flow_params* p, int ts, double* dq_norm, double* r_rho) {
   if (!c || !c->ok) return FLOW_ERR_ARG;
   int rc = check_params(c, p);
@@ -2381,6 +2383,74 @@ int flow_autotune(flow_ctx* c, const flow_params* p, int ts, int steps, int* var
     variants[0] = c->var[0];
     variants[1] = c->var[1];
   }
+  return rc & FLOW_ERR_CUDA ? rc : read_status(c);
+}
+
+int flow_autotune_sweep(flow_ctx* c, const flow_params* p, int ts, int steps, int allow_df,
+                        int* choice, double* ms) {
+  if (!c || !c->ok || ts < 1) return FLOW_ERR_ARG;
+  if (c->precision != 3) {
+    set_error("flow_autotune_sweep: precision mode 3 only");
+    return FLOW_ERR_ARG;
+  }
+  int rc = check_params(c, p);
+  if (rc) return rc;
+  cudaSetDevice(c->device);
+  if (steps < 1) steps = 4;
+  if ((rc = flow_save_state(c))) return rc;
+  if ((rc = ensure_hist(c, 1))) return rc;
+  const int saved_timing = c->timing, saved_ring = c->ring, saved_df = c->sweep_df;
+  long kc[8];
+  double km[8];
+  std::copy(c->kcount, c->kcount + 8, kc);
+  std::copy(c->kms, c->kms + 8, km);
+  // candidates: the three ring shapes with one launch per colour, and the
+  // 64-row shape with one launch per sweep (allow_df)
+  const int nc = kRingShapes + 1;
+  int best = -1;
+  double best_ms = 1e30;
+  for (int k = 0; k < nc && !rc; k++) {
+    const int shape = k < kRingShapes ? k : 0, df = k < kRingShapes ? 0 : 1;
+    if (ms) ms[k] = 1e30;
+    if (!c->ring_ok[shape] || (df && !allow_df)) continue;
+    c->ring = shape;
+    c->sweep_df = df;
+    apply_ring(c);
+    rc |= flow_restore_state(c);
+    reset_run(c, 0.);
+    c->timing = 0;
+    rc |= enqueue_step(c, p, ts, -1, 1);  // warm-up, untimed
+    cudaStreamSynchronize(c->stream);
+    harvest(c);
+    c->kcount[4] = 0;
+    c->kms[4] = 0.;
+    c->timing = 1;
+    for (int i = 0; i < steps && !rc; i++) rc |= enqueue_step(c, p, ts + 1 + i, -1, 0);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) rc |= FLOW_ERR_CUDA;
+    harvest(c);
+    const double t = c->kcount[4] ? c->kms[4] / c->kcount[4] : 1e30;
+    if (ms) ms[k] = t;
+    if (t < best_ms) {
+      best_ms = t;
+      best = k;
+    }
+  }
+  if (best < 0) {
+    c->ring = saved_ring;
+    c->sweep_df = saved_df;
+  } else {
+    c->ring = best < kRingShapes ? best : 0;
+    c->sweep_df = best < kRingShapes ? 0 : 1;
+  }
+  apply_ring(c);
+  c->timing = saved_timing;
+  std::copy(kc, kc + 8, c->kcount);
+  std::copy(km, km + 8, c->kms);
+  cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream);
+  rc |= flow_restore_state(c);
+  reset_run(c, 0.);
+  drop_graphs(c);
+  if (choice) *choice = ring_rows(c->ring) + (c->sweep_df ? 1000 : 0);
   return rc & FLOW_ERR_CUDA ? rc : read_status(c);
 }
 

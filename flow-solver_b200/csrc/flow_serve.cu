@@ -37,7 +37,11 @@ thread_local std::string g_serve_error;
 // bit-identical results and their speed depends only on the device and the
 // mesh, so a choice measured once holds for every later admission.
 std::mutex g_tuned_mutex;
-std::map<std::tuple<int, int, int, int>, std::pair<int, int>> g_tuned;
+struct Tuned {
+  int node = -1, flux = -1;  // kernel variants (flow_autotune)
+  int sweep = 0;             // mode 3 sweep shape (flow_autotune_sweep), 0: not tuned
+};
+std::map<std::tuple<int, int, int, int>, Tuned> g_tuned;
 // one tuning run at a time, so that concurrent admissions do not time their
 // variants against each other's kernels
 std::mutex g_tuning_run_mutex;
@@ -203,24 +207,34 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     auto lookup = [&]() {
       std::lock_guard<std::mutex> lock(g_tuned_mutex);
       auto it = g_tuned.find(key);
-      return it != g_tuned.end() ? it->second : std::make_pair(-1, -1);
+      return it != g_tuned.end() ? it->second : Tuned();
     };
-    std::pair<int, int> found = lookup();
+    Tuned found = lookup();
     std::unique_lock<std::mutex> run_lock(g_tuning_run_mutex, std::defer_lock);
-    if (found.first < 0) {
+    if (found.node < 0) {
       run_lock.lock();
       found = lookup();  // another admission may have tuned this bucket meanwhile
     }
-    if (found.first >= 0) {
-      rc = flow_set_variants(c, found.first, found.second);
+    const int mode = flow_precision_of(c);
+    if (found.node >= 0) {
+      rc = flow_set_variants(c, found.node, found.flux);
+      if (!rc && mode == 3 && found.sweep > 0) {
+        rc = flow_set_sweep_ring(c, found.sweep % 1000);
+        if (!rc && found.sweep >= 1000) rc = flow_set_sweep_dataflow(c, 1);
+      }
     } else {
+      Tuned t;
       int v[2] = {0, 0};
-      const int trc = flow_autotune(c, p, 1, autotune_steps, v, nullptr);
+      int trc = flow_autotune(c, p, 1, autotune_steps, v, nullptr);
+      t.node = v[0];
+      t.flux = v[1];
+      if (!(trc & FLOW_ERR_CUDA) && mode == 3)
+        trc |= flow_autotune_sweep(c, p, 1, autotune_steps, 0, &t.sweep, nullptr);
       if (trc & FLOW_ERR_CUDA) {
         rc = trc;  // other bits: the tuning steps' physics, not fatal
       } else {
         std::lock_guard<std::mutex> lock(g_tuned_mutex);
-        g_tuned[key] = std::make_pair(v[0], v[1]);
+        g_tuned[key] = t;
       }
     }
   }

@@ -34,10 +34,10 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_residuals", "flow_residual_stage", "flow_linear_solve", "flow_body_forces", "flow_surface_cp",
            "flow_write_surface_cp", "flow_write_tecplot", "flow_write_restart", "flow_get",
            "flow_size", "flow_set",
-           "flow_set_sweep_mode", "flow_set_precision", "flow_set_chunk", "flow_set_sweep_ring", "flow_set_sweep_dataflow", "flow_chunk_starts", "flow_set_graphs",
+           "flow_set_sweep_mode", "flow_set_precision", "flow_precision_of", "flow_set_chunk", "flow_set_sweep_ring", "flow_set_sweep_dataflow", "flow_chunk_starts", "flow_set_graphs",
            "flow_set_capture_fault", "flow_capture_fallbacks", "flow_set_jacobian",
            "flow_set_exact_rms",
-           "flow_autotune", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
+           "flow_autotune", "flow_autotune_sweep", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
            "flow_linear_residual_noalloc", "flow_arena_create", "flow_arena_destroy",
@@ -133,6 +133,7 @@ def _load_locked():
     L.flow_set.argtypes = [vp, C.c_char_p, DP, C.c_long]
     L.flow_set_sweep_mode.argtypes = [vp, C.c_int]
     L.flow_set_precision.argtypes = [vp, C.c_int]
+    L.flow_precision_of.argtypes = [vp]
     L.flow_set_graphs.argtypes = [vp, C.c_int]
     L.flow_set_capture_fault.argtypes = [vp, C.c_int]
     L.flow_set_jacobian.argtypes = [vp, C.c_int]
@@ -144,6 +145,7 @@ def _load_locked():
     L.flow_set_sweep_dataflow.argtypes = [vp, C.c_int]
     L.flow_autotune.argtypes = [vp, PP, C.c_int, C.c_int, IP, DP]
     L.flow_set_variants.argtypes = [vp, C.c_int, C.c_int]
+    L.flow_autotune_sweep.argtypes = [vp, PP, C.c_int, C.c_int, C.c_int, IP, DP]
     L.flow_set_sweep_schedule.argtypes = [vp, C.c_int, C.c_int]
     L.flow_chunk_starts.argtypes = [vp, IP, C.c_int, IP, IP]
     L.flow_save_state.argtypes = [vp]
@@ -601,6 +603,15 @@ class Solver:
         _check(self.L.flow_autotune(self.ctx, C.byref(self.p), int(ts), int(steps), v, ms),
                "flow_autotune")
         return (v[0], v[1]), [round(x, 4) for x in ms]
+
+    def autotune_sweep(self, ts: int = 2, steps: int = 4, allow_df: bool = False):
+        """Pick the fastest mode 3 sweep shape; returns (rows + 1000*one_launch, ms)."""
+        ch = C.c_int(0)
+        ms = (C.c_double * 4)()
+        _check(self.L.flow_autotune_sweep(self.ctx, C.byref(self.p), int(ts), int(steps),
+                                          int(bool(allow_df)), C.byref(ch), ms),
+               "flow_autotune_sweep")
+        return ch.value, [round(x, 4) for x in ms]
 
     def set_sweep_schedule(self, sweeps: int, until_step: int = 0):
         """`sweeps` Gauss-Seidel sweeps up to `until_step` (0: end of the CFL ramp)."""

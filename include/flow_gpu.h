@@ -306,6 +306,8 @@ int flow_set_sweep_mode(flow_ctx *ctx, int mode);
  * most 8 off-diagonal blocks per row and a matrix bandwidth whose chunk
  * windows fit in shared memory; otherwise switching to it fails. */
 int flow_set_precision(flow_ctx *ctx, int mode);
+/* The context's precision mode (0..3; -1 for a null context). */
+int flow_precision_of(flow_ctx *ctx);
 /* Face Jacobians of the precision form (no reference counterpart): mode 0
  * (default) the reference's forward differences (jacobian.C:45-185, eight
  * extra Roe fluxes per face); mode 1 the approximate Roe Jacobian
@@ -427,6 +429,18 @@ double flow_last_device_ms(flow_ctx *ctx);
 int flow_autotune(flow_ctx *ctx, const flow_params *p, int ts, int steps, int *variants,
                   double *ms);
 int flow_set_variants(flow_ctx *ctx, int node_prepare, int flux);
+/* The sweep of precision mode 3 in the shape that runs fastest on this mesh:
+ * the record ring of 64, 32 or 16-row sub-levels with one launch per colour
+ * (colours per launch = 1), and, with allow_df, the 64-row ring with the
+ * whole sweep in one launch (flow_set_sweep_dataflow; its chunks wait for
+ * their neighbours on the device, so among many solves it holds SMs that
+ * others could use).  Every shape gives the same bits.  Timed like
+ * flow_autotune, the state put back; *choice = the rows of the chosen ring,
+ * plus 1000 for one launch per sweep; ms[4] (may be NULL) the sweep times
+ * (1e30 where a shape does not fit or is not allowed).  The sweep count is
+ * not chosen here: it changes the iterates, not only their speed. */
+int flow_autotune_sweep(flow_ctx *ctx, const flow_params *p, int ts, int steps, int allow_df,
+                        int *choice, double *ms);
 
 /* ---- Device arena (no counterpart in the reference) ----------------------
  * One cudaMalloc of `bytes` on `device`, carved into the buffers of the
