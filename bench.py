@@ -515,7 +515,11 @@ def run_batch(args, bw):
     # ---- roofline: k_node_prepare4 on the largest mesh of the batch, served form ----
     # the served configuration of that mesh: its precision form and Jacobian,
     # the kernel variants the autotuner picks for it
-    big = max(prep, key=lambda p: p.req.nodes)
+    # (the largest one whose solve stays physical: some requests of the stream
+    # reach a non-physical state within a few steps, in the reference too)
+    ok = [i for i in range(len(prep)) if bw.fp64_status is None
+          or bw.fp64_status[i] in (0, capi.ERR_NOT_CONVERGED)]
+    big = max((prep[i] for i in ok), key=lambda p: p.req.nodes)
     s = capi.Solver.from_mesh(big.mesh, big.params, device=local)
     s.set_precision(bw.precision)
     s.set_jacobian(bw.jacobian)

@@ -259,30 +259,15 @@ __device__ __forceinline__ double max_wave(const double* q, double nx, double ny
 
 // limiter.C:672-700: one reconstructed value's Venkatakrishnan bound
 // (phi(y) = (y^2+2y)/(y^2+y+2), no epsilon), folded into phi with MIN().
-//
-// phi starts at 1 and only falls, so a point whose computed bound is at
-// least 1 leaves it unchanged.  For y in [2.001, 1e14] the computed bound is
-// at least 1: numerator - denominator is y - 2 in exact arithmetic, and the
-// three roundings on either side (each at most 2^-53 of t^2+2t+2) stay far
-// below it; a quotient of a numerator above its denominator rounds to 1 or
-// more.  Such points are recognised from two products instead of the two
-// divisions: a >= 2.002 d and a <= 0.9e14 d (signs folded for d < 0) put
-// fl(a/d) inside that range even after the products' and the quotient's own
-// roundings, for any normal d.  Every other point, a NaN phi or a NaN
-// operand takes the reference's expressions, so phi is the same bits.
 __device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0, double qmin,
                                               double qmax) {
   double d = qrec - q0;
   if (d > 0.) {
-    const double a = qmax - q0;
-    if (ph == ph && d >= 1e-290 && a >= 2.002 * d && a <= 0.9e14 * d) return ph;
-    double t = a / (qrec - q0);
+    double t = (qmax - q0) / (qrec - q0);
     t = (t * t + 2. * t) / (t * t + t + 2.);
     return ph <= t ? ph : t;
   } else if (d < 0.) {
-    const double a = qmin - q0;
-    if (ph == ph && d <= -1e-290 && a <= 2.002 * d && a >= 0.9e14 * d) return ph;
-    double t = a / (qrec - q0);
+    double t = (qmin - q0) / (qrec - q0);
     t = (t * t + 2. * t) / (t * t + t + 2.);
     return ph <= t ? ph : t;
   }

@@ -33,10 +33,11 @@ def _alone(pr):
     except capi.FlowError:
         s.set_precision(1)  # what the server does for a mesh mode 3 cannot take
     s.set_state(pr.Q0)
-    steps, _r0, _r1 = s.converge(1, MAX_STEPS, 1e-10, chunk=32, check=False)
+    steps, r0, r1 = s.converge(1, MAX_STEPS, 1e-10, chunk=32, check=False)
+    st = s.status() or (0 if r1 < 1e-10 * r0 else capi.ERR_NOT_CONVERGED)
     q = s.get("Q")
     s.close()
-    return steps, q
+    return steps, st, q
 
 
 def _stream_pass(prep, arena):
@@ -78,9 +79,11 @@ def test_threaded_admission_of_the_batch_matches_solves_run_alone():
     arena = capi.Arena(16 << 30)
     for _ in range(3):
         got = _stream_pass(prep, arena)
-        for i, (steps, q) in enumerate(alone):
+        for i, (steps, st, q) in enumerate(alone):
             c, q2 = got[i]
-            assert c["status"] in (0, capi.ERR_NOT_CONVERGED), (i, c["status"])
+            # a request that turns non-physical does so alone too, at the same step
+            assert c["status"] == st, (i, c["status"], st)
             assert c["steps"] == steps, (i, c["steps"], steps)
-            assert np.array_equal(q[4:], q2[4:]), i
+            if q2 is not None:
+                assert np.array_equal(q[4:], q2[4:]), i
     arena.close()
