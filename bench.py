@@ -69,7 +69,7 @@ REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
 BENCH_BUDGET_S = 1500.      # wall-clock target of a whole batch run (warm-up and checks included)
 SERVE_RATES = (0.5, 2.0)    # requests/s of the serving measurement in the batch run
 SERVE_REQUESTS = 16
-SERVE_MIN_LEFT_S = 240.     # run the serving measurement only with this much time left
+SERVE_MIN_LEFT_S = 200.     # run the serving measurement only with this much time left
 REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
 STAGE_THREADS = max(1, min(8, os.cpu_count() or 1))  # concurrent admissions per batch pass
 CPU_BASELINE_STEPS = 6      # pseudo-time steps timed for cpu_baseline
@@ -490,7 +490,8 @@ def run_batch(args, bw):
         # the streamed (end-to-end) passes repeat the value passes' work from
         # host buffers; as many as the run's time target leaves room for, at
         # least 3 and at most K (every rank runs the same number)
-        left = BENCH_BUDGET_S - (time.time() - t_run0) - 120.
+        # room kept for the FP64 model, the CPU baseline and the serving runs
+        left = BENCH_BUDGET_S - (time.time() - t_run0) - 120. - SERVE_MIN_LEFT_S
         n_e2e = int(max(3, min(args.steps, left // max(1.1 * t_pass, 1e-3))))
         n_e2e = int(allreduce_max(pg, n_e2e)) if pg is not None else n_e2e
         log(f"[rank {rank}] {bw.name}: value passes done at {time.time() - t_run0:.0f} s; "

@@ -172,7 +172,7 @@ struct flow_ctx {
   // optional per-kernel event timing
   int timing = 0;
   std::vector<cudaEvent_t> event_pool;
-  struct Pending { int cls; cudaEvent_t a, b; };
+  struct Pending { int cls; cudaEvent_t a, b; int weight; };
   std::vector<Pending> pending;
   long kcount[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   double kms[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -224,6 +224,7 @@ struct flow_ctx {
   int jac_mode = 0;  // face Jacobians of the precision form (flow_set_jacobian)
   bool fused_ok = false;  // every row has at most kRecBlocks off-diagonal blocks
   int exact_rms = 0;      // every b-Ax RMS in the reference's order (flow_set_exact_rms)
+  int sweep_pairs = 1;    // mode 3: a colour's two passes in a row as one launch
   // staged node kernel (node_prepare variant 3): largest per-tile slices and
   // whether its shared memory fits, per order of the kernel
   StageCaps stage_caps{};
@@ -338,8 +339,9 @@ cudaEvent_t get_event(flow_ctx* c) {
 struct Timed {
   flow_ctx* c;
   int cls;
+  int weight;  // launches of the class the bracket counts as
   cudaEvent_t a = nullptr;
-  Timed(flow_ctx* ctx, int k) : c(ctx), cls(k) {
+  Timed(flow_ctx* ctx, int k, int w = 1) : c(ctx), cls(k), weight(w) {
     if (c->timing) {
       a = get_event(c);
       cudaEventRecord(a, c->stream);
@@ -349,7 +351,7 @@ struct Timed {
     if (c->timing) {
       cudaEvent_t b = get_event(c);
       cudaEventRecord(b, c->stream);
-      c->pending.push_back({cls, a, b});
+      c->pending.push_back({cls, a, b, weight});
     }
   }
 };
@@ -360,7 +362,7 @@ void harvest(flow_ctx* c) {
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
       c->kms[p.cls] += ms;
-      c->kcount[p.cls] += 1;
+      c->kcount[p.cls] += p.weight;
     }
     c->event_pool.push_back(p.a);
     c->event_pool.push_back(p.b);
@@ -509,6 +511,40 @@ int launch_linear_solve_mixed(flow_ctx* c, const flow_params* p) {
     // coloured chunks of the reference order, in-place FP32 iterate
     const ChunkTables& ct = c->ct;
     const size_t smem = 16 * kRecStride * kRingRecords + sizeof(float4) * ct.maxwin;
+    if (c->sweep_pairs && !(c->sweep_df && ct.ring == 0) && p->subits > 1) {
+      // the (sweep, colour) passes in order; where one sweep ends with the
+      // colour the next begins with, the two passes are one launch
+      std::vector<std::pair<int, int>> passes;
+      for (int it = 0; it < p->subits; it++)
+        for (int ci = 0; ci < ct.ncol; ci++)
+          passes.push_back({it, it % 2 == 0 ? ci : ct.ncol - 1 - ci});
+      Timed t(c, 4, p->subits);
+      for (size_t k = 0; k < passes.size(); k++) {
+        const int it = passes[k].first, col = passes[k].second, dir = it % 2;
+        const int nb = c->h_col_ptr[col + 1] - c->h_col_ptr[col];
+        const bool pair = k + 1 < passes.size() && passes[k + 1].second == col;
+        const int last = (pair ? passes[k + 1].first : it) == p->subits - 1;
+        if (pair) k++;
+        if (nb <= 0) continue;
+        if (pair) {
+          auto kern = dir == 0 ? (ct.ring == 2 ? k_sweep_chunk_pair<0, 16>
+                                  : ct.ring == 1 ? k_sweep_chunk_pair<0, 32>
+                                                 : k_sweep_chunk_pair<0, 64>)
+                               : (ct.ring == 2 ? k_sweep_chunk_pair<1, 16>
+                                  : ct.ring == 1 ? k_sweep_chunk_pair<1, 32>
+                                                 : k_sweep_chunk_pair<1, 64>);
+          kern<<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
+        } else {
+          auto kern = dir == 0 ? (ct.ring == 2 ? k_sweep_chunk<0, 16>
+                                  : ct.ring == 1 ? k_sweep_chunk<0, 32> : k_sweep_chunk<0, 64>)
+                               : (ct.ring == 2 ? k_sweep_chunk<1, 16>
+                                  : ct.ring == 1 ? k_sweep_chunk<1, 32> : k_sweep_chunk<1, 64>);
+          kern<<<nb, 256, smem, c->stream>>>(c->s, ct, c->mt.dq32, col, last);
+        }
+        rc |= launch_check(c);
+      }
+      return rc;
+    }
     for (int it = 0; it < p->subits; it++) {
       Timed t(c, 4);
       const int last = it == p->subits - 1, dir = it % 2;
@@ -937,7 +973,10 @@ bool ensure_kernel_attrs(int device) {
   const int chunk_cap = 227 * 1024 - kChunkStaticSmem;
   const int cta = (int)sizeof(SweepSmem);
   bool ok = preload_kernels();
-  for (const void* f : {(const void*)k_sweep_chunk_df<0>, (const void*)k_sweep_chunk_df<1>,
+  for (const void* f : {(const void*)k_sweep_chunk_pair<0, 64>, (const void*)k_sweep_chunk_pair<1, 64>,
+                        (const void*)k_sweep_chunk_pair<0, 32>, (const void*)k_sweep_chunk_pair<1, 32>,
+                        (const void*)k_sweep_chunk_pair<0, 16>, (const void*)k_sweep_chunk_pair<1, 16>,
+                        (const void*)k_sweep_chunk_df<0>, (const void*)k_sweep_chunk_df<1>,
                         (const void*)k_sweep_chunk<0, 64>, (const void*)k_sweep_chunk<1, 64>,
                         (const void*)k_sweep_chunk<0, 32>, (const void*)k_sweep_chunk<1, 32>,
                         (const void*)k_sweep_chunk<0, 16>, (const void*)k_sweep_chunk<1, 16>})
@@ -1784,6 +1823,18 @@ int flow_set_jacobian(flow_ctx* c, int mode) {
   cudaStreamSynchronize(c->stream);
   drop_graphs(c);
   c->jac_mode = mode;
+  return 0;
+}
+
+int flow_set_sweep_pairs(flow_ctx* c, int on) {
+  if (!c || !c->ok) {
+    set_error("flow_set_sweep_pairs: null context");
+    return FLOW_ERR_ARG;
+  }
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  drop_graphs(c);
+  c->sweep_pairs = on ? 1 : 0;
   return 0;
 }
 

@@ -1448,9 +1448,12 @@ __global__ void k_fill_sweep_records(SweepRec* __restrict__ rec, const int* __re
 // kernel (DF true) queues the records first, calls wait_deps() (which
 // returns once the chunk's earlier-colour neighbours have finished this
 // sweep, every thread past a barrier) and only then reads the window.
+// reuse_window: the chunk's window is already in shared memory, current (the
+// CTA's previous pass over the same chunk left it there).
 template <int DIR, int ROWS, bool DF, class Wait>
 __device__ __forceinline__ void sweep_chunk_body(const DevState& s, const ChunkTables& ct,
-                                                 float* dq32, int q, int last, Wait&& wait_deps) {
+                                                 float* dq32, int q, int last, int* ss,
+                                                 Wait&& wait_deps, bool reuse_window = false) {
   constexpr int SLOTS = kRingRecords / ROWS;
   static_assert(SLOTS * ROWS == kRingRecords && SLOTS >= 3 && 4 * ROWS <= 256,
                 "ring shape");
@@ -1462,14 +1465,15 @@ __device__ __forceinline__ void sweep_chunk_body(const DevState& s, const ChunkT
   const int nwin = w.y - w.x + 1;
   float4* X = reinterpret_cast<float4*>(dq32);
   auto load_window = [&]() {
-    for (int i = tid; i < nwin; i += blockDim.x) cp_async16(win + i, X + w.x + i);
+    if (!reuse_window)
+      for (int i = tid; i < nwin; i += blockDim.x) cp_async16(win + i, X + w.x + i);
     cp_async_commit();
   };
   if (!DF) load_window();
   const int S0 = ct.chunk_sub[DIR][q], nsub = ct.chunk_sub[DIR][q + 1] - S0;
-  // the chunk's sub-level starts, read once into shared memory (they sit on
-  // the loop's critical path); a chunk has at most kChunkSubMax sub-levels
-  __shared__ int ss[kChunkSubMax + 1];
+  // the chunk's sub-level starts, read once into shared memory ss (the
+  // caller's kChunkSubMax + 1 ints; they sit on the loop's critical path); a
+  // chunk has at most kChunkSubMax sub-levels
   for (int i = tid; i <= nsub && i <= kChunkSubMax; i += blockDim.x)
     ss[i] = ct.sub_start[DIR][S0 + i];
   __syncthreads();
@@ -1553,7 +1557,25 @@ __global__ void __launch_bounds__(256) k_sweep_chunk(DevState s, ChunkTables ct,
                                                      int colour, int last) {
   if (*s.stop) return;  // the run has converged
   const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
-  sweep_chunk_body<DIR, ROWS, false>(s, ct, dq32, q, last, [] {});
+  __shared__ int ss[kChunkSubMax + 1];
+  sweep_chunk_body<DIR, ROWS, false>(s, ct, dq32, q, last, ss, [] {});
+}
+
+// Two passes of one colour back to back: the DIR pass of a sweep (it ends
+// with this colour) and the opposite pass of the next sweep (it starts with
+// it).  Chunks of one colour read only rows of other colours and their own,
+// and no other colour runs between the two passes, so each chunk sweeps
+// itself twice with its window kept in shared memory: what two launches
+// compute, with one launch, one window load and no barrier between them.
+template <int DIR, int ROWS>
+__global__ void __launch_bounds__(256) k_sweep_chunk_pair(DevState s, ChunkTables ct,
+                                                          float* dq32, int colour, int last) {
+  if (*s.stop) return;  // the run has converged
+  const int q = ct.col_chunks[ct.col_ptr[colour] + blockIdx.x];
+  __shared__ int ss[kChunkSubMax + 1];
+  sweep_chunk_body<DIR, ROWS, false>(s, ct, dq32, q, 0, ss, [] {});
+  __syncthreads();  // the first pass's window is complete before the second reads it
+  sweep_chunk_body<1 - DIR, ROWS, false>(s, ct, dq32, q, last, ss, [] {}, true);
 }
 
 // A whole mode 3 sweep in one launch (one CTA per chunk): CTAs take chunks
@@ -1607,7 +1629,8 @@ __global__ void __launch_bounds__(256) k_sweep_chunk_df(DevState s, ChunkTables 
     }
     __syncthreads();
   };
-  sweep_chunk_body<DIR, 64, true>(s, ct, dq32, q, last, wait_deps);
+  __shared__ int ss[kChunkSubMax + 1];
+  sweep_chunk_body<DIR, 64, true>(s, ct, dq32, q, last, ss, wait_deps);
   // publish: every thread's iterate writes before the chunk's flag
   __threadfence();
   __syncthreads();

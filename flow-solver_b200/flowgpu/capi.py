@@ -36,7 +36,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_size", "flow_set",
            "flow_set_sweep_mode", "flow_set_precision", "flow_precision_of", "flow_set_chunk", "flow_set_sweep_ring", "flow_set_sweep_dataflow", "flow_chunk_starts", "flow_set_graphs",
            "flow_set_capture_fault", "flow_capture_fallbacks", "flow_set_jacobian",
-           "flow_set_exact_rms",
+           "flow_set_exact_rms", "flow_set_sweep_pairs",
            "flow_autotune", "flow_autotune_sweep", "flow_set_variants", "flow_set_sweep_schedule", "flow_save_state", "flow_restore_state", "flow_set_timing",
            "flow_kernel_times", "flow_stream", "flow_status", "flow_clear_status",
            "flow_last_error", "flow_launch_count", "flow_last_device_ms",
@@ -138,6 +138,7 @@ def _load_locked():
     L.flow_set_capture_fault.argtypes = [vp, C.c_int]
     L.flow_set_jacobian.argtypes = [vp, C.c_int]
     L.flow_set_exact_rms.argtypes = [vp, C.c_int]
+    L.flow_set_sweep_pairs.argtypes = [vp, C.c_int]
     L.flow_capture_fallbacks.restype = C.c_long
     L.flow_capture_fallbacks.argtypes = [vp]
     L.flow_set_chunk.argtypes = [vp, C.c_int, C.c_int]
@@ -637,6 +638,10 @@ class Solver:
     def set_jacobian(self, mode: int):
         """Precision-form face Jacobians: 0 forward differences, 1 approximate Roe."""
         _check(self.L.flow_set_jacobian(self.ctx, int(mode)), "flow_set_jacobian")
+
+    def set_sweep_pairs(self, on: bool):
+        """Mode 3: a colour's two passes in a row as one launch (default on)."""
+        _check(self.L.flow_set_sweep_pairs(self.ctx, int(bool(on))), "flow_set_sweep_pairs")
 
     def set_exact_rms(self, on: bool):
         """Sum every b-Ax RMS in the reference's row order (flow_set_exact_rms)."""

@@ -328,6 +328,15 @@ int flow_set_jacobian(flow_ctx *ctx, int mode);
  * while the CFL ramps keep the early, poorly conditioned Newton steps from
  * overshooting when the precision form solves them too accurately. */
 int flow_set_sweep_schedule(flow_ctx *ctx, int sweeps, int until_step);
+/* Paired passes of the mode 3 sweeps (no counterpart in the reference): a
+ * symmetric Gauss-Seidel step ends each forward sweep with the colour the
+ * backward sweep begins with (and each backward sweep with the colour the
+ * next forward begins with).  on != 0 (the default) runs those two passes
+ * of a colour as one launch in which every chunk sweeps itself twice with
+ * its window kept in shared memory: S sweeps over C colours take S*C - S + 1
+ * launches instead of S*C, with the same bits (chunks of one colour read
+ * only rows of other colours, which do not change between the two passes). */
+int flow_set_sweep_pairs(flow_ctx *ctx, int on);
 /* Chunk limits of precision mode 3 (0: defaults, rows = twice the matrix
  * bandwidth up to 2048, levels = 32). */
 int flow_set_chunk(flow_ctx *ctx, int rows, int levels);

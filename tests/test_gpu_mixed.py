@@ -199,3 +199,30 @@ def test_approximate_jacobian_converges_to_the_fp64_answer(order):
     (n0, f0), (n1, f1) = out[0], out[3]
     assert abs(f1[0] - f0[0]) <= 1e-8 * max(1.0, abs(f0[0]))
     assert abs(f1[1] - f0[1]) <= 1e-8 * max(1.0, abs(f0[1]))
+
+
+@pytest.mark.parametrize("subits,ring,order", [(4, 0, 3), (3, 0, 3), (2, 32, 3), (4, 16, 1),
+                                               (5, 0, 1)])
+def test_paired_colour_passes_bitwise(subits, ring, order):
+    """Mode 3 with a colour's two passes in a row as one launch (the default)
+    against one launch per pass: the same iterates, step by step, with graph
+    chunks, for several sweep counts and ring shapes."""
+    from flowgpu import capi, workloads
+    from flowgpu.prep import Mesh
+    wl = workloads.Workload("pairs", 128, 32, order == 3, order, 0.8 if order == 3 else 0.5,
+                            subits=subits)
+    mesh = Mesh.from_case(wl.write(), order=order)
+    fp = wl.params()
+    out = []
+    for pairs in (False, True):
+        s = capi.Solver.from_mesh(mesh, fp, device=0)
+        s.set_precision(3)
+        s.set_sweep_ring(ring)
+        s.set_sweep_pairs(pairs)
+        s.set_state(mesh.initial_state(fp))
+        steps, r0, r1 = s.converge(1, 200, 1e-10, chunk=16, check=False)
+        out.append((steps, r0, r1, s.get("Q"), s.get("dQ"), s.status()))
+        s.close()
+    (n0, a0, b0, q0, d0, st0), (n1, a1, b1, q1, d1, st1) = out
+    assert st0 == st1 and n0 == n1 and a0 == a1 and b0 == b1
+    assert np.array_equal(q0, q1) and np.array_equal(d0, d1)
