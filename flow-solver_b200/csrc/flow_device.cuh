@@ -259,19 +259,21 @@ __device__ __forceinline__ double max_wave(const double* q, double nx, double ny
 
 // limiter.C:672-700: one reconstructed value's Venkatakrishnan bound
 // (phi(y) = (y^2+2y)/(y^2+y+2), no epsilon), folded into phi with MIN().
+// Written without branches: the reference's two branches differ only in the
+// numerator (qmax - q0 above, qmin - q0 below), so the numerator is selected
+// and the quotients formed for every point; where the difference is zero or
+// NaN (the reference's third branch) the quotients are discarded and the
+// fold takes MIN(phi, 1).  The same expressions on the same operands give the
+// same bits, and the divisions of a lane's face points no longer wait on one
+// another's branches.
 __device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0, double qmin,
                                               double qmax) {
-  double d = qrec - q0;
-  if (d > 0.) {
-    double t = (qmax - q0) / (qrec - q0);
-    t = (t * t + 2. * t) / (t * t + t + 2.);
-    return ph <= t ? ph : t;
-  } else if (d < 0.) {
-    double t = (qmin - q0) / (qrec - q0);
-    t = (t * t + 2. * t) / (t * t + t + 2.);
-    return ph <= t ? ph : t;
-  }
-  return ph <= 1.0 ? ph : 1.0;
+  const double d = qrec - q0;
+  const bool up = d > 0., down = d < 0.;
+  double t = (up ? qmax - q0 : qmin - q0) / (qrec - q0);
+  t = (t * t + 2. * t) / (t * t + t + 2.);
+  const double b = (up || down) ? t : 1.0;
+  return ph <= b ? ph : b;
 }
 
 // linear_algebra.C:571-596 lu() on a 4x4 row-major block, in place.

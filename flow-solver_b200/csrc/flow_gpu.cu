@@ -375,9 +375,10 @@ void harvest(flow_ctx* c) {
 // k_node_prepare4: variant 0, 1, 2 -> 0 (compiler's choice), 10, 12 blocks.
 // k_subedge_flux:  variant 0, 1, 2 -> 4, 5, 3 blocks.
 constexpr int kVariants = 3;
-// k_node_prepare4 has a fourth: variant 3 = k_node_stage (gathers staged in
-// shared memory), where its shared memory fits the mesh.
-constexpr int kNodeVariants = 4;
+// k_node_prepare4 has two more: variant 3 = k_node_stage (gathers staged in
+// shared memory), where its shared memory fits the mesh; variant 4 =
+// k_node_prepare16 (each node's chains split over 16 lanes).
+constexpr int kNodeVariants = 5;
 constexpr size_t kStageSmemMax = 110 * 1024;  // two CTAs per SM at most
 template <class F>
 void launch_variant(int v, F&& f) {
@@ -402,6 +403,12 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   // the LSQ gradient (k=1, or the second-order start-up steps of k=2) is
   // the k=1 kernel's work
   const bool k1 = c->order == 1 || a.do_grad;
+  if (c->var[0] == 4) {
+    const int nb16 = grid_blocks(16 * c->nn, 128);
+    if (k1) k_node_prepare16<1><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+    else k_node_prepare16<3><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+    return launch_check(c);
+  }
   if (c->var[0] == 3 && c->stage_ok[k1 ? 0 : 1]) {
     const int tiles = grid_blocks(c->nn, kStageNodes);
     if (k1)
@@ -936,6 +943,7 @@ bool preload_kernels() {
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
         (const void*)k_boundary_add4<true>, (const void*)k_boundary_add4<false>,
         (const void*)k_node_stage<1>, (const void*)k_node_stage<3>,
+        (const void*)k_node_prepare16<1>, (const void*)k_node_prepare16<3>,
         (const void*)k_faces_assemble<0, 1>, (const void*)k_faces_assemble<1, 1>,
         (const void*)k_faces_assemble<0, 2>, (const void*)k_faces_assemble<1, 2>,
         (const void*)k_diag_lu,
@@ -2359,7 +2367,7 @@ int flow_restore_state(flow_ctx* c) {
 int flow_set_variants(flow_ctx* c, int node_prepare, int flux) {
   if (!c || !c->ok || node_prepare < 0 || node_prepare >= kNodeVariants || flux < 0 ||
       flux >= kVariants) {
-    set_error("flow_set_variants: null context, node variant outside 0..3 or flux outside 0..2");
+    set_error("flow_set_variants: null context, node variant outside 0..4 or flux outside 0..2");
     return FLOW_ERR_ARG;
   }
   if (node_prepare == 3 && !c->stage_ok[0] && !c->stage_ok[1]) {

@@ -269,6 +269,222 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
 }
 
 // ---------------------------------------------------------------------------
+// k_node_prepare4 with each node's serial chains split over 16 lanes (a
+// half-warp): lane l = 4 g + v owns variable v in group g.  Nothing is summed
+// in another order:
+// * the wave-speed sum: lane j forms face j's term, every lane adds the terms
+//   in face order from shuffles;
+// * the k=1 gradient: its x sum in group 0, its y sum in group 1, each over
+//   every edge in order;
+// * the k=2 derivatives: the five columns of V S^-1 U^T b are independent
+//   sums; group g sums column g (group 0 also column 4) over the stencil rows
+//   in order, and every lane then forms h and the point value from the five;
+// * the 1-ring min/max and the limiter's MIN over face points are folds of
+//   MIN/MAX: over values none of which is NaN (and the limiter bound is
+//   never -0) they equal the minimum / maximum whatever the order, so the
+//   four groups fold a quarter of the faces each and the results are
+//   combined.  Where any value of the node is NaN the fold is order-
+//   dependent, and every lane then folds all faces in the reference's order.
+__device__ __forceinline__ double hshfl(double x, unsigned mask, int lane) {
+  return __shfl_sync(mask, x, lane);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_node_prepare16(DevMesh m, DevState s, StepArgs a) {
+  if (*s.stop) return;  // the run has converged
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = (tid >> 4) + 1, l = tid & 15, v = l & 3, g = l >> 2;
+  const int hbase = threadIdx.x & 16;
+  const unsigned hmask = 0xFFFFu << hbase;
+  if (n > m.nn) return;  // whole half-warps leave together
+  const double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
+  const double q0v = v == 0 ? q4.x : v == 1 ? q4.y : v == 2 ? q4.z : q4.w;
+
+  // ---- wave-speed sum (cv_calc.C:819-953), terms formed in parallel ----
+  const double rho = q4.x, uu = q4.y / rho, vv = q4.z / rho;
+  const double P = (a.gamma - 1.0) * (q4.w - 0.5 * rho * (uu * uu + vv * vv));
+  const double cs = sqrt((a.gamma * P) / rho);
+  double ev = 0.;
+  int bad = 0;
+  const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
+  for (int base = s0; base < s1; base += 16) {
+    double term = 0.;
+    if (base + l < s1) {
+      const double4 gg = m.sub_geo[m.nsub[base + l] >> 1];
+      const double theta = uu * gg.x + vv * gg.y;
+      const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+      const double w = tpc >= tmc ? tpc : tmc;
+      if (!isfinite(w)) bad = 1;
+      term = (w * gg.z);
+    }
+    const int cnt = min(16, s1 - base);
+    for (int j = 0; j < cnt; j++) ev += hshfl(term, hmask, hbase + j);
+  }
+  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+  for (int k = b0; k < b1; k++) {
+    const double* xn = s.xn_bedges + 3 * m.nbed[k];
+    const double theta = uu * xn[0] + vv * xn[1];
+    const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+    const double w = tpc >= tmc ? tpc : tmc;
+    if (!isfinite(w)) bad = 1;
+    ev += (w * xn[2]);
+  }
+  bad = __any_sync(hmask, bad);
+  if (l == 0) {
+    const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
+    s.dt[n] = dt;
+    if (bad) atomicOr(s.status, ERR_EIGEN);
+    if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
+  }
+  if (!a.do_grad && !a.do_derivs && !a.do_lim) return;
+
+  // ---- the k=1 gradient (x in group 0, y in group 1) and the 1-ring
+  //      min/max (a quarter of the edges per group) ----
+  const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
+  double qmin = q0v, qmax = q0v, gsum = 0.;
+  int nan = 0;
+  for (int k = e0; k < e1; k++) {
+    const int ed = m.nedg[k];
+    const int side = ed & 1;
+    const bool mine = ((k - e0) & 3) == g;
+    const bool grad = ORDER == 1 && a.do_grad && g < 2;
+    if (!mine && !grad) continue;
+    const double qo = s.nQ[4 * (long)m.nedg_nbr[k] + v];
+    if (mine) {
+      if (qo != qo) nan = 1;
+      qmin = qmin <= qo ? qmin : qo;
+      qmax = qmax >= qo ? qmax : qo;
+    }
+    if (grad) {
+      const double4 w = m.edge_w[ed >> 1];
+      const double dq = side ? (q0v - qo) : (qo - q0v);  // nQ[R] - nQ[L]
+      if (side == 0) gsum += (g == 0 ? w.x : w.y) * dq;
+      else gsum -= (g == 0 ? w.z : w.w) * dq;
+    }
+  }
+  double g0 = 0., g1 = 0.;
+  if (ORDER == 1 && a.do_grad) {
+    g0 = hshfl(gsum, hmask, hbase + v);
+    g1 = hshfl(gsum, hmask, hbase + 4 + v);
+    if (g == 0) reinterpret_cast<double2*>(s.grad + 8 * (long)n)[v] = make_double2(g0, g1);
+  }
+
+  // ---- k=2: column g (and 4) of V S^-1 U^T b of variable v ----
+  double h[5] = {0., 0., 0., 0., 0.}, pv = 0.;
+  if (ORDER == 3 && a.do_derivs) {
+    const int t0 = m.st_ptr[n], t1 = m.st_ptr[n + 1];
+    const int mrows = t1 - t0;
+    const double* U = m.svd_U1 + 5 * (long)t0;
+    double accA = 0., accB = 0.;
+#pragma unroll 4
+    for (int k = 0; k < mrows; k++) {
+      const int nb = m.st_idx[t0 + k];
+      const double bv = m.st_w[t0 + k] * (s.nQ[4 * (long)nb + v] - q0v);
+      accA += bv * U[5 * k + g];
+      if (g == 0) accB += bv * U[5 * k + 4];
+    }
+    const double* S = m.svd_S + 5 * (long)n;
+    const double tA = accA / S[g];
+    const double tB = g == 0 ? accB / S[4] : 0.;
+    double t1v[5];
+    t1v[0] = hshfl(tA, hmask, hbase + v);
+    t1v[1] = hshfl(tA, hmask, hbase + 4 + v);
+    t1v[2] = hshfl(tA, hmask, hbase + 8 + v);
+    t1v[3] = hshfl(tA, hmask, hbase + 12 + v);
+    t1v[4] = hshfl(tB, hmask, hbase + v);
+    const double* VT = m.svd_VT + 25 * (long)n;
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      double sum = 0.;
+#pragma unroll
+      for (int c = 0; c < 5; c++) sum += VT[j * 5 + c] * t1v[c];
+      h[j] = sum;
+    }
+    const double* mo = m.moments + 9 * (long)n;
+    pv = q0v - mo[0] * h[0] - mo[1] * h[1] - mo[2] * h[2] * 0.5 - mo[3] * h[3] * 0.5 -
+         mo[4] * h[4];
+    if (g == 0) {
+      double* hd = s.hess5 + 20 * (long)n + 5 * v;
+#pragma unroll
+      for (int c = 0; c < 5; c++) hd[c] = h[c];
+      s.pv[4 * (long)n + v] = pv;
+    }
+  }
+
+  if (!a.do_lim) return;
+  // ---- Venkatakrishnan bound of variable v over every face point ----
+  const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
+  auto fold_faces = [&](double mn, double mx, int first, int stride, int& sawnan) {
+    double ph = 1.0;
+    for (int k = s0 + first; k < s1; k += stride) {
+      const int sd = m.nsub[k];
+      const int sub = sd >> 1, side = sd & 1;
+      if (ORDER == 1) {
+        const double4 d = m.sub_dx[sub];
+        const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
+        const double qr = q0v + (g0 * dx0 + g1 * dx1);
+        ph = venkat_fold(ph, qr, q0v, mn, mx);
+        if (ph != ph) sawnan = 1;
+      } else {
+        const double* xg = m.sub_xg + 6 * (long)sub;
+#pragma unroll
+        for (int gpt = 0; gpt < 3; gpt++) {
+          const double dx0 = xg[2 * gpt] - xn0, dx1 = xg[2 * gpt + 1] - xn1;
+          double qr = pv;
+          qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
+                 h[4] * dx0 * dx1);
+          ph = venkat_fold(ph, qr, q0v, mn, mx);
+          if (ph != ph) sawnan = 1;
+        }
+      }
+    }
+    return ph;
+  };
+  // this variable's 1-ring min/max from the four groups
+  double mn = qmin, mx = qmax;
+#pragma unroll
+  for (int gg = 1; gg < 4; gg++) {
+    const double omn = hshfl(qmin, hmask, hbase + ((g + gg) & 3) * 4 + v);
+    const double omx = hshfl(qmax, hmask, hbase + ((g + gg) & 3) * 4 + v);
+    mn = mn <= omn ? mn : omn;
+    mx = mx >= omx ? mx : omx;
+  }
+  int sawnan = 0;
+  double ph = fold_faces(mn, mx, g, 4, sawnan);
+  double pg = ph;
+#pragma unroll
+  for (int gg = 1; gg < 4; gg++) {
+    const double o = hshfl(ph, hmask, hbase + ((g + gg) & 3) * 4 + v);
+    pg = pg <= o ? pg : o;
+  }
+  if (__any_sync(hmask, nan | sawnan)) {
+    // a NaN makes the folds order-dependent: the reference's order throughout
+    mn = q0v;
+    mx = q0v;
+    for (int k = e0; k < e1; k++) {
+      const double qo = s.nQ[4 * (long)m.nedg_nbr[k] + v];
+      mn = mn <= qo ? mn : qo;
+      mx = mx >= qo ? mx : qo;
+    }
+    int unused = 0;
+    pg = fold_faces(mn, mx, 0, 1, unused);
+  }
+  // min over the variables in order 0..3 (limiter.C:895-906)
+  const double p1 = hshfl(pg, hmask, hbase + 1);
+  const double p2 = hshfl(pg, hmask, hbase + 2);
+  const double p3 = hshfl(pg, hmask, hbase + 3);
+  double pmin = hshfl(pg, hmask, hbase);
+  pmin = pmin <= p1 ? pmin : p1;
+  pmin = pmin <= p2 ? pmin : p2;
+  pmin = pmin <= p3 ? pmin : p3;
+  if (g == 0) {
+    const double out = v == 0 ? pmin : pg;
+    reinterpret_cast<double2*>(s.phi + 8 * (long)n)[v] = make_double2(out, out);
+    if (out < 0.0 || out > 1.0) atomicOr(s.status, ERR_LIMITER);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // k_node_prepare4 with its gathers staged in shared memory: the same per-lane
 // arithmetic in the same order (so the same bits), but a CTA of kStageNodes
 // consecutive nodes first copies its slices of the incidence lists and the

@@ -420,21 +420,23 @@ long flow_launch_count(flow_ctx *ctx);
 double flow_last_device_ms(flow_ctx *ctx);
 
 /* ---- Autotuner (no counterpart in the reference) -------------------------
- * k_node_prepare4 comes in four variants, k_subedge_flux in three; the
+ * k_node_prepare4 comes in five variants, k_subedge_flux in three; the
  * results are bit-identical, the speed depends on the mesh.  Variants 0..2
  * of both set the minimum resident blocks per SM the compiler must allow
  * (how many registers a thread may hold); node variant 3 is the staged
  * kernel (a CTA of 32 nodes copies its incidence and stencil slices, then
  * gathers every face record and neighbour state into shared memory with
  * asynchronous copies before the arithmetic), offered where its shared
- * memory fits the mesh.  flow_autotune times each variant over `steps`
+ * memory fits the mesh; node variant 4 gives each node 16 lanes instead of
+ * 4 (its stencil columns, gradient components and face points spread over
+ * them, every sum still in the reference's order).  flow_autotune times each variant over `steps`
  * pseudo-time steps from step index `ts` (CUDA events, after one warm-up
  * step), keeps the fastest, and puts the solution state back as it was
  * with a clear status (the returned status still reports what the timing
- * steps ran into).  variants[2] receives the choice, ms[7] (may be NULL)
- * the average kernel times per variant (ms[0..3] node, ms[4..6] flux;
+ * steps ran into).  variants[2] receives the choice, ms[8] (may be NULL)
+ * the average kernel times per variant (ms[0..4] node, ms[5..7] flux;
  * 1e30 for a variant that does not fit).  flow_set_variants sets a choice
- * directly (node 0..3, flux 0..2). */
+ * directly (node 0..4, flux 0..2). */
 int flow_autotune(flow_ctx *ctx, const flow_params *p, int ts, int steps, int *variants,
                   double *ms);
 int flow_set_variants(flow_ctx *ctx, int node_prepare, int flux);
