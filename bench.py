@@ -69,6 +69,7 @@ REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
 BENCH_BUDGET_S = 1500.      # wall-clock target of a whole batch run (warm-up and checks included)
 SERVE_RATES = (0.5, 2.0)    # requests/s of the serving measurement in the batch run
 SERVE_REQUESTS = 16
+SERVE_STALL = 1200           # stall retirement window of the serving runs (as batch64's)
 SERVE_MIN_LEFT_S = 200.     # run the serving measurement only with this much time left
 REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
 STAGE_THREADS = max(1, min(8, os.cpu_count() or 1))  # concurrent admissions per batch pass
@@ -726,13 +727,15 @@ def batch_cpu_baseline(prep, bw) -> dict:
 def measure_fp64(args, bw):
     """Record the FP64 drop-in's step count, status and forces on every
     request of the batch (the reference's own, since the drop-in is
-    bit-identical).  The solves run side by side in one server in precision
-    mode 0; a served solve's iterates are those it has alone."""
+    bit-identical) with `--subits` Gauss-Seidel sweeps per step (default 2).
+    The solves run side by side in one server in precision mode 0; a served
+    solve's iterates are those it has alone."""
     import torch
     from flowgpu import capi, serve
     torch.cuda.set_device(0)
+    sweeps = args.subits or 2
     reqs = [serve.sample_request(i, seed=bw.seed) for i in range(bw.n)]
-    prep = serve.prepare_all(reqs, 2, bw.max_steps, bw.drop)
+    prep = serve.prepare_all(reqs, sweeps, bw.max_steps, bw.drop)
     free, _ = torch.cuda.mem_get_info(0)
     arena = capi.Arena(int(min(free * 0.85, 150e9)))
     # 16 at a time: the FP64 drop-in's ordered sweeps poll across the GPU
@@ -742,7 +745,8 @@ def measure_fp64(args, bw):
     steps = tuple(x["steps"] for x in recs)
     status = tuple(x["status"] for x in recs)
     forces = tuple(tuple(x["forces"]) if x["status"] == 0 else None for x in recs)
-    print(json.dumps({"workload": bw.name, "fp64_steps": steps, "fp64_status": status,
+    print(json.dumps({"workload": bw.name, "subits": sweeps, "fp64_steps": steps,
+                      "fp64_status": status,
                       "seconds": round(r["makespan_s"], 2), "fp64_forces": forces}),
           flush=True)
 
@@ -1016,7 +1020,7 @@ def serving_run(rate: float, n: int, arena, budget: int, jacobian: int = 0,
             for i in range(n)]
     r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
                           precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
-                          stall=2000, ramp_sweeps=2, jacobian=jacobian)
+                          stall=SERVE_STALL, ramp_sweeps=2, jacobian=jacobian)
     recs = r["records"]
     conv = [x for x in recs if x.get("status") == 0]
     return {"value": round(len(conv) / r["span_s"], 5), "unit": UNIT,
@@ -1033,7 +1037,7 @@ def serving_run(rate: float, n: int, arena, budget: int, jacobian: int = 0,
             "status": [x.get("status") for x in recs],
             "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
                        "jacobian": jacobian, "ramp_sweeps_on_meshes_from_250k_nodes": 2,
-                       "stall_retire_steps": 2000, "arena_bytes": budget, "stream_seed": 1,
+                       "stall_retire_steps": SERVE_STALL, "arena_bytes": budget, "stream_seed": 1,
                        "first_request": index0, "nodes_range": [4000, 500000]}}
 
 
@@ -1050,7 +1054,7 @@ def run_serve(args):
     with ClockSampler(0) as clk:
         r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
                               precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
-                              stall=2000, ramp_sweeps=2,
+                              stall=SERVE_STALL, ramp_sweeps=2,
                               jacobian=workloads.BATCHES[workloads.DEFAULT_BENCH].jacobian)
     arena.close()
     recs = r["records"]
@@ -1070,7 +1074,7 @@ def run_serve(args):
             "status": [x.get("status") for x in recs],
             "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
                        "ramp_sweeps_on_meshes_from_250k_nodes": 2,
-                       "stall_retire_steps": 2000, "arena_bytes": budget, "stream_seed": 1,
+                       "stall_retire_steps": SERVE_STALL, "arena_bytes": budget, "stream_seed": 1,
                        "nodes_range": [4000, 500000]},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -1123,7 +1127,8 @@ def main():
     ap.add_argument("--node-variant", type=int, default=-1,
                     help="with --profile-steps: node kernel variant (3: staged in shared memory)")
     ap.add_argument("--subits", type=int, default=0,
-                    help="with --profile-steps: Gauss-Seidel sweeps per step (0: the workload's)")
+                    help="with --profile-steps: Gauss-Seidel sweeps per step (0: the workload's); "
+                         "with --measure-fp64: the FP64 drop-in's sweeps (0: 2)")
     ap.add_argument("--serve-rate", type=float, default=0.,
                     help="run the serving form: Poisson arrivals at this rate (requests/s)")
     ap.add_argument("--serve-requests", type=int, default=16)

@@ -179,6 +179,8 @@ struct flow_ctx {
   // device snapshot of the solution state
   double *snapQ = nullptr, *snapnQ = nullptr, *snappQ = nullptr, *snapXnb = nullptr;
   double* xnb0 = nullptr;  // boundary normals as created (restored by flow_set_state)
+  // state at the start of the last two chunks of a served run (by flag slot)
+  double* ckpt[2] = {nullptr, nullptr};
   // one-CTA ordered sweep: stage tables (null when the matrix bandwidth is too
   // large for its dQ window, then the multi-CTA sweep is used)
   SweepTables sweep_tb{};
@@ -2875,8 +2877,67 @@ int run_norms(flow_ctx* c, double* r_first, double* r_last) {
   return 0;
 }
 
+int checkpoint_enable(flow_ctx* c) {
+  if (!c || !c->ok) return FLOW_ERR_ARG;
+  if (c->ckpt[0]) return 0;
+  const size_t nq = 4 * (size_t)(c->nn + c->ng + 1);
+  double* a = c->buf.alloc<double>(nq);
+  double* b = a ? c->buf.alloc<double>(nq) : nullptr;
+  if (!a || !b) {
+    set_error("checkpoint allocation failed");
+    return carve_error(c);
+  }
+  c->ckpt[0] = a;
+  c->ckpt[1] = b;
+  return 0;
+}
+
+int checkpoint_save(flow_ctx* c, int slot) {
+  if (!c->ckpt[slot]) return 0;
+  const size_t bytes = sizeof(double) * 4 * (size_t)(c->nn + c->ng + 1);
+  return cudaMemcpyAsync(c->ckpt[slot], c->s.Q, bytes, cudaMemcpyDeviceToDevice, c->stream) ==
+                 cudaSuccess
+             ? 0
+             : FLOW_ERR_CUDA;
+}
+
+int checkpoint_restore(flow_ctx* c, int slot, int step) {
+  if (!c || !c->ok || !c->ckpt[slot] || step < 1) return FLOW_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error(cudaGetErrorString(cudaGetLastError()));
+    return FLOW_ERR_CUDA;
+  }
+  const size_t bytes = sizeof(double) * 4 * (size_t)(c->nn + c->ng + 1);
+  // the step counters as they stood before `step`: the device-side step
+  // index of graph replays continues from citer, and steps_done == 0 makes
+  // step 1 the run's first again
+  const int before = step - 1;
+  bool ok = cudaMemcpyAsync(c->s.Q, c->ckpt[slot], bytes, cudaMemcpyDeviceToDevice,
+                            c->stream) == cudaSuccess &&
+            cudaMemcpyAsync(c->s.nQ, c->s.Q, bytes, cudaMemcpyDeviceToDevice, c->stream) ==
+                cudaSuccess &&
+            cudaMemcpyAsync(c->s.citer, &before, sizeof(int), cudaMemcpyHostToDevice,
+                            c->stream) == cudaSuccess &&
+            cudaMemcpyAsync(c->s.steps_done, &before, sizeof(int), cudaMemcpyHostToDevice,
+                            c->stream) == cudaSuccess &&
+            cudaMemsetAsync(c->s.status, 0, sizeof(int), c->stream) == cudaSuccess &&
+            cudaMemsetAsync(c->s.stop, 0, sizeof(int), c->stream) == cudaSuccess &&
+            cudaMemsetAsync(c->s.skip, 0, sizeof(int), c->stream) == cudaSuccess;
+  // the first k=2 boundary pass rewrites the curved-wall normals
+  if (ok && step == 1)
+    ok = cudaMemcpyAsync(c->s.xn_bedges, c->xnb0, sizeof(double) * 3 * (size_t)(c->nbe + 1),
+                         cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess;
+  if (!ok || cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error(cudaGetErrorString(cudaGetLastError()));
+    return FLOW_ERR_CUDA;
+  }
+  return 0;
+}
+
 cudaStream_t stream_of(flow_ctx* c) { return c->stream; }
 int device_of(flow_ctx* c) { return c->device; }
+int jacobian_of(flow_ctx* c) { return c && c->ok && c->precision != 0 ? c->jac_mode : 0; }
 int state_of(flow_ctx* c, const double** Q, int* nn, int* ng) {
   if (!c || !c->ok) return FLOW_ERR_ARG;
   *Q = c->s.Q;

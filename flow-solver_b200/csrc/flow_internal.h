@@ -37,6 +37,19 @@ double run_ms(flow_ctx* c, int slot);
 int run_norms(flow_ctx* c, double* r_first, double* r_last);
 cudaStream_t stream_of(flow_ctx* c);
 int device_of(flow_ctx* c);
+// The face Jacobians the context's steps build (flow_set_jacobian; 0 when
+// the context runs the FP64 drop-in, which always takes the reference's).
+int jacobian_of(flow_ctx* c);
+// Chunk checkpoints of a served run: checkpoint_enable carves two copies of
+// GRID::Q from the context's buffers; checkpoint_save(slot) queues a copy of
+// the state into copy `slot` on the context's stream (before the chunk that
+// posts flag slot `slot`; nothing when not enabled); checkpoint_restore
+// waits for the stream, puts copy `slot` back as the state before step
+// `step` and clears the run's error bits and stop flag, so that the next
+// enqueue_steps(step, ...) runs from there.
+int checkpoint_enable(flow_ctx* c);
+int checkpoint_save(flow_ctx* c, int slot);
+int checkpoint_restore(flow_ctx* c, int slot, int step);
 // The context's resident state GRID::Q ((nn+nn_ghost+1)*4 doubles on the
 // device) and its node counts; FLOW_ERR_ARG for a null or failed context.
 int state_of(flow_ctx* c, const double** Q, int* nn, int* ng);

@@ -62,6 +62,9 @@ struct Slot {
   double r_first = 0., r_last = 0., ms = 0.;
   double best = 1.;     // best ||R_rho|| relative to the first step, kept by factors of 10
   int best_step = 0;    // step at which it last improved tenfold
+  int chunk_first[2] = {0, 0};  // first step of the chunk posting each flag slot
+  int recoverable = 0;  // approximate face Jacobians with chunk checkpoints kept
+  int recovered_at = 0; // step it went back to with the forward-difference Jacobians
 };
 
 }  // namespace
@@ -78,6 +81,7 @@ struct flow_server {
   long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
   int priority_policy = 0;                // 1: larger meshes get greater stream priority
   int jacobian = 0;                       // face Jacobians of precision-form solves
+  int recovery = 1;                       // roll back a failed approximate-Jacobian solve
   // guards the slot table and the counters: stage may run on several host
   // threads at once (each builds its context outside the lock) beside
   // progress / start / result / release
@@ -98,7 +102,10 @@ void finish(Slot& sl, int status, int steps, int flag_slot) {
 int issue_chunk(flow_server* sv, Slot& sl) {
   const int K = std::min(sv->chunk, sl.max_steps - sl.issued);
   if (K <= 0) return 0;
-  int rc = flow::internal::enqueue_steps(sl.ctx, &sl.p, 1 + sl.issued, K);
+  int rc = sl.recoverable ? flow::internal::checkpoint_save(sl.ctx, sl.next_flag) : 0;
+  if (rc) return rc;
+  sl.chunk_first[sl.next_flag] = 1 + sl.issued;
+  rc = flow::internal::enqueue_steps(sl.ctx, &sl.p, 1 + sl.issued, K);
   if (rc) return rc;
   sl.issued += K;
   rc = flow::internal::post_flags(sl.ctx, sl.next_flag);
@@ -106,6 +113,31 @@ int issue_chunk(flow_server* sv, Slot& sl) {
   sl.next_flag ^= 1;
   sl.inflight++;
   return 0;
+}
+
+// Error bits of a state that went non-physical (a negative pressure or
+// density on the way to a wave speed, dt, the limiter or a far-field state).
+constexpr int kNonPhysical = FLOW_ERR_EIGEN | FLOW_ERR_DT | FLOW_ERR_LIMITER | FLOW_ERR_BC;
+
+// A solve on the approximate face Jacobians whose chunk (flag slot fs) ended
+// non-physical: the approximation's Newton steps can overshoot where the CFL
+// ramp makes them large.  Put back the state of that chunk's first step and
+// carry on from there with the forward-difference Jacobians, which converge
+// where the FP64 drop-in does.  The steps after the failure are run once
+// more; they count in the solve's device time.
+int recover(flow_server* sv, Slot& sl, int fs) {
+  const int step = sl.chunk_first[fs];
+  int rc = flow::internal::checkpoint_restore(sl.ctx, fs, step);
+  if (!rc) rc = flow_set_jacobian(sl.ctx, 0);
+  if (rc) return rc;
+  sl.recoverable = 0;
+  sl.recovered_at = step;
+  sl.issued = step - 1;
+  sl.inflight = 0;
+  sl.next_flag = sl.oldest_flag = 0;
+  rc = issue_chunk(sv, sl);
+  if (!rc) rc = issue_chunk(sv, sl);
+  return rc;
 }
 
 }  // namespace
@@ -152,6 +184,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   }
   int idx = -1;
   int autotune_steps = 0, sched_sweeps = 0, sched_until = 0, priority_policy = 0, jacobian = 0;
+  int recovery = 0;
   long sched_min_nodes = 0;
   {
     std::lock_guard<std::mutex> lock(sv->mu);
@@ -168,6 +201,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     sched_min_nodes = sv->sched_min_nodes;
     priority_policy = sv->priority_policy;
     jacobian = sv->jacobian;
+    recovery = sv->recovery;
   }
   auto unreserve = [&]() {
     std::lock_guard<std::mutex> lock(sv->mu);
@@ -187,6 +221,8 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   // bandwidth is too large for that is served in mode 1 instead
   if (rc == FLOW_ERR_ARG && precision == 3) rc = flow_set_precision(c, 1);
   if (!rc && precision != 0 && jacobian != 0) rc = flow_set_jacobian(c, jacobian);
+  const int recoverable = !rc && recovery && flow::internal::jacobian_of(c) != 0;
+  if (recoverable) rc = flow::internal::checkpoint_enable(c);
   if (!rc && precision != 0 && sched_sweeps > 0 && flow_size(c, "dt") - 1 >= sched_min_nodes)
     rc = flow_set_sweep_schedule(c, sched_sweeps, sched_until);
   if (!rc && priority_policy == 1) {
@@ -254,6 +290,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   sl.drop = drop;
   sl.max_steps = max_steps;
   sl.tag = tag;
+  sl.recoverable = recoverable;
   sl.state = 3;  // staged: inputs on the device, nothing launched
   if (slot_out) *slot_out = idx;
   if (hold) return 0;
@@ -312,6 +349,11 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
       const int fs = sl.oldest_flag;
       sl.oldest_flag ^= 1;
       sl.inflight--;
+      if (r > 0 && sl.recoverable && !stop && status && !(status & ~kNonPhysical)) {
+        const int rc = recover(sv, sl, fs);
+        if (!rc) continue;  // running again from the failed chunk's first step
+        status |= rc;
+      }
       // stall: no tenfold drop of the best residual within stall_steps steps
       if (rr < sl.best * 0.1) {
         sl.best = rr;
@@ -335,6 +377,7 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
         cpl.r_last = sl.r_last;
         cpl.device_ms = sl.ms;
         cpl.launches = flow_launch_count(sl.ctx);
+        cpl.recovered_at = sl.recovered_at;
         continue;
       }
       if (sl.issued < sl.max_steps) {
@@ -353,6 +396,7 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
           cpl.r_last = sl.r_last;
           cpl.device_ms = sl.ms;
           cpl.launches = flow_launch_count(sl.ctx);
+        cpl.recovered_at = sl.recovered_at;
         }
       }
     }
@@ -430,6 +474,13 @@ int flow_server_set_jacobian(flow_server* sv, int mode) {
   if (!sv || mode < 0 || mode > 2) return FLOW_ERR_ARG;
   std::lock_guard<std::mutex> lock(sv->mu);
   sv->jacobian = mode;
+  return 0;
+}
+
+int flow_server_set_recovery(flow_server* sv, int on) {
+  if (!sv) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  sv->recovery = on ? 1 : 0;
   return 0;
 }
 

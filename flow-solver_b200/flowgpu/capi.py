@@ -27,6 +27,11 @@ ERR_NOT_CONVERGED = 256
 ERR_BUDGET = 512
 ERR_STALLED = 1024
 ERR_SWEEP_TIMEOUT = 64
+ERR_EIGEN = 4
+ERR_DT = 8
+ERR_LIMITER = 16
+ERR_BC = 32
+ERR_NONPHYSICAL = ERR_EIGEN | ERR_DT | ERR_LIMITER | ERR_BC
 
 # exported symbols, in include/flow_gpu.h order
 SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_run",
@@ -48,6 +53,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_server_set_autotune", "flow_server_set_stall",
            "flow_server_set_sweep_schedule", "flow_set_stream_priority",
            "flow_server_set_priority_policy", "flow_server_set_jacobian",
+           "flow_server_set_recovery",
            "flow_selftest_sweep_timeout")
 
 
@@ -193,6 +199,7 @@ def _load_locked():
     L.flow_set_stream_priority.argtypes = [vp, C.c_int]
     L.flow_server_set_priority_policy.argtypes = [vp, C.c_int]
     L.flow_server_set_jacobian.argtypes = [vp, C.c_int]
+    L.flow_server_set_recovery.argtypes = [vp, C.c_int]
     L.flow_selftest_sweep_timeout.argtypes = [vp, C.c_long, IP]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
@@ -230,7 +237,8 @@ NOALLOC_MAX_ROWS = 262144
 class FlowCompletion(C.Structure):
     _fields_ = [("tag", C.c_longlong), ("slot", C.c_int), ("status", C.c_int),
                 ("steps", C.c_int), ("r_first", C.c_double), ("r_last", C.c_double),
-                ("device_ms", C.c_double), ("launches", C.c_longlong)]
+                ("device_ms", C.c_double), ("launches", C.c_longlong),
+                ("recovered_at", C.c_int)]
 
 
 class Arena:
@@ -264,7 +272,7 @@ class Server:
 
     def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64, autotune: int = 0,
                  stall: int = 0, ramp_sweeps: int = 0, ramp_min_nodes: int = 250000,
-                 priority_policy: int = 0, jacobian: int = 0):
+                 priority_policy: int = 0, jacobian: int = 0, recovery: bool = True):
         self.L = load()
         st = C.c_int(0)
         self.arena = arena
@@ -283,6 +291,8 @@ class Server:
                    "priority policy")
         if jacobian:
             _check(self.L.flow_server_set_jacobian(self.h, int(jacobian)), "jacobian")
+        if not recovery:
+            _check(self.L.flow_server_set_recovery(self.h, 0), "recovery")
         self._keep = {}
         self._out = (FlowCompletion * 64)()
 
@@ -314,7 +324,7 @@ class Server:
                                            C.byref(n)), "flow_server_progress")
         return [{"tag": c.tag, "slot": c.slot, "status": c.status, "steps": c.steps,
                  "r_first": c.r_first, "r_last": c.r_last, "device_ms": c.device_ms,
-                 "launches": c.launches}
+                 "launches": c.launches, "recovered_at": c.recovered_at}
                 for c in self._out[:n.value]]
 
     def result(self, slot: int, want_q: bool = True):

@@ -495,6 +495,8 @@ typedef struct {
   double r_last;     /* ||R_rho|| of the last step */
   double device_ms;  /* device time from the start of the run to retirement */
   long long launches; /* kernel launches the solve issued (graph replays included) */
+  int recovered_at;  /* 0, or the step a solve on the approximate face Jacobians went back
+                        to after a non-physical state (flow_server_set_recovery) */
 } flow_completion;
 flow_server *flow_server_create(flow_arena *arena, int chunk, int max_slots, int *status);
 void flow_server_destroy(flow_server *srv);
@@ -542,6 +544,16 @@ int flow_server_set_priority_policy(flow_server *srv, int policy);
 /* flow_set_jacobian(mode) for every precision-form solve admitted later
  * (0, the default: forward differences). */
 int flow_server_set_jacobian(flow_server *srv, int mode);
+/* Recovery of precision-form solves on the approximate face Jacobians
+ * (flow_set_jacobian 1 or 2; no reference counterpart).  on != 0 (the
+ * default): the server keeps the state at the start of each solve's last two
+ * chunks (two copies of GRID::Q carved from the arena at admission); when a
+ * chunk ends with a non-physical state (FLOW_ERR_EIGEN, _DT, _LIMITER or
+ * _BC) it puts the state of that chunk's first step back, switches the solve
+ * to the forward-difference Jacobians (mode 0) and runs on from there, once
+ * per solve.  flow_completion::recovered_at reports the step.  on == 0: such
+ * a solve retires with its error bits, as a context run alone does. */
+int flow_server_set_recovery(flow_server *srv, int on);
 /* flow_set_sweep_schedule for every precision-form solve admitted later on
  * a mesh of at least min_nodes nodes (measured: the 1.05M-node O-grid needs
  * 2 sweeps during the CFL ramp, meshes up to 124k nodes converge faster

@@ -233,3 +233,70 @@ def test_arena_without_room_refuses_before_building_the_context():
     assert srv.running() == 0
     srv.close()
     arena.close()
+
+
+def _request44():
+    """Request 44 of the 64-solve batch stream (seed 0): an 81,796-node k=2
+    O-grid at Mach 0.677 whose approximate-Jacobian Newton steps go
+    non-physical near step 550 of the CFL ramp; the FP64 drop-in and the
+    forward-difference Jacobians converge it."""
+    from flowgpu import serve, workloads
+    bw = workloads.BATCHES["batch64"]
+    return serve.prepare(serve.sample_request(44, seed=0), bw.subits, bw.max_steps, bw.drop)
+
+
+def test_failed_approximate_jacobian_solve_rolls_back_and_converges():
+    """The served solve goes back to its failed chunk's first step with the
+    forward-difference Jacobians: its state is bit for bit that of a context
+    run alone on the approximate Jacobians up to that step and on the
+    forward-difference ones after it, and its forces are within 1e-8 of the
+    FP64 drop-in's.  With recovery off it retires in that chunk with
+    non-physical error bits, as the context alone fails."""
+    from flowgpu import capi
+    pr = _request44()
+    mesh, fp, q0 = pr.mesh, pr.params, pr.Q0
+    arena = capi.Arena(4 << 30)
+    got = {}
+    for recovery in (True, False):
+        srv = capi.Server(arena, chunk=32, max_slots=2, jacobian=2, recovery=recovery)
+        srv.submit(mesh, fp, q0, precision=3, drop=1e-10, max_steps=6000, tag=int(recovery))
+        while int(recovery) not in got:
+            for c in srv.progress(wait_us=5000):
+                q, f = srv.result(c["slot"]) if c["status"] == 0 else (None, None)
+                got[c["tag"]] = (c, q, f)
+                srv.release(c["slot"])
+        srv.close()
+    c, q, f = got[1]
+    assert c["status"] == 0 and c["recovered_at"] > 1, c
+    s = c["recovered_at"]
+    assert (s - 1) % 32 == 0
+    # alone: approximate Jacobians for steps 1 .. s-1, forward differences after
+    alone = capi.Solver.from_mesh(mesh, fp, device=0)
+    alone.set_precision(3)
+    alone.set_jacobian(2)
+    alone.set_state(q0)
+    alone.run(1, s - 1)
+    alone.set_jacobian(0)
+    alone.run(s, c["steps"] - s + 1)
+    assert np.array_equal(alone.get("Q")[4:], q[4:])
+    alone.close()
+    fp64 = capi.Solver.from_mesh(mesh, fp, device=0)
+    fp64.set_state(q0)
+    fp64.converge(1, 6000, 1e-10, check=False)
+    assert fp64.status() == 0
+    f64 = fp64.body_forces()
+    fp64.close()
+    assert max(abs(f[0] - f64[0]), abs(f[1] - f64[1])) < 1e-8
+    # recovery off: the error bits of the context alone
+    c0 = got[0][0]
+    assert c0["recovered_at"] == 0
+    assert c0["status"] & capi.ERR_NONPHYSICAL and not c0["status"] & ~capi.ERR_NONPHYSICAL
+    assert c0["steps"] < s + 32
+    alone = capi.Solver.from_mesh(mesh, fp, device=0)
+    alone.set_precision(3)
+    alone.set_jacobian(2)
+    alone.set_state(q0)
+    alone.converge(1, 6000, 1e-10, chunk=32, check=False)
+    assert alone.status() & capi.ERR_NONPHYSICAL
+    alone.close()
+    arena.close()
