@@ -10,9 +10,10 @@ log-uniform, 4:1 O-grids; Mach 0.3..0.85, angle of attack -4..6 degrees,
 k=1 or k=2), admitted together to the serving engine (one device arena, one
 stream per solve, CUDA-graph chunks of pseudo-time steps) in the precision
 form (FP64 residual, FP32 blocks, Gauss-Seidel in coloured chunks of the
-reference order), each retired at a 1e-10 drop of ||R_rho||, at its step
-limit or when it stalls.  A "step" of this benchmark is one pass over the
-batch.
+reference order; approximate Roe face Jacobians, with a one-chunk roll-back
+to the forward-difference ones for a solve they drive non-physical), each
+retired at a 1e-10 drop of ||R_rho||, at its step limit or when it stalls.
+A "step" of this benchmark is one pass over the batch.
 
 * value: converged solves / device time of the passes (CUDA events), with
   every mesh and initial state already on the device (staged).
@@ -23,11 +24,13 @@ batch.
 * latency: p50/p95/p99 of the per-solve device time from start to retirement.
 * plain_fp64: the same requests solved one at a time by the FP64 drop-in
   (bit-identical to the reference), modelled: the recorded FP64 step count
-  of each request x its measured FP64 ms/step; two requests are also solved
+  of each request x its measured FP64 ms/step, at whichever recorded sweep
+  count (2 or 4 per step) solves it soonest; two requests are also solved
   to convergence in the run and the model's error on them is printed.
-* roofline: k_node_prepare4 (the largest kernel of a step) on the batch's
-  largest mesh, compulsory bytes over its measured duration against the
-  measured HBM copy bandwidth.
+* roofline: the kernel class with the largest share of a step (node
+  preparation, face fluxes, assembly or the chunk sweeps) on the batch's
+  largest mesh that the FP64 drop-in solves, compulsory bytes over its
+  measured duration against the measured HBM copy bandwidth.
 * cpu_baseline: the reference (oracle/_ref, built from its own sources) on
   one host core, timed on the smallest meshes of the batch and scaled by node
   count to every request's recorded step count.
@@ -580,43 +583,58 @@ def run_batch(args, bw):
     # ---- plain FP64 drop-in on the same requests, one at a time ----
     plain = None
     if bw.fp64_steps is not None and rank == 0 and world == 1:
-        tot = 0.
-        per = []
+        # recorded runs of the drop-in: (sweeps, steps, status) per request
+        recorded = [(2, bw.fp64_steps, bw.fp64_status)]
+        if bw.fp64_steps4 is not None:
+            recorded.append((4, bw.fp64_steps4, bw.fp64_status4))
         n = 96
+        tot, per, chosen, conv64 = 0., [], [], 0
         for i, pr in enumerate(prep):
-            s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params, subits=2),
-                                      device=local)
-            s.set_state(pr.Q0)
-            s.converge(1, n, 1e-300, chunk=32, check=False)
-            ms_step = s.last_device_ms() / n
-            s.close()
-            per.append(round(ms_step, 4))
-            tot += bw.fp64_steps[i] * ms_step / 1e3
-        conv64 = sum(1 for st in bw.fp64_status if st == 0)
+            ms = {}
+            for sw, _steps, _status in recorded:
+                s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params, subits=sw),
+                                          device=local)
+                s.set_state(pr.Q0)
+                s.converge(1, n, 1e-300, chunk=32, check=False)
+                ms[sw] = s.last_device_ms() / n
+                s.close()
+            # the sweep count that solves this request soonest (converged
+            # runs first): a choice made with hindsight, so the baseline is
+            # the drop-in at its best, not at one fixed setting
+            runs = [(sw, steps[i], status[i]) for sw, steps, status in recorded]
+            pool = [r for r in runs if r[2] == 0] or runs
+            sw, steps_i, status_i = min(pool, key=lambda r: r[1] * ms[r[0]])
+            per.append(round(ms[sw], 4))
+            chosen.append((sw, steps_i, status_i))
+            tot += steps_i * ms[sw] / 1e3
+            conv64 += status_i == 0
         # the model checked on two requests solved to convergence here: the
         # converged ones whose modelled time is largest below 6 s
-        est = {i: bw.fp64_steps[i] * per[i] / 1e3 for i in range(len(prep))
-               if bw.fp64_status[i] == 0}
+        est = {i: chosen[i][1] * per[i] / 1e3 for i in range(len(prep)) if chosen[i][2] == 0}
         pick = sorted((i for i in est if est[i] < 6.0), key=lambda i: -est[i])[:2]
         checks = []
         for i in pick:
             pr = prep[i]
-            s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params, subits=2),
+            s = capi.Solver.from_mesh(pr.mesh, dataclasses.replace(pr.params,
+                                                                    subits=chosen[i][0]),
                                       device=local)
             s.set_state(pr.Q0)
             steps_i, _r0, _r1 = s.converge(1, bw.max_steps, bw.drop, chunk=32, check=False)
             real = s.last_device_ms() / 1e3
             s.close()
-            checks.append({"request": i, "nodes": pr.req.nodes, "steps": steps_i,
-                           "recorded_steps": bw.fp64_steps[i], "modelled_s": round(est[i], 3),
-                           "measured_s": round(real, 3),
+            checks.append({"request": i, "nodes": pr.req.nodes, "sweeps": chosen[i][0],
+                           "steps": steps_i, "recorded_steps": chosen[i][1],
+                           "modelled_s": round(est[i], 3), "measured_s": round(real, 3),
                            "model_error": round(est[i] / real - 1.0, 4)})
         plain = {"value": round(conv64 / tot, 5), "unit": UNIT, "converged": conv64,
-                 "seconds": round(tot, 2), "ms_per_step": per, "modelled": True,
-                 "how": "recorded FP64 step count of each request (capped at max_steps; the "
+                 "seconds": round(tot, 2), "ms_per_step": per,
+                 "sweeps": [c[0] for c in chosen], "modelled": True,
+                 "how": "per request, the recorded FP64 step count (capped at max_steps; the "
                         "drop-in runs every solve to its drop or max_steps, as the reference's "
                         "driver does) x its FP64 drop-in ms/step measured over 96 steps (graph "
-                        "chunks), solved one after the other",
+                        "chunks), at whichever of the recorded sweep counts ("
+                        + ", ".join(str(r[0]) for r in recorded) + ") converges it soonest; "
+                        "solved one after the other",
                  "model_checked_on": checks}
 
     cpu = None

@@ -276,6 +276,35 @@ __device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0,
   return ph <= b ? ph : b;
 }
 
+// The zero an IEEE division of a zero dividend by a non-zero divisor gives:
+// the sign is the XOR of the operands' signs.
+__device__ __forceinline__ double zero_quotient(double num, double den) {
+  return __longlong_as_double((__double_as_longlong(num) ^ __double_as_longlong(den)) &
+                              (long long)0x8000000000000000ULL);
+}
+
+// venkat_fold with both quotients formed from non-zero operands only: a zero
+// dividend (a node that is its ring's extreme on the side the reconstruction
+// goes, or a bound of zero) gives zero_quotient without dividing, and the
+// divisor of a discarded quotient (a zero or NaN difference) is 1.  Every
+// other quotient is the same division, so phi has the same bits.
+__device__ __forceinline__ double venkat_fold_nz(double ph, double qrec, double q0, double qmin,
+                                                 double qmax) {
+  const double d = qrec - q0;
+  const bool up = d > 0., down = d < 0.;
+  const bool used = up || down;
+  const double num = up ? qmax - q0 : qmin - q0;
+  const double den = used ? d : 1.0;
+  const bool z1 = num == 0.;
+  const double y = (z1 ? 1.0 : num) / den;
+  const double t = z1 ? zero_quotient(num, den) : y;
+  const double tn = t * t + 2. * t, td = t * t + t + 2.;
+  const bool z2 = tn == 0.;
+  const double f = (z2 ? 1.0 : tn) / td;
+  const double b = used ? (z2 ? zero_quotient(tn, td) : f) : 1.0;
+  return ph <= b ? ph : b;
+}
+
 // linear_algebra.C:571-596 lu() on a 4x4 row-major block, in place.
 __device__ __forceinline__ void lu4(double* A) {
 #pragma unroll

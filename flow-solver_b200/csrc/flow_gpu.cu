@@ -377,16 +377,24 @@ void harvest(flow_ctx* c) {
 // k_node_prepare4: variant 0, 1, 2 -> 0 (compiler's choice), 10, 12 blocks.
 // k_subedge_flux:  variant 0, 1, 2 -> 4, 5, 3 blocks.
 constexpr int kVariants = 3;
-// k_node_prepare4 has two more: variant 3 = k_node_stage (gathers staged in
+// k_node_prepare4 has five more: variant 3 = k_node_stage (gathers staged in
 // shared memory), where its shared memory fits the mesh; variant 4 =
-// k_node_prepare16 (each node's chains split over 16 lanes).
-constexpr int kNodeVariants = 5;
+// k_node_prepare16 (each node's chains split over 16 lanes); variants 5, 6,
+// 7 = variant 0 with WS = 1 (the warp meets after every loop), 2 (the
+// limiter's quotients from non-zero operands) and 3 (both).
+constexpr int kNodeVariants = 8;
 constexpr size_t kStageSmemMax = 110 * 1024;  // two CTAs per SM at most
 template <class F>
 void launch_variant(int v, F&& f) {
   if (v == 1) f(std::integral_constant<int, 10>());
   else if (v == 2) f(std::integral_constant<int, 12>());
   else f(std::integral_constant<int, 0>());
+}
+template <class F>
+void launch_ws_variant(int v, F&& f) {
+  if (v == 5) f(std::integral_constant<int, 1>());
+  else if (v == 6) f(std::integral_constant<int, 2>());
+  else f(std::integral_constant<int, 3>());
 }
 template <class F>
 void launch_flux_variant(int v, F&& f) {
@@ -419,6 +427,17 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
     else
       k_node_stage<3><<<tiles, 128, stage_smem_bytes(3, c->stage_caps), c->stream>>>(
           c->m, c->s, a, c->stage_caps);
+    return launch_check(c);
+  }
+  if (c->var[0] >= 5) {
+    if (k1)
+      launch_ws_variant(c->var[0], [&](auto W) {
+        k_node_prepare4<1, 0, W.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+      });
+    else
+      launch_ws_variant(c->var[0], [&](auto W) {
+        k_node_prepare4<3, 0, W.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+      });
     return launch_check(c);
   }
   if (k1)
@@ -940,6 +959,9 @@ bool preload_kernels() {
         (const void*)k_node_prepare4<1, 0>, (const void*)k_node_prepare4<1, 10>,
         (const void*)k_node_prepare4<1, 12>, (const void*)k_node_prepare4<3, 0>,
         (const void*)k_node_prepare4<3, 10>, (const void*)k_node_prepare4<3, 12>,
+        (const void*)k_node_prepare4<1, 0, 1>, (const void*)k_node_prepare4<1, 0, 2>,
+        (const void*)k_node_prepare4<1, 0, 3>, (const void*)k_node_prepare4<3, 0, 1>,
+        (const void*)k_node_prepare4<3, 0, 2>, (const void*)k_node_prepare4<3, 0, 3>,
         (const void*)k_assemble4<true, 0>, (const void*)k_assemble4<false, 0>,
         (const void*)k_assemble4<true, 1>, (const void*)k_assemble4<false, 1>,
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
@@ -2369,7 +2391,7 @@ int flow_restore_state(flow_ctx* c) {
 int flow_set_variants(flow_ctx* c, int node_prepare, int flux) {
   if (!c || !c->ok || node_prepare < 0 || node_prepare >= kNodeVariants || flux < 0 ||
       flux >= kVariants) {
-    set_error("flow_set_variants: null context, node variant outside 0..4 or flux outside 0..2");
+    set_error("flow_set_variants: null context, node variant outside 0..7 or flux outside 0..2");
     return FLOW_ERR_ARG;
   }
   if (node_prepare == 3 && !c->stage_ok[0] && !c->stage_ok[1]) {

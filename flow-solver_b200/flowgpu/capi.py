@@ -610,7 +610,7 @@ class Solver:
         """Pick the fastest kernel variants on this mesh; returns
         ((node_prepare variant, flux variant), per-variant ms)."""
         v = (C.c_int * 2)()
-        ms = (C.c_double * 8)()
+        ms = (C.c_double * 11)()
         _check(self.L.flow_autotune(self.ctx, C.byref(self.p), int(ts), int(steps), v, ms),
                "flow_autotune")
         return (v[0], v[1]), [round(x, 4) for x in ms]

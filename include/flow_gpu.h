@@ -429,14 +429,19 @@ double flow_last_device_ms(flow_ctx *ctx);
  * asynchronous copies before the arithmetic), offered where its shared
  * memory fits the mesh; node variant 4 gives each node 16 lanes instead of
  * 4 (its stencil columns, gradient components and face points spread over
- * them, every sum still in the reference's order).  flow_autotune times each variant over `steps`
+ * them, every sum still in the reference's order); node variants 5, 6 and 7
+ * are variant 0 with the warp's eight nodes meeting after every loop over
+ * faces or stencil rows (5), with the limiter's quotients formed from
+ * non-zero operands only (6: a zero dividend gives its signed zero without
+ * a division, an unused quotient divides by 1), or both (7); every variant
+ * gives the same bits.  flow_autotune times each variant over `steps`
  * pseudo-time steps from step index `ts` (CUDA events, after one warm-up
  * step), keeps the fastest, and puts the solution state back as it was
  * with a clear status (the returned status still reports what the timing
- * steps ran into).  variants[2] receives the choice, ms[8] (may be NULL)
- * the average kernel times per variant (ms[0..4] node, ms[5..7] flux;
+ * steps ran into).  variants[2] receives the choice, ms[11] (may be NULL)
+ * the average kernel times per variant (ms[0..7] node, ms[8..10] flux;
  * 1e30 for a variant that does not fit).  flow_set_variants sets a choice
- * directly (node 0..4, flux 0..2). */
+ * directly (node 0..7, flux 0..2). */
 int flow_autotune(flow_ctx *ctx, const flow_params *p, int ts, int steps, int *variants,
                   double *ms);
 int flow_set_variants(flow_ctx *ctx, int node_prepare, int flux);

@@ -8,7 +8,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("precision,order", [(0, 3), (3, 3), (0, 1), (3, 1)])
 def test_variants_are_bit_identical_and_autotune_restores_state(precision, order):
-    """Variant 3 of the node kernel is the shared-memory-staged one."""
+    """Variant 3 of the node kernel is the shared-memory-staged one, 4 the
+    16-lane one, 5-7 the warp-reconverging / non-zero-quotient ones."""
     from flowgpu import capi, workloads
     from flowgpu.prep import Mesh
     wl = workloads.Workload("tune", 64, 16, order == 3, order, 0.8 if order == 3 else 0.5,
@@ -16,7 +17,7 @@ def test_variants_are_bit_identical_and_autotune_restores_state(precision, order
     mesh = Mesh.from_case(wl.write(), order=order)
     fp = wl.params()
     runs = []
-    for v in [(0, 0), (1, 1), (2, 2), (3, 0), (4, 2), None]:
+    for v in [(0, 0), (1, 1), (2, 2), (3, 0), (4, 2), (5, 0), (6, 1), (7, 2), None]:
         s = capi.Solver.from_mesh(mesh, fp, device=0)
         s.set_precision(precision)
         s.set_state(mesh.initial_state(fp))
@@ -24,7 +25,7 @@ def test_variants_are_bit_identical_and_autotune_restores_state(precision, order
         if v is None:
             q_before = s.get("Q")
             chosen, ms = s.autotune(ts=4, steps=2)
-            assert 0 <= chosen[0] <= 4 and 0 <= chosen[1] <= 2 and all(t > 0 for t in ms)
+            assert 0 <= chosen[0] <= 7 and 0 <= chosen[1] <= 2 and all(t > 0 for t in ms)
             assert ms[3] < 1e30  # the staged kernel fits this mesh and was timed
             assert np.array_equal(q_before, s.get("Q"))
         else:
