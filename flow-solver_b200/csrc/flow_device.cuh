@@ -276,6 +276,22 @@ __device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0,
   return ph <= b ? ph : b;
 }
 
+// venkat_fold with the quotients of a discarded point (qrec == q0, or a NaN
+// difference) formed as 1/1 instead of from a zero divisor: where the state
+// is uniform (the free stream of the first steps) every face point is such
+// a point.  The points the fold keeps divide the same operands as before.
+__device__ __forceinline__ double venkat_fold_used(double ph, double qrec, double q0,
+                                                   double qmin, double qmax) {
+  const double d = qrec - q0;
+  const bool up = d > 0., down = d < 0.;
+  const bool used = up || down;
+  const double num = used ? (up ? qmax - q0 : qmin - q0) : 1.0;
+  double t = num / (used ? d : 1.0);
+  t = (t * t + 2. * t) / (t * t + t + 2.);
+  const double b = used ? t : 1.0;
+  return ph <= b ? ph : b;
+}
+
 // The zero an IEEE division of a zero dividend by a non-zero divisor gives:
 // the sign is the XOR of the operands' signs.
 __device__ __forceinline__ double zero_quotient(double num, double den) {
@@ -303,6 +319,14 @@ __device__ __forceinline__ double venkat_fold_nz(double ph, double qrec, double 
   const double f = (z2 ? 1.0 : tn) / td;
   const double b = used ? (z2 ? zero_quotient(tn, td) : f) : 1.0;
   return ph <= b ? ph : b;
+}
+
+template <int LIM>
+__device__ __forceinline__ double venkat_fold_lim(double ph, double qrec, double q0, double qmin,
+                                                  double qmax) {
+  if (LIM == 1) return venkat_fold_used(ph, qrec, q0, qmin, qmax);
+  if (LIM == 2) return venkat_fold_nz(ph, qrec, q0, qmin, qmax);
+  return venkat_fold(ph, qrec, q0, qmin, qmax);
 }
 
 // linear_algebra.C:571-596 lu() on a 4x4 row-major block, in place.

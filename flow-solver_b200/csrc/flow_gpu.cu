@@ -379,9 +379,10 @@ void harvest(flow_ctx* c) {
 constexpr int kVariants = 3;
 // k_node_prepare4 has five more: variant 3 = k_node_stage (gathers staged in
 // shared memory), where its shared memory fits the mesh; variant 4 =
-// k_node_prepare16 (each node's chains split over 16 lanes); variants 5, 6,
-// 7 = variant 0 with WS = 1 (the warp meets after every loop), 2 (the
-// limiter's quotients from non-zero operands) and 3 (both).
+// k_node_prepare16 (each node's chains split over 16 lanes); variants 5 and
+// 6 = variant 0 with LIM = 1 (a discarded limiter quotient formed as 1/1)
+// and 2 (besides, a zero dividend's quotient without a division); variant 7
+// = variant 4 with LIM = 1.
 constexpr int kNodeVariants = 8;
 constexpr size_t kStageSmemMax = 110 * 1024;  // two CTAs per SM at most
 template <class F>
@@ -391,10 +392,9 @@ void launch_variant(int v, F&& f) {
   else f(std::integral_constant<int, 0>());
 }
 template <class F>
-void launch_ws_variant(int v, F&& f) {
+void launch_lim_variant(int v, F&& f) {
   if (v == 5) f(std::integral_constant<int, 1>());
-  else if (v == 6) f(std::integral_constant<int, 2>());
-  else f(std::integral_constant<int, 3>());
+  else f(std::integral_constant<int, 2>());
 }
 template <class F>
 void launch_flux_variant(int v, F&& f) {
@@ -413,10 +413,15 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   // the LSQ gradient (k=1, or the second-order start-up steps of k=2) is
   // the k=1 kernel's work
   const bool k1 = c->order == 1 || a.do_grad;
-  if (c->var[0] == 4) {
+  if (c->var[0] == 4 || c->var[0] == 7) {
     const int nb16 = grid_blocks(16 * c->nn, 128);
-    if (k1) k_node_prepare16<1><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
-    else k_node_prepare16<3><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+    if (c->var[0] == 7) {
+      if (k1) k_node_prepare16<1, 1><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+      else k_node_prepare16<3, 1><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+    } else {
+      if (k1) k_node_prepare16<1><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+      else k_node_prepare16<3><<<nb16, 128, 0, c->stream>>>(c->m, c->s, a);
+    }
     return launch_check(c);
   }
   if (c->var[0] == 3 && c->stage_ok[k1 ? 0 : 1]) {
@@ -431,11 +436,11 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   }
   if (c->var[0] >= 5) {
     if (k1)
-      launch_ws_variant(c->var[0], [&](auto W) {
+      launch_lim_variant(c->var[0], [&](auto W) {
         k_node_prepare4<1, 0, W.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
       });
     else
-      launch_ws_variant(c->var[0], [&](auto W) {
+      launch_lim_variant(c->var[0], [&](auto W) {
         k_node_prepare4<3, 0, W.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
       });
     return launch_check(c);
@@ -960,14 +965,14 @@ bool preload_kernels() {
         (const void*)k_node_prepare4<1, 12>, (const void*)k_node_prepare4<3, 0>,
         (const void*)k_node_prepare4<3, 10>, (const void*)k_node_prepare4<3, 12>,
         (const void*)k_node_prepare4<1, 0, 1>, (const void*)k_node_prepare4<1, 0, 2>,
-        (const void*)k_node_prepare4<1, 0, 3>, (const void*)k_node_prepare4<3, 0, 1>,
-        (const void*)k_node_prepare4<3, 0, 2>, (const void*)k_node_prepare4<3, 0, 3>,
+        (const void*)k_node_prepare4<3, 0, 1>, (const void*)k_node_prepare4<3, 0, 2>,
         (const void*)k_assemble4<true, 0>, (const void*)k_assemble4<false, 0>,
         (const void*)k_assemble4<true, 1>, (const void*)k_assemble4<false, 1>,
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
         (const void*)k_boundary_add4<true>, (const void*)k_boundary_add4<false>,
         (const void*)k_node_stage<1>, (const void*)k_node_stage<3>,
         (const void*)k_node_prepare16<1>, (const void*)k_node_prepare16<3>,
+        (const void*)k_node_prepare16<1, 1>, (const void*)k_node_prepare16<3, 1>,
         (const void*)k_faces_assemble<0, 1>, (const void*)k_faces_assemble<1, 1>,
         (const void*)k_faces_assemble<0, 2>, (const void*)k_faces_assemble<1, 2>,
         (const void*)k_diag_lu,

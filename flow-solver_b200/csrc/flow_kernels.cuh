@@ -124,20 +124,17 @@ __device__ __forceinline__ void cp_async_wait() {
 // formed by every lane of the quad from node constants computed once.
 // MINB: resident blocks per SM the compiler must allow (0: its own choice);
 // the autotuner picks the variant that runs fastest on a given mesh.
-// WS bit 0: the warp's eight quads, whose loops run for different numbers
-// of faces and stencil rows, meet again after every loop (__syncwarp);
-// bit 1: the limiter's quotients from non-zero operands (venkat_fold_nz).
-// Neither changes an operation on the data, so every variant has the same bits.
-template <int ORDER, int MINB, int WS = 0>
+// LIM: the limiter's fold -- 0 venkat_fold; 1 venkat_fold_used (a quotient
+// the fold discards is formed as 1/1); 2 venkat_fold_nz (besides, a zero
+// dividend gives its signed zero without dividing).  All give the same bits.
+template <int ORDER, int MINB, int LIM = 0>
 __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = (tid >> 2) + 1, v = tid & 3;
   const int qbase = threadIdx.x & ~3 & 31;
   const unsigned qmask = 0xFu << qbase;
-  const bool live = n <= m.nn;
-  const unsigned wmask = (WS & 1) ? __ballot_sync(0xFFFFFFFFu, live) : 0u;
-  if (!live) return;  // whole quads leave together
+  if (n > m.nn) return;  // whole quads leave together
   const double4 q4 = reinterpret_cast<const double4*>(s.nQ)[n];
   const double q0v = v == 0 ? q4.x : v == 1 ? q4.y : v == 2 ? q4.z : q4.w;
 
@@ -166,7 +163,6 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
     if (!isfinite(w)) bad = 1;
     ev += (w * xn[2]);
   }
-  if (WS & 1) __syncwarp(wmask);
   if (v == 0) {
     const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
     s.dt[n] = dt;
@@ -199,7 +195,6 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
       }
     }
   }
-  if (WS & 1) __syncwarp(wmask);
   if (ORDER == 1 && a.do_grad)
     reinterpret_cast<double2*>(s.grad + 8 * (long)n)[v] = make_double2(g0, g1);
 
@@ -217,8 +212,7 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
 #pragma unroll
       for (int c = 0; c < 5; c++) acc[c] += bv * U[5 * k + c];
     }
-    if (WS & 1) __syncwarp(wmask);
-    const double* VT = m.svd_VT + 25 * (long)n;
+      const double* VT = m.svd_VT + 25 * (long)n;
     const double* S = m.svd_S + 5 * (long)n;
     double t1v[5];
 #pragma unroll
@@ -251,7 +245,7 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
       const double4 d = m.sub_dx[sub];
       const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
       const double qr = q0v + (g0 * dx0 + g1 * dx1);
-      ph = (WS & 2) ? venkat_fold_nz(ph, qr, q0v, qmin, qmax) : venkat_fold(ph, qr, q0v, qmin, qmax);
+      ph = venkat_fold_lim<LIM>(ph, qr, q0v, qmin, qmax);
     } else {
       const double* xg = m.sub_xg + 6 * (long)sub;
 #pragma unroll
@@ -260,12 +254,10 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
         double qr = pv;
         qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
                h[4] * dx0 * dx1);
-        ph = (WS & 2) ? venkat_fold_nz(ph, qr, q0v, qmin, qmax)
-                      : venkat_fold(ph, qr, q0v, qmin, qmax);
+        ph = venkat_fold_lim<LIM>(ph, qr, q0v, qmin, qmax);
       }
     }
   }
-  if (WS & 1) __syncwarp(wmask);
   // min over the variables in order 0..3 (limiter.C:895-906)
   const double p1 = __shfl_sync(qmask, ph, qbase + 1);
   const double p2 = __shfl_sync(qmask, ph, qbase + 2);
@@ -300,7 +292,8 @@ __device__ __forceinline__ double hshfl(double x, unsigned mask, int lane) {
   return __shfl_sync(mask, x, lane);
 }
 
-template <int ORDER>
+// LIM: the limiter's fold, as in k_node_prepare4.
+template <int ORDER, int LIM = 0>
 __global__ void __launch_bounds__(128) k_node_prepare16(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -434,7 +427,7 @@ __global__ void __launch_bounds__(128) k_node_prepare16(DevMesh m, DevState s, S
         const double4 d = m.sub_dx[sub];
         const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
         const double qr = q0v + (g0 * dx0 + g1 * dx1);
-        ph = venkat_fold(ph, qr, q0v, mn, mx);
+        ph = venkat_fold_lim<LIM>(ph, qr, q0v, mn, mx);
         if (ph != ph) sawnan = 1;
       } else {
         const double* xg = m.sub_xg + 6 * (long)sub;
@@ -444,7 +437,7 @@ __global__ void __launch_bounds__(128) k_node_prepare16(DevMesh m, DevState s, S
           double qr = pv;
           qr += (h[0] * dx0 + h[1] * dx1 + h[2] * dx0 * dx0 * 0.5 + h[3] * dx1 * dx1 * 0.5 +
                  h[4] * dx0 * dx1);
-          ph = venkat_fold(ph, qr, q0v, mn, mx);
+          ph = venkat_fold_lim<LIM>(ph, qr, q0v, mn, mx);
           if (ph != ph) sawnan = 1;
         }
       }

@@ -138,12 +138,12 @@ def test_long_residual_history(ref_lib, nc, nr, curved, order, mach, steps):
 @pytest.mark.parametrize("nc,nr,curved,order,steps", [
     (128, 32, False, 1, 4), (128, 32, True, 3, 4), (12, 4, True, 3, 4), (8, 3, False, 1, 4),
 ])
-@pytest.mark.parametrize("variant", [3, 4, 7])
+@pytest.mark.parametrize("variant", [3, 4, 5, 6, 7])
 def test_node_kernel_variants_bitwise(ref_lib, nc, nr, curved, order, steps, variant):
-    """Node variant 3 (gathers staged in shared memory), 4 (16 lanes a node)
-    and 7 (the warp meeting after every loop, the limiter's quotients from
-    non-zero operands), step by step against the reference, including meshes
-    smaller than one tile of 32 nodes."""
+    """Node variant 3 (gathers staged in shared memory), 4 (16 lanes a node),
+    5 and 6 (the limiter's quotients from no zero divisor / no zero operand)
+    and 7 (16 lanes, the limiter of 5), step by step against the reference, including meshes smaller than one
+    tile of 32 nodes."""
     case = ParityCase(nc, nr, curved, order)
     gpu = _solver(case)
     gpu.set_variants(variant, 0)
