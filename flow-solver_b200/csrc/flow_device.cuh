@@ -276,56 +276,34 @@ __device__ __forceinline__ double venkat_fold(double ph, double qrec, double q0,
   return ph <= b ? ph : b;
 }
 
-// venkat_fold with the quotients of a discarded point (qrec == q0, or a NaN
-// difference) formed as 1/1 instead of from a zero divisor: where the state
-// is uniform (the free stream of the first steps) every face point is such
-// a point.  The points the fold keeps divide the same operands as before.
-__device__ __forceinline__ double venkat_fold_used(double ph, double qrec, double q0,
-                                                   double qmin, double qmax) {
-  const double d = qrec - q0;
-  const bool up = d > 0., down = d < 0.;
-  const bool used = up || down;
-  const double num = used ? (up ? qmax - q0 : qmin - q0) : 1.0;
-  double t = num / (used ? d : 1.0);
-  t = (t * t + 2. * t) / (t * t + t + 2.);
-  const double b = used ? t : 1.0;
-  return ph <= b ? ph : b;
-}
-
-// The zero an IEEE division of a zero dividend by a non-zero divisor gives:
-// the sign is the XOR of the operands' signs.
-__device__ __forceinline__ double zero_quotient(double num, double den) {
-  return __longlong_as_double((__double_as_longlong(num) ^ __double_as_longlong(den)) &
-                              (long long)0x8000000000000000ULL);
-}
-
-// venkat_fold with both quotients formed from non-zero operands only: a zero
-// dividend (a node that is its ring's extreme on the side the reconstruction
-// goes, or a bound of zero) gives zero_quotient without dividing, and the
-// divisor of a discarded quotient (a zero or NaN difference) is 1.  Every
-// other quotient is the same division, so phi has the same bits.
+// venkat_fold without a division of a zero or by a zero: a point the fold
+// discards (qrec == q0, or a NaN difference) and a point whose bound is the
+// node's own value (qmax == q0 going up, qmin == q0 going down: a zero
+// dividend) divide 1 by 1 instead.  The first folds in 1 as before; the
+// second folds in +0, the bits the reference's quotients give there
+// (0/d = +-0, then (+0 + +-0) / (+0 +- 0 + 2) = +0).  Every other point
+// divides the same operands, so phi has the same bits.  Where the state is
+// uniform (the free stream of the first steps) most points are of the two
+// kinds, and a division of or by zero leaves the fast path of the division.
 __device__ __forceinline__ double venkat_fold_nz(double ph, double qrec, double q0, double qmin,
                                                  double qmax) {
   const double d = qrec - q0;
   const bool up = d > 0., down = d < 0.;
   const bool used = up || down;
   const double num = up ? qmax - q0 : qmin - q0;
-  const double den = used ? d : 1.0;
-  const bool z1 = num == 0.;
-  const double y = (z1 ? 1.0 : num) / den;
-  const double t = z1 ? zero_quotient(num, den) : y;
-  const double tn = t * t + 2. * t, td = t * t + t + 2.;
-  const bool z2 = tn == 0.;
-  const double f = (z2 ? 1.0 : tn) / td;
-  const double b = used ? (z2 ? zero_quotient(tn, td) : f) : 1.0;
+  const bool flat = num == 0.;
+  const bool div = used && !flat;
+  double t = (div ? num : 1.0) / (div ? d : 1.0);
+  t = (t * t + 2. * t) / (t * t + t + 2.);
+  const double b = used ? (flat ? 0.0 : t) : 1.0;
   return ph <= b ? ph : b;
 }
 
+// The limiter fold of a node kernel: 0 venkat_fold, 1 venkat_fold_nz.
 template <int LIM>
 __device__ __forceinline__ double venkat_fold_lim(double ph, double qrec, double q0, double qmin,
                                                   double qmax) {
-  if (LIM == 1) return venkat_fold_used(ph, qrec, q0, qmin, qmax);
-  if (LIM == 2) return venkat_fold_nz(ph, qrec, q0, qmin, qmax);
+  if (LIM == 1) return venkat_fold_nz(ph, qrec, q0, qmin, qmax);
   return venkat_fold(ph, qrec, q0, qmin, qmax);
 }
 

@@ -124,9 +124,8 @@ __device__ __forceinline__ void cp_async_wait() {
 // formed by every lane of the quad from node constants computed once.
 // MINB: resident blocks per SM the compiler must allow (0: its own choice);
 // the autotuner picks the variant that runs fastest on a given mesh.
-// LIM: the limiter's fold -- 0 venkat_fold; 1 venkat_fold_used (a quotient
-// the fold discards is formed as 1/1); 2 venkat_fold_nz (besides, a zero
-// dividend gives its signed zero without dividing).  All give the same bits.
+// LIM: the limiter's fold -- 0 venkat_fold, 1 venkat_fold_nz (no division
+// of or by zero); both give the same bits.
 template <int ORDER, int MINB, int LIM = 0>
 __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged

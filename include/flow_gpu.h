@@ -429,12 +429,11 @@ double flow_last_device_ms(flow_ctx *ctx);
  * asynchronous copies before the arithmetic), offered where its shared
  * memory fits the mesh; node variant 4 gives each node 16 lanes instead of
  * 4 (its stencil columns, gradient components and face points spread over
- * them, every sum still in the reference's order); node variants 5 and 6
- * are variant 0 with the limiter's discarded quotients (a face point whose
- * reconstruction equals the node's value) formed as 1/1 instead of from a
- * zero divisor (5), and besides with a zero dividend's quotient given as its
- * signed zero without a division (6); node variant 7 is variant 4 with the
- * discarded quotients of variant 5; every variant gives the same bits.
+ * them, every sum still in the reference's order); node variants 5, 6 and
+ * 7 are variants 0, 1 and 4 with a limiter that divides no zero and by no
+ * zero (a face point whose reconstruction equals the node's value, or whose
+ * bound is the node's own value, folds in the value the reference's
+ * quotients give there without dividing); every variant gives the same bits.
  * flow_autotune times each variant over `steps`
  * pseudo-time steps from step index `ts` (CUDA events, after one warm-up
  * step), keeps the fastest, and puts the solution state back as it was

@@ -9,8 +9,8 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("precision,order", [(0, 3), (3, 3), (0, 1), (3, 1)])
 def test_variants_are_bit_identical_and_autotune_restores_state(precision, order):
     """Variant 3 of the node kernel is the shared-memory-staged one, 4 the
-    16-lane one, 5 and 6 the ones whose limiter forms no quotient from a zero
-    divisor (5) or operand (6), 7 the 16-lane one with the limiter of 5."""
+    16-lane one, 5-7 variants 0, 1 and 4 with the limiter that divides no
+    zero and by no zero."""
     from flowgpu import capi, workloads
     from flowgpu.prep import Mesh
     wl = workloads.Workload("tune", 64, 16, order == 3, order, 0.8 if order == 3 else 0.5,

@@ -141,8 +141,8 @@ def test_long_residual_history(ref_lib, nc, nr, curved, order, mach, steps):
 @pytest.mark.parametrize("variant", [3, 4, 5, 6, 7])
 def test_node_kernel_variants_bitwise(ref_lib, nc, nr, curved, order, steps, variant):
     """Node variant 3 (gathers staged in shared memory), 4 (16 lanes a node),
-    5 and 6 (the limiter's quotients from no zero divisor / no zero operand)
-    and 7 (16 lanes, the limiter of 5), step by step against the reference, including meshes smaller than one
+    5-7 (variants 0, 1 and 4 with the limiter that divides no zero and by no
+    zero), step by step against the reference, including meshes smaller than one
     tile of 32 nodes."""
     case = ParityCase(nc, nr, curved, order)
     gpu = _solver(case)
