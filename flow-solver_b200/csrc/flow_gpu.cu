@@ -203,7 +203,6 @@ struct flow_ctx {
   const int* ring_chunk_sub[kRingShapes][2] = {};
   bool ring_ok[kRingShapes] = {};
   int ring = 0;  // requested shape: sub-levels of ring_rows(ring) rows
-  int l2_ahead = 0;  // mode 3 sweep: sub-levels prefetched to L2 past the ring
   int sweep_df = 0;  // 1: one-launch (dataflow) mode 3 sweeps (flow_set_sweep_dataflow)
   bool has_edge_w = false;  // the grid view carried LSQ edge weights
   bool has_stencils = false;  // order 3: the view carried the k=2 stencils and SVD factors
@@ -1098,7 +1097,6 @@ void apply_ring(flow_ctx* c) {
     c->ct.chunk_sub[dir] = c->ring_chunk_sub[shape][dir];
   }
   c->ct.ring = shape;
-  c->ct.l2_ahead = c->l2_ahead;
 }
 
 int build_chunks_with(flow_ctx* c, int bw, int cmax, int lmax) {
@@ -1746,19 +1744,6 @@ int flow_set_precision(flow_ctx* c, int mode) {
     if (rc) return rc;
   }
   c->precision = mode;
-  return 0;
-}
-
-int flow_set_sweep_prefetch(flow_ctx* c, int ahead) {
-  if (!c || !c->ok || ahead < 0 || ahead > 64) {
-    set_error("flow_set_sweep_prefetch: null context or ahead outside 0..64");
-    return FLOW_ERR_ARG;
-  }
-  cudaSetDevice(c->device);
-  cudaStreamSynchronize(c->stream);
-  drop_graphs(c);
-  c->l2_ahead = ahead;
-  c->ct.l2_ahead = ahead;
   return 0;
 }
 

@@ -111,11 +111,6 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
-// Bulk prefetch of `bytes` (a multiple of 16, from a 16-byte aligned
-// address of this GPU's memory) into L2; no data reaches the SM.
-__device__ __forceinline__ void prefetch_l2_bulk(const void* src, unsigned bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
-}
 
 // ---------------------------------------------------------------------------
 // Per node: cv_calc_eigenvalue_contribution (cv_calc.C:819-953) and the dt /
@@ -1714,20 +1709,6 @@ __device__ __forceinline__ void sweep_chunk_body(const DevState& s, const ChunkT
     }
     cp_async_commit();  // one group per sub-level, empty past the end
   };
-  // records of the sub-levels past the ring are prefetched into L2 ahead of
-  // their cp.async, which then waits on L2 rather than HBM (the ring's
-  // bytes in flight per SM, not the DRAM bandwidth, set a sub-level's time)
-  const int ahead = ct.l2_ahead;
-  auto prefetch = [&](int u) {
-    if (tid == 0 && u < nsub) {
-      const int r0 = ss[u], r1 = ss[u + 1];
-      if (r1 > r0)
-        prefetch_l2_bulk(recs + (long)r0 * kRecInts,
-                         (unsigned)(r1 - r0) * (unsigned)sizeof(SweepRec));
-    }
-  };
-  if (ahead > 0)
-    for (int k = SLOTS - 1; k < SLOTS - 1 + ahead; k++) prefetch(k);
   for (int k = 0; k < SLOTS - 1; k++) issue(k);
   const int quad = tid >> 2, r = tid & 3;
   const int qbase = tid & 31 & ~3;
@@ -1741,7 +1722,6 @@ __device__ __forceinline__ void sweep_chunk_body(const DevState& s, const ChunkT
   }
   __syncthreads();
   for (int u = 0; u < nsub; u++) {
-    if (ahead > 0) prefetch(u + SLOTS - 1 + ahead);
     issue(u + SLOTS - 1);  // into the slot sub-level u-1 left
     if (quad < ss[u + 1] - ss[u]) {
       const SweepRec& R = *reinterpret_cast<const SweepRec*>(

@@ -108,7 +108,6 @@ struct ChunkTables {
   const int* chunk_sub[2];   // first sub-level of each chunk, plus the end
   const int* pos[2];         // record index of each row (1..nn)
   int ring;                  // ring shape of the sub-level tables: rows 64 >> ring
-  int l2_ahead;              // sub-levels past the ring whose records are prefetched to L2
   // one-launch (dataflow) sweeps
   const int* task_chunk[2];  // per direction: chunks in dispensing (colour) order
   const int* colour;         // colour of each chunk

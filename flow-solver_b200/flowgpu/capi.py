@@ -53,7 +53,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_server_set_autotune", "flow_server_set_stall",
            "flow_server_set_sweep_schedule", "flow_set_stream_priority",
            "flow_server_set_priority_policy", "flow_server_set_jacobian",
-           "flow_server_set_recovery", "flow_set_sweep_prefetch",
+           "flow_server_set_recovery",
            "flow_selftest_sweep_timeout")
 
 
@@ -200,7 +200,6 @@ def _load_locked():
     L.flow_server_set_priority_policy.argtypes = [vp, C.c_int]
     L.flow_server_set_jacobian.argtypes = [vp, C.c_int]
     L.flow_server_set_recovery.argtypes = [vp, C.c_int]
-    L.flow_set_sweep_prefetch.argtypes = [vp, C.c_int]
     L.flow_selftest_sweep_timeout.argtypes = [vp, C.c_long, IP]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
@@ -649,10 +648,6 @@ class Solver:
     def set_jacobian(self, mode: int):
         """Precision-form face Jacobians: 0 forward differences, 1 approximate Roe."""
         _check(self.L.flow_set_jacobian(self.ctx, int(mode)), "flow_set_jacobian")
-
-    def set_sweep_prefetch(self, ahead: int):
-        """Mode 3: sub-levels of sweep records prefetched to L2 past the ring."""
-        _check(self.L.flow_set_sweep_prefetch(self.ctx, int(ahead)), "flow_set_sweep_prefetch")
 
     def set_sweep_pairs(self, on: bool):
         """Mode 3: a colour's two passes in a row as one launch (default on)."""

@@ -457,11 +457,6 @@ int flow_set_variants(flow_ctx *ctx, int node_prepare, int flux);
  * not chosen here: it changes the iterates, not only their speed. */
 int flow_autotune_sweep(flow_ctx *ctx, const flow_params *p, int ts, int steps, int allow_df,
                         int *choice, double *ms);
-/* Mode 3 sweeps (no reference counterpart): a chunk prefetches into L2 the
- * records of the `ahead` sub-levels past those its shared-memory ring holds
- * (one bulk prefetch a sub-level; 0, the default, turns it off), so that the
- * ring's copies wait on L2 rather than HBM.  The same results. */
-int flow_set_sweep_prefetch(flow_ctx *ctx, int ahead);
 
 /* ---- Device arena (no counterpart in the reference) ----------------------
  * One cudaMalloc of `bytes` on `device`, carved into the buffers of the
