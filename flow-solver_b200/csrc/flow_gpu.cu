@@ -484,11 +484,11 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
     rc |= launch_check(c);
     return rc;
   }
+  // the approximate Roe Jacobian only in the precision form
+  const bool approx = jac && c->jac_mode != 0 && c->precision != 0;
   {
     Timed t(c, 1);
     int nbs = grid_blocks(c->ns, 128);
-    // the approximate Roe Jacobian only in the precision form
-    const bool approx = jac && c->jac_mode != 0 && c->precision != 0;
     if (a.recon == 1) {
       launch_flux_variant(c->var[1], [&](auto V) {
         if (approx) k_subedge_flux<1, true, V.value, 1><<<nbs, 128, 0, c->stream>>>(c->m, c->s, a);
@@ -517,10 +517,12 @@ int launch_residuals(flow_ctx* c, const StepArgs& a, int jac) {
     const MixedTables& mt = c->mt;
     const ChunkTables& ct = c->ct;
     if (c->precision == 3) {
-      if (jac) k_assemble4<true, 2><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      if (approx) k_assemble4<true, 2, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      else if (jac) k_assemble4<true, 2><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
       else k_assemble4<false, 2><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
     } else if (c->precision != 0) {
-      if (jac) k_assemble4<true, 1><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      if (approx) k_assemble4<true, 1, true><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
+      else if (jac) k_assemble4<true, 1><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
       else k_assemble4<false, 1><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
     } else {
       if (jac) k_assemble4<true, 0><<<nbn, 128, 0, c->stream>>>(c->m, c->s, a, mt, ct);
@@ -968,6 +970,7 @@ bool preload_kernels() {
         (const void*)k_assemble4<true, 0>, (const void*)k_assemble4<false, 0>,
         (const void*)k_assemble4<true, 1>, (const void*)k_assemble4<false, 1>,
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,
+        (const void*)k_assemble4<true, 1, true>, (const void*)k_assemble4<true, 2, true>,
         (const void*)k_boundary_add4<true>, (const void*)k_boundary_add4<false>,
         (const void*)k_node_stage<1>, (const void*)k_node_stage<3>,
         (const void*)k_node_prepare16<1>, (const void*)k_node_prepare16<3>,

@@ -753,10 +753,12 @@ __device__ __forceinline__ void face_flux_approx(double4 g, double gamma, const 
   roe_core(g.x, g.y, g.z, gamma, ogm1, qL, qR, SL, SR, bg, flux, Rm);
   euler_jacobian(qL, g.x, g.y, gamma, dL);
   euler_jacobian(qR, g.x, g.y, gamma, dR);
+  // each entry rounded to FP32: the blocks these feed are FP32, and the
+  // face-to-assembly round trip carries half the bytes
 #pragma unroll
   for (int k = 0; k < 16; k++) {
-    JL[k] = 0.5 * (dL[k] + Rm[k]) * g.z;
-    JR[k] = 0.5 * (dR[k] - Rm[k]) * g.z;
+    JL[k] = (double)__double2float_rn(0.5 * (dL[k] + Rm[k]) * g.z);
+    JR[k] = (double)__double2float_rn(0.5 * (dR[k] - Rm[k]) * g.z);
   }
 }
 
@@ -769,6 +771,17 @@ __device__ __forceinline__ void face_flux_approx(double4 g, double gamma, const 
 // precision form) writes FP32 off-diagonal blocks and FP32 LU factors with
 // reciprocal pivots instead of the FP64 row: into the mode 1/2 tables
 // (MIXED 1) or into the row's forward and backward sweep records (MIXED 2).
+
+// Row q of face `sub`'s Jacobian block J (JL or JR): FP64, or FP32 entries
+// (JF) widened exactly.
+template <bool JF>
+__device__ __forceinline__ double4 face_jac_row(const double* J, int sub, int q) {
+  if (JF) {
+    const float4 f = reinterpret_cast<const float4*>(J)[4 * (long)sub + q];
+    return make_double4(f.x, f.y, f.z, f.w);
+  }
+  return reinterpret_cast<const double4*>(J + 16 * (long)sub)[q];
+}
 
 // The V/dt diagonal row q of node n's block (build_matrix).
 __device__ __forceinline__ void diag_row(const DevMesh& m, const DevState& s, const StepArgs& a,
@@ -873,7 +886,9 @@ __device__ __forceinline__ void assemble_row(const DevMesh& m, const DevState& s
   }
 }
 
-template <bool JAC, int MIXED>
+// JF: the face Jacobians are the approximate ones, stored as FP32
+// (k_subedge_flux<., true, ., 1>).
+template <bool JAC, int MIXED, bool JF = false>
 __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepArgs a,
                                                    MixedTables mt, ChunkTables ct) {
   if (*s.stop) return;  // the run has converged
@@ -893,8 +908,7 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
     if (side == 0) r += f;
     else r -= f;
     if (JAC) {
-      const double4 J =
-          reinterpret_cast<const double4*>((side ? s.JR : s.JL) + 16 * (long)sub)[q];
+      const double4 J = face_jac_row<JF>(side ? s.JR : s.JL, sub, q);
       if (side == 0) {
         D0 += J.x; D1 += J.y; D2 += J.z; D3 += J.w;
       } else {
@@ -910,7 +924,7 @@ __global__ void __launch_bounds__(128) k_assemble4(DevMesh m, DevState s, StepAr
     for (int t = 0; t < 2; t++) {
       const int sub = t == 0 ? cs.x : cs.y;
       if (sub < 0) break;
-      const double4 J = reinterpret_cast<const double4*>(src + 16 * (long)sub)[q];
+      const double4 J = face_jac_row<JF>(src, sub, q);
       if (cs.z == 0) {
         B0 += J.x; B1 += J.y; B2 += J.z; B3 += J.w;
       } else {
@@ -1079,12 +1093,15 @@ __global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState 
     double JL[16], JR[16];
     face_flux_approx(g, a.gamma, qL, qR, flux, JL, JR);
     reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
-    double4* JLo = reinterpret_cast<double4*>(s.JL + 16 * (long)sub);
-    double4* JRo = reinterpret_cast<double4*>(s.JR + 16 * (long)sub);
+    // FP32-valued entries stored as FP32 (16 floats a face and side)
+    float4* JLo = reinterpret_cast<float4*>(s.JL) + 4 * (long)sub;
+    float4* JRo = reinterpret_cast<float4*>(s.JR) + 4 * (long)sub;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-      JLo[r] = make_double4(JL[4 * r], JL[4 * r + 1], JL[4 * r + 2], JL[4 * r + 3]);
-      JRo[r] = make_double4(JR[4 * r], JR[4 * r + 1], JR[4 * r + 2], JR[4 * r + 3]);
+      JLo[r] = make_float4((float)JL[4 * r], (float)JL[4 * r + 1], (float)JL[4 * r + 2],
+                           (float)JL[4 * r + 3]);
+      JRo[r] = make_float4((float)JR[4 * r], (float)JR[4 * r + 1], (float)JR[4 * r + 2],
+                           (float)JR[4 * r + 3]);
     }
     return;
   }

@@ -505,7 +505,8 @@ static void euler_jacobian(const double *Q, double nx, double ny, double gamma, 
 /* Precision form, jac_approx: dF/dqL = (A(qL) + |A~|) len/2 and
  * dF/dqR = (A(qR) - |A~|) len/2, |A~| the Roe dissipation matrix of the face
  * (no reference counterpart; the reference's boundary faces use this form,
- * jacobian.C:681-962), accumulated like numerical_jacobian's blocks. */
+ * jacobian.C:681-962), each entry rounded to FP32 (the blocks it feeds are
+ * FP32) and accumulated in double like numerical_jacobian's blocks. */
 static void approximate_jacobian(orc_grid *g, const orc_params *p, int L, int R,
                                  const double *QL, const double *QR, double nx, double ny,
                                  double len)
@@ -516,8 +517,8 @@ static void approximate_jacobian(orc_grid *g, const orc_params *p, int L, int R,
   euler_jacobian(QR, nx, ny, p->gamma, dR);
   for (int i = 0; i < 4; i++)
     for (int k = 0; k < 4; k++) {
-      dL[i][k] = 0.5 * (dL[i][k] + Rm[i * 4 + k]) * len;
-      dR[i][k] = 0.5 * (dR[i][k] - Rm[i * 4 + k]) * len;
+      dL[i][k] = (double)(float)(0.5 * (dL[i][k] + Rm[i * 4 + k]) * len);
+      dR[i][k] = (double)(float)(0.5 * (dR[i][k] - Rm[i * 4 + k]) * len);
     }
   add_block(&g->LHS[(long)g->iau[L] * 16], dL, 1.0);
   add_block(&g->LHS[(long)g->iau[R] * 16], dR, -1.0);
