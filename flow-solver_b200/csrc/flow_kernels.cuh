@@ -175,14 +175,14 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   const int e0 = m.nedg_ptr[n], e1 = m.nedg_ptr[n + 1];
   #pragma unroll 4
   for (int k = e0; k < e1; k++) {
-    const int ed = m.nedg[k];
-    const int e = ed >> 1, side = ed & 1;
-    const int2 lr = m.edge_lr[e];
-    const int other = side ? lr.x : lr.y;
-    const double qo = s.nQ[4 * (long)other + v];
+    // the neighbour straight from the node's incidence list (nedg_nbr), so
+    // its state is one dependent load away, not two
+    const double qo = s.nQ[4 * (long)m.nedg_nbr[k] + v];
     qmin = qmin <= qo ? qmin : qo;
     qmax = qmax >= qo ? qmax : qo;
     if (ORDER == 1 && a.do_grad) {
+      const int ed = m.nedg[k];
+      const int e = ed >> 1, side = ed & 1;
       const double4 w = m.edge_w[e];
       const double dq = side ? (q0v - qo) : (qo - q0v);  // nQ[R] - nQ[L]
       if (side == 0) {

@@ -33,7 +33,7 @@ def node_prepare_bytes(mesh) -> int:
                write dt 8, phi 64 (k=1: grad 64; k=2: derivatives 160, point values 32)
     per subedge      two incidence entries 8, normal/length 32,
                      face point offsets 32 (k=1) or 3 Gauss points 48 (k=2)
-    per edge         two incidence entries 8, end nodes 8 (k=1: LSQ weights 32)
+    per edge         two neighbour entries 8 (k=1: two incidence entries 8, LSQ weights 32)
     per bedge        incidence entry 4, normal/length 24
     per stencil entry (k=2) index 4, weight 8, the row of U's first 5 columns 40
     """
@@ -41,7 +41,7 @@ def node_prepare_bytes(mesh) -> int:
     k2 = mesh.order == 3
     per_node = 32 + 16 + 8 + 12 + 8 + 64 + ((72 + 200 + 40 + 4 + 160 + 32) if k2 else 64)
     per_sub = 8 + 32 + (48 if k2 else 32)
-    per_edge = 8 + 8 + (0 if k2 else 32)
+    per_edge = 8 + (0 if k2 else 8 + 32)
     per_bedge = 4 + 24
     return int(z["nn"] * per_node + z["ns"] * per_sub + z["ne"] * per_edge +
                z["nbe"] * per_bedge + z["stencil"] * 52)
