@@ -537,14 +537,15 @@ def run_batch(args, bw):
     s.close()
     peaks, peak_kind = measured_peaks()
     fused = bw.jacobian == 1 and bw.precision != 0
+    approx = bw.jacobian != 0 and bw.precision != 0
     # algorithmic bytes per launch of each kernel class (flowgpu/roofline.py)
     names = {"node_prepare": "k_node_stage" if variants[0] == 3 else "k_node_prepare4",
              "subedge_flux": "k_faces_assemble" if fused else "k_subedge_flux",
              "assemble": "k_assemble4"}
     per_launch = {"node_prepare": roofline.node_prepare_bytes(big.mesh),
                   "subedge_flux": (roofline.faces_assemble_bytes(big.mesh) if fused else
-                                   roofline.subedge_flux_bytes(big.mesh)),
-                  "assemble": roofline.assemble_bytes(big.mesh, bw.precision)}
+                                   roofline.subedge_flux_bytes(big.mesh, approx=approx)),
+                  "assemble": roofline.assemble_bytes(big.mesh, bw.precision, approx=approx)}
     if bw.precision == 3:  # one sweep: its colour launches
         names["sweep"] = "k_sweep_chunk (one sweep)"
         per_launch["sweep"] = roofline.chunk_sweep_bytes(big.mesh)

@@ -74,27 +74,31 @@ def chunk_sweep_bytes(mesh) -> int:
     return int(z["nn"] * (640 + 16 + 16))
 
 
-def subedge_flux_bytes(mesh, jacobian: bool = True) -> int:
+def subedge_flux_bytes(mesh, jacobian: bool = True, approx: bool = False) -> int:
     """k_subedge_flux: per subedge its end nodes 8, normal/length 32 and the
     two node states 64 read (k=1 reconstruction: the two nodes' gradients
     128, limiters 16 and the face-point offsets 32), the flux 32 written and,
-    with the Jacobian, dF/dqL and dF/dqR 256."""
+    with the Jacobian, dF/dqL and dF/dqR: 256 (FP64) or, for the approximate
+    Jacobian of the precision form, 128 (FP32)."""
     z = _sizes(mesh)
-    per = 8 + 32 + 64 + (0 if mesh.order == 3 else 128 + 16 + 32) + 32 + (256 if jacobian else 0)
+    jac = (128 if approx else 256) if jacobian else 0
+    per = 8 + 32 + 64 + (0 if mesh.order == 3 else 128 + 16 + 32) + 32 + jac
     return int(z["ns"] * per)
 
 
-def assemble_bytes(mesh, precision: int = 3) -> int:
+def assemble_bytes(mesh, precision: int = 3, approx: bool = False) -> int:
     """k_assemble4: per subedge incidence (two a subedge) its entry 4, the
-    face's flux 32 and Jacobian 128 read; per off-diagonal block its
+    face's flux 32 and Jacobian block J read; per off-diagonal block its
     subedge pair 16 and the one or two face Jacobians (two a block on these
-    meshes) 256 read; per node dt, cv_area 16 read, R and RHS 64 written and
+    meshes) 2J read; per node dt, cv_area 16 read, R and RHS 64 written and
     its row written: two 640-byte sweep records (mode 3), or FP64 blocks
-    128 a block and LU factors 128 (mode 0)."""
+    128 a block and LU factors 128 (mode 0).  J = 128 (FP64) or 64 (the
+    approximate Jacobian's FP32 blocks)."""
     z = _sizes(mesh)
     offd = z["nnz"] - z["nn"]
+    J = 64 if approx else 128
     row = 2 * 640 if precision == 3 else 128 * z["nnz"] / max(z["nn"], 1) + 128
-    return int(2 * z["ns"] * (4 + 32 + 128) + offd * (16 + 256) + z["nn"] * (16 + 64 + row))
+    return int(2 * z["ns"] * (4 + 32 + J) + offd * (16 + 2 * J) + z["nn"] * (16 + 64 + row))
 
 
 def faces_assemble_bytes(mesh) -> int:
