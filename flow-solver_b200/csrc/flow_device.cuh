@@ -299,11 +299,11 @@ __device__ __forceinline__ double venkat_fold_nz(double ph, double qrec, double 
   return ph <= b ? ph : b;
 }
 
-// The limiter fold of a node kernel: 0 venkat_fold, 1 venkat_fold_nz.
+// The limiter fold of a node kernel: 0 venkat_fold, 1 or 2 venkat_fold_nz.
 template <int LIM>
 __device__ __forceinline__ double venkat_fold_lim(double ph, double qrec, double q0, double qmin,
                                                   double qmax) {
-  if (LIM == 1) return venkat_fold_nz(ph, qrec, q0, qmin, qmax);
+  if (LIM >= 1) return venkat_fold_nz(ph, qrec, q0, qmin, qmax);
   return venkat_fold(ph, qrec, q0, qmin, qmax);
 }
 

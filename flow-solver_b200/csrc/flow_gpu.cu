@@ -381,7 +381,8 @@ constexpr int kVariants = 3;
 // shared memory), where its shared memory fits the mesh; variant 4 =
 // k_node_prepare16 (each node's chains split over 16 lanes); variants 5, 6
 // and 7 = variants 0, 1 and 4 with the limiter fold that divides no zero
-// and by no zero (LIM = 1, venkat_fold_nz).
+// and by no zero (venkat_fold_nz), variant 5 with the wave-speed face terms
+// in the limiter's face loop too (LIM = 2; variants 6 and 7 LIM = 1).
 constexpr int kNodeVariants = 8;
 constexpr size_t kStageSmemMax = 110 * 1024;  // two CTAs per SM at most
 template <class F>
@@ -390,10 +391,11 @@ void launch_variant(int v, F&& f) {
   else if (v == 2) f(std::integral_constant<int, 12>());
   else f(std::integral_constant<int, 0>());
 }
+// node variants 5 and 6: (MINB, LIM) = (0, 2) and (10, 1)
 template <class F>
 void launch_lim_variant(int v, F&& f) {
-  if (v == 6) f(std::integral_constant<int, 10>());
-  else f(std::integral_constant<int, 0>());
+  if (v == 6) f(std::integral_constant<int, 10>(), std::integral_constant<int, 1>());
+  else f(std::integral_constant<int, 0>(), std::integral_constant<int, 2>());
 }
 template <class F>
 void launch_flux_variant(int v, F&& f) {
@@ -435,12 +437,12 @@ int launch_node_prepare(flow_ctx* c, const StepArgs& a) {
   }
   if (c->var[0] >= 5) {
     if (k1)
-      launch_lim_variant(c->var[0], [&](auto W) {
-        k_node_prepare4<1, W.value, 1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+      launch_lim_variant(c->var[0], [&](auto W, auto L) {
+        k_node_prepare4<1, W.value, L.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
       });
     else
-      launch_lim_variant(c->var[0], [&](auto W) {
-        k_node_prepare4<3, W.value, 1><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
+      launch_lim_variant(c->var[0], [&](auto W, auto L) {
+        k_node_prepare4<3, W.value, L.value><<<nb, 128, 0, c->stream>>>(c->m, c->s, a);
       });
     return launch_check(c);
   }
@@ -965,8 +967,8 @@ bool preload_kernels() {
         (const void*)k_node_prepare4<1, 0>, (const void*)k_node_prepare4<1, 10>,
         (const void*)k_node_prepare4<1, 12>, (const void*)k_node_prepare4<3, 0>,
         (const void*)k_node_prepare4<3, 10>, (const void*)k_node_prepare4<3, 12>,
-        (const void*)k_node_prepare4<1, 0, 1>, (const void*)k_node_prepare4<1, 10, 1>,
-        (const void*)k_node_prepare4<3, 0, 1>, (const void*)k_node_prepare4<3, 10, 1>,
+        (const void*)k_node_prepare4<1, 0, 2>, (const void*)k_node_prepare4<1, 10, 1>,
+        (const void*)k_node_prepare4<3, 0, 2>, (const void*)k_node_prepare4<3, 10, 1>,
         (const void*)k_assemble4<true, 0>, (const void*)k_assemble4<false, 0>,
         (const void*)k_assemble4<true, 1>, (const void*)k_assemble4<false, 1>,
         (const void*)k_assemble4<true, 2>, (const void*)k_assemble4<false, 2>,

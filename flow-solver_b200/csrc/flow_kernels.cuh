@@ -124,8 +124,9 @@ __device__ __forceinline__ void cp_async_wait() {
 // formed by every lane of the quad from node constants computed once.
 // MINB: resident blocks per SM the compiler must allow (0: its own choice);
 // the autotuner picks the variant that runs fastest on a given mesh.
-// LIM: the limiter's fold -- 0 venkat_fold, 1 venkat_fold_nz (no division
-// of or by zero); both give the same bits.
+// LIM: 0 venkat_fold; 1 venkat_fold_nz (no division of or by zero); 2 the
+// same, with the wave-speed face terms formed in the limiter's face loop (one
+// walk of the node's faces, more registers).  All give the same bits.
 template <int ORDER, int MINB, int LIM = 0>
 __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState s, StepArgs a) {
   if (*s.stop) return;  // the run has converged
@@ -138,35 +139,51 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   const double q0v = v == 0 ? q4.x : v == 1 ? q4.y : v == 2 ? q4.z : q4.w;
 
   // ---- wave-speed sum (cv_calc.C:819-953): node constants first ----
-  const double rho = q4.x, uu = q4.y / rho, vv = q4.z / rho;
-  const double P = (a.gamma - 1.0) * (q4.w - 0.5 * rho * (uu * uu + vv * vv));
-  const double cs = sqrt((a.gamma * P) / rho);
+  double uu, vv, cs;
+  auto node_consts = [&](const double4& q) {
+    const double rho = q.x;
+    uu = q.y / rho;
+    vv = q.z / rho;
+    const double P = (a.gamma - 1.0) * (q.w - 0.5 * rho * (uu * uu + vv * vv));
+    cs = sqrt((a.gamma * P) / rho);
+  };
   double ev = 0.;
   int bad = 0;
   const int s0 = m.nsub_ptr[n], s1 = m.nsub_ptr[n + 1];
-  #pragma unroll 4
-  for (int k = s0; k < s1; k++) {
-    const double4 g = m.sub_geo[m.nsub[k] >> 1];
+  auto wave_term = [&](const double4& g) {
     const double theta = uu * g.x + vv * g.y;
     const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
     const double w = tpc >= tmc ? tpc : tmc;
     if (!isfinite(w)) bad = 1;
     ev += (w * g.z);
-  }
-  const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
-  for (int k = b0; k < b1; k++) {
-    const double* xn = s.xn_bedges + 3 * m.nbed[k];
-    const double theta = uu * xn[0] + vv * xn[1];
-    const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
-    const double w = tpc >= tmc ? tpc : tmc;
-    if (!isfinite(w)) bad = 1;
-    ev += (w * xn[2]);
-  }
-  if (v == 0) {
-    const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
-    s.dt[n] = dt;
-    if (bad) atomicOr(s.status, ERR_EIGEN);
-    if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
+  };
+  // the boundary edges' terms after the faces', then dt and V/dt
+  auto finish_wave = [&]() {
+    const int b0 = m.nbed_ptr[n], b1 = m.nbed_ptr[n + 1];
+    for (int k = b0; k < b1; k++) {
+      const double* xn = s.xn_bedges + 3 * m.nbed[k];
+      const double theta = uu * xn[0] + vv * xn[1];
+      const double tpc = fabs(theta + cs), tmc = fabs(theta - cs);
+      const double w = tpc >= tmc ? tpc : tmc;
+      if (!isfinite(w)) bad = 1;
+      ev += (w * xn[2]);
+    }
+    if (v == 0) {
+      const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
+      s.dt[n] = dt;
+      if (bad) atomicOr(s.status, ERR_EIGEN);
+      if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
+    }
+  };
+  // LIM 2 with the limiter on: the face terms are summed inside the
+  // limiter's pass over the same faces (the same order), one walk of the
+  // node's incidence list instead of two
+  const bool merged = LIM == 2 && a.do_lim;
+  if (!merged) {
+    node_consts(q4);
+    #pragma unroll 4
+    for (int k = s0; k < s1; k++) wave_term(m.sub_geo[m.nsub[k] >> 1]);
+    finish_wave();
   }
   if (!a.do_grad && !a.do_derivs && !a.do_lim) return;
 
@@ -236,10 +253,14 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
   // ---- Venkatakrishnan bound of variable v over every face point ----
   double ph = 1.0;
   const double xn0 = m.x[2 * n], xn1 = m.x[2 * n + 1];
+  // the node constants formed again here rather than held through the
+  // gradient and stencil loops (the same expressions: the same bits)
+  if (merged) node_consts(reinterpret_cast<const double4*>(s.nQ)[n]);
   #pragma unroll 4
   for (int k = s0; k < s1; k++) {
     const int sd = m.nsub[k];
     const int sub = sd >> 1, side = sd & 1;
+    if (merged) wave_term(m.sub_geo[sub]);
     if (ORDER == 1) {
       const double4 d = m.sub_dx[sub];
       const double dx0 = side ? d.z : d.x, dx1 = side ? d.w : d.y;
@@ -257,6 +278,7 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
       }
     }
   }
+  if (merged) finish_wave();
   // min over the variables in order 0..3 (limiter.C:895-906)
   const double p1 = __shfl_sync(qmask, ph, qbase + 1);
   const double p2 = __shfl_sync(qmask, ph, qbase + 2);

@@ -433,7 +433,9 @@ double flow_last_device_ms(flow_ctx *ctx);
  * 7 are variants 0, 1 and 4 with a limiter that divides no zero and by no
  * zero (a face point whose reconstruction equals the node's value, or whose
  * bound is the node's own value, folds in the value the reference's
- * quotients give there without dividing); every variant gives the same bits.
+ * quotients give there without dividing), variant 5 also forming the
+ * wave-speed face terms in the limiter's walk over the faces; every variant
+ * gives the same bits.
  * flow_autotune times each variant over `steps`
  * pseudo-time steps from step index `ts` (CUDA events, after one warm-up
  * step), keeps the fastest, and puts the solution state back as it was
