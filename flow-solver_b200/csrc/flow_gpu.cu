@@ -203,6 +203,7 @@ struct flow_ctx {
   const int* ring_chunk_sub[kRingShapes][2] = {};
   bool ring_ok[kRingShapes] = {};
   int ring = 0;  // requested shape: sub-levels of ring_rows(ring) rows
+  bool grad_written = false;  // the caller wrote the gradient (flow_set "grad")
   int sweep_df = 0;  // 1: one-launch (dataflow) mode 3 sweeps (flow_set_sweep_dataflow)
   bool has_edge_w = false;  // the grid view carried LSQ edge weights
   bool has_stencils = false;  // order 3: the view carried the k=2 stencils and SVD factors
@@ -714,6 +715,21 @@ int launch_step_args(flow_ctx* c, const flow_params* p, int citer) {
   return launch_check(c);
 }
 
+// What k_begin_step clears at the start of a step (solve.C:298-348: grad and
+// hess <- 0, phi <- 1), less what the step's node kernel then writes for
+// every node: phi when the limiter runs, the k=2 derivatives when they are
+// formed, the gradient when it is formed.  The gradient is cleared on steps
+// that do not form it only where some step of the run, or the caller
+// (flow_set "grad"), writes it; otherwise it keeps the zeros it was created
+// with.
+int begin_flags(const flow_ctx* c, const flow_params* p, const StepArgs& a) {
+  int f = 0;
+  if (!a.do_lim) f |= kBeginResetPhi;
+  if (c->order == 3 && !a.do_derivs) f |= kBeginZeroHess;
+  if (!a.do_grad && (c->order == 1 || p->soits > 0 || c->grad_written)) f |= kBeginZeroGrad;
+  return f;
+}
+
 // One solve() call (solve.C:44-933), device-only.  device_ts: the step index
 // advances on the device (for captured chunks of steps; ts then only selects
 // the order phase, which must be the same for every step of the chunk) and
@@ -725,14 +741,15 @@ int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int f
   c->citer = ts;
   rc |= launch_step_args(c, p, device_ts ? 0 : ts);
   if (device_ts) first = -1;
-  k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 1);
-  rc |= launch_check(c);
   StepArgs a = make_args(p, ts);
+  const int clear = begin_flags(c, p, a);
+  k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, kBeginCopyQ | clear);
+  rc |= launch_check(c);
   for (int mi = 1; mi <= p->iter; mi++) {
     int jac = ((mi - 1) % p->jufreq == 0) || mi == 1;
     if (mi > 1) {
       // phi <- 1 at every Newton iteration (solve.C:344-348)
-      k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 0);
+      k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, clear);
       rc |= launch_check(c);
     }
     rc |= launch_node_prepare(c, a);
@@ -2117,7 +2134,8 @@ int flow_reconstruct(flow_ctx* c, const flow_params* p, int ts) {
   c->citer = ts;
   rc |= launch_step_args(c, p, ts);
   // grad, hess <- 0 and phi <- 1 (solve.C:298-348), keeping the current nQ
-  k_begin_step<<<grid_blocks(c->nn + c->ng, 256), 256, 0, c->stream>>>(c->m, c->s, 1, 0);
+  k_begin_step<<<grid_blocks(c->nn + c->ng, 256), 256, 0, c->stream>>>(
+      c->m, c->s, kBeginResetPhi | kBeginZeroGrad | kBeginZeroHess);
   rc |= launch_check(c);
   rc |= launch_node_prepare(c, a);
   if (rc) return rc;
@@ -2279,7 +2297,15 @@ int flow_set(flow_ctx* c, const char* name, const double* in, long n) {
   else if (nm == "dQ") dst = c->s.dQ;
   else if (nm == "R") dst = c->s.R;
   else if (nm == "RHS") dst = c->s.RHS;
-  else if (nm == "grad") dst = c->s.grad;
+  else if (nm == "grad") {
+    dst = c->s.grad;
+    if (!c->grad_written) {
+      // from now on the steps that do not form a gradient clear it again
+      cudaStreamSynchronize(c->stream);
+      drop_graphs(c);
+      c->grad_written = true;
+    }
+  }
   else if (nm == "phi") dst = c->s.phi;
   else if (nm == "dt") dst = c->s.dt;
   else if (nm == "LHS") dst = c->s.LHS;

@@ -66,27 +66,33 @@ __global__ void k_step_args(DevState s, int citer, int method, int ramp, double 
   s.scalars[3] = cfl;
 }
 
-__global__ void k_begin_step(DevMesh m, DevState s, int reset_phi, int copy_q) {
+// flags: kBeginCopyQ nQ <- Q; kBeginResetPhi phi <- 1; kBeginZeroGrad
+// grad <- 0; kBeginZeroHess the k=2 derivatives <- 0.  The host leaves out
+// what the step's node kernel overwrites for every node anyway.
+constexpr int kBeginCopyQ = 1, kBeginResetPhi = 2, kBeginZeroGrad = 4, kBeginZeroHess = 8;
+__global__ void k_begin_step(DevMesh m, DevState s, int flags) {
   if (*s.stop) return;  // the run has converged
   int total = m.nn + m.ng;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= total;
        i += gridDim.x * blockDim.x) {
-    if (copy_q) {
+    if (flags & kBeginCopyQ) {
       const double4* q = reinterpret_cast<const double4*>(s.Q) + i;
       reinterpret_cast<double4*>(s.nQ)[i] = *q;
     }
     if (i <= m.nn) {
       double4 z = make_double4(0., 0., 0., 0.);
-      double4* g = reinterpret_cast<double4*>(s.grad) + 2 * i;
-      g[0] = z;
-      g[1] = z;
-      if (m.order == 3) {
+      if (flags & kBeginZeroGrad) {
+        double4* g = reinterpret_cast<double4*>(s.grad) + 2 * i;
+        g[0] = z;
+        g[1] = z;
+      }
+      if (m.order == 3 && (flags & kBeginZeroHess)) {
         // 20 doubles a node, 32-byte aligned: five vector stores
         double4* h = reinterpret_cast<double4*>(s.hess5 + 20 * (long)i);
 #pragma unroll
         for (int k = 0; k < 5; k++) h[k] = z;
       }
-      if (reset_phi) {
+      if (flags & kBeginResetPhi) {
         double4 o = make_double4(1., 1., 1., 1.);
         double4* p = reinterpret_cast<double4*>(s.phi) + 2 * i;
         p[0] = o;
