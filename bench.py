@@ -72,7 +72,9 @@ REF_SAMPLE_STEPS = 2        # pseudo-time steps per reference-arm bench step
 BENCH_BUDGET_S = 1500.      # wall-clock target of a whole batch run (warm-up and checks included)
 SERVE_RATES = (0.5, 2.0)    # requests/s of the serving measurement in the batch run
 SERVE_REQUESTS = 16
-SERVE_STALL = 1200           # stall retirement window of the serving runs (as batch64's)
+# stall retirement of the serving runs (as batch64's): no halving of the best
+# residual within max(160, 1.4 sqrt(nodes)) steps
+SERVE_STALL, SERVE_STALL_DROP, SERVE_STALL_PER_SQRT = 160, 2.0, 1.4
 SERVE_MIN_LEFT_S = 200.     # run the serving measurement only with this much time left
 REF_ARM_TIMEOUT_S = 900     # bound on the reference arm's whole sample
 STAGE_THREADS = max(1, min(8, os.cpu_count() or 1))  # concurrent admissions per batch pass
@@ -363,7 +365,8 @@ def run_batch(args, bw):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n, autotune=bw.autotune,
                           stall=bw.stall, priority_policy=bw.priority_policy,
-                          jacobian=bw.jacobian)
+                          jacobian=bw.jacobian, stall_drop=bw.stall_drop,
+                          stall_per_sqrt=bw.stall_per_sqrt)
         torch.cuda.synchronize()
         ev[0].record()
         # context + mesh arrays + state to the device, several requests at a
@@ -403,7 +406,8 @@ def run_batch(args, bw):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
         srv = capi.Server(arena, chunk=bw.chunk, max_slots=bw.n, autotune=bw.autotune,
                           stall=bw.stall, priority_policy=bw.priority_policy,
-                          jacobian=bw.jacobian)
+                          jacobian=bw.jacobian, stall_drop=bw.stall_drop,
+                          stall_per_sqrt=bw.stall_per_sqrt)
         torch.cuda.synchronize()
         ev[0].record()
         recs = {}
@@ -670,7 +674,9 @@ def run_batch(args, bw):
                                         "coloured chunks of the reference order"}.get(
                                             bw.precision, f"mode {bw.precision}"),
                        "gs_sweeps": bw.subits, "drop": bw.drop, "max_steps": bw.max_steps,
-                       "stall_retire_steps": bw.stall, "autotune_steps": bw.autotune,
+                       "stall_retire": {"drop": bw.stall_drop, "min_steps": bw.stall,
+                                        "steps_per_sqrt_node": bw.stall_per_sqrt},
+                       "autotune_steps": bw.autotune,
                        "priority_policy": bw.priority_policy,
                        "converged_per_pass": n_conv // max(args.steps, 1),
                        "stalled_per_pass": n_stall // max(args.steps, 1),
@@ -1039,7 +1045,8 @@ def serving_run(rate: float, n: int, arena, budget: int, jacobian: int = 0,
             for i in range(n)]
     r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
                           precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
-                          stall=SERVE_STALL, ramp_sweeps=2, jacobian=jacobian)
+                          stall=SERVE_STALL, ramp_sweeps=2, jacobian=jacobian,
+                          stall_drop=SERVE_STALL_DROP, stall_per_sqrt=SERVE_STALL_PER_SQRT)
     recs = r["records"]
     conv = [x for x in recs if x.get("status") == 0]
     return {"value": round(len(conv) / r["span_s"], 5), "unit": UNIT,
@@ -1056,7 +1063,7 @@ def serving_run(rate: float, n: int, arena, budget: int, jacobian: int = 0,
             "status": [x.get("status") for x in recs],
             "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
                        "jacobian": jacobian, "ramp_sweeps_on_meshes_from_250k_nodes": 2,
-                       "stall_retire_steps": SERVE_STALL, "arena_bytes": budget, "stream_seed": 1,
+                       "stall_retire": {"drop": SERVE_STALL_DROP, "min_steps": SERVE_STALL, "steps_per_sqrt_node": SERVE_STALL_PER_SQRT}, "arena_bytes": budget, "stream_seed": 1,
                        "first_request": index0, "nodes_range": [4000, 500000]}}
 
 
@@ -1074,7 +1081,8 @@ def run_serve(args):
         r = serve.run_poisson(reqs, rate, arena, subits=4, max_steps=8000, drop=1e-8,
                               precision=3, chunk=32, max_slots=64, seed=1, autotune=4,
                               stall=SERVE_STALL, ramp_sweeps=2,
-                              jacobian=workloads.BATCHES[workloads.DEFAULT_BENCH].jacobian)
+                              jacobian=workloads.BATCHES[workloads.DEFAULT_BENCH].jacobian,
+                              stall_drop=SERVE_STALL_DROP, stall_per_sqrt=SERVE_STALL_PER_SQRT)
     arena.close()
     recs = r["records"]
     conv = [x for x in recs if x.get("status") == 0]
@@ -1093,7 +1101,7 @@ def run_serve(args):
             "status": [x.get("status") for x in recs],
             "config": {"drop": 1e-8, "max_steps": 8000, "precision": 3, "gs_sweeps": 4,
                        "ramp_sweeps_on_meshes_from_250k_nodes": 2,
-                       "stall_retire_steps": SERVE_STALL, "arena_bytes": budget, "stream_seed": 1,
+                       "stall_retire": {"drop": SERVE_STALL_DROP, "min_steps": SERVE_STALL, "steps_per_sqrt_node": SERVE_STALL_PER_SQRT}, "arena_bytes": budget, "stream_seed": 1,
                        "nodes_range": [4000, 500000]},
             "clocks": clk.summary()}
     print(json.dumps(line), flush=True)

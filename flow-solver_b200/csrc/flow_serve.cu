@@ -60,8 +60,9 @@ struct Slot {
   int oldest_flag = 0; // flag slot of the oldest chunk in flight
   int status = 0, steps = 0;
   double r_first = 0., r_last = 0., ms = 0.;
-  double best = 1.;     // best ||R_rho|| relative to the first step, kept by factors of 10
-  int best_step = 0;    // step at which it last improved tenfold
+  double best = 1.;     // best ||R_rho|| relative to the first step, kept by the stall factor
+  int best_step = 0;    // step at which it last improved by that factor
+  int stall_window = 0; // steps without such an improvement that retire it (0: never)
   int chunk_first[2] = {0, 0};  // first step of the chunk posting each flag slot
   int recoverable = 0;  // approximate face Jacobians with chunk checkpoints kept
   int recovered_at = 0; // step it went back to with the forward-difference Jacobians
@@ -76,7 +77,9 @@ struct flow_server {
   std::vector<Slot> slots;
   int running = 0;
   int autotune_steps = 0;  // 0: no autotuning at admission
-  int stall_steps = 0;     // 0: no stall retirement
+  int stall_steps = 0;     // 0: no stall retirement; else the window (its minimum with a rule)
+  double stall_drop = 10.;       // the improvement the best residual must make within the window
+  double stall_per_sqrt = 0.;    // window steps per square root of the mesh's nodes (0: fixed)
   int sched_sweeps = 0, sched_until = 0;  // sweep schedule of precision-form solves
   long sched_min_nodes = 0;               // ... on meshes of at least this many nodes
   int priority_policy = 0;                // 1: larger meshes get greater stream priority
@@ -184,7 +187,8 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   }
   int idx = -1;
   int autotune_steps = 0, sched_sweeps = 0, sched_until = 0, priority_policy = 0, jacobian = 0;
-  int recovery = 0;
+  int recovery = 0, stall_steps = 0;
+  double stall_per_sqrt = 0.;
   long sched_min_nodes = 0;
   {
     std::lock_guard<std::mutex> lock(sv->mu);
@@ -202,6 +206,8 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     priority_policy = sv->priority_policy;
     jacobian = sv->jacobian;
     recovery = sv->recovery;
+    stall_steps = sv->stall_steps;
+    stall_per_sqrt = sv->stall_per_sqrt;
   }
   auto unreserve = [&]() {
     std::lock_guard<std::mutex> lock(sv->mu);
@@ -282,6 +288,16 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
     unreserve();
     return rc;
   }
+  // the stall window of this solve: the fixed window, or the rule's
+  // steps per square root of the mesh's nodes (at least the fixed window),
+  // rounded up to whole chunks
+  int stall_window = stall_steps;
+  if (stall_steps > 0 && stall_per_sqrt > 0.) {
+    const double nn = (double)(flow_size(c, "dt") - 1);
+    const int chunk = sv->chunk;
+    const int w = (int)std::ceil(stall_per_sqrt * std::sqrt(std::max(nn, 1.)) / chunk) * chunk;
+    stall_window = std::max(stall_steps, w);
+  }
   std::lock_guard<std::mutex> lock(sv->mu);
   Slot& sl = sv->slots[idx];
   sl = Slot();
@@ -291,6 +307,7 @@ int flow_server_stage(flow_server* sv, const flow_grid_view* g, const flow_param
   sl.max_steps = max_steps;
   sl.tag = tag;
   sl.recoverable = recoverable;
+  sl.stall_window = stall_window;
   sl.state = 3;  // staged: inputs on the device, nothing launched
   if (slot_out) *slot_out = idx;
   if (hold) return 0;
@@ -354,12 +371,13 @@ int flow_server_progress(flow_server* sv, int wait_us, flow_completion* out, int
         if (!rc) continue;  // running again from the failed chunk's first step
         status |= rc;
       }
-      // stall: no tenfold drop of the best residual within stall_steps steps
-      if (rr < sl.best * 0.1) {
+      // stall: the best residual has not dropped by the stall factor within
+      // the solve's window
+      if (rr < sl.best / sv->stall_drop) {
         sl.best = rr;
         sl.best_step = steps;
       }
-      if (!stop && !status && sv->stall_steps > 0 && steps - sl.best_step >= sv->stall_steps)
+      if (!stop && !status && sl.stall_window > 0 && steps - sl.best_step >= sl.stall_window)
         status = FLOW_ERR_STALLED;
       bool done = stop || status || (sl.issued >= sl.max_steps && sl.inflight == 0);
       if (done) {
@@ -460,6 +478,14 @@ int flow_server_set_priority_policy(flow_server* sv, int policy) {
   if (!sv || policy < 0 || policy > 1) return FLOW_ERR_ARG;
   std::lock_guard<std::mutex> lock(sv->mu);
   sv->priority_policy = policy;
+  return 0;
+}
+
+int flow_server_set_stall_rule(flow_server* sv, double drop, double steps_per_sqrt_node) {
+  if (!sv || !(drop > 1.) || !(steps_per_sqrt_node >= 0.)) return FLOW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(sv->mu);
+  sv->stall_drop = drop;
+  sv->stall_per_sqrt = steps_per_sqrt_node;
   return 0;
 }
 

@@ -53,7 +53,7 @@ SYMBOLS = ("flow_create", "flow_destroy", "flow_set_state", "flow_solve", "flow_
            "flow_server_set_autotune", "flow_server_set_stall",
            "flow_server_set_sweep_schedule", "flow_set_stream_priority",
            "flow_server_set_priority_policy", "flow_server_set_jacobian",
-           "flow_server_set_recovery",
+           "flow_server_set_recovery", "flow_server_set_stall_rule",
            "flow_selftest_sweep_timeout")
 
 
@@ -200,6 +200,7 @@ def _load_locked():
     L.flow_server_set_priority_policy.argtypes = [vp, C.c_int]
     L.flow_server_set_jacobian.argtypes = [vp, C.c_int]
     L.flow_server_set_recovery.argtypes = [vp, C.c_int]
+    L.flow_server_set_stall_rule.argtypes = [vp, C.c_double, C.c_double]
     L.flow_selftest_sweep_timeout.argtypes = [vp, C.c_long, IP]
     # host preprocessing (include/flow_prep.h)
     L.flow_prep_read.restype = vp
@@ -272,7 +273,8 @@ class Server:
 
     def __init__(self, arena: Arena, chunk: int = 32, max_slots: int = 64, autotune: int = 0,
                  stall: int = 0, ramp_sweeps: int = 0, ramp_min_nodes: int = 250000,
-                 priority_policy: int = 0, jacobian: int = 0, recovery: bool = True):
+                 priority_policy: int = 0, jacobian: int = 0, recovery: bool = True,
+                 stall_drop: float = 10., stall_per_sqrt: float = 0.):
         self.L = load()
         st = C.c_int(0)
         self.arena = arena
@@ -293,6 +295,9 @@ class Server:
             _check(self.L.flow_server_set_jacobian(self.h, int(jacobian)), "jacobian")
         if not recovery:
             _check(self.L.flow_server_set_recovery(self.h, 0), "recovery")
+        if stall_drop != 10. or stall_per_sqrt:
+            _check(self.L.flow_server_set_stall_rule(self.h, float(stall_drop),
+                                                     float(stall_per_sqrt)), "stall rule")
         self._keep = {}
         self._out = (FlowCompletion * 64)()
 

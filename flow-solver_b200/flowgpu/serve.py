@@ -148,7 +148,8 @@ def run_sequential(prepared, precision: int = 0, chunk: int = 64, device: int = 
 def run_poisson(reqs, rate_per_s: float, arena: capi.Arena, subits: int, max_steps: int,
                 drop: float, precision: int = 1, chunk: int = 32, max_slots: int = 64,
                 seed: int = 0, prep_threads: int = 8, autotune: int = 0,
-                stall: int = 0, ramp_sweeps: int = 0, jacobian: int = 0) -> dict:
+                stall: int = 0, ramp_sweeps: int = 0, jacobian: int = 0,
+                stall_drop: float = 10., stall_per_sqrt: float = 0.) -> dict:
     """Open-loop Poisson arrivals at `rate_per_s`: each request is prepared
     on arrival by a worker thread, which then admits it (stages its context
     on the device and starts it) as soon as the arena has room; the main
@@ -159,7 +160,8 @@ def run_poisson(reqs, rate_per_s: float, arena: capi.Arena, subits: int, max_ste
     arrivals = np.cumsum(gaps) - gaps[0]
     capi.load()
     srv = capi.Server(arena, chunk=chunk, max_slots=max_slots, autotune=autotune, stall=stall,
-                      ramp_sweeps=ramp_sweeps, jacobian=jacobian)
+                      ramp_sweeps=ramp_sweeps, jacobian=jacobian, stall_drop=stall_drop,
+                      stall_per_sqrt=stall_per_sqrt)
     recs = [dict() for _ in reqs]
     lock = threading.Lock()
     room = threading.Condition(lock)  # signalled whenever a solve is released

@@ -103,11 +103,14 @@ class BatchWorkload:
     max_steps, other values failed (a non-physical state).  Measured with
     ``bench.py --measure-fp64``.
 
-    ``stall``: the server retires a solve whose best ||R_rho|| has not
-    dropped tenfold for this many steps (on batch64's requests served in
-    precision mode 3 with 4 sweeps and the approximate face Jacobians, the
-    longest run without a tenfold drop before convergence is 736 steps, on
-    the 147,456-node request 46; the window is 1.6 times that);
+    ``stall``, ``stall_drop``, ``stall_per_sqrt``: the server retires a solve
+    whose best ||R_rho|| has not dropped by the factor ``stall_drop`` within
+    max(``stall``, ``stall_per_sqrt`` * sqrt(nodes)) steps.  On batch64's
+    requests served in precision mode 3 with 4 sweeps and the approximate
+    face Jacobians, the longest run without a halving before convergence
+    grows with the mesh (32 steps at 2k nodes, 128 at 41k, 320 at 181k: at
+    most 0.75 sqrt(nodes)); the window max(160, 1.4 sqrt(nodes)) is at least
+    1.9 times each converging solve's longest such run;
     ``autotune``: steps per kernel variant timed at admission."""
     name: str
     seed: int
@@ -120,6 +123,8 @@ class BatchWorkload:
     fp64_steps: tuple | None = None
     fp64_status: tuple | None = None
     stall: int = 0
+    stall_drop: float = 10.
+    stall_per_sqrt: float = 0.
     autotune: int = 0
     fp64_forces: tuple | None = None  # raw lift/drag of the FP64 drop-in per request
     priority_policy: int = 0          # 1: larger meshes on higher-priority streams
@@ -131,7 +136,7 @@ class BatchWorkload:
 BATCHES = {
     # the batching form as specified: 64 independent solves in one arena
     # (requests 0..63 of stream 0 on rank 0, the next 64 on rank 1, ...)
-    "batch64": BatchWorkload("batch64", 0, 64, 8000, 1e-10, 3, 4, stall=1200, autotune=4,
+    "batch64": BatchWorkload("batch64", 0, 64, 8000, 1e-10, 3, 4, stall=160, stall_drop=2., stall_per_sqrt=1.4, autotune=4,
                              priority_policy=1, jacobian=2,
                              fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065, 1395, 1487, 8000, 3827, 1262, 8000, 415, 3035, 64, 8000, 1475, 810, 8000, 7340, 3346, 64, 278, 536, 8000, 64, 1087, 2309, 415, 2513, 930, 8000, 8000, 8000, 64, 8000, 64, 3705, 8000, 6900, 1978, 5921, 8000, 4285, 1743, 1794, 8000, 3477, 8000, 2040, 64, 1585, 64, 64, 912, 8000, 2687),
                              fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256, 0, 0, 256, 0, 0, 44, 256, 0, 0, 256, 0, 0, 44, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256, 256, 256, 44, 256, 44, 0, 256, 0, 0, 0, 256, 0, 0, 0, 256, 0, 256, 0, 44, 0, 44, 44, 0, 256, 0),
@@ -140,7 +145,7 @@ BATCHES = {
                              fp64_forces=(None, None, (-0.025777386029756044, -0.0054055864833447076), None, (-0.0010171575037174392, -0.001240139392816858), None, (-0.027248649454864958, -0.003062564172084038), (-0.12773519262622307, -0.018852769853473013), None, None, (-0.018041588523432805, -0.002214218243070119), (0.002168299510290521, -0.0016691959198755204), (0.028612422320067932, -0.005656445411432563), (-0.0017219682626121772, -0.0013359229295129356), (-0.03246397561528733, -0.0029672357554528374), None, (-0.07621782393542069, -0.0048012799301380355), (-0.20986626352195453, -0.028688895204014832), None, (0.04666059516157848, -0.008005804230765284), (0.019087319252602365, -0.001482639953373573), None, None, (0.039936872659750385, -0.0038141957773608157), (0.0003257405055705526, -0.001822215172047123), None, (-0.19177442021253613, -0.01723684073456574), (0.0432973120624181, -0.00339450845774449), None, (0.03188269948663082, -0.007280141883886639), (0.018382161826746297, -0.0106550912117282), None, None, (-0.024456547136083084, -0.005018145472129145), (0.010818981126226179, -0.002387014107041504), (-0.04440898199151, -0.0075415065311262445), (0.0655803205867983, -0.004950069442132337), (-0.0023400526814139192, -0.001771997899719281), None, None, None, None, None, None, (-0.02007443256463631, -0.0037642781088572694), None, (-0.06933146954849441, -0.0035062312826888565), (-0.08868317689152848, -0.007610661826188901), (0.04559064820540709, -0.0026394350417630777), None, (-0.17617304809434906, -0.016650205797371188), (-0.026475309051357494, -0.008758498911407755), (0.004735135354381516, -0.0016012204784226426), None, (0.02617089666340069, -0.001790390307587515), None, (0.07619508554929875, -0.005998724380028264), None, (0.0537048432982277, -0.005541582009699136), None, None, (-0.0355744365642943, -0.005129144991253361), None, (0.19662866543828933, -0.02542728332062686))),
     # its first 16 requests: a quarter of the work, for quick runs
     "batch16": BatchWorkload(
-        "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=1200, autotune=4, priority_policy=1,
+        "batch16", 0, 16, 8000, 1e-10, 3, 4, stall=160, stall_drop=2., stall_per_sqrt=1.4, autotune=4, priority_policy=1,
         fp64_steps=(8000, 8000, 324, 8000, 4441, 8000, 921, 392, 8000, 64, 1249, 1148, 1065,
                     1395, 1487, 8000),
         fp64_status=(256, 256, 0, 256, 0, 256, 0, 0, 256, 44, 0, 0, 0, 0, 0, 256),

@@ -544,6 +544,14 @@ int flow_server_set_autotune(flow_server *srv, int steps);
  * limit cycle or a stalled solve that will not reach its drop.  0 (default)
  * turns it off: solves then run to their drop or max_steps. */
 int flow_server_set_stall(flow_server *srv, int steps);
+/* The stall test of later admissions (no reference counterpart): retire a
+ * solve whose best ||R_rho|| has not dropped by the factor `drop` (> 1;
+ * default 10) within its window; with steps_per_sqrt_node > 0 the window of
+ * a mesh of n nodes is max(steps, steps_per_sqrt_node * sqrt(n)) rounded up
+ * to whole chunks (the gaps between a converging solve's improvements grow
+ * with the mesh), with 0 (the default) the fixed `steps` of
+ * flow_server_set_stall. */
+int flow_server_set_stall_rule(flow_server *srv, double drop, double steps_per_sqrt_node);
 /* Priority policy for later admissions: 0 (default) one priority for all;
  * 1 the larger the mesh, the greater its stream priority (the longest solves
  * of a batch keep the GPU first, the small ones fill the gaps). */

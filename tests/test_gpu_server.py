@@ -89,10 +89,13 @@ def test_admission_waits_for_arena_room():
     arena.close()
 
 
-def test_stalled_solves_are_retired_and_converging_ones_are_not():
+@pytest.mark.parametrize("rule", [None, (2.0, 1.4)])
+def test_stalled_solves_are_retired_and_converging_ones_are_not(rule):
     """A k=1 solve caught in the limiter's limit cycle is retired as stalled
     long before its step limit; a converging solve served next to it takes
-    exactly the steps it takes alone."""
+    exactly the steps it takes alone: with the fixed window (a tenfold drop
+    within 600 steps) and with the size-scaled rule (a halving within
+    max(160, 1.4 sqrt(nodes)) steps)."""
     from flowgpu import capi
     (wl1, m1) = _case(64, 16, False, 1, 0.5, 1.25, 2)
     (wl2, m2) = _case(32, 8, True, 3, 0.8, 1.25, 4)
@@ -104,7 +107,11 @@ def test_stalled_solves_are_retired_and_converging_ones_are_not():
     alone.close()
     assert r1 < 1e-10 * r0
     arena = capi.Arena(1 << 30)
-    srv = capi.Server(arena, chunk=16, max_slots=4, stall=600)
+    if rule is None:
+        srv = capi.Server(arena, chunk=16, max_slots=4, stall=600)
+    else:
+        srv = capi.Server(arena, chunk=16, max_slots=4, stall=160, stall_drop=rule[0],
+                          stall_per_sqrt=rule[1])
     fp1 = wl1.params()
     srv.submit(m1, fp1, m1.initial_state(fp1), precision=3, max_steps=3000, tag=1)
     srv.submit(m2, fp2, m2.initial_state(fp2), precision=3, max_steps=3000, tag=2)
