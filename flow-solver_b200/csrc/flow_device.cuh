@@ -245,6 +245,44 @@ __device__ __forceinline__ void euler_jacobian(const double* q, double nx, doubl
   d[15] = gamma * th;
 }
 
+// euler_jacobian one row at a time: the state's scalars once, then row r's
+// four entries by the same expressions (the same bits as d[4r .. 4r+3]).
+struct EulerJacSide {
+  double u, v, th, ph, ger;
+};
+__device__ __forceinline__ EulerJacSide euler_jacobian_side(const double* q, double nx,
+                                                            double ny, double gamma) {
+  EulerJacSide S;
+  const double rho = q[0];
+  S.u = q[1] / q[0];
+  S.v = q[2] / q[0];
+  S.th = S.u * nx + S.v * ny;
+  S.ph = 0.5 * (gamma - 1.) * (S.u * S.u + S.v * S.v);
+  S.ger = gamma * q[3] / rho;
+  return S;
+}
+__device__ __forceinline__ void euler_jacobian_row(const EulerJacSide& S, double nx, double ny,
+                                                   double gamma, int r, double* d) {
+  if (r == 0) {
+    d[0] = 0.; d[1] = nx; d[2] = ny; d[3] = 0.;
+  } else if (r == 1) {
+    d[0] = S.ph * nx - S.u * S.th;
+    d[1] = (2. - gamma) * S.u * nx + S.th;
+    d[2] = S.u * ny - (gamma - 1.) * S.v * nx;
+    d[3] = (gamma - 1.) * nx;
+  } else if (r == 2) {
+    d[0] = S.ph * ny - S.v * S.th;
+    d[1] = S.v * nx - (gamma - 1.) * S.u * ny;
+    d[2] = S.th + (2. - gamma) * S.v * ny;
+    d[3] = (gamma - 1.) * ny;
+  } else {
+    d[0] = (2. * S.ph - S.ger) * S.th;
+    d[1] = (1. - gamma) * S.u * S.th + nx * (S.ger - S.ph);
+    d[2] = (1. - gamma) * S.v * S.th + ny * (S.ger - S.ph);
+    d[3] = gamma * S.th;
+  }
+}
+
 // cv_calc.C:840-866: max(|theta+c|, |theta-c|) for one node state.
 __device__ __forceinline__ double max_wave(const double* q, double nx, double ny, double gamma) {
   double rho = q[0];

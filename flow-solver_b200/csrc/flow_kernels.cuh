@@ -1118,18 +1118,34 @@ __global__ void __launch_bounds__(128, MINB) k_subedge_flux(DevMesh m, DevState 
   face_states<RECON>(m, s, sub, lr, qL, qR);
   double flux[4];
   if (JAC && JMODE == 1) {
-    double JL[16], JR[16];
-    face_flux_approx(g, a.gamma, qL, qR, flux, JL, JR);
+    // face_flux_approx's arithmetic with the physical Jacobians formed and
+    // stored a row at a time (fewer values live at once; the same bits)
+    const double ogm1 = 1.0 / (a.gamma - 1.0);
+    RoeSide SL, SR;
+    roe_side(qL, g.x, g.y, g.z, a.gamma, SL);
+    roe_side(qR, g.x, g.y, g.z, a.gamma, SR);
+    const double bg = roe_weight(SL.rho, SR.rho);
+    double Rm[16];
+    roe_core(g.x, g.y, g.z, a.gamma, ogm1, qL, qR, SL, SR, bg, flux, Rm);
     reinterpret_cast<double4*>(s.F)[sub] = make_double4(flux[0], flux[1], flux[2], flux[3]);
+    const EulerJacSide EL = euler_jacobian_side(qL, g.x, g.y, a.gamma);
+    const EulerJacSide ER = euler_jacobian_side(qR, g.x, g.y, a.gamma);
     // FP32-valued entries stored as FP32 (16 floats a face and side)
     float4* JLo = reinterpret_cast<float4*>(s.JL) + 4 * (long)sub;
     float4* JRo = reinterpret_cast<float4*>(s.JR) + 4 * (long)sub;
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-      JLo[r] = make_float4((float)JL[4 * r], (float)JL[4 * r + 1], (float)JL[4 * r + 2],
-                           (float)JL[4 * r + 3]);
-      JRo[r] = make_float4((float)JR[4 * r], (float)JR[4 * r + 1], (float)JR[4 * r + 2],
-                           (float)JR[4 * r + 3]);
+      double dl[4], dr[4];
+      euler_jacobian_row(EL, g.x, g.y, a.gamma, r, dl);
+      euler_jacobian_row(ER, g.x, g.y, a.gamma, r, dr);
+      float jl[4], jr[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        jl[k] = __double2float_rn(0.5 * (dl[k] + Rm[4 * r + k]) * g.z);
+        jr[k] = __double2float_rn(0.5 * (dr[k] - Rm[4 * r + k]) * g.z);
+      }
+      JLo[r] = make_float4(jl[0], jl[1], jl[2], jl[3]);
+      JRo[r] = make_float4(jr[0], jr[1], jr[2], jr[3]);
     }
     return;
   }
