@@ -2,6 +2,7 @@
 proper colouring of the block pattern, and the multicolour FP32 solve drives
 the nonlinear residual down like the FP64 one."""
 import numpy as np
+import pytest
 
 
 def _grid(nc, nr, curved, order):
@@ -33,8 +34,12 @@ def test_greedy_colouring_is_proper():
         assert col[j] == min(set(range(nc + 1)) - earlier)
 
 
-def test_mixed_solve_reduces_the_residual():
+@pytest.mark.parametrize("approx", [0, 1])
+def test_mixed_solve_reduces_the_residual(approx):
+    """With the forward-difference face Jacobians and with the approximate
+    Roe ones rounded to FP32 (jac_approx)."""
     mesh, og, p = _grid(32, 8, True, 3)
+    p.jac_approx = approx
     nn = mesh.sizes["nn"]
     norms = []
     for ts in range(1, 41):
