@@ -739,11 +739,14 @@ int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int f
   int rc = 0;
   int total = c->nn + c->ng;
   c->citer = ts;
-  rc |= launch_step_args(c, p, device_ts ? 0 : ts);
   if (device_ts) first = -1;
   StepArgs a = make_args(p, ts);
   const int clear = begin_flags(c, p, a);
-  k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(c->m, c->s, kBeginCopyQ | clear);
+  // the step index and CFL (k_step_args) by the first thread of the step's
+  // first kernel
+  k_begin_step<<<grid_blocks(total, 256), 256, 0, c->stream>>>(
+      c->m, c->s, kBeginCopyQ | kBeginStepArgs | clear, device_ts ? 0 : ts, p->method, p->ramp,
+      p->CFL);
   rc |= launch_check(c);
   for (int mi = 1; mi <= p->iter; mi++) {
     int jac = ((mi - 1) % p->jufreq == 0) || mi == 1;
@@ -757,11 +760,9 @@ int enqueue_step(flow_ctx* c, const flow_params* p, int ts, int hist_slot, int f
     flow_params pe = *p;  // the sweep schedule may lower the sweep count early on
     pe.subits = sweeps_at(c, p, ts);
     rc |= launch_linear_solve(c, &pe, false);
-    k_finish_step<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->m, c->s, mi == p->iter);
-    rc |= launch_check(c);
-    bool last = mi == p->iter;
-    k_finalize_step<<<1, kRedThreads, 0, c->stream>>>(
-        c->s, last && hist_slot >= 0 ? c->d_hist : nullptr,
+    const bool last = mi == p->iter;
+    k_finish_step<<<kRedBlocks, kRedThreads, 0, c->stream>>>(
+        c->m, c->s, last, last && hist_slot >= 0 ? c->d_hist : nullptr,
         last && hist_slot >= 0 ? c->d_hist + c->hist_cap : nullptr, hist_slot < 0 ? 0 : hist_slot,
         last ? (first < 0 ? -1 : first) : 0);
     rc |= launch_check(c);
@@ -1014,7 +1015,7 @@ bool preload_kernels() {
         (const void*)k_fill_sweep_records, (const void*)k_prepare_sweep,
         (const void*)k_lin_residual, (const void*)k_finalize_rms, (const void*)k_exact_rms,
         (const void*)k_finish_step,
-        (const void*)k_finalize_step, (const void*)k_body_forces,
+        (const void*)k_body_forces,
         (const void*)k_body_forces_sum})
     ok = ok && cudaFuncGetAttributes(&fa, f) == cudaSuccess;
   return ok;
@@ -1656,7 +1657,8 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   s.stop = c->buf.alloc<int>(1);
   s.steps_done = c->buf.alloc<int>(1);
   s.citer = c->buf.alloc<int>(1);
-  s.partial = c->buf.alloc<double>(2 * kRedBlocks);
+  // the partial sums of the step's reductions, then k_finish_step's block count
+  s.partial = c->buf.alloc<double>(2 * kRedBlocks + 2);
   s.scalars = c->buf.alloc<double>(8);
   if (!s.Q || !s.nQ || !s.pQ || !s.dQ || !s.dQ2 || !s.R || !s.RHS || !s.grad || !s.phi || !s.hess5 ||
       !s.pv || !s.dt || !s.LHS || !s.LUd || !s.xn_bedges || !s.F || !s.JL || !s.JR || !s.Fb ||
@@ -1688,6 +1690,7 @@ static flow_ctx* create_impl(flow_arena* arena, const flow_grid_view* g, const f
   zero(s.steps_done, 4);
   zero(s.citer, 4);
   zero(s.scalars, 64);
+  zero(s.partial, (2 * kRedBlocks + 2) * 8);
   if (!zero_ok) return fail(c, FLOW_ERR_CUDA, "clearing the device state failed");
   std::vector<double> xnb((size_t)(nbe + 1) * 3, 0.);
   std::copy(g->xn_bedges, g->xn_bedges + xnb.size(), xnb.begin());

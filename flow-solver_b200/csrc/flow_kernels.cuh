@@ -52,8 +52,8 @@ struct StepArgs {
 // Step index and CFL of the step about to run (init_memory.C:200-216).
 // citer > 0 sets the index; citer == 0 takes the one after the previous step,
 // which lets a captured sequence of steps replay with an advancing ramp.
-__global__ void k_step_args(DevState s, int citer, int method, int ramp, double CFL) {
-  if (*s.stop) return;  // the run has converged
+__device__ __forceinline__ void step_args_body(DevState& s, int citer, int method, int ramp,
+                                               double CFL) {
   const int ci = citer > 0 ? citer : *s.citer + 1;
   *s.citer = ci;
   double cfl;
@@ -65,13 +65,23 @@ __global__ void k_step_args(DevState s, int citer, int method, int ramp, double 
     cfl = CFL;
   s.scalars[3] = cfl;
 }
+__global__ void k_step_args(DevState s, int citer, int method, int ramp, double CFL) {
+  if (*s.stop) return;  // the run has converged
+  step_args_body(s, citer, method, ramp, CFL);
+}
 
 // flags: kBeginCopyQ nQ <- Q; kBeginResetPhi phi <- 1; kBeginZeroGrad
-// grad <- 0; kBeginZeroHess the k=2 derivatives <- 0.  The host leaves out
-// what the step's node kernel overwrites for every node anyway.
-constexpr int kBeginCopyQ = 1, kBeginResetPhi = 2, kBeginZeroGrad = 4, kBeginZeroHess = 8;
-__global__ void k_begin_step(DevMesh m, DevState s, int flags) {
+// grad <- 0; kBeginZeroHess the k=2 derivatives <- 0; kBeginStepArgs the
+// step index and CFL (k_step_args, by one thread; nothing else in this
+// kernel reads them).  The host leaves out what the step's node kernel
+// overwrites for every node anyway.
+constexpr int kBeginCopyQ = 1, kBeginResetPhi = 2, kBeginZeroGrad = 4, kBeginZeroHess = 8,
+              kBeginStepArgs = 16;
+__global__ void k_begin_step(DevMesh m, DevState s, int flags, int citer = 0, int method = 0,
+                             int ramp = 0, double CFL = 0.) {
   if (*s.stop) return;  // the run has converged
+  if ((flags & kBeginStepArgs) && blockIdx.x == 0 && threadIdx.x == 0)
+    step_args_body(s, citer, method, ramp, CFL);
   int total = m.nn + m.ng;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= total;
        i += gridDim.x * blockDim.x) {
@@ -2039,11 +2049,43 @@ __global__ void __launch_bounds__(256) k_exact_rms(DevMesh m, DevState s) {
   }
 }
 
+// The step's norms from the per-block partial sums (summed in block order,
+// the same bits whatever block forms them), the history, the run's first
+// residual, the step count and the stop flag.
+__device__ __forceinline__ void finalize_step_body(DevState& s, double* sh, double* hist_dq,
+                                                   double* hist_r, int slot, int first) {
+  double a = 0., b = 0.;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) {
+    a += __ldcg(s.partial + i);
+    b += __ldcg(s.partial + kRedBlocks + i);
+  }
+  double ta = block_sum(a, sh);
+  double tb = block_sum(b, sh);
+  if (threadIdx.x == 0) {
+    s.scalars[1] = ta;
+    s.scalars[2] = tb;
+    double r = sqrt(tb);
+    if (hist_dq) hist_dq[slot] = sqrt(ta);
+    if (hist_r) hist_r[slot] = r;
+    // first < 0: the first step of the run is the one with no step done yet
+    if (first > 0 || (first < 0 && *s.steps_done == 0)) s.scalars[6] = r;
+    *s.steps_done += 1;
+    // stop once ||R_rho|| < drop * ||R_rho|| of the first step
+    if (s.scalars[7] > 0. && r < s.scalars[7] * s.scalars[6]) *s.stop = 1;
+  }
+}
+
 // nQ += dQ, pQ <- Q, Q <- nQ (solve.C:901-928) and partial sums of |dQ|^2
-// and |R_rho|^2.
-__global__ void __launch_bounds__(kRedThreads) k_finish_step(DevMesh m, DevState s, int last) {
-  if (*s.stop) return;  // the run has converged
+// and |R_rho|^2; the last block to finish sums the partials
+// (finalize_step_body), so the step needs no separate one-block launch.
+// The blocks count themselves in the word after the partials, which the
+// last block sets back to zero.
+__global__ void __launch_bounds__(kRedThreads) k_finish_step(DevMesh m, DevState s, int last,
+                                                            double* hist_dq, double* hist_r,
+                                                            int slot, int first) {
+  if (*s.stop) return;  // the run has converged (every block sees the same flag)
   __shared__ double sh[kRedThreads];
+  __shared__ int is_last;
   double dq2 = 0., r2 = 0.;
   const int total = m.nn + m.ng;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x + 1; i <= total;
@@ -2064,35 +2106,18 @@ __global__ void __launch_bounds__(kRedThreads) k_finish_step(DevMesh m, DevState
   }
   double a = block_sum(dq2, sh);
   double b = block_sum(r2, sh);
+  unsigned* done = reinterpret_cast<unsigned*>(s.partial + 2 * kRedBlocks);
   if (threadIdx.x == 0) {
     s.partial[blockIdx.x] = a;
     s.partial[kRedBlocks + blockIdx.x] = b;
+    __threadfence();  // the partials are visible before the count says so
+    is_last = atomicAdd(done, 1u) == gridDim.x - 1;
   }
-}
-
-__global__ void k_finalize_step(DevState s, double* hist_dq, double* hist_r, int slot,
-                                int first) {
-  if (*s.stop) return;  // the run has converged
-  __shared__ double sh[kRedThreads];
-  double a = 0., b = 0.;
-  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) {
-    a += s.partial[i];
-    b += s.partial[kRedBlocks + i];
-  }
-  double ta = block_sum(a, sh);
-  double tb = block_sum(b, sh);
-  if (threadIdx.x == 0) {
-    s.scalars[1] = ta;
-    s.scalars[2] = tb;
-    double r = sqrt(tb);
-    if (hist_dq) hist_dq[slot] = sqrt(ta);
-    if (hist_r) hist_r[slot] = r;
-    // first < 0: the first step of the run is the one with no step done yet
-    if (first > 0 || (first < 0 && *s.steps_done == 0)) s.scalars[6] = r;
-    *s.steps_done += 1;
-    // stop once ||R_rho|| < drop * ||R_rho|| of the first step
-    if (s.scalars[7] > 0. && r < s.scalars[7] * s.scalars[6]) *s.stop = 1;
-  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  finalize_step_body(s, sh, hist_dq, hist_r, slot, first);
+  if (threadIdx.x == 0) *done = 0u;
 }
 
 // ---------------------------------------------------------------------------
