@@ -2,7 +2,10 @@
 //
 // One pseudo-time step is a fixed sequence of launches on the context's
 // stream:
-//   k_begin_step      nQ <- Q, grad/hess <- 0, phi <- 1        (solve.C:298-348)
+//   k_begin_step      step index and CFL, nQ <- Q, and what the node kernel
+//                     will not overwrite of grad/hess <- 0, phi <- 1
+//                                                               (init_memory.C:200-224,
+//                                                                solve.C:298-348)
 //   k_node_prepare    per node: wave-speed sum, dt and V/dt    (build_matrix)
 //                     + LSQ gradient or k=2 derivatives + Venkatakrishnan phi
 //   k_subedge_flux    per subedge: reconstructed Roe flux and the 8-flux
@@ -12,7 +15,10 @@
 //   k_assemble        per node: R, RHS, the node's LHS row, LU of the diagonal
 //   k_sweep_ordered   block Gauss-Seidel sweeps in reference row order
 //   k_lin_residual    b - Ax RMS after a sweep                  (linear_algebra.C:348-387)
-//   k_finish_step     nQ += dQ, pQ <- Q, Q <- nQ, norms         (solve.C:883-928)
+//   k_finish_step     nQ += dQ, pQ <- Q, Q <- nQ, norms, the stop flag
+//                                                               (solve.C:883-928)
+// (the precision form replaces the sweeps and the RMS by k_sweep_chunk /
+// k_sweep_chunk_pair and its face Jacobians may be the approximate ones)
 // Face results are written once per face and gathered per node in ascending
 // face order, which reproduces the reference's sequential scatter sums
 // exactly without atomics.
@@ -185,7 +191,7 @@ __global__ void __launch_bounds__(128, MINB) k_node_prepare4(DevMesh m, DevState
       ev += (w * xn[2]);
     }
     if (v == 0) {
-      const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
+      const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of the step (step_args_body)
       s.dt[n] = dt;
       if (bad) atomicOr(s.status, ERR_EIGEN);
       if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
@@ -372,7 +378,7 @@ __global__ void __launch_bounds__(128) k_node_prepare16(DevMesh m, DevState s, S
   }
   bad = __any_sync(hmask, bad);
   if (l == 0) {
-    const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of k_step_args
+    const double dt = s.scalars[3] * (m.cv_area[n] / ev);  // cfl of the step (step_args_body)
     s.dt[n] = dt;
     if (bad) atomicOr(s.status, ERR_EIGEN);
     if (dt <= 0. || !isfinite(dt)) atomicOr(s.status, ERR_DT);
