@@ -521,69 +521,76 @@ def run_batch(args, bw):
     e2e = n_conv_all / max(args.steps, 1) * n_e2e / (stream_ms_max / 1e3)
     e2e_staged = n_conv_all / (e2e_ms_max / 1e3)
 
-    # ---- roofline: k_node_prepare4 on the largest mesh of the batch, served form ----
-    # the served configuration of that mesh: its precision form and Jacobian,
-    # the kernel variants the autotuner picks for it
-    # (the largest one whose solve stays physical: some requests of the stream
-    # reach a non-physical state within a few steps, in the reference too)
-    ok = [i for i in range(len(prep)) if bw.fp64_status is None
-          or bw.fp64_status[i] in (0, capi.ERR_NOT_CONVERGED)]
-    big = max((prep[i] for i in ok), key=lambda p: p.req.nodes)
-    s = capi.Solver.from_mesh(big.mesh, big.params, device=local)
-    s.set_precision(bw.precision)
-    s.set_jacobian(bw.jacobian)
-    s.set_state(big.Q0)
-    variants, _ = s.autotune(ts=2, steps=4)
-    s.run(1, 8)
-    s.set_timing(True)
-    s.run(9, 24)
-    kt = s.kernel_times()
-    s.close()
-    peaks, peak_kind = measured_peaks()
-    fused = bw.jacobian == 1 and bw.precision != 0
-    approx = bw.jacobian != 0 and bw.precision != 0
-    # algorithmic bytes per launch of each kernel class (flowgpu/roofline.py)
-    names = {"node_prepare": "k_node_stage" if variants[0] == 3 else "k_node_prepare4",
-             "subedge_flux": "k_faces_assemble" if fused else "k_subedge_flux",
-             "assemble": "k_assemble4"}
-    per_launch = {"node_prepare": roofline.node_prepare_bytes(big.mesh),
-                  "subedge_flux": (roofline.faces_assemble_bytes(big.mesh) if fused else
-                                   roofline.subedge_flux_bytes(big.mesh, approx=approx)),
-                  "assemble": roofline.assemble_bytes(big.mesh, bw.precision, approx=approx)}
-    if bw.precision == 3:  # one sweep: its colour launches
-        names["sweep"] = "k_sweep_chunk (one sweep)"
-        per_launch["sweep"] = roofline.chunk_sweep_bytes(big.mesh)
-    total_ms = max(sum(v[1] for v in kt.values()), 1e-30)
-    top = max(per_launch, key=lambda k: kt[k][1])  # the class with the largest device time
-    cnt, ms = kt[top]
-    k_ms = ms / max(cnt, 1)
-    achieved = per_launch[top] / (k_ms * 1e-3) / 1e9
-    roof = {"bound": "hbm", "kernel": names[top], "mesh": f"{big.req.nc}x{big.req.nr}",
-            "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "peak_kind": peak_kind,
-            "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
-            "traffic": ncu_traffic(f"{bw.name}:{big.req.nc}x{big.req.nr}",
-                                   f"{names[top]}_dram_bytes"),
-            "algorithmic_bytes_per_launch": per_launch[top], "avg_launch_ms": round(k_ms, 4),
-            "share_of_step": round(ms / total_ms, 3), "variants": list(variants),
-            "others": {names[k]: {"avg_launch_ms": round(kt[k][1] / max(kt[k][0], 1), 4),
-                                  "achieved_gbs": round(per_launch[k] / max(
-                                      kt[k][1] / max(kt[k][0], 1), 1e-9) * 1e-6, 1),
-                                  "share_of_step": round(kt[k][1] / total_ms, 3)}
-                       for k in per_launch if k != top and kt[k][0]},
-            "kernels_ms": {k: round(t / max(c, 1), 4) for k, (c, t) in kt.items() if c}}
-    scnt, sms = kt["sweep"]
-    if bw.precision == 3 and scnt:
-        sw_bytes = roofline.chunk_sweep_bytes(big.mesh)
-        sw_ms = sms / scnt
-        sw_ach = sw_bytes / (sw_ms * 1e-3) / 1e9
-        roof_sweep = {"bound": "latency (dependency levels inside a chunk)",
-                      "kernel": "k_sweep_chunk (one sweep = one launch per chunk colour)",
-                      "achieved": round(sw_ach, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                      "frac": round(sw_ach / peaks["hbm_gbs"], 4),
-                      "algorithmic_bytes_per_sweep": sw_bytes, "avg_sweep_ms": round(sw_ms, 4),
-                      "share_of_step": round(sms / max(sum(v[1] for v in kt.values()), 1e-30), 3)}
-    else:
-        roof_sweep = None
+    # ---- roofline, on rank 0 only: its requests are the ones whose FP64
+    # statuses are recorded (other ranks serve other requests of the stream) ----
+    def roofline_lines():
+        # the kernel class with the largest share of the step on the largest
+        # mesh of the batch, served form
+        # the served configuration of that mesh: its precision form and Jacobian,
+        # the kernel variants the autotuner picks for it
+        # (the largest one whose solve stays physical: some requests of the stream
+        # reach a non-physical state within a few steps, in the reference too)
+        ok = [i for i in range(len(prep)) if bw.fp64_status is None
+              or bw.fp64_status[i] in (0, capi.ERR_NOT_CONVERGED)]
+        big = max((prep[i] for i in ok), key=lambda p: p.req.nodes)
+        s = capi.Solver.from_mesh(big.mesh, big.params, device=local)
+        s.set_precision(bw.precision)
+        s.set_jacobian(bw.jacobian)
+        s.set_state(big.Q0)
+        variants, _ = s.autotune(ts=2, steps=4)
+        s.run(1, 8)
+        s.set_timing(True)
+        s.run(9, 24)
+        kt = s.kernel_times()
+        s.close()
+        peaks, peak_kind = measured_peaks()
+        fused = bw.jacobian == 1 and bw.precision != 0
+        approx = bw.jacobian != 0 and bw.precision != 0
+        # algorithmic bytes per launch of each kernel class (flowgpu/roofline.py)
+        names = {"node_prepare": "k_node_stage" if variants[0] == 3 else "k_node_prepare4",
+                 "subedge_flux": "k_faces_assemble" if fused else "k_subedge_flux",
+                 "assemble": "k_assemble4"}
+        per_launch = {"node_prepare": roofline.node_prepare_bytes(big.mesh),
+                      "subedge_flux": (roofline.faces_assemble_bytes(big.mesh) if fused else
+                                       roofline.subedge_flux_bytes(big.mesh, approx=approx)),
+                      "assemble": roofline.assemble_bytes(big.mesh, bw.precision, approx=approx)}
+        if bw.precision == 3:  # one sweep: its colour launches
+            names["sweep"] = "k_sweep_chunk (one sweep)"
+            per_launch["sweep"] = roofline.chunk_sweep_bytes(big.mesh)
+        total_ms = max(sum(v[1] for v in kt.values()), 1e-30)
+        top = max(per_launch, key=lambda k: kt[k][1])  # the class with the largest device time
+        cnt, ms = kt[top]
+        k_ms = ms / max(cnt, 1)
+        achieved = per_launch[top] / (k_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": names[top], "mesh": f"{big.req.nc}x{big.req.nr}",
+                "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+                "traffic": ncu_traffic(f"{bw.name}:{big.req.nc}x{big.req.nr}",
+                                       f"{names[top]}_dram_bytes"),
+                "algorithmic_bytes_per_launch": per_launch[top], "avg_launch_ms": round(k_ms, 4),
+                "share_of_step": round(ms / total_ms, 3), "variants": list(variants),
+                "others": {names[k]: {"avg_launch_ms": round(kt[k][1] / max(kt[k][0], 1), 4),
+                                      "achieved_gbs": round(per_launch[k] / max(
+                                          kt[k][1] / max(kt[k][0], 1), 1e-9) * 1e-6, 1),
+                                      "share_of_step": round(kt[k][1] / total_ms, 3)}
+                           for k in per_launch if k != top and kt[k][0]},
+                "kernels_ms": {k: round(t / max(c, 1), 4) for k, (c, t) in kt.items() if c}}
+        scnt, sms = kt["sweep"]
+        if bw.precision == 3 and scnt:
+            sw_bytes = roofline.chunk_sweep_bytes(big.mesh)
+            sw_ms = sms / scnt
+            sw_ach = sw_bytes / (sw_ms * 1e-3) / 1e9
+            roof_sweep = {"bound": "latency (dependency levels inside a chunk)",
+                          "kernel": "k_sweep_chunk (one sweep = one launch per chunk colour)",
+                          "achieved": round(sw_ach, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                          "frac": round(sw_ach / peaks["hbm_gbs"], 4),
+                          "algorithmic_bytes_per_sweep": sw_bytes, "avg_sweep_ms": round(sw_ms, 4),
+                          "share_of_step": round(sms / max(sum(v[1] for v in kt.values()), 1e-30), 3)}
+        else:
+            roof_sweep = None
+        return roof, roof_sweep
+
+    roof, roof_sweep = roofline_lines() if rank == 0 else (None, None)
 
     # ---- plain FP64 drop-in on the same requests, one at a time ----
     plain = None
