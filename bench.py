@@ -614,8 +614,7 @@ def run_batch(args, bw):
             # runs first): a choice made with hindsight, so the baseline is
             # the drop-in at its best, not at one fixed setting
             runs = [(sw, steps[i], status[i]) for sw, steps, status in recorded]
-            pool = [r for r in runs if r[2] == 0] or runs
-            sw, steps_i, status_i = min(pool, key=lambda r: r[1] * ms[r[0]])
+            sw, steps_i, status_i = serve.fastest_recorded_run(runs, ms)
             per.append(round(ms[sw], 4))
             chosen.append((sw, steps_i, status_i))
             tot += steps_i * ms[sw] / 1e3

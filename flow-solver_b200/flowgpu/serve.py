@@ -84,6 +84,17 @@ def prepare_all(reqs, subits: int, max_steps: int, drop: float, threads: int = 8
         return list(ex.map(lambda r: prepare(r, subits, max_steps, drop), reqs))
 
 
+def fastest_recorded_run(runs, ms_per_step) -> tuple:
+    """The FP64 drop-in's run of one request that solves it soonest.
+
+    runs: (sweeps, steps, status) per recorded sweep count; ms_per_step:
+    {sweeps: measured ms per step}.  Runs that converged (status 0) are
+    preferred; among them (or among all, when none converged) the one with
+    the least steps x ms/step.  Returns (sweeps, steps, status)."""
+    pool = [r for r in runs if r[2] == 0] or list(runs)
+    return min(pool, key=lambda r: r[1] * ms_per_step[r[0]])
+
+
 def percentiles(xs, ps=(50, 95, 99)) -> dict:
     if not xs:
         return {f"p{p}": None for p in ps}

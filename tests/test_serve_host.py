@@ -32,6 +32,29 @@ def test_percentiles_and_longest_first_packing():
     assert bench._lpt_makespan([1, 1, 1], 8) == 1
 
 
+def test_plain_fp64_takes_the_recorded_run_that_solves_soonest():
+    from flowgpu import serve
+    ms = {2: 1.0, 4: 1.7}
+    # both converge: 4 sweeps take fewer steps but cost more a step
+    assert serve.fastest_recorded_run([(2, 1000, 0), (4, 500, 0)], ms) == (4, 500, 0)
+    assert serve.fastest_recorded_run([(2, 1000, 0), (4, 700, 0)], ms) == (2, 1000, 0)
+    # a converged run beats a faster one that fails or stops at max_steps
+    assert serve.fastest_recorded_run([(2, 3000, 0), (4, 64, 44)], ms) == (2, 3000, 0)
+    assert serve.fastest_recorded_run([(2, 8000, 256), (4, 900, 0)], ms) == (4, 900, 0)
+    # none converges: the cheapest of them
+    assert serve.fastest_recorded_run([(2, 8000, 256), (4, 64, 44)], ms) == (4, 64, 44)
+
+
+def test_roofline_approximate_jacobian_halves_the_face_blocks():
+    from flowgpu import roofline, workloads
+    from flowgpu.prep import Mesh
+    wl = workloads.Workload("rl_a", 64, 16, True, 3, 0.8)
+    m = Mesh.from_case(wl.write(), order=3)
+    ns = m.sizes["ns"] if "ns" in m.sizes else m.sizes["nsubedges"]
+    assert roofline.subedge_flux_bytes(m) - roofline.subedge_flux_bytes(m, approx=True) == 128 * ns
+    assert roofline.assemble_bytes(m, 3, approx=True) < roofline.assemble_bytes(m, 3)
+
+
 def test_roofline_bytes_scale_with_the_mesh():
     from flowgpu import roofline, workloads
     from flowgpu.prep import Mesh
