@@ -125,9 +125,10 @@ constexpr int kNonPhysical = FLOW_ERR_EIGEN | FLOW_ERR_DT | FLOW_ERR_LIMITER | F
 // A solve on the approximate face Jacobians whose chunk (flag slot fs) ended
 // non-physical: the approximation's Newton steps can overshoot where the CFL
 // ramp makes them large.  Put back the state of that chunk's first step and
-// carry on from there with the forward-difference Jacobians, which converge
-// where the FP64 drop-in does.  The steps after the failure are run once
-// more; they count in the solve's device time.
+// carry on from there with the forward-difference Jacobians (the reference's
+// derivatives of the flux the residual uses), once per solve.  The steps
+// after the failure are run once more; they count in the solve's device
+// time.
 int recover(flow_server* sv, Slot& sl, int fs) {
   const int step = sl.chunk_first[fs];
   int rc = flow::internal::checkpoint_restore(sl.ctx, fs, step);
